@@ -1,0 +1,364 @@
+#!/usr/bin/env python
+"""bench.py — H-LU factor+solve/s at <= 1e-10 backward error (FP64 HODLR, N = 8192).
+
+Workload (one "step"): restore the H-matrix (kernel 1/(r+1e-3) on 8192 Morton-sorted points
+of U[0,1]^2, diagonal shifted by 2 * max off-diagonal row sum, weak admissibility, leaf 256,
+rank 16), H-LU factorization on the persistent VM, then solve + FP64 iterative refinement
+until ||b - Ax||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= 1e-10.  Inputs are synthetic and
+seeded.  Multi-GPU: independent replicas, one per rank (no collective on the data path).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import importlib.util
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+WORKLOAD = dict(n=8192, dim=2, kernel="inv", p0=1e-3, leaf=256, rank=16, admissibility=0, seed=1234, tol=1e-10)
+WORKLOAD_NAME = "hodlr-inv2d-n8192-leaf256-rank16-fp64-ir1e-10"
+METRIC = "H-LU factor+solve/s at 1e-10 residual (FP64 HODLR N=8192)"
+
+
+def load_pp():
+    pkg = os.path.join(ROOT, "pastel-palettes_b200")
+    spec = importlib.util.spec_from_file_location("pastel_palettes_b200", os.path.join(pkg, "__init__.py"),
+                                                  submodule_search_locations=[pkg])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["pastel_palettes_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx = max(mx, float(f[2]))
+                except ValueError:
+                    continue
+                for nm, v in zip(names, f[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        except OSError:
+            pass
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def program_bytes(pp, h, which=0, nrhs=1):
+    """Compulsory operand bytes of one launch: targets read + written, inputs read once."""
+    info = h.program_info(which, nrhs)
+    tasks, _, _, _ = h.encode_program(which, nrhs, [0] * 5)
+    total = 0
+    for t in tasks:
+        op, m, n, k, l = int(t["op"]), int(t["m"]), int(t["n"]), int(t["k"]), int(t["l"])
+        if op == 1:
+            e = 2 * m * n
+        elif op in (2, 4, 5):
+            e = 2 * m * n + m * m // 2
+        elif op == 3:
+            e = 2 * m * n + n * n // 2
+        elif op == 6:
+            e = (2 if t["beta"] != 0 else 1) * m * n + m * k + k * n
+        elif op == 9:
+            e = 2 * (m * k + n * k) + (m + n) * l + n * k
+        else:
+            e = 0
+        total += 8 * e
+    return total, info
+
+
+def build_problem(pp, ctx, rank):
+    w = WORKLOAD
+    return pp.make_kernel_problem(ctx, w["n"], w["dim"], w["kernel"], w["p0"], w["leaf"], w["rank"],
+                                  w["admissibility"], seed=w["seed"] + rank)
+
+
+def fp64_peak_tflops(torch):
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(3):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = min(best, s.elapsed_time(e) / 1e3)
+    del a, b
+    return 2.0 * n ** 3 / best / 1e12
+
+
+# ----------------------------------------------------------------------------- CPU arm
+def cpu_steps(pp, oracle, h, prob, steps, threads):
+    """Factor + solve + refinement on the host cores with the oracle (restated reference
+    routines) executed over the same DAG; returns seconds per step and refinement steps."""
+    n = prob.n
+    b = pp.rhs(n, 1, seed=7)
+    A_rows = None
+    fac = oracle.HostArenas(h, 0)
+    original = fac.matrix.copy()
+    sol = oracle.HostArenas(h, 1, 1)
+    times, iters = [], []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        fac.matrix[:] = original
+        fac.run(threads=threads)
+        sol.matrix[:] = fac.matrix
+        x = np.zeros((n, 1))
+        r = b.copy()
+        it = 0
+        while True:
+            sol.rhs[:n] = r.ravel()
+            sol.run(threads=1)
+            x += sol.rhs[:n].reshape(n, 1)
+            it += 1
+            if A_rows is None:
+                A_rows = prob.dense()
+            r = b - A_rows @ x
+            err = np.abs(r).max() / (prob.norm_inf * np.abs(x).max() + np.abs(b).max())
+            if err <= WORKLOAD["tol"] or it >= 30:
+                break
+        times.append(time.perf_counter() - t0)
+        iters.append(it)
+    return times, iters
+
+
+def run_reference_arm(args, pp, rank, world):
+    if rank != 0:
+        return
+    import oracle
+    ctx = pp.Context(device=-1)
+    h, prob = build_problem(pp, ctx, 0)
+    threads = os.cpu_count() or 1
+    times, iters = cpu_steps(pp, oracle, h, prob, args.warmup + args.steps, threads)
+    t = times[args.warmup:]
+    value = len(t) / sum(t)
+    line = {"metric": METRIC, "value": value, "unit": "factor+solve/s", "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(t) / len(t),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD_NAME, **{k: v for k, v in WORKLOAD.items()}},
+            "cpu_baseline": {"value": value, "unit": "factor+solve/s", "cores": threads, "kind": "port",
+                             "sample": f"{len(t)} full steps of the workload (oracle over the same DAG, "
+                                       f"{threads} threads; refinement {iters[-1]} solves)"},
+            "e2e": {"value": value, "unit": "factor+solve/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- GPU arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pp = load_pp()
+    if args.impl == "reference":
+        run_reference_arm(args, pp, rank, world)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    ctx = pp.Context(device=local)
+    h, prob = build_problem(pp, ctx, rank)
+    h.pin_host()
+    s = torch.cuda.current_stream()
+    h.upload(s)
+    h.keep_original(s)
+    b = torch.from_numpy(pp.rhs(prob.n, 1, seed=7)).cuda()
+    ref = pp.Refiner(h, ctx, prob, stream=s)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
+
+    def step():
+        h.restore(s)
+        h.factor(s)
+        x, hist = ref.solve(b, tol=WORKLOAD["tol"])
+        return x, hist
+
+    for _ in range(args.warmup):
+        x, hist = step()
+    h.sync(s)
+    if hist[-1] > WORKLOAD["tol"]:
+        raise SystemExit(f"refinement did not reach {WORKLOAD['tol']}: {hist}")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # --- device-timed steps (inputs resident in HBM), L2 flushed between steps
+    launches0 = ref.launches
+    n_iters = []
+    total = 0.0
+    with Clocks(local) as clk:
+        barrier()
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            x, hist = step()
+            e1.record(s)
+            e1.synchronize()
+            total += e0.elapsed_time(e1) / 1e3
+            n_iters.append(len(hist))
+        barrier()
+    h.sync(s)
+    gpu_launches = 2 * args.steps + (ref.launches - launches0)
+    t = torch.tensor([total], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_max = t.item()
+    value = world * args.steps / total_max
+
+    # --- end to end through the C ABI with host buffers: H2D matrix + rhs, factor,
+    #     refinement, D2H solution (and the scalar norms the refinement reads back)
+    b_host = torch.from_numpy(pp.rhs(prob.n, 1, seed=7)).pin_memory()
+    x_host = torch.empty_like(b_host).pin_memory()
+    e2e_total = 0.0
+    d2h_extra = 0
+    barrier()
+    for _ in range(max(3, args.steps // 2)):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        h.upload(s)
+        bd = b_host.to("cuda", non_blocking=True)
+        h.factor(s)
+        xd, hist = ref.solve(bd, tol=WORKLOAD["tol"])
+        x_host.copy_(xd, non_blocking=True)
+        e1.record(s)
+        e1.synchronize()
+        e2e_total += e0.elapsed_time(e1) / 1e3
+        d2h_extra = 16 * len(hist)
+    e2e_steps = max(3, args.steps // 2)
+    t = torch.tensor([e2e_total], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * e2e_steps / t.item()
+    h.restore(s)
+
+    # --- roofline of the dominant kernel (the factor VM launch), timed alone
+    fac_ms = []
+    for _ in range(args.steps):
+        h.restore(s)
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        h.factor(s)
+        e1.record(s)
+        e1.synchronize()
+        fac_ms.append(e0.elapsed_time(e1))
+    h.sync(s)
+    sol_ms = []
+    r = torch.empty_like(b)
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        h.solve(b, r, s)
+        e1.record(s)
+        e1.synchronize()
+        sol_ms.append(e0.elapsed_time(e1))
+    fbytes, finfo = program_bytes(pp, h, 0)
+    hbm_peak, peak_kind = peaks()
+    fac_s = float(np.mean(fac_ms)) / 1e3
+    fp64_peak = fp64_peak_tflops(torch)
+    achieved_gbs = fbytes / fac_s / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved_gbs / hbm_peak, "traffic": None,
+                "kernel": "vm_kernel (factor launch)", "launch_ms": 1e3 * fac_s,
+                "algorithmic_bytes": fbytes, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "fp64": {"achieved_tflops": finfo["flops"] / fac_s / 1e12, "peak_tflops": fp64_peak,
+                         "frac": finfo["flops"] / fac_s / 1e12 / fp64_peak,
+                         "peak_source": "measured in this run: torch float64 matmul 8192^3"},
+                "solve_launch_ms": float(np.mean(sol_ms))}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle
+        threads = os.cpu_count() or 1
+        hc, pc = build_problem(pp, pp.Context(device=-1), 0)
+        times, iters = cpu_steps(pp, oracle, hc, pc, 2, threads)
+        cpu = {"value": 1.0 / times[-1], "unit": "factor+solve/s", "cores": threads, "kind": "port",
+               "sample": f"1 full step of the same workload after 1 warm-up (oracle over the same DAG, "
+                         f"{threads} threads, {iters[-1]} refinement solves)"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "factor+solve/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1e3 * total_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": WORKLOAD_NAME, **WORKLOAD, "l2": "flushed between steps (256 MiB write)",
+                           "parallelism": f"replicas{world}", "factor_tasks": finfo["n_tasks"],
+                           "factor_flops": finfo["flops"], "refinement_solves": int(np.median(n_iters))},
+                "e2e": {"value": e2e_value, "unit": "factor+solve/s",
+                        "h2d_bytes_per_step": h.arena_bytes() + 8 * prob.n,
+                        "d2h_bytes_per_step": 8 * prob.n + d2h_extra},
+                "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": gpu_launches}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

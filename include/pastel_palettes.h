@@ -1,0 +1,169 @@
+/* pastel_palettes.h — C ABI of the B200-native H-LU engine (libpastel_palettes.so).
+ *
+ * Drop-in boundary for the factor / solve path of Pastel-Palettes.  Every entry point
+ * names the reference interface it replaces (file:line in the reference project).
+ * Plain C: pointers, sizes and status codes only.  Device pointers are CUDA device
+ * addresses; `stream` is a cudaStream_t passed as void* (0 = legacy default stream).
+ *
+ * Conventions
+ *  - Matrices are row-major FP64 (the reference kernel's layout, src/kernel.cu:42).
+ *  - The caller owns host buffers; the library owns device copies of H-matrices and
+ *    their factors until pp_hmatrix_destroy.
+ *  - A context is used from one host thread at a time.
+ *  - No CPU fallback: without a usable CUDA device every compute entry point returns
+ *    PP_CUDA_ERROR.
+ */
+#ifndef PASTEL_PALETTES_H
+#define PASTEL_PALETTES_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum pp_status {
+  PP_OK = 0,
+  PP_INVALID_ARG = 1,
+  PP_OOM = 2,
+  PP_TIMEOUT = 3,     /* a device wait gave up (bounded spin) */
+  PP_NUMERICAL = 4,   /* non-finite result / zero pivot        */
+  PP_CUDA_ERROR = 5,
+  PP_UNSUPPORTED = 6,
+  PP_INTERNAL = 7
+} pp_status;
+
+typedef struct pp_context pp_context;
+typedef struct pp_hmatrix pp_hmatrix;
+
+typedef struct pp_config {
+  int tile;              /* dense blocks above this are split before they reach an instruction (<= 64) */
+  int ctas_per_sm;       /* persistent VM CTAs per SM (0 = occupancy maximum)                        */
+  long long spin_limit;  /* polls of an empty ready slot before a VM CTA reports PP_TIMEOUT            */
+  unsigned long long seed;  /* seed of the random sketch used by accum                                */
+} pp_config;
+
+typedef struct pp_block_info {
+  int kind;       /* 0 dense, 1 low-rank, 2 hierarchical */
+  int row0, col0, m, n;
+  int rank, kmax, level;
+  int children[4];
+} pp_block_info;
+
+typedef struct pp_program_info {
+  int n_tasks;
+  long long n_edges;
+  long long flops;                  /* algorithmic FLOPs of all instructions */
+  long long op_count[10];           /* instructions per pp_op               */
+  long long arena_elems[5];         /* matrix, work, scratch, rhs, rand     */
+  double host_build_ms;             /* op generation + DAG + encoding        */
+} pp_program_info;
+
+/* --- context ----------------------------------------------------------- */
+/* replaces the device set-up of dev_hierarchical_GETRF (src/launcher.cu:119-123) */
+pp_status pp_context_create(int device, const pp_config* cfg, pp_context** out);
+void pp_context_destroy(pp_context* ctx);
+/* copies the last error message (NUL-terminated) into buf; returns its length */
+int pp_last_error(const pp_context* ctx, char* buf, size_t size);
+int pp_device_sm_count(const pp_context* ctx);
+
+/* --- matrix/Dense + matrix/Hierarchical --------------------------------- */
+/* all-dense 2 x 2 partition down to `leaf` (matrix/Hierarchical.h:4-7 is an empty stub in
+ * the reference; the tree interface follows its use at src/launcher.cu:126,138-139) */
+pp_status pp_hmatrix_create_dense(pp_context* ctx, int n, int leaf, pp_hmatrix** out);
+/* geometric block tree over points in cluster order; admissibility 0 = weak, 1 = standard */
+pp_status pp_hmatrix_create_geometric(pp_context* ctx, int n, int dim, const double* points, int leaf,
+                                      int admissibility, double eta, int kmax, pp_hmatrix** out);
+void pp_hmatrix_destroy(pp_hmatrix* h);
+int pp_hmatrix_num_blocks(const pp_hmatrix* h);
+int pp_hmatrix_root(const pp_hmatrix* h);
+pp_status pp_hmatrix_block_info(const pp_hmatrix* h, int block, pp_block_info* info);
+/* host data of one block (Dense(m, n, lda), matrix/Dense.h:6-18; row-major here) */
+pp_status pp_hmatrix_set_dense(pp_hmatrix* h, int block, const double* a, int lda);
+pp_status pp_hmatrix_set_lowrank(pp_hmatrix* h, int block, const double* U, int ldu, const double* V, int ldv,
+                                 int rank);
+pp_status pp_hmatrix_upload(pp_hmatrix* h, void* stream);
+pp_status pp_hmatrix_download(pp_hmatrix* h, void* stream);
+/* page-locks the host image so uploads / downloads run at full PCIe rate */
+pp_status pp_hmatrix_pin_host(pp_hmatrix* h);
+/* keeps a device copy of the uploaded (unfactored) matrix; pp_hmatrix_restore copies it
+ * back over the factors (device to device, stream ordered) for repeated factorizations */
+pp_status pp_hmatrix_keep_original(pp_hmatrix* h, void* stream);
+pp_status pp_hmatrix_restore(pp_hmatrix* h, void* stream);
+/* dense n x n image of the host copy (after download: the L\U factors) */
+pp_status pp_hmatrix_to_dense(const pp_hmatrix* h, double* out);
+long long pp_hmatrix_storage_elems(const pp_hmatrix* h);
+/* host image of the block arena (row-major blocks at the offsets of the block tree);
+ * writable: pp_hmatrix_to_dense and pp_hmatrix_upload read it */
+double* pp_hmatrix_host_arena(pp_hmatrix* h, long long* elems);
+/* device base of the matrix arena (read-only view for residual / export helpers) */
+const double* pp_hmatrix_device_arena(const pp_hmatrix* h);
+
+/* --- factor / solve (launcher.cuh) --------------------------------------- */
+/* H-LU factorization in place on the device, stream ordered.
+ * replaces dev_hierarchical_GETRF (include/launcher.cuh:18, src/launcher.cu:117-217) */
+pp_status pp_hlu_factor(pp_hmatrix* h, void* stream);
+/* X := A^-1 B with the device factors: B, X device, row-major n x nrhs (may alias).
+ * no reference counterpart (the reference has no solve) */
+pp_status pp_hlu_solve(pp_hmatrix* h, const double* b_dev, double* x_dev, int nrhs, void* stream);
+/* waits for `stream`; returns PP_TIMEOUT / PP_INTERNAL if the last VM launch of h failed */
+pp_status pp_hmatrix_sync(pp_hmatrix* h, void* stream);
+/* introspection of the factor (which = 0) or solve (which = 1, nrhs) program */
+pp_status pp_hmatrix_program_info(pp_hmatrix* h, int which, int nrhs, pp_program_info* info);
+/* reference-signature driver: dev_hierarchical_GETRF(h, num_blocks, num_threads, kernel_size)
+ * (include/launcher.cuh:18).  num_blocks > 0 caps the persistent grid; num_threads must be
+ * 256 or 0; kernel_size is accepted and ignored (one launch covers the whole DAG). */
+pp_status pp_dev_hierarchical_getrf(pp_hmatrix* h, int num_blocks, int num_threads, int kernel_size);
+
+/* --- residuals (FP64 refinement) ----------------------------------------- */
+/* r := b - A x, A dense row-major (device); x, b, r device n x nrhs */
+pp_status pp_dense_residual_dev(pp_context* ctx, const double* A, int lda, int n, const double* x, const double* b,
+                                double* r, int nrhs, void* stream);
+/* r := b - A x, A_ij = K(|p_i - p_j|) + shift * (i == j) evaluated on the fly.
+ * kernel: 0 = 1/(r+p0), 1 = 1/(4 pi (r+p0)), 2 = exp(-r/p0), 3 = Matern-3/2 length p0 */
+pp_status pp_kernel_residual_dev(pp_context* ctx, int kernel, double p0, double shift, const double* pts_dev,
+                                 int dim, int n, const double* x, const double* b, double* r, int nrhs,
+                                 void* stream);
+
+/* --- rts (DAG primitives, rts/ops.h, rts/dependency.h) ------------------- */
+/* DataMap2D::checkOverlap (rts/ops.cpp:7-40); regions: ptr, pitch, width (bytes), height */
+int pp_datamap2d_check_overlap(uintptr_t ptr_a, size_t pitch_a, size_t width_a, size_t height_a, uintptr_t ptr_b,
+                               size_t pitch_b, size_t width_b, size_t height_b);
+/* Operation::checkDependencyFrom (rts/ops.cpp:42-61): regions as flat arrays of
+ * (ptr, pitch, width, height) with read_only flags; returns a dependency_t bit set
+ * (1 flow, 2 anti, 4 out) */
+int pp_operation_dependency(int n_from, const uint64_t* regions_from, const int* ro_from, int n_to,
+                            const uint64_t* regions_to, const int* ro_to);
+
+/* --- program export (tests, oracle, reference-format streams) ------------ */
+/* Encodes the factor (which = 0) or solve (which = 1) program with caller-chosen arena
+ * bases (host or device addresses; arena order matrix, work, scratch, rhs, rand).
+ * tasks: n_tasks records of 160 bytes (pp_task.h); succ: n_edges; indeg: n_tasks.  */
+pp_status pp_hmatrix_encode_program(pp_hmatrix* h, int which, int nrhs, double* const* bases, void* tasks,
+                                    int32_t* succ, int32_t* indeg, int32_t* order);
+/* typed DAG of the factor / solve program: edge e runs from[e] -> to[e] with dependency_t
+ * bits type[e] (1 flow, 2 anti, 4 out); the dependency_table of rts/dependency.h:24-53 */
+pp_status pp_hmatrix_program_edges(pp_hmatrix* h, int which, int nrhs, int64_t* from, int64_t* to, int32_t* type);
+/* Runs an arbitrary task table (host array of n pp_task records with device operand
+ * pointers; successor lists and in-degrees as pp_hmatrix_encode_program returns them) on
+ * the VM and waits.  spin_limit <= 0 uses the context's.  Returns PP_TIMEOUT when a ready
+ * slot is never filled (e.g. an in-degree that no predecessor can bring to zero).
+ * Counterpart of launchKernelWithArgs (include/launcher.cuh:15-16) for decoded streams. */
+pp_status pp_vm_execute(pp_context* ctx, const void* tasks, int n_tasks, const int32_t* succ, long long n_succ,
+                        const int32_t* indeg, long long spin_limit, int grid, void* stream);
+/* random sketch the accum instructions read (arena `rand`, row-major n x kmax, ld = rank) */
+pp_status pp_hmatrix_rand_host(pp_hmatrix* h, double* out, long long count);
+/* Reference-format instruction streams of the factor program (src/kernel.cu:1384-1522)
+ * for `workers` workers; pointer index = arena index above.  Returns the stream words
+ * concatenated, lengths[workers], and the per-worker scratch the reference's accum needs.
+ * operation enum: nop 0, getrf 1, trsml 2, trsmr 3, gemm 4, gemm_plus 5, gemm_3x 6,
+ * gemm_4x 7, accum 8; opcodes: finish 0, execute 1, signal_wait 2. */
+pp_status pp_refstream_encode(pp_hmatrix* h, int workers, int32_t* words, long long capacity, int32_t* lengths,
+                              long long* tmp_elems_per_worker);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

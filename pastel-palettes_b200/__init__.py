@@ -1,0 +1,581 @@
+"""pastel_palettes_b200 — Python host mirror of the B200 H-LU engine.
+
+Thin ctypes layer over libpastel_palettes.so (C ABI: include/pastel_palettes.h).  The
+names follow the reference's host interface (Pastel-Palettes matrix/Dense.h,
+matrix/Hierarchical.h, rts/ops.h, include/launcher.cuh):
+
+  Hierarchical        block tree + device copy        (matrix/Hierarchical.h:4-7; usage
+                                                        src/launcher.cu:126,138-139)
+  dev_hierarchical_GETRF(h, num_blocks, num_threads, kernel_size)
+                                                       (include/launcher.cuh:18)
+  DataMap2D.checkOverlap                               (rts/ops.h:9-20, rts/ops.cpp:7-40)
+  Operation.checkDependencyFrom                        (rts/ops.h:22-36, rts/ops.cpp:42-61)
+
+plus what the reference lacks: solve, FP64 residuals, and the synthetic problem builders
+of the benchmark configurations.  There is no CPU fallback: compute calls go to the CUDA
+library or raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import time
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpastel_palettes.so")
+
+PP_OK, PP_INVALID_ARG, PP_OOM, PP_TIMEOUT, PP_NUMERICAL, PP_CUDA_ERROR, PP_UNSUPPORTED, PP_INTERNAL = range(8)
+STATUS_NAMES = ["OK", "INVALID_ARG", "OOM", "TIMEOUT", "NUMERICAL", "CUDA_ERROR", "UNSUPPORTED", "INTERNAL"]
+OP_NAMES = ["nop", "getrf", "trsml", "trsmr", "trsmrt", "trsmu", "gemm", "gemm3", "gemm4", "accum"]
+DENSE, LOWRANK, HIER = 0, 1, 2
+ARENAS = ["matrix", "work", "scratch", "rhs", "rand"]
+
+# pp_task (pastel-palettes_b200/csrc/pp_task.h), 160 bytes
+TASK_DTYPE = np.dtype(
+    [("op", "<i4"), ("flags", "<i4"), ("m", "<i4"), ("n", "<i4"), ("k", "<i4"), ("l", "<i4"), ("o", "<i4"),
+     ("ctrl", "<i4"), ("ld", "<i4", 6), ("p", "<u8", 6), ("tmp", "<u8"), ("alpha", "<f8"), ("beta", "<f8"),
+     ("succ_begin", "<i4"), ("n_succ", "<i4"), ("prec", "<i4"), ("instance", "<i4"), ("aux", "<i4"),
+     ("pad", "<i4", 3)])
+assert TASK_DTYPE.itemsize == 160
+
+
+class PPError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS_NAMES[status] if 0 <= status < len(STATUS_NAMES) else status}: {msg}")
+        self.status = status
+
+
+class _Config(C.Structure):
+    _fields_ = [("tile", C.c_int), ("ctas_per_sm", C.c_int), ("spin_limit", C.c_longlong), ("seed", C.c_ulonglong)]
+
+
+class _BlockInfo(C.Structure):
+    _fields_ = [("kind", C.c_int), ("row0", C.c_int), ("col0", C.c_int), ("m", C.c_int), ("n", C.c_int),
+                ("rank", C.c_int), ("kmax", C.c_int), ("level", C.c_int), ("children", C.c_int * 4)]
+
+
+class _ProgramInfo(C.Structure):
+    _fields_ = [("n_tasks", C.c_int), ("n_edges", C.c_longlong), ("flops", C.c_longlong),
+                ("op_count", C.c_longlong * 10), ("arena_elems", C.c_longlong * 5), ("host_build_ms", C.c_double)]
+
+
+_lib = None
+
+
+def lib():
+    """The loaded C library; raises if it was not built (no silent fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `make -C pastel-palettes_b200/csrc`")
+        L = C.CDLL(LIB_PATH)
+        vp, i, ll, d, dp = C.c_void_p, C.c_int, C.c_longlong, C.c_double, C.POINTER(C.c_double)
+        sig = {
+            "pp_context_create": (i, [i, C.POINTER(_Config), C.POINTER(vp)]),
+            "pp_context_destroy": (None, [vp]),
+            "pp_last_error": (i, [vp, C.c_char_p, C.c_size_t]),
+            "pp_device_sm_count": (i, [vp]),
+            "pp_hmatrix_create_dense": (i, [vp, i, i, C.POINTER(vp)]),
+            "pp_hmatrix_create_geometric": (i, [vp, i, i, dp, i, i, d, i, C.POINTER(vp)]),
+            "pp_hmatrix_destroy": (None, [vp]),
+            "pp_hmatrix_num_blocks": (i, [vp]),
+            "pp_hmatrix_root": (i, [vp]),
+            "pp_hmatrix_block_info": (i, [vp, i, C.POINTER(_BlockInfo)]),
+            "pp_hmatrix_set_dense": (i, [vp, i, dp, i]),
+            "pp_hmatrix_set_lowrank": (i, [vp, i, dp, i, dp, i, i]),
+            "pp_hmatrix_upload": (i, [vp, vp]),
+            "pp_hmatrix_download": (i, [vp, vp]),
+            "pp_hmatrix_pin_host": (i, [vp]),
+            "pp_hmatrix_keep_original": (i, [vp, vp]),
+            "pp_hmatrix_restore": (i, [vp, vp]),
+            "pp_hmatrix_to_dense": (i, [vp, dp]),
+            "pp_hmatrix_storage_elems": (ll, [vp]),
+            "pp_hmatrix_host_arena": (dp, [vp, C.POINTER(ll)]),
+            "pp_hmatrix_device_arena": (vp, [vp]),
+            "pp_hlu_factor": (i, [vp, vp]),
+            "pp_hlu_solve": (i, [vp, vp, vp, i, vp]),
+            "pp_hmatrix_sync": (i, [vp, vp]),
+            "pp_hmatrix_program_info": (i, [vp, i, i, C.POINTER(_ProgramInfo)]),
+            "pp_dev_hierarchical_getrf": (i, [vp, i, i, i]),
+            "pp_dense_residual_dev": (i, [vp, vp, i, i, vp, vp, vp, i, vp]),
+            "pp_kernel_residual_dev": (i, [vp, i, d, d, vp, i, i, vp, vp, vp, i, vp]),
+            "pp_datamap2d_check_overlap": (i, [C.c_uint64, C.c_size_t, C.c_size_t, C.c_size_t,
+                                               C.c_uint64, C.c_size_t, C.c_size_t, C.c_size_t]),
+            "pp_operation_dependency": (i, [i, vp, vp, i, vp, vp]),
+            "pp_hmatrix_encode_program": (i, [vp, i, i, vp, vp, vp, vp, vp]),
+            "pp_hmatrix_rand_host": (i, [vp, dp, ll]),
+            "pp_hmatrix_program_edges": (i, [vp, i, i, vp, vp, vp]),
+            "pp_vm_execute": (i, [vp, vp, i, vp, ll, vp, ll, i, vp]),
+            "pp_refstream_encode": (i, [vp, i, vp, ll, vp, C.POINTER(ll)]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _stream_handle(stream):
+    if stream is None:
+        return None
+    return C.c_void_p(getattr(stream, "cuda_stream", stream))
+
+
+def exported_symbols():
+    """Names declared in include/pastel_palettes.h (for the load test)."""
+    hdr = os.path.join(os.path.dirname(_HERE), "include", "pastel_palettes.h")
+    import re
+    src = open(hdr).read()
+    return sorted(set(re.findall(r"\b(pp_[a-z0-9_]+)\s*\(", src)))
+
+
+class Context:
+    """Device context (device >= 0) or host-only planning context (device = -1)."""
+
+    def __init__(self, device=0, tile=64, ctas_per_sm=0, spin_limit=1 << 24, seed=0x5EED5EED):
+        cfg = _Config(tile, ctas_per_sm, spin_limit, seed)
+        h = C.c_void_p()
+        st = lib().pp_context_create(device, C.byref(cfg), C.byref(h))
+        if st != PP_OK:
+            raise PPError(st, f"pp_context_create(device={device}) failed")
+        self._h = h
+        self.device = device
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().pp_context_destroy(self._h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def last_error(self):
+        buf = C.create_string_buffer(1024)
+        lib().pp_last_error(self._h, buf, 1024)
+        return buf.value.decode()
+
+    def check(self, st, what):
+        if st != PP_OK:
+            raise PPError(st, f"{what}: {self.last_error()}")
+
+    @property
+    def sm_count(self):
+        return lib().pp_device_sm_count(self._h)
+
+    # --- FP64 residuals (device pointers of torch tensors)
+    def dense_residual(self, A, x, b, r, stream=None):
+        n, nrhs = x.shape
+        self.check(lib().pp_dense_residual_dev(self._h, A.data_ptr(), A.stride(0), n, x.data_ptr(), b.data_ptr(),
+                                               r.data_ptr(), nrhs, _stream_handle(stream)), "dense_residual")
+
+    def vm_execute(self, tasks, succ, indeg, spin_limit=0, grid=0, stream=None):
+        """Run a task table (TASK_DTYPE array with device pointers) on the VM and wait."""
+        tasks = np.ascontiguousarray(tasks, dtype=TASK_DTYPE)
+        succ = np.ascontiguousarray(succ, dtype=np.int32)
+        indeg = np.ascontiguousarray(indeg, dtype=np.int32)
+        self.check(lib().pp_vm_execute(self._h, tasks.ctypes.data, len(tasks), succ.ctypes.data if succ.size else None,
+                                       succ.size, indeg.ctypes.data, spin_limit, grid, _stream_handle(stream)),
+                   "vm_execute")
+
+    def kernel_residual(self, kernel, p0, shift, pts, x, b, r, stream=None):
+        n, nrhs = x.shape
+        self.check(lib().pp_kernel_residual_dev(self._h, kernel, p0, shift, pts.data_ptr(), pts.shape[1], n,
+                                                x.data_ptr(), b.data_ptr(), r.data_ptr(), nrhs,
+                                                _stream_handle(stream)), "kernel_residual")
+
+
+class Hierarchical:
+    """A block tree (dense / low-rank / 2x2 hierarchical blocks) and its device copy."""
+
+    def __init__(self, ctx, handle):
+        self.ctx = ctx
+        self._h = handle
+
+    @classmethod
+    def dense(cls, ctx, n, leaf):
+        h = C.c_void_p()
+        ctx.check(lib().pp_hmatrix_create_dense(ctx.handle, n, leaf, C.byref(h)), "create_dense")
+        return cls(ctx, h)
+
+    @classmethod
+    def geometric(cls, ctx, points, leaf, admissibility=0, eta=1.0, kmax=16):
+        pts = np.ascontiguousarray(points, dtype=np.float64)
+        n, dim = pts.shape
+        h = C.c_void_p()
+        ctx.check(lib().pp_hmatrix_create_geometric(ctx.handle, n, dim, _ptr(pts), leaf, admissibility, eta, kmax,
+                                                    C.byref(h)), "create_geometric")
+        return cls(ctx, h)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().pp_hmatrix_destroy(self._h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    # --- structure (getNy_abs / getNx_abs / getRootIndex)
+    def blocks(self):
+        out = []
+        for b in range(lib().pp_hmatrix_num_blocks(self._h)):
+            info = _BlockInfo()
+            lib().pp_hmatrix_block_info(self._h, b, C.byref(info))
+            out.append(dict(id=b, kind=info.kind, row0=info.row0, col0=info.col0, m=info.m, n=info.n,
+                            rank=info.rank, kmax=info.kmax, level=info.level, children=list(info.children)))
+        return out
+
+    @property
+    def n(self):
+        info = _BlockInfo()
+        lib().pp_hmatrix_block_info(self._h, self.root, C.byref(info))
+        return info.m
+
+    def getNy_abs(self):
+        return self.n
+
+    def getNx_abs(self):
+        return self.n
+
+    @property
+    def root(self):
+        return lib().pp_hmatrix_root(self._h)
+
+    def getRootIndex(self):
+        return self.root
+
+    def storage_elems(self):
+        return lib().pp_hmatrix_storage_elems(self._h)
+
+    # --- data
+    def set_dense(self, block, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        self.ctx.check(lib().pp_hmatrix_set_dense(self._h, block, _ptr(a), a.shape[1]), "set_dense")
+
+    def set_lowrank(self, block, U, V):
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        V = np.ascontiguousarray(V, dtype=np.float64)
+        self.ctx.check(lib().pp_hmatrix_set_lowrank(self._h, block, _ptr(U), U.shape[1], _ptr(V), V.shape[1],
+                                                    U.shape[1]), "set_lowrank")
+
+    def host_arena(self):
+        """Writable numpy view of the host image of the block arena."""
+        n = C.c_longlong()
+        p = lib().pp_hmatrix_host_arena(self._h, C.byref(n))
+        return np.ctypeslib.as_array(p, shape=(max(n.value, 1),))[: n.value]
+
+    def to_dense(self):
+        out = np.zeros((self.n, self.n))
+        self.ctx.check(lib().pp_hmatrix_to_dense(self._h, _ptr(out)), "to_dense")
+        return out
+
+    def upload(self, stream=None):
+        self.ctx.check(lib().pp_hmatrix_upload(self._h, _stream_handle(stream)), "upload")
+
+    def download(self, stream=None):
+        self.ctx.check(lib().pp_hmatrix_download(self._h, _stream_handle(stream)), "download")
+
+    def device_arena_ptr(self):
+        return lib().pp_hmatrix_device_arena(self._h)
+
+    def pin_host(self):
+        self.ctx.check(lib().pp_hmatrix_pin_host(self._h), "pin_host")
+
+    def keep_original(self, stream=None):
+        self.ctx.check(lib().pp_hmatrix_keep_original(self._h, _stream_handle(stream)), "keep_original")
+
+    def restore(self, stream=None):
+        self.ctx.check(lib().pp_hmatrix_restore(self._h, _stream_handle(stream)), "restore")
+
+    def arena_bytes(self):
+        return 8 * self.host_arena().size
+
+    # --- factor / solve
+    def factor(self, stream=None):
+        self.ctx.check(lib().pp_hlu_factor(self._h, _stream_handle(stream)), "hlu_factor")
+
+    def solve(self, b, x, stream=None):
+        """x := A^-1 b with device tensors (n x nrhs row-major, float64)."""
+        nrhs = b.shape[1] if b.dim() == 2 else 1
+        self.ctx.check(lib().pp_hlu_solve(self._h, b.data_ptr(), x.data_ptr(), nrhs, _stream_handle(stream)),
+                       "hlu_solve")
+
+    def sync(self, stream=None):
+        self.ctx.check(lib().pp_hmatrix_sync(self._h, _stream_handle(stream)), "sync")
+
+    def program_info(self, which=0, nrhs=1):
+        info = _ProgramInfo()
+        self.ctx.check(lib().pp_hmatrix_program_info(self._h, which, nrhs, C.byref(info)), "program_info")
+        return dict(n_tasks=info.n_tasks, n_edges=info.n_edges, flops=info.flops,
+                    op_count={OP_NAMES[i]: info.op_count[i] for i in range(10)},
+                    arena_elems={ARENAS[i]: info.arena_elems[i] for i in range(5)},
+                    host_build_ms=info.host_build_ms)
+
+    def encode_program(self, which, nrhs, bases):
+        """Task table bound to the given arena base addresses (ints); returns
+        (tasks structured array, succ, indeg, ready)."""
+        info = self.program_info(which, nrhs)
+        n, e = info["n_tasks"], info["n_edges"]
+        tasks = np.zeros(n, dtype=TASK_DTYPE)
+        succ = np.zeros(max(e, 1), dtype=np.int32)
+        indeg = np.zeros(n, dtype=np.int32)
+        order = np.zeros(n, dtype=np.int32)
+        b = (C.c_void_p * 5)(*[C.c_void_p(int(x)) for x in bases])
+        self.ctx.check(lib().pp_hmatrix_encode_program(self._h, which, nrhs, b, tasks.ctypes.data,
+                                                       succ.ctypes.data, indeg.ctypes.data, order.ctypes.data),
+                       "encode_program")
+        ready = order[order >= 0]
+        return tasks, succ[:e], indeg, ready
+
+    def edges(self, which=0, nrhs=1):
+        """Typed DAG edges (from, to, dependency_t bits) of the factor / solve program."""
+        e = self.program_info(which, nrhs)["n_edges"]
+        f = np.zeros(max(e, 1), dtype=np.int64)
+        t = np.zeros(max(e, 1), dtype=np.int64)
+        ty = np.zeros(max(e, 1), dtype=np.int32)
+        self.ctx.check(lib().pp_hmatrix_program_edges(self._h, which, nrhs, f.ctypes.data, t.ctypes.data,
+                                                      ty.ctypes.data), "program_edges")
+        return f[:e], t[:e], ty[:e]
+
+    def rand_host(self):
+        n = self.program_info(0)["arena_elems"]["rand"]
+        out = np.zeros(max(n, 1))
+        self.ctx.check(lib().pp_hmatrix_rand_host(self._h, _ptr(out), n), "rand_host")
+        return out[:n]
+
+    def refstreams(self, workers=1):
+        """Reference-format instruction streams of the factor program (one per worker)."""
+        lengths = np.zeros(workers, dtype=np.int32)
+        tmp = C.c_longlong()
+        self.ctx.check(lib().pp_refstream_encode(self._h, workers, None, 0, lengths.ctypes.data, C.byref(tmp)),
+                       "refstream size")
+        words = np.zeros(int(lengths.sum()), dtype=np.int32)
+        self.ctx.check(lib().pp_refstream_encode(self._h, workers, words.ctypes.data, words.size,
+                                                 lengths.ctypes.data, C.byref(tmp)), "refstream")
+        return words, lengths, tmp.value
+
+
+def dev_hierarchical_GETRF(h, num_blocks=0, num_threads=0, kernel_size=0):
+    """Reference signature (include/launcher.cuh:18): factor h in place and wait."""
+    h.ctx.check(lib().pp_dev_hierarchical_getrf(h.handle, num_blocks, num_threads, kernel_size),
+                "dev_hierarchical_GETRF")
+
+
+class DataMap2D:
+    """Pitched 2-D byte region (rts/ops.h:9-20)."""
+
+    def __init__(self, ptr, pitch, width, height):
+        self.ptr, self.pitch, self.width, self.height = int(ptr), int(pitch), int(width), int(height)
+
+    def checkOverlap(self, other):
+        return bool(lib().pp_datamap2d_check_overlap(self.ptr, self.pitch, self.width, self.height, other.ptr,
+                                                     other.pitch, other.width, other.height))
+
+
+class Operation:
+    """R/W region list of one operation (rts/ops.h:22-36); `data` holds (read_only, DataMap2D)."""
+
+    def __init__(self, data=()):
+        self.data = list(data)
+
+    def _flat(self):
+        r = np.array([[d.ptr, d.pitch, d.width, d.height] for _, d in self.data], dtype=np.uint64).reshape(-1, 4)
+        ro = np.array([1 if f else 0 for f, _ in self.data], dtype=np.int32)
+        return np.ascontiguousarray(r), ro
+
+    def checkDependencyFrom(self, op_from):
+        rf, rof = op_from._flat()
+        rt, rot = self._flat()
+        return lib().pp_operation_dependency(len(op_from.data), rf.ctypes.data, rof.ctypes.data, len(self.data),
+                                             rt.ctypes.data, rot.ctypes.data)
+
+    def checkDependencyTo(self, op_to):
+        return op_to.checkDependencyFrom(self)
+
+
+# --------------------------------------------------------------------------- problems
+KERNELS = {"inv": 0, "laplace": 1, "exp": 2, "matern32": 3}
+
+
+def kernel_eval(kind, d, p0):
+    if kind == 0:
+        return 1.0 / (d + p0)
+    if kind == 1:
+        return 1.0 / (4.0 * np.pi * (d + p0))
+    if kind == 2:
+        return np.exp(-d / p0)
+    s = np.sqrt(3.0) * d / p0
+    return (1.0 + s) * np.exp(-s)
+
+
+def morton_order(pts):
+    """Indices sorting points of [0,1]^d along a Z-order (Morton) curve."""
+    n, dim = pts.shape
+    bits = 21 if dim <= 3 else 10
+    q = np.clip((pts * (1 << bits)).astype(np.uint64), 0, (1 << bits) - 1)
+    key = np.zeros(n, dtype=np.uint64)
+    for b in range(bits):
+        for d in range(dim):
+            key |= ((q[:, d] >> np.uint64(b)) & np.uint64(1)) << np.uint64(b * dim + d)
+    return np.argsort(key, kind="stable")
+
+
+def truncated_svd(A, k, rng):
+    """Rank-k truncated SVD of A as (U*s, V): exact for small blocks, randomized with
+    oversampling 10 and two power iterations otherwise."""
+    m, n = A.shape
+    k = min(k, m, n)
+    if min(m, n) <= 2 * k + 16:
+        u, s, vt = np.linalg.svd(A, full_matrices=False)
+        return u[:, :k] * s[:k], vt[:k].T.copy()
+    p = min(k + 10, min(m, n))
+    Y = A @ rng.standard_normal((n, p))
+    Q, _ = np.linalg.qr(Y)
+    for _ in range(2):
+        Q, _ = np.linalg.qr(A.T @ Q)
+        Q, _ = np.linalg.qr(A @ Q)
+    B = Q.T @ A
+    ub, s, vt = np.linalg.svd(B, full_matrices=False)
+    U = (Q @ ub[:, :k]) * s[:k]
+    return U, vt[:k].T.copy()
+
+
+class KernelProblem:
+    """Points, kernel and diagonal shift of a kernel-matrix configuration."""
+
+    def __init__(self, n, dim, kernel, p0, shift, points, offdiag_max=None):
+        self.n, self.dim, self.kernel, self.p0, self.shift, self.points = n, dim, kernel, p0, shift, points
+        if offdiag_max is None:
+            offdiag_max = offdiag_rowsum_max(points, kernel, p0)
+        # all kernels here are positive: max row sum of |A| = K(0) + shift + off-diagonal row sum
+        self.norm_inf = float(kernel_eval(kernel, 0.0, p0)) + shift + offdiag_max
+
+    def entries(self, rows, cols):
+        X, Y = self.points[rows], self.points[cols]
+        d = np.sqrt(np.maximum(((X[:, None, :] - Y[None, :, :]) ** 2).sum(-1), 0.0))
+        A = kernel_eval(self.kernel, d, self.p0)
+        ri = np.asarray(rows)[:, None] if not isinstance(rows, slice) else np.arange(rows.start, rows.stop)[:, None]
+        ci = np.asarray(cols)[None, :] if not isinstance(cols, slice) else np.arange(cols.start, cols.stop)[None, :]
+        return A + self.shift * (ri == ci)
+
+    def dense(self):
+        return self.entries(slice(0, self.n), slice(0, self.n))
+
+
+def offdiag_rowsum_max(points, kernel, p0, block=2048):
+    n = points.shape[0]
+    best = 0.0
+    for i0 in range(0, n, block):
+        X = points[i0:i0 + block]
+        s = np.zeros(X.shape[0])
+        for j0 in range(0, n, block):
+            Y = points[j0:j0 + block]
+            d = np.sqrt(((X[:, None, :] - Y[None, :, :]) ** 2).sum(-1))
+            K = np.abs(kernel_eval(kernel, d, p0))
+            if i0 == j0:
+                np.fill_diagonal(K, 0.0)
+            s += K.sum(1)
+        best = max(best, float(s.max()))
+    return best
+
+
+def fill_kernel_hmatrix(h, prob, seed=7):
+    """Dense blocks evaluated exactly; low-rank blocks by truncated SVD at their kmax."""
+    rng = np.random.default_rng(seed)
+    for b in h.blocks():
+        if b["kind"] == DENSE:
+            h.set_dense(b["id"], prob.entries(slice(b["row0"], b["row0"] + b["m"]),
+                                              slice(b["col0"], b["col0"] + b["n"])))
+        elif b["kind"] == LOWRANK:
+            A = prob.entries(slice(b["row0"], b["row0"] + b["m"]), slice(b["col0"], b["col0"] + b["n"]))
+            U, V = truncated_svd(A, b["kmax"], rng)
+            h.set_lowrank(b["id"], U, V)
+
+
+def make_dense_problem(ctx, n=1024, leaf=256, seed=1234):
+    """Configuration 1: A = U[-1,1]^{n x n} + n I, all-dense 2x2 tree down to `leaf`."""
+    rng = np.random.default_rng(seed)
+    A = rng.uniform(-1.0, 1.0, (n, n)) + n * np.eye(n)
+    h = Hierarchical.dense(ctx, n, leaf)
+    for b in h.blocks():
+        if b["kind"] == DENSE:
+            h.set_dense(b["id"], A[b["row0"]:b["row0"] + b["m"], b["col0"]:b["col0"] + b["n"]])
+    return h, A
+
+
+def make_kernel_problem(ctx, n, dim, kernel, p0, leaf, rank, admissibility=0, eta=1.0, shift=None,
+                        shift_factor=2.0, seed=1234):
+    """Kernel-matrix configuration: points U[0,1]^dim (Morton order), A_ij = K(|x_i - x_j|),
+    diagonal shifted by `shift` or by shift_factor * max off-diagonal row sum."""
+    rng = np.random.default_rng(seed)
+    pts = rng.uniform(0.0, 1.0, (n, dim))
+    pts = pts[morton_order(pts)]
+    kid = KERNELS[kernel] if isinstance(kernel, str) else kernel
+    off = offdiag_rowsum_max(pts, kid, p0)
+    if shift is None:
+        shift = shift_factor * off
+    prob = KernelProblem(n, dim, kid, p0, shift, pts, off)
+    h = Hierarchical.geometric(ctx, pts, leaf, admissibility, eta, rank)
+    fill_kernel_hmatrix(h, prob, seed + 1)
+    return h, prob
+
+
+def rhs(n, nrhs=1, seed=99):
+    return np.random.default_rng(seed).uniform(-1.0, 1.0, (n, nrhs))
+
+
+class Refiner:
+    """FP64 iterative refinement around the H-LU solve (no reference counterpart):
+    x_0 = (LU)^-1 b;  r = b - A x (FP64, A evaluated exactly: kernel entries on the fly or
+    the dense FP64 matrix);  x += (LU)^-1 r; until the normwise backward error
+    ||r||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= tol."""
+
+    def __init__(self, h, ctx, prob=None, dense=None, norm_inf=None, stream=None):
+        import torch
+        self.h, self.ctx, self.prob, self.stream = h, ctx, prob, stream
+        if prob is not None:
+            self.pts = torch.from_numpy(np.ascontiguousarray(prob.points)).cuda()
+            self.norm_inf = prob.norm_inf
+        else:
+            self.A = torch.from_numpy(np.ascontiguousarray(dense)).cuda()
+            self.norm_inf = float(np.abs(dense).sum(1).max()) if norm_inf is None else norm_inf
+        self.launches = 0
+
+    def residual(self, x, b, r):
+        if self.prob is not None:
+            self.ctx.kernel_residual(self.prob.kernel, self.prob.p0, self.prob.shift, self.pts, x, b, r, self.stream)
+        else:
+            self.ctx.dense_residual(self.A, x, b, r, self.stream)
+        self.launches += 1
+
+    def solve(self, b, tol=1e-10, max_iter=30, x=None):
+        import torch
+        x = torch.zeros_like(b) if x is None else x
+        r = b.clone()
+        dx = torch.empty_like(b)
+        bn = b.abs().max().item()
+        hist = []
+        for it in range(max_iter):
+            self.h.solve(r, dx, self.stream)
+            self.launches += 2
+            x += dx
+            self.residual(x, b, r)
+            err = r.abs().max().item() / (self.norm_inf * x.abs().max().item() + bn)
+            hist.append(err)
+            if err <= tol:
+                break
+        return x, hist
+
+
+def timed(fn, *a, **k):
+    t0 = time.perf_counter()
+    r = fn(*a, **k)
+    return r, time.perf_counter() - t0

@@ -1,0 +1,621 @@
+// capi.cpp — extern "C" boundary of the engine (include/pastel_palettes.h).
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/pastel_palettes.h"
+#include "hmatrix.h"
+#include "hops.h"
+#include "rts.h"
+#include "vm.cuh"
+
+struct pp_context {
+  int device = -1;   // -1: host-only context (planning, encoding; no compute)
+  int sm_count = 0;
+  int blocks_per_sm = 0;
+  pp_config cfg{};
+  std::string err;
+};
+
+namespace {
+
+struct VmPlan {
+  pp::Program prog;
+  bool built = false;
+  bool on_device = false;
+  int n_tasks = 0, n_ready = 0;
+  pp_task* d_tasks = nullptr;
+  int32_t *d_succ = nullptr, *d_indeg = nullptr, *d_ready = nullptr, *d_counters = nullptr, *d_slots = nullptr;
+  pp_vm_state* d_state = nullptr;
+  double *d_work = nullptr, *d_scratch = nullptr, *d_rhs = nullptr;
+  int64_t work_elems = 0, scratch_elems = 0, rhs_elems = 0;
+  double build_ms = 0;
+  int grid = 0;
+  void release() {
+    cudaFree(d_tasks); cudaFree(d_succ); cudaFree(d_indeg); cudaFree(d_ready); cudaFree(d_counters);
+    cudaFree(d_slots); cudaFree(d_state); cudaFree(d_work); cudaFree(d_scratch); cudaFree(d_rhs);
+    d_tasks = nullptr; d_succ = d_indeg = d_ready = d_counters = d_slots = nullptr; d_state = nullptr;
+    d_work = d_scratch = d_rhs = nullptr;
+    on_device = false;
+  }
+};
+
+uint64_t splitmix64(uint64_t& s) {
+  uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+}  // namespace
+
+struct pp_hmatrix {
+  pp_context* ctx = nullptr;
+  std::unique_ptr<pp::Hierarchical> H;
+  double* d_arena = nullptr;
+  double* d_orig = nullptr;
+  double* d_rand = nullptr;
+  bool pinned = false;
+  std::vector<double> rand_host;
+  VmPlan factor;
+  std::map<int, std::unique_ptr<VmPlan>> solves;
+  VmPlan* last = nullptr;
+  ~pp_hmatrix() {
+    factor.release();
+    for (auto& kv : solves) kv.second->release();
+    if (pinned) cudaHostUnregister(H->host.data());
+    cudaFree(d_arena);
+    cudaFree(d_orig);
+    cudaFree(d_rand);
+  }
+};
+
+namespace {
+
+pp_status fail(pp_context* c, pp_status s, const std::string& msg) {
+  if (c) c->err = msg;
+  return s;
+}
+
+pp_status cuda_fail(pp_context* c, cudaError_t e, const char* what) {
+  return fail(c, e == cudaErrorMemoryAllocation ? PP_OOM : PP_CUDA_ERROR,
+              std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define PP_CUDA(call)                                          \
+  do {                                                         \
+    cudaError_t e_ = (call);                                   \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call);   \
+  } while (0)
+
+bool has_device(const pp_context* c) { return c && c->device >= 0; }
+
+void make_rand(pp_hmatrix* h) {
+  const int64_t count = h->factor.prog.arena_elems.size() > (size_t)pp::AR_RAND
+                            ? h->factor.prog.arena_elems[pp::AR_RAND]
+                            : 0;
+  h->rand_host.resize((size_t)count);
+  uint64_t s = h->ctx->cfg.seed;
+  for (int64_t i = 0; i < count; ++i) {
+    const uint64_t z = splitmix64(s);
+    // uniform in [-1, 1): 53 random bits
+    h->rand_host[(size_t)i] = (double)(z >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+  }
+}
+
+// op generation + DAG for the factor (which = 0) or solve (which = 1) program
+pp_status build_program(pp_hmatrix* h, int which, int nrhs, VmPlan& plan) {
+  pp_context* ctx = h->ctx;
+  if (plan.built) return PP_OK;
+  auto t0 = std::chrono::steady_clock::now();
+  try {
+    pp::Generator g(plan.prog, *h->H, ctx->cfg.tile, h->H->n);
+    if (which == 0) g.getrf_program();
+    else g.solve_program(nrhs);
+    plan.prog.build_dag();
+  } catch (const std::exception& e) {
+    plan.prog = pp::Program();
+    return fail(ctx, PP_UNSUPPORTED, std::string("program generation: ") + e.what());
+  }
+  plan.n_tasks = (int)plan.prog.tasks.size();
+  plan.work_elems = plan.prog.arena_elems[pp::AR_WORK];
+  plan.scratch_elems = plan.prog.arena_elems[pp::AR_SCRATCH];
+  plan.rhs_elems = plan.prog.arena_elems[pp::AR_RHS];
+  plan.built = true;
+  plan.build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return PP_OK;
+}
+
+pp_status plan_to_device(pp_hmatrix* h, VmPlan& plan) {
+  pp_context* ctx = h->ctx;
+  if (plan.on_device) return PP_OK;
+  if (!has_device(ctx)) return fail(ctx, PP_CUDA_ERROR, "no CUDA device in this context");
+  if (!h->d_arena) return fail(ctx, PP_INVALID_ARG, "H-matrix not uploaded");
+  auto t0 = std::chrono::steady_clock::now();
+  const int n = plan.n_tasks;
+  auto alloc = [&](void** p, size_t bytes) { return cudaMalloc(p, bytes ? bytes : 8); };
+  PP_CUDA(alloc((void**)&plan.d_work, sizeof(double) * plan.work_elems));
+  PP_CUDA(alloc((void**)&plan.d_scratch, sizeof(double) * plan.scratch_elems));
+  PP_CUDA(alloc((void**)&plan.d_rhs, sizeof(double) * plan.rhs_elems));
+  std::vector<double*> bases = {h->d_arena, plan.d_work, plan.d_scratch, plan.d_rhs, h->d_rand};
+  std::vector<pp_task> tasks;
+  std::vector<int32_t> succ, indeg, ready;
+  plan.prog.encode(bases, tasks, succ, indeg, ready);
+  plan.n_ready = (int)ready.size();
+  PP_CUDA(alloc((void**)&plan.d_tasks, sizeof(pp_task) * n));
+  PP_CUDA(alloc((void**)&plan.d_succ, sizeof(int32_t) * succ.size()));
+  PP_CUDA(alloc((void**)&plan.d_indeg, sizeof(int32_t) * n));
+  PP_CUDA(alloc((void**)&plan.d_ready, sizeof(int32_t) * ready.size()));
+  PP_CUDA(alloc((void**)&plan.d_counters, sizeof(int32_t) * n));
+  PP_CUDA(alloc((void**)&plan.d_slots, sizeof(int32_t) * n));
+  PP_CUDA(alloc((void**)&plan.d_state, sizeof(pp_vm_state)));
+  PP_CUDA(cudaMemcpy(plan.d_tasks, tasks.data(), sizeof(pp_task) * n, cudaMemcpyHostToDevice));
+  if (!succ.empty()) PP_CUDA(cudaMemcpy(plan.d_succ, succ.data(), sizeof(int32_t) * succ.size(), cudaMemcpyHostToDevice));
+  PP_CUDA(cudaMemcpy(plan.d_indeg, indeg.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+  if (!ready.empty()) PP_CUDA(cudaMemcpy(plan.d_ready, ready.data(), sizeof(int32_t) * ready.size(), cudaMemcpyHostToDevice));
+  PP_CUDA(cudaMemset(plan.d_state, 0, sizeof(pp_vm_state)));
+  const int per_sm = ctx->cfg.ctas_per_sm > 0 ? std::min(ctx->cfg.ctas_per_sm, ctx->blocks_per_sm) : ctx->blocks_per_sm;
+  plan.grid = std::max(1, std::min(n, ctx->sm_count * std::max(1, per_sm)));
+  plan.on_device = true;
+  plan.build_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return PP_OK;
+}
+
+pp_status launch_plan(pp_hmatrix* h, VmPlan& plan, cudaStream_t s, int grid_cap) {
+  pp_context* ctx = h->ctx;
+  if (plan.work_elems > 0) PP_CUDA(cudaMemsetAsync(plan.d_work, 0, sizeof(double) * plan.work_elems, s));
+  pp_vm_launch L;
+  L.tasks = plan.d_tasks;
+  L.n_tasks = plan.n_tasks;
+  L.succ = plan.d_succ;
+  L.indeg = plan.d_indeg;
+  L.ready = plan.d_ready;
+  L.n_ready = plan.n_ready;
+  L.counters = plan.d_counters;
+  L.slots = plan.d_slots;
+  L.state = plan.d_state;
+  L.spin_limit = ctx->cfg.spin_limit;
+  L.grid = grid_cap > 0 ? std::min(plan.grid, grid_cap) : plan.grid;
+  PP_CUDA(pp_vm_run(L, s));
+  h->last = &plan;
+  return PP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+pp_status pp_context_create(int device, const pp_config* cfg, pp_context** out) {
+  if (!out) return PP_INVALID_ARG;
+  *out = nullptr;
+  auto* c = new (std::nothrow) pp_context();
+  if (!c) return PP_OOM;
+  c->cfg.tile = 64;
+  c->cfg.ctas_per_sm = 0;
+  c->cfg.spin_limit = 1ll << 24;
+  c->cfg.seed = 0x5eed5eedull;
+  if (cfg) {
+    if (cfg->tile > 0) c->cfg.tile = cfg->tile;
+    c->cfg.ctas_per_sm = cfg->ctas_per_sm;
+    if (cfg->spin_limit > 0) c->cfg.spin_limit = cfg->spin_limit;
+    if (cfg->seed) c->cfg.seed = cfg->seed;
+  }
+  if (c->cfg.tile < 8 || c->cfg.tile > PP_VM_TILE) { delete c; return PP_INVALID_ARG; }
+  c->device = device;
+  if (device >= 0) {
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || device >= count) { delete c; return PP_CUDA_ERROR; }
+    if (cudaSetDevice(device) != cudaSuccess) { delete c; return PP_CUDA_ERROR; }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) { delete c; return PP_CUDA_ERROR; }
+    c->sm_count = prop.multiProcessorCount;
+    if (pp_vm_prepare() != cudaSuccess) { delete c; return PP_CUDA_ERROR; }
+    c->blocks_per_sm = pp_vm_blocks_per_sm();
+    if (c->blocks_per_sm < 1) { delete c; return PP_CUDA_ERROR; }
+  }
+  *out = c;
+  return PP_OK;
+}
+
+void pp_context_destroy(pp_context* ctx) { delete ctx; }
+
+int pp_last_error(const pp_context* ctx, char* buf, size_t size) {
+  if (!ctx) return 0;
+  if (buf && size) {
+    std::strncpy(buf, ctx->err.c_str(), size - 1);
+    buf[size - 1] = 0;
+  }
+  return (int)ctx->err.size();
+}
+
+int pp_device_sm_count(const pp_context* ctx) { return ctx ? ctx->sm_count : 0; }
+
+static pp_status wrap_hmatrix(pp_context* ctx, pp::Hierarchical* H, pp_hmatrix** out) {
+  auto* h = new (std::nothrow) pp_hmatrix();
+  if (!h) { delete H; return PP_OOM; }
+  h->ctx = ctx;
+  h->H.reset(H);
+  *out = h;
+  return PP_OK;
+}
+
+pp_status pp_hmatrix_create_dense(pp_context* ctx, int n, int leaf, pp_hmatrix** out) {
+  if (!ctx || !out || n <= 0 || leaf <= 0) return fail(ctx, PP_INVALID_ARG, "pp_hmatrix_create_dense: bad argument");
+  try {
+    return wrap_hmatrix(ctx, pp::Hierarchical::dense_tiled(n, leaf), out);
+  } catch (const std::exception& e) {
+    return fail(ctx, PP_INVALID_ARG, e.what());
+  }
+}
+
+pp_status pp_hmatrix_create_geometric(pp_context* ctx, int n, int dim, const double* points, int leaf,
+                                      int admissibility, double eta, int kmax, pp_hmatrix** out) {
+  if (!ctx || !out || !points || n <= 0 || dim <= 0 || leaf <= 0 || kmax <= 0 || kmax > PP_VM_MAX_RANK ||
+      (admissibility != 0 && admissibility != 1))
+    return fail(ctx, PP_INVALID_ARG, "pp_hmatrix_create_geometric: bad argument");
+  try {
+    return wrap_hmatrix(ctx, pp::Hierarchical::geometric(n, dim, points, leaf, admissibility, eta, kmax), out);
+  } catch (const std::exception& e) {
+    return fail(ctx, PP_INVALID_ARG, e.what());
+  }
+}
+
+void pp_hmatrix_destroy(pp_hmatrix* h) { delete h; }
+
+int pp_hmatrix_num_blocks(const pp_hmatrix* h) { return h ? (int)h->H->nodes.size() : 0; }
+int pp_hmatrix_root(const pp_hmatrix* h) { return h ? h->H->root : -1; }
+
+pp_status pp_hmatrix_block_info(const pp_hmatrix* h, int b, pp_block_info* info) {
+  if (!h || !info || b < 0 || b >= (int)h->H->nodes.size()) return PP_INVALID_ARG;
+  const pp::HNode& nd = h->H->nodes[b];
+  info->kind = (int)nd.kind;
+  info->row0 = nd.r0;
+  info->col0 = nd.c0;
+  info->m = nd.m;
+  info->n = nd.n;
+  info->rank = nd.rank;
+  info->kmax = nd.kmax;
+  info->level = nd.level;
+  for (int i = 0; i < 4; ++i) info->children[i] = nd.ch[i];
+  return PP_OK;
+}
+
+pp_status pp_hmatrix_set_dense(pp_hmatrix* h, int b, const double* a, int lda) {
+  if (!h || !a) return PP_INVALID_ARG;
+  try {
+    if (lda < h->H->nodes.at(b).n) return fail(h->ctx, PP_INVALID_ARG, "lda smaller than the block width");
+    h->H->set_dense(b, a, lda);
+  } catch (const std::exception& e) {
+    return fail(h->ctx, PP_INVALID_ARG, e.what());
+  }
+  return PP_OK;
+}
+
+pp_status pp_hmatrix_set_lowrank(pp_hmatrix* h, int b, const double* U, int ldu, const double* V, int ldv, int rank) {
+  if (!h || !U || !V) return PP_INVALID_ARG;
+  try {
+    if (h->factor.built && rank != h->H->nodes.at(b).rank)
+      return fail(h->ctx, PP_INVALID_ARG, "rank change after the factor program was built");
+    h->H->set_lowrank(b, U, ldu, V, ldv, rank);
+  } catch (const std::exception& e) {
+    return fail(h->ctx, PP_INVALID_ARG, e.what());
+  }
+  return PP_OK;
+}
+
+pp_status pp_hmatrix_upload(pp_hmatrix* h, void* stream) {
+  if (!h) return PP_INVALID_ARG;
+  pp_context* ctx = h->ctx;
+  if (!has_device(ctx)) return fail(ctx, PP_CUDA_ERROR, "no CUDA device in this context");
+  const size_t bytes = sizeof(double) * (size_t)std::max<int64_t>(h->H->arena_elems, 1);
+  if (!h->d_arena) PP_CUDA(cudaMalloc((void**)&h->d_arena, bytes));
+  PP_CUDA(cudaMemcpyAsync(h->d_arena, h->H->host.data(), sizeof(double) * h->H->arena_elems, cudaMemcpyHostToDevice,
+                          (cudaStream_t)stream));
+  // the random sketch depends on the factor program's arena sizes
+  pp_status st = build_program(h, 0, 0, h->factor);
+  if (st != PP_OK) return st;
+  if (!h->d_rand) {
+    make_rand(h);
+    PP_CUDA(cudaMalloc((void**)&h->d_rand, sizeof(double) * std::max<size_t>(h->rand_host.size(), 1)));
+    PP_CUDA(cudaMemcpy(h->d_rand, h->rand_host.data(), sizeof(double) * h->rand_host.size(), cudaMemcpyHostToDevice));
+  }
+  return PP_OK;
+}
+
+pp_status pp_hmatrix_download(pp_hmatrix* h, void* stream) {
+  if (!h) return PP_INVALID_ARG;
+  pp_context* ctx = h->ctx;
+  if (!h->d_arena) return fail(ctx, PP_INVALID_ARG, "H-matrix not uploaded");
+  PP_CUDA(cudaMemcpyAsync(h->H->host.data(), h->d_arena, sizeof(double) * h->H->arena_elems, cudaMemcpyDeviceToHost,
+                          (cudaStream_t)stream));
+  PP_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+  return PP_OK;
+}
+
+pp_status pp_hmatrix_pin_host(pp_hmatrix* h) {
+  if (!h) return PP_INVALID_ARG;
+  pp_context* ctx = h->ctx;
+  if (!has_device(ctx)) return fail(ctx, PP_CUDA_ERROR, "no CUDA device in this context");
+  if (h->pinned || h->H->host.empty()) return PP_OK;
+  PP_CUDA(cudaHostRegister(h->H->host.data(), sizeof(double) * h->H->host.size(), cudaHostRegisterDefault));
+  h->pinned = true;
+  return PP_OK;
+}
+
+pp_status pp_hmatrix_keep_original(pp_hmatrix* h, void* stream) {
+  if (!h) return PP_INVALID_ARG;
+  pp_context* ctx = h->ctx;
+  if (!h->d_arena) return fail(ctx, PP_INVALID_ARG, "H-matrix not uploaded");
+  const size_t bytes = sizeof(double) * (size_t)h->H->arena_elems;
+  if (!h->d_orig) PP_CUDA(cudaMalloc((void**)&h->d_orig, std::max<size_t>(bytes, 8)));
+  PP_CUDA(cudaMemcpyAsync(h->d_orig, h->d_arena, bytes, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+  return PP_OK;
+}
+
+pp_status pp_hmatrix_restore(pp_hmatrix* h, void* stream) {
+  if (!h) return PP_INVALID_ARG;
+  pp_context* ctx = h->ctx;
+  if (!h->d_orig) return fail(ctx, PP_INVALID_ARG, "no original kept (pp_hmatrix_keep_original)");
+  PP_CUDA(cudaMemcpyAsync(h->d_arena, h->d_orig, sizeof(double) * (size_t)h->H->arena_elems,
+                          cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+  return PP_OK;
+}
+
+pp_status pp_hmatrix_to_dense(const pp_hmatrix* h, double* out) {
+  if (!h || !out) return PP_INVALID_ARG;
+  h->H->to_dense(out);
+  return PP_OK;
+}
+
+long long pp_hmatrix_storage_elems(const pp_hmatrix* h) { return h ? h->H->storage_elems() : 0; }
+
+double* pp_hmatrix_host_arena(pp_hmatrix* h, long long* elems) {
+  if (!h) return nullptr;
+  if (elems) *elems = h->H->arena_elems;
+  return h->H->host.data();
+}
+const double* pp_hmatrix_device_arena(const pp_hmatrix* h) { return h ? h->d_arena : nullptr; }
+
+pp_status pp_hlu_factor(pp_hmatrix* h, void* stream) {
+  if (!h) return PP_INVALID_ARG;
+  pp_status st = build_program(h, 0, 0, h->factor);
+  if (st != PP_OK) return st;
+  st = plan_to_device(h, h->factor);
+  if (st != PP_OK) return st;
+  return launch_plan(h, h->factor, (cudaStream_t)stream, 0);
+}
+
+static VmPlan* solve_plan(pp_hmatrix* h, int nrhs) {
+  auto it = h->solves.find(nrhs);
+  if (it != h->solves.end()) return it->second.get();
+  auto p = std::make_unique<VmPlan>();
+  VmPlan* raw = p.get();
+  h->solves.emplace(nrhs, std::move(p));
+  return raw;
+}
+
+pp_status pp_hlu_solve(pp_hmatrix* h, const double* b_dev, double* x_dev, int nrhs, void* stream) {
+  if (!h || !b_dev || !x_dev || nrhs <= 0) return fail(h ? h->ctx : nullptr, PP_INVALID_ARG, "pp_hlu_solve: bad argument");
+  pp_context* ctx = h->ctx;
+  VmPlan* plan = solve_plan(h, nrhs);
+  pp_status st = build_program(h, 1, nrhs, *plan);
+  if (st != PP_OK) return st;
+  st = plan_to_device(h, *plan);
+  if (st != PP_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t bytes = sizeof(double) * (size_t)h->H->n * nrhs;
+  PP_CUDA(cudaMemcpyAsync(plan->d_rhs, b_dev, bytes, cudaMemcpyDeviceToDevice, s));
+  st = launch_plan(h, *plan, s, 0);
+  if (st != PP_OK) return st;
+  PP_CUDA(cudaMemcpyAsync(x_dev, plan->d_rhs, bytes, cudaMemcpyDeviceToDevice, s));
+  return PP_OK;
+}
+
+pp_status pp_hmatrix_sync(pp_hmatrix* h, void* stream) {
+  if (!h) return PP_INVALID_ARG;
+  pp_context* ctx = h->ctx;
+  PP_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+  if (!h->last) return PP_OK;
+  pp_vm_state s;
+  PP_CUDA(cudaMemcpy(&s, h->last->d_state, sizeof(s), cudaMemcpyDeviceToHost));
+  if (s.error == PP_VM_TIMEOUT)
+    return fail(ctx, PP_TIMEOUT, "VM: ready-queue slot " + std::to_string(s.err_info) + " never filled");
+  if (s.error == PP_VM_BAD_TASK)
+    return fail(ctx, PP_INTERNAL, "VM: task " + std::to_string(s.err_info) + " has unsupported shape");
+  if (s.done != h->last->n_tasks)
+    return fail(ctx, PP_INTERNAL, "VM: " + std::to_string(s.done) + " of " + std::to_string(h->last->n_tasks) + " tasks ran");
+  return PP_OK;
+}
+
+pp_status pp_hmatrix_program_info(pp_hmatrix* h, int which, int nrhs, pp_program_info* info) {
+  if (!h || !info || (which != 0 && which != 1) || (which == 1 && nrhs <= 0)) return PP_INVALID_ARG;
+  VmPlan* plan = which == 0 ? &h->factor : solve_plan(h, nrhs);
+  pp_status st = build_program(h, which, nrhs, *plan);
+  if (st != PP_OK) return st;
+  std::memset(info, 0, sizeof(*info));
+  info->n_tasks = plan->n_tasks;
+  info->n_edges = plan->prog.edges;
+  info->flops = plan->prog.total_flops();
+  for (int op = 0; op < 10; ++op) info->op_count[op] = plan->prog.count_op(op);
+  for (int a = 0; a < 5; ++a) info->arena_elems[a] = plan->prog.arena_elems[a];
+  info->host_build_ms = plan->build_ms;
+  return PP_OK;
+}
+
+pp_status pp_dev_hierarchical_getrf(pp_hmatrix* h, int num_blocks, int num_threads, int kernel_size) {
+  (void)kernel_size;
+  if (!h) return PP_INVALID_ARG;
+  pp_context* ctx = h->ctx;
+  if (num_threads != 0 && num_threads != PP_VM_THREADS)
+    return fail(ctx, PP_INVALID_ARG, "num_threads must be 0 or 256");
+  pp_status st = build_program(h, 0, 0, h->factor);
+  if (st != PP_OK) return st;
+  if (!h->d_arena) {
+    st = pp_hmatrix_upload(h, nullptr);
+    if (st != PP_OK) return st;
+  }
+  st = plan_to_device(h, h->factor);
+  if (st != PP_OK) return st;
+  st = launch_plan(h, h->factor, nullptr, num_blocks > 0 ? num_blocks : 0);
+  if (st != PP_OK) return st;
+  return pp_hmatrix_sync(h, nullptr);
+}
+
+pp_status pp_dense_residual_dev(pp_context* ctx, const double* A, int lda, int n, const double* x, const double* b,
+                                double* r, int nrhs, void* stream) {
+  if (!has_device(ctx)) return fail(ctx, PP_CUDA_ERROR, "no CUDA device in this context");
+  if (!A || !x || !b || !r || n <= 0 || nrhs <= 0 || lda < n) return fail(ctx, PP_INVALID_ARG, "dense residual: bad argument");
+  PP_CUDA(pp_dense_residual(A, lda, n, x, b, r, nrhs, (cudaStream_t)stream));
+  return PP_OK;
+}
+
+pp_status pp_kernel_residual_dev(pp_context* ctx, int kernel, double p0, double shift, const double* pts, int dim,
+                                 int n, const double* x, const double* b, double* r, int nrhs, void* stream) {
+  if (!has_device(ctx)) return fail(ctx, PP_CUDA_ERROR, "no CUDA device in this context");
+  if (!pts || !x || !b || !r || n <= 0 || nrhs <= 0 || nrhs > 16 || dim < 1 || dim > 3 || kernel < 0 || kernel > 3)
+    return fail(ctx, PP_INVALID_ARG, "kernel residual: bad argument");
+  PP_CUDA(pp_kernel_residual(kernel, p0, 0.0, shift, pts, dim, n, x, b, r, nrhs, (cudaStream_t)stream));
+  return PP_OK;
+}
+
+int pp_datamap2d_check_overlap(uintptr_t pa, size_t pitch_a, size_t width_a, size_t height_a, uintptr_t pb,
+                               size_t pitch_b, size_t width_b, size_t height_b) {
+  pp::DataMap2D a(pa, pitch_a, width_a, height_a), b(pb, pitch_b, width_b, height_b);
+  return a.checkOverlap(b) ? 1 : 0;
+}
+
+int pp_operation_dependency(int n_from, const uint64_t* rf, const int* ro_from, int n_to, const uint64_t* rt,
+                            const int* ro_to) {
+  pp::Operation from, to;
+  for (int i = 0; i < n_from; ++i)
+    from.data.emplace_back(ro_from[i] != 0, pp::DataMap2D(rf[4 * i], rf[4 * i + 1], rf[4 * i + 2], rf[4 * i + 3]));
+  for (int i = 0; i < n_to; ++i)
+    to.data.emplace_back(ro_to[i] != 0, pp::DataMap2D(rt[4 * i], rt[4 * i + 1], rt[4 * i + 2], rt[4 * i + 3]));
+  return (int)to.checkDependencyFrom(from);
+}
+
+pp_status pp_hmatrix_encode_program(pp_hmatrix* h, int which, int nrhs, double* const* bases, void* tasks,
+                                    int32_t* succ, int32_t* indeg, int32_t* order) {
+  if (!h || !bases || !tasks || !indeg || (which != 0 && which != 1)) return PP_INVALID_ARG;
+  VmPlan* plan = which == 0 ? &h->factor : solve_plan(h, nrhs);
+  pp_status st = build_program(h, which, nrhs, *plan);
+  if (st != PP_OK) return st;
+  std::vector<double*> b(bases, bases + pp::PP_ARENAS);
+  std::vector<pp_task> t;
+  std::vector<int32_t> s, d, r;
+  plan->prog.encode(b, t, s, d, r);
+  std::memcpy(tasks, t.data(), sizeof(pp_task) * t.size());
+  if (succ && !s.empty()) std::memcpy(succ, s.data(), sizeof(int32_t) * s.size());
+  std::memcpy(indeg, d.data(), sizeof(int32_t) * d.size());
+  if (order) {
+    for (size_t i = 0; i < t.size(); ++i) order[i] = i < r.size() ? r[i] : -1;
+  }
+  return PP_OK;
+}
+
+pp_status pp_hmatrix_program_edges(pp_hmatrix* h, int which, int nrhs, int64_t* from, int64_t* to, int32_t* type) {
+  if (!h || !from || !to || !type || (which != 0 && which != 1)) return PP_INVALID_ARG;
+  VmPlan* plan = which == 0 ? &h->factor : solve_plan(h, nrhs);
+  pp_status st = build_program(h, which, nrhs, *plan);
+  if (st != PP_OK) return st;
+  int64_t e = 0;
+  std::vector<int64_t> lis;
+  for (int t = 0; t < plan->n_tasks; ++t) {
+    plan->prog.deps.getDepFrom(t, lis);
+    for (int64_t s : lis) {
+      from[e] = t;
+      to[e] = s;
+      type[e] = (int32_t)plan->prog.deps.lookup(t, s);
+      ++e;
+    }
+  }
+  return PP_OK;
+}
+
+pp_status pp_vm_execute(pp_context* ctx, const void* tasks, int n, const int32_t* succ, long long n_succ,
+                        const int32_t* indeg, long long spin_limit, int grid, void* stream) {
+  if (!ctx || !tasks || !indeg || n <= 0 || n_succ < 0 || (n_succ > 0 && !succ))
+    return fail(ctx, PP_INVALID_ARG, "pp_vm_execute: bad argument");
+  if (!has_device(ctx)) return fail(ctx, PP_CUDA_ERROR, "no CUDA device in this context");
+  const pp_task* T = static_cast<const pp_task*>(tasks);
+  std::vector<int32_t> ready;
+  for (int i = 0; i < n; ++i) {
+    if (T[i].n_succ < 0 || T[i].succ_begin < 0 || (long long)T[i].succ_begin + T[i].n_succ > n_succ)
+      return fail(ctx, PP_INVALID_ARG, "pp_vm_execute: successor range outside succ");
+    if (indeg[i] == 0) ready.push_back(i);
+  }
+  for (long long q = 0; q < n_succ; ++q)
+    if (succ[q] < 0 || succ[q] >= n) return fail(ctx, PP_INVALID_ARG, "pp_vm_execute: successor id out of range");
+  VmPlan p;
+  p.n_tasks = n;
+  p.n_ready = (int)ready.size();
+  PP_CUDA(cudaMalloc((void**)&p.d_tasks, sizeof(pp_task) * n));
+  PP_CUDA(cudaMalloc((void**)&p.d_succ, sizeof(int32_t) * std::max<long long>(n_succ, 1)));
+  PP_CUDA(cudaMalloc((void**)&p.d_indeg, sizeof(int32_t) * n));
+  PP_CUDA(cudaMalloc((void**)&p.d_ready, sizeof(int32_t) * std::max<size_t>(ready.size(), 1)));
+  PP_CUDA(cudaMalloc((void**)&p.d_counters, sizeof(int32_t) * n));
+  PP_CUDA(cudaMalloc((void**)&p.d_slots, sizeof(int32_t) * n));
+  PP_CUDA(cudaMalloc((void**)&p.d_state, sizeof(pp_vm_state)));
+  PP_CUDA(cudaMemcpy(p.d_tasks, T, sizeof(pp_task) * n, cudaMemcpyHostToDevice));
+  if (n_succ > 0) PP_CUDA(cudaMemcpy(p.d_succ, succ, sizeof(int32_t) * n_succ, cudaMemcpyHostToDevice));
+  PP_CUDA(cudaMemcpy(p.d_indeg, indeg, sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+  if (!ready.empty()) PP_CUDA(cudaMemcpy(p.d_ready, ready.data(), sizeof(int32_t) * ready.size(), cudaMemcpyHostToDevice));
+  pp_vm_launch L;
+  L.tasks = p.d_tasks; L.n_tasks = n; L.succ = p.d_succ; L.indeg = p.d_indeg; L.ready = p.d_ready;
+  L.n_ready = p.n_ready; L.counters = p.d_counters; L.slots = p.d_slots; L.state = p.d_state;
+  L.spin_limit = spin_limit > 0 ? spin_limit : ctx->cfg.spin_limit;
+  L.grid = grid > 0 ? grid : std::max(1, std::min(n, ctx->sm_count * ctx->blocks_per_sm));
+  cudaStream_t s = (cudaStream_t)stream;
+  PP_CUDA(pp_vm_run(L, s));
+  PP_CUDA(cudaStreamSynchronize(s));
+  pp_vm_state st;
+  PP_CUDA(cudaMemcpy(&st, p.d_state, sizeof(st), cudaMemcpyDeviceToHost));
+  p.release();
+  if (st.error == PP_VM_TIMEOUT) return fail(ctx, PP_TIMEOUT, "VM: ready-queue slot " + std::to_string(st.err_info) + " never filled");
+  if (st.error == PP_VM_BAD_TASK) return fail(ctx, PP_INTERNAL, "VM: task " + std::to_string(st.err_info) + " has unsupported shape");
+  if (st.done != n) return fail(ctx, PP_INTERNAL, "VM: " + std::to_string(st.done) + " of " + std::to_string(n) + " tasks ran");
+  return PP_OK;
+}
+
+pp_status pp_hmatrix_rand_host(pp_hmatrix* h, double* out, long long count) {
+  if (!h || !out) return PP_INVALID_ARG;
+  pp_status st = build_program(h, 0, 0, h->factor);
+  if (st != PP_OK) return st;
+  if (h->rand_host.empty()) make_rand(h);
+  if (count > (long long)h->rand_host.size()) return fail(h->ctx, PP_INVALID_ARG, "rand_host: count too large");
+  std::memcpy(out, h->rand_host.data(), sizeof(double) * count);
+  return PP_OK;
+}
+
+pp_status pp_refstream_encode(pp_hmatrix* h, int workers, int32_t* words, long long capacity, int32_t* lengths,
+                              long long* tmp_elems) {
+  if (!h || workers <= 0 || !lengths) return PP_INVALID_ARG;
+  pp_status st = build_program(h, 0, 0, h->factor);
+  if (st != PP_OK) return st;
+  std::vector<std::vector<int32_t>> streams;
+  std::string err;
+  int64_t tmp = 0;
+  if (!h->factor.prog.encode_reference(workers, streams, err, &tmp)) return fail(h->ctx, PP_UNSUPPORTED, err);
+  long long total = 0;
+  for (auto& s : streams) total += (long long)s.size();
+  for (int w = 0; w < workers; ++w) lengths[w] = (int32_t)streams[w].size();
+  if (tmp_elems) *tmp_elems = tmp;
+  if (!words) return PP_OK;  // size query
+  if (total > capacity) return fail(h->ctx, PP_INVALID_ARG, "refstream: capacity too small");
+  long long at = 0;
+  for (auto& s : streams) {
+    std::memcpy(words + at, s.data(), sizeof(int32_t) * s.size());
+    at += (long long)s.size();
+  }
+  return PP_OK;
+}
+
+}  // extern "C"

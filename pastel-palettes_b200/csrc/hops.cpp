@@ -1,0 +1,712 @@
+// hops.cpp — H-LU operation generator, DAG construction and encoders.
+#include "hops.h"
+
+#include <algorithm>
+#include <stdexcept>
+
+namespace pp {
+
+// ----------------------------------------------------------------------------- views
+View View::sub(int i, int j, int mm, int nn) const {
+  View v = *this;
+  v.m = mm;
+  v.n = nn;
+  if (!t) { v.r0 += i; v.c0 += j; }
+  else { v.r0 += j; v.c0 += i; }
+  return v;
+}
+
+View View::T() const {
+  View v = *this;
+  v.t = !t;
+  std::swap(v.m, v.n);
+  return v;
+}
+
+static Mat transpose(const Mat& X) {
+  Mat Y = X;
+  std::swap(Y.m, Y.n);
+  if (X.kind == Mat::D) Y.d = X.d.T();
+  else if (X.kind == Mat::LR) { Y.u = X.v; Y.v = X.u; }
+  else Y.tr = !X.tr;
+  return Y;
+}
+
+// ----------------------------------------------------------------------------- flops
+static int64_t flops_getrf(int64_t m, int64_t n) {
+  int64_t f = 0;
+  const int64_t mn = std::min(m, n);
+  for (int64_t i = 0; i < mn; ++i) f += (m - i - 1) + 2 * (m - i - 1) * (n - i - 1);
+  return f;
+}
+
+// ----------------------------------------------------------------------------- program
+int Program::add_instance() {
+  int id = n_instances++;
+  arena_elems.resize((size_t)n_instances * PP_ARENAS, 0);
+  return id;
+}
+
+int Program::add_obj_at(int arena, int64_t off, int rows, int cols, int ld, bool tracked) {
+  objs.push_back({arena, off, rows, cols, ld, tracked});
+  return (int)objs.size() - 1;
+}
+
+int Program::add_obj(int arena, int rows, int cols, bool tracked) {
+  int64_t off = (arena_elems[arena] + 3) & ~int64_t(3);
+  arena_elems[arena] = off + (int64_t)rows * cols;
+  return add_obj_at(arena, off, rows, cols, cols, tracked);
+}
+
+int64_t Program::total_flops() const {
+  int64_t s = 0;
+  for (auto& t : tasks) s += t.flops;
+  return s;
+}
+
+int64_t Program::count_op(int op) const {
+  int64_t c = 0;
+  for (auto& t : tasks) c += t.t.op == op;
+  return c;
+}
+
+static inline bool rect_overlap(const Region& a, const Region& b) {
+  return a.r0 < b.r0 + b.nr && b.r0 < a.r0 + a.nr && a.c0 < b.c0 + b.nc && b.c0 < a.c0 + a.nc;
+}
+static inline bool rect_covers(const Region& a, const Region& b) {
+  return a.r0 <= b.r0 && b.r0 + b.nr <= a.r0 + a.nr && a.c0 <= b.c0 && b.c0 + b.nc <= a.c0 + a.nc;
+}
+
+// Program order is a valid sequential execution; an edge joins every pair of tasks
+// whose regions overlap with at least one write (flow / anti / out).  Scanning an
+// object's earlier accesses newest-first stops at a write that covers the current
+// region: anything older that overlaps it is already ordered before that write.
+// Accesses fully covered by a later write are dropped for the same reason.
+void Program::build_dag() {
+  const int n = (int)tasks.size();
+  succ.assign(n, {});
+  pred.assign(n, {});
+  deps.clear();
+  struct Acc { int task; Region r; };
+  std::vector<std::vector<Acc>> acc(objs.size());
+  std::vector<int> mark(n, -1), depbits(n, 0);
+  std::vector<int> touched;
+  edges = 0;
+  for (int t = 0; t < n; ++t) {
+    touched.clear();
+    for (const Region& r : tasks[t].regions) {
+      auto& L = acc[r.obj];
+      for (int q = (int)L.size() - 1; q >= 0; --q) {
+        const Acc& a = L[q];
+        if (a.task == t || !rect_overlap(a.r, r)) continue;
+        int d = 0;
+        if (!a.r.ro && r.ro) d |= (int)dependency_t::flow;
+        if (a.r.ro && !r.ro) d |= (int)dependency_t::anti;
+        if (!a.r.ro && !r.ro) d |= (int)dependency_t::out;
+        if (d) {
+          if (mark[a.task] != t) { mark[a.task] = t; depbits[a.task] = 0; touched.push_back(a.task); }
+          depbits[a.task] |= d;
+        }
+        if (!a.r.ro && rect_covers(a.r, r)) break;
+      }
+    }
+    for (const Region& r : tasks[t].regions) {
+      auto& L = acc[r.obj];
+      if (!r.ro)
+        L.erase(std::remove_if(L.begin(), L.end(), [&](const Acc& a) { return rect_covers(r, a.r); }), L.end());
+      L.push_back({t, r});
+    }
+    std::sort(touched.begin(), touched.end());
+    for (int p : touched) {
+      pred[t].push_back(p);
+      succ[p].push_back(t);
+      deps.update(p, t, (dependency_t)depbits[p]);
+      ++edges;
+    }
+  }
+  blevel.assign(n, 0);
+  for (int t = n - 1; t >= 0; --t) {
+    int64_t b = 0;
+    for (int s : succ[t]) b = std::max(b, blevel[s]);
+    blevel[t] = b + std::max<int64_t>(tasks[t].flops, 1 << 14);
+  }
+}
+
+h_ops_dag Program::to_dag() const {
+  h_ops_dag d;
+  d.length = (int)tasks.size();
+  d.succ = succ;
+  d.pred = pred;
+  d.flops.resize(tasks.size());
+  for (size_t i = 0; i < tasks.size(); ++i) d.flops[i] = tasks[i].flops;
+  return d;
+}
+
+void Program::encode(const std::vector<double*>& bases, std::vector<pp_task>& out, std::vector<int32_t>& succ_out,
+                     std::vector<int32_t>& indeg_out, std::vector<int32_t>& ready_out) const {
+  const int n = (int)tasks.size();
+  out.resize(n);
+  succ_out.clear();
+  indeg_out.resize(n);
+  ready_out.clear();
+  std::vector<int> s;
+  for (int t = 0; t < n; ++t) {
+    const HTask& h = tasks[t];
+    pp_task x = h.t;
+    for (int k = 0; k < 6; ++k) {
+      if (!h.has[k]) { x.p[k] = nullptr; continue; }
+      const View& v = h.opnd[k];
+      const PObj& o = objs[v.obj];
+      double* base = bases.at(o.arena);
+      x.p[k] = base ? base + o.off + (int64_t)v.r0 * o.ld + v.c0 : nullptr;
+      x.ld[k] = o.ld;
+    }
+    if (h.scratch_elems > 0) {
+      double* base = bases.at(h.t.instance * PP_ARENAS + AR_SCRATCH);
+      x.tmp = base ? base + h.scratch_off : nullptr;
+    } else {
+      x.tmp = nullptr;
+    }
+    s = succ[t];
+    std::stable_sort(s.begin(), s.end(), [&](int a, int b) { return blevel[a] > blevel[b]; });
+    x.succ_begin = (int32_t)succ_out.size();
+    x.n_succ = (int32_t)s.size();
+    succ_out.insert(succ_out.end(), s.begin(), s.end());
+    indeg_out[t] = (int32_t)pred[t].size();
+    if (pred[t].empty()) ready_out.push_back(t);
+    out[t] = x;
+  }
+  std::stable_sort(ready_out.begin(), ready_out.end(), [&](int a, int b) { return blevel[a] > blevel[b]; });
+}
+
+void Program::merge(const Program& o) {
+  const int obj0 = (int)objs.size(), task0 = (int)tasks.size(), inst0 = n_instances;
+  for (const PObj& p : o.objs) {
+    PObj q = p;
+    q.arena += inst0 * PP_ARENAS;
+    objs.push_back(q);
+  }
+  n_instances += o.n_instances;
+  arena_elems.insert(arena_elems.end(), o.arena_elems.begin(), o.arena_elems.end());
+  for (const HTask& h : o.tasks) {
+    HTask g = h;
+    g.t.instance += inst0;
+    for (int k = 0; k < 6; ++k)
+      if (g.has[k]) g.opnd[k].obj += obj0;
+    for (Region& r : g.regions) r.obj += obj0;
+    tasks.push_back(std::move(g));
+  }
+  succ.resize(tasks.size());
+  pred.resize(tasks.size());
+  blevel.resize(tasks.size());
+  for (size_t t = 0; t < o.tasks.size(); ++t) {
+    for (int x : o.succ[t]) succ[task0 + t].push_back(x + task0);
+    for (int x : o.pred[t]) pred[task0 + t].push_back(x + task0);
+    blevel[task0 + t] = o.blevel[t];
+  }
+  edges += o.edges;
+}
+
+// ----------------------------------------------------------------------------- reference format
+// Word layout of src/kernel.cu:1404-1501 (operation arguments after opcode, signal, operation).
+namespace refisa {
+enum { finish = 0, execute = 1, signal_wait = 2 };
+enum { nop = 0, getrf = 1, trsml = 2, trsmr = 3, gemm = 4, gemm_plus = 5, gemm_3x = 6, gemm_4x = 7, accum = 8 };
+}  // namespace refisa
+
+bool Program::encode_reference(int workers, std::vector<std::vector<int32_t>>& streams, std::string& err,
+                               int64_t* tmp_elems_per_worker) const {
+  if (workers <= 0) { err = "workers must be positive"; return false; }
+  h_ops_dag dag = to_dag();
+  instructions_scheduler sched(dag, workers);
+  streams.assign(workers, {});
+  int64_t tmp_need = 0;
+  auto ptr_off = [&](const HTask& h, int k, int32_t& ptr, int32_t& off) -> bool {
+    const View& v = h.opnd[k];
+    const PObj& o = objs[v.obj];
+    int64_t e = o.off + (int64_t)v.r0 * o.ld + v.c0;
+    if (e > INT32_MAX) { err = "element offset exceeds the reference's int32 format"; return false; }
+    ptr = o.arena;
+    off = (int32_t)e;
+    return true;
+  };
+  for (int w = 0; w < workers; ++w) {
+    auto& S = streams[w];
+    for (const auto& en : sched.getSchedule(w)) {
+      if (!en.exe) {
+        S.insert(S.end(), {refisa::signal_wait, en.inst, 64});
+        continue;
+      }
+      const HTask& h = tasks[en.inst];
+      const pp_task& x = h.t;
+      auto T = [&](int k) { return (x.flags & PP_T(k)) ? 1 : 0; };
+      int32_t p[6] = {0}, o[6] = {0};
+      for (int k = 0; k < 6; ++k)
+        if (h.has[k] && !ptr_off(h, k, p[k], o[k])) return false;
+      S.push_back(refisa::execute);
+      S.push_back(en.inst);
+      switch (x.op) {
+        case PP_OP_GETRF:
+          S.insert(S.end(), {refisa::getrf, p[0], o[0], x.n, x.m, x.ld[0]});
+          break;
+        case PP_OP_TRSML:
+          S.insert(S.end(), {refisa::trsml, p[0], p[1], o[0], o[1], x.n, x.m, x.m, x.ld[0], x.ld[1], 0});
+          break;
+        case PP_OP_TRSMR:
+          S.insert(S.end(), {refisa::trsmr, p[0], p[1], o[0], o[1], x.n, x.m, x.n, x.ld[0], x.ld[1], 0});
+          break;
+        case PP_OP_TRSMRT:
+          S.insert(S.end(), {refisa::trsmr, p[0], p[1], o[0], o[1], x.m, x.n, x.m, x.ld[0], x.ld[1], 1});
+          break;
+        case PP_OP_GEMM: {
+          int opn;
+          if (x.beta == 1.0 && x.alpha == -1.0) opn = refisa::gemm;
+          else if (x.beta == 1.0 && x.alpha == 1.0) opn = refisa::gemm_plus;
+          else { err = "GEMM with alpha/beta outside the reference's gemm / gemm_plus"; return false; }
+          S.insert(S.end(), {opn, p[0], p[1], p[2], o[0], o[1], o[2], x.m, x.n, x.k, x.ld[0], x.ld[1], x.ld[2],
+                             T(1), T(2)});
+          break;
+        }
+        case PP_OP_GEMM3:
+          if (x.alpha != -1.0) { err = "GEMM3 alpha must be -1 in the reference format"; return false; }
+          S.insert(S.end(), {refisa::gemm_3x, p[0], p[1], p[2], p[3], o[0], o[1], o[2], o[3], x.m, x.n, x.k, x.l,
+                             x.ld[0], x.ld[1], x.ld[2], x.ld[3], T(1), T(2), T(3), x.ctrl});
+          tmp_need = std::max<int64_t>(tmp_need, h.scratch_elems);
+          break;
+        case PP_OP_GEMM4: {
+          if (x.alpha != -1.0) { err = "GEMM4 alpha must be -1 in the reference format"; return false; }
+          // the reference keeps t1 at my_tmp[0] and t2 at my_tmp[offset]
+          const int32_t offset = x.aux;
+          S.insert(S.end(), {refisa::gemm_4x, p[0], p[1], p[2], p[3], p[4], o[0], o[1], o[2], o[3], o[4], x.m, x.n,
+                             x.k, x.l, x.o, x.ld[0], x.ld[1], x.ld[2], x.ld[3], x.ld[4], T(1), T(2), T(3), T(4),
+                             x.ctrl, offset});
+          tmp_need = std::max<int64_t>(tmp_need, h.scratch_elems);
+          break;
+        }
+        case PP_OP_ACCUM: {
+          if (x.alpha != 1.0 || T(2) || T(3)) { err = "accum with a sign or transposed factors has no reference form"; return false; }
+          if (x.ld[4] != x.k) { err = "accum random sketch must have ld = rank"; return false; }
+          // my_tmp: U (ny x k1) | V (nx x k1) | Q (max(ny x k1, k1 x k2))
+          const int64_t off1 = (int64_t)x.m * x.k, off2 = off1 + (int64_t)x.n * x.k;
+          const int64_t qsz = std::max<int64_t>((int64_t)x.m * x.k, (int64_t)x.k * std::max(x.k, x.l));
+          tmp_need = std::max<int64_t>(tmp_need, off2 + qsz);
+          S.insert(S.end(), {refisa::accum, p[0], p[1], p[2], p[3], o[0], o[1], o[2], o[3], x.n, x.m, x.k, x.l,
+                             x.ld[0], x.ld[1], x.ld[2], x.ld[3], (int32_t)off1, (int32_t)off2});
+          break;
+        }
+        default:
+          err = "instruction has no reference-format counterpart (op " + std::to_string(x.op) + ")";
+          return false;
+      }
+    }
+    S.push_back(refisa::finish);
+  }
+  if (tmp_elems_per_worker) *tmp_elems_per_worker = tmp_need;
+  return true;
+}
+
+// ----------------------------------------------------------------------------- generator
+Generator::Generator(Program& P, Hierarchical& H, int tile, int max_n_rand)
+    : P_(P), H_(H), T_(tile), max_n_rand_(max_n_rand) {
+  if (tile < 8) throw std::invalid_argument("tile must be >= 8");
+  inst_ = P.add_instance();
+  const int ar = P.arena_id(inst_, AR_MATRIX);
+  P.arena_elems[ar] = H.arena_elems;
+  node_obj_.resize(H.objs.size());
+  for (size_t i = 0; i < H.objs.size(); ++i)
+    node_obj_[i] = P.add_obj_at(ar, H.objs[i].off, H.objs[i].rows, H.objs[i].cols, H.objs[i].ld, true);
+  for (auto& x : rand_ld_obj_) x = -1;
+  int kmax = 1;
+  for (auto& nd : H.nodes)
+    if (nd.kind == HNode::LR) kmax = std::max(kmax, nd.kmax);
+  P.arena_elems[P.arena_id(inst_, AR_RAND)] = (int64_t)std::max(max_n_rand, H.n) * kmax;
+}
+
+int Generator::rand_obj(int k1) {
+  if (k1 < 1 || k1 > 64) throw std::invalid_argument("rank outside 1..64");
+  if (rand_ld_obj_[k1] < 0)
+    rand_ld_obj_[k1] = P_.add_obj_at(P_.arena_id(inst_, AR_RAND), 0, std::max(max_n_rand_, H_.n), k1, k1, false);
+  return rand_ld_obj_[k1];
+}
+
+Mat Generator::asD(const View& v) const {
+  Mat M;
+  M.kind = Mat::D;
+  M.m = v.m;
+  M.n = v.n;
+  M.d = v;
+  return M;
+}
+
+Mat Generator::node(int id, bool tr) const {
+  const HNode& nd = H_.nodes.at(id);
+  Mat M;
+  M.m = tr ? nd.n : nd.m;
+  M.n = tr ? nd.m : nd.n;
+  if (nd.kind == HNode::D) {
+    M.kind = Mat::D;
+    View v;
+    v.obj = node_obj_[nd.obj];
+    v.m = nd.m;
+    v.n = nd.n;
+    M.d = tr ? v.T() : v;
+  } else if (nd.kind == HNode::LR) {
+    M.kind = Mat::LR;
+    View u, v;
+    u.obj = node_obj_[nd.obj];
+    u.m = nd.m;
+    u.n = nd.rank;
+    v.obj = node_obj_[nd.objV];
+    v.m = nd.n;
+    v.n = nd.rank;
+    M.k = nd.rank;
+    M.u = tr ? v : u;
+    M.v = tr ? u : v;
+  } else {
+    M.kind = Mat::H;
+    M.node = id;
+    M.tr = tr;
+  }
+  return M;
+}
+
+Mat Generator::child(const Mat& X, int i, int j) const {
+  const HNode& nd = H_.nodes.at(X.node);
+  return X.tr ? node(nd.ch[j * 2 + i], true) : node(nd.ch[i * 2 + j], false);
+}
+
+int Generator::hsplit_r(const Mat& X) const { return X.kind == Mat::H ? child(X, 0, 0).m : -1; }
+int Generator::hsplit_c(const Mat& X) const { return X.kind == Mat::H ? child(X, 0, 0).n : -1; }
+
+int Generator::tri_split(const Mat& X) const {
+  if (X.kind == Mat::H) return hsplit_r(X);
+  if (X.kind == Mat::D && X.m > T_) {
+    int s = X.m / 2;
+    if (X.m >= 32) s = (s + 7) & ~7;
+    return s;
+  }
+  return -1;
+}
+
+void Generator::partition(const Mat& X, int rs, int cs, Mat out[2][2], int& nr, int& nc) const {
+  nr = rs < 0 ? 1 : 2;
+  nc = cs < 0 ? 1 : 2;
+  const int roff[2] = {0, rs < 0 ? 0 : rs}, coff[2] = {0, cs < 0 ? 0 : cs};
+  const int rsz[2] = {rs < 0 ? X.m : rs, rs < 0 ? 0 : X.m - rs};
+  const int csz[2] = {cs < 0 ? X.n : cs, cs < 0 ? 0 : X.n - cs};
+  if (X.kind == Mat::H) {
+    if (rs != hsplit_r(X) || cs != hsplit_c(X))
+      throw std::runtime_error("partition: block structures of the operands do not match");
+    for (int i = 0; i < 2; ++i)
+      for (int j = 0; j < 2; ++j) out[i][j] = child(X, i, j);
+    return;
+  }
+  for (int i = 0; i < nr; ++i)
+    for (int j = 0; j < nc; ++j) {
+      Mat M;
+      M.kind = X.kind;
+      M.m = rsz[i];
+      M.n = csz[j];
+      if (X.kind == Mat::D) {
+        M.d = X.d.sub(roff[i], coff[j], rsz[i], csz[j]);
+      } else {
+        M.k = X.k;
+        M.u = X.u.sub(roff[i], 0, rsz[i], X.k);
+        M.v = X.v.sub(coff[j], 0, csz[j], X.k);
+      }
+      out[i][j] = M;
+    }
+}
+
+View Generator::tmp(int rows, int cols) {
+  View v;
+  v.obj = P_.add_obj(P_.arena_id(inst_, AR_WORK), rows, cols, true);
+  v.m = rows;
+  v.n = cols;
+  return v;
+}
+
+HTask& Generator::emit(int op) {
+  P_.tasks.emplace_back();
+  HTask& t = P_.tasks.back();
+  t.t.op = op;
+  t.t.instance = inst_;
+  t.t.alpha = 1.0;
+  t.t.beta = 1.0;
+  return t;
+}
+
+void Generator::bind(HTask& t, int slot, const View& v, bool write) {
+  t.opnd[slot] = v;
+  t.has[slot] = true;
+  const PObj& o = P_.objs[v.obj];
+  t.t.ld[slot] = o.ld;
+  if (v.t) t.t.flags |= PP_T(slot);
+  if (v.r0 < 0 || v.c0 < 0 || v.r0 + v.srows() > o.rows || v.c0 + v.scols() > o.cols)
+    throw std::logic_error("operand view outside its storage object");
+  if (o.tracked) t.regions.push_back({v.obj, v.r0, v.c0, v.srows(), v.scols(), !write});
+}
+
+// --------------------------------------------------------------------------- H-LU
+void Generator::getrf_program() { getrf(node(H_.root)); }
+
+void Generator::solve_program(int nrhs) {
+  rhs_obj_ = P_.add_obj(P_.arena_id(inst_, AR_RHS), H_.n, nrhs, true);
+  View b;
+  b.obj = rhs_obj_;
+  b.m = H_.n;
+  b.n = nrhs;
+  trsml(node(H_.root), asD(b));
+  trsmu(node(H_.root), asD(b));
+}
+
+void Generator::getrf(const Mat& A) {
+  if (A.kind == Mat::LR) throw std::logic_error("getrf on a low-rank block");
+  const int s = tri_split(A);
+  if (s < 0) {
+    HTask& t = emit(PP_OP_GETRF);
+    bind(t, 0, A.d, true);
+    t.t.m = A.m;
+    t.t.n = A.n;
+    t.flops = flops_getrf(A.m, A.n);
+    return;
+  }
+  Mat p[2][2];
+  int nr, nc;
+  partition(A, s, A.kind == Mat::H ? hsplit_c(A) : s, p, nr, nc);
+  getrf(p[0][0]);
+  trsml(p[0][0], p[0][1]);
+  trsmr(p[0][0], p[1][0]);
+  gemm(p[1][1], p[1][0], p[0][1], -1);
+  getrf(p[1][1]);
+}
+
+void Generator::trsml(const Mat& L, const Mat& B) {
+  if (B.kind == Mat::LR) { trsml(L, asD(B.u)); return; }
+  const int s = tri_split(L);
+  if (s < 0) {
+    if (B.kind != Mat::D || B.d.t) throw std::logic_error("trsml: target must be a dense untransposed block");
+    for (int c = 0; c < B.n; c += T_) {
+      const int w = std::min(T_, B.n - c);
+      HTask& t = emit(PP_OP_TRSML);
+      bind(t, 0, B.d.sub(0, c, B.m, w), true);
+      bind(t, 1, L.d, false);
+      t.t.m = B.m;
+      t.t.n = w;
+      t.flops = (int64_t)w * B.m * (B.m - 1);
+    }
+    return;
+  }
+  Mat Lp[2][2], Bp[2][2];
+  int a, b, br, bc;
+  partition(L, s, L.kind == Mat::H ? hsplit_c(L) : s, Lp, a, b);
+  partition(B, s, hsplit_c(B), Bp, br, bc);
+  for (int j = 0; j < bc; ++j) {
+    trsml(Lp[0][0], Bp[0][j]);
+    gemm(Bp[1][j], Lp[1][0], Bp[0][j], -1);
+    trsml(Lp[1][1], Bp[1][j]);
+  }
+}
+
+void Generator::trsmr(const Mat& U, const Mat& B) {
+  if (B.kind == Mat::LR) { trsmrt(U, B.v); return; }
+  const int s = tri_split(U);
+  if (s < 0) {
+    if (B.kind != Mat::D || B.d.t) throw std::logic_error("trsmr: target must be a dense untransposed block");
+    const int rows = std::max(T_, 4096 / std::max(1, B.n));
+    for (int r = 0; r < B.m; r += rows) {
+      const int h = std::min(rows, B.m - r);
+      HTask& t = emit(PP_OP_TRSMR);
+      bind(t, 0, B.d.sub(r, 0, h, B.n), true);
+      bind(t, 1, U.d, false);
+      t.t.m = h;
+      t.t.n = B.n;
+      t.flops = (int64_t)h * B.n * B.n;
+    }
+    return;
+  }
+  Mat Up[2][2], Bp[2][2];
+  int a, b, br, bc;
+  partition(U, s, U.kind == Mat::H ? hsplit_c(U) : s, Up, a, b);
+  partition(B, hsplit_r(B), s, Bp, br, bc);
+  for (int i = 0; i < br; ++i) {
+    trsmr(Up[0][0], Bp[i][0]);
+    gemm(Bp[i][1], Bp[i][0], Up[0][1], -1);
+    trsmr(Up[1][1], Bp[i][1]);
+  }
+}
+
+void Generator::trsmrt(const Mat& U, const View& V) {
+  if (V.t) throw std::logic_error("trsmrt: V must be untransposed");
+  const int s = tri_split(U);
+  if (s < 0) {
+    for (int c = 0; c < V.n; c += T_) {
+      const int w = std::min(T_, V.n - c);
+      HTask& t = emit(PP_OP_TRSMRT);
+      bind(t, 0, V.sub(0, c, V.m, w), true);
+      bind(t, 1, U.d, false);
+      t.t.m = V.m;
+      t.t.n = w;
+      t.flops = (int64_t)w * V.m * V.m;
+    }
+    return;
+  }
+  Mat Up[2][2];
+  int a, b;
+  partition(U, s, U.kind == Mat::H ? hsplit_c(U) : s, Up, a, b);
+  View V0 = V.sub(0, 0, s, V.n), V1 = V.sub(s, 0, V.m - s, V.n);
+  trsmrt(Up[0][0], V0);
+  gemm(asD(V1), transpose(Up[0][1]), asD(V0), -1);
+  trsmrt(Up[1][1], V1);
+}
+
+void Generator::trsmu(const Mat& U, const Mat& B) {
+  if (B.kind == Mat::LR) { trsmu(U, asD(B.u)); return; }
+  const int s = tri_split(U);
+  if (s < 0) {
+    if (B.kind != Mat::D || B.d.t) throw std::logic_error("trsmu: target must be a dense untransposed block");
+    for (int c = 0; c < B.n; c += T_) {
+      const int w = std::min(T_, B.n - c);
+      HTask& t = emit(PP_OP_TRSMU);
+      bind(t, 0, B.d.sub(0, c, B.m, w), true);
+      bind(t, 1, U.d, false);
+      t.t.m = B.m;
+      t.t.n = w;
+      t.flops = (int64_t)w * B.m * B.m;
+    }
+    return;
+  }
+  Mat Up[2][2], Bp[2][2];
+  int a, b, br, bc;
+  partition(U, s, U.kind == Mat::H ? hsplit_c(U) : s, Up, a, b);
+  partition(B, s, hsplit_c(B), Bp, br, bc);
+  for (int j = 0; j < bc; ++j) {
+    trsmu(Up[1][1], Bp[1][j]);
+    gemm(Bp[0][j], Up[0][1], Bp[1][j], -1);
+    trsmu(Up[0][0], Bp[0][j]);
+  }
+}
+
+void Generator::gemm_tiles(const View& C, const View& A, const View& B, int alpha) {
+  if (C.t) throw std::logic_error("gemm target must be untransposed");
+  if (A.m != C.m || B.n != C.n || A.n != B.m) throw std::logic_error("gemm dimension mismatch");
+  const int TN = std::min(C.n, 64);
+  const int TM = std::min(C.m, std::max(64, 4096 / std::max(TN, 1)));
+  for (int i = 0; i < C.m; i += TM)
+    for (int j = 0; j < C.n; j += TN) {
+      const int mi = std::min(TM, C.m - i), nj = std::min(TN, C.n - j);
+      HTask& t = emit(PP_OP_GEMM);
+      bind(t, 0, C.sub(i, j, mi, nj), true);
+      bind(t, 1, A.sub(i, 0, mi, A.n), false);
+      bind(t, 2, B.sub(0, j, B.m, nj), false);
+      t.t.m = mi;
+      t.t.n = nj;
+      t.t.k = A.n;
+      t.t.alpha = (double)alpha;
+      t.t.beta = 1.0;
+      t.flops = 2LL * mi * nj * A.n;
+    }
+}
+
+void Generator::gemm(const Mat& C, const Mat& A, const Mat& B, int alpha) {
+  if (A.m != C.m || B.n != C.n || A.n != B.m) throw std::logic_error("gemm: dimension mismatch");
+  if (A.kind == Mat::LR || B.kind == Mat::LR) {
+    LRP p = lr_product(A, B, alpha);
+    lr_update(C, p.x, p.y, p.sign);
+    return;
+  }
+  if (C.kind == Mat::LR) {
+    if (A.kind == Mat::D && B.kind == Mat::D) { accum(C, A.d, B.d.T(), alpha); return; }
+    throw std::runtime_error("unsupported: hierarchical product accumulated into a low-rank block");
+  }
+  if (C.kind == Mat::D && A.kind == Mat::D && B.kind == Mat::D) {
+    gemm_tiles(C.d, A.d, B.d, alpha);
+    return;
+  }
+  int rs = hsplit_r(C);
+  if (rs < 0) rs = hsplit_r(A);
+  int cs = hsplit_c(C);
+  if (cs < 0) cs = hsplit_c(B);
+  int ks = hsplit_c(A);
+  if (ks < 0) ks = hsplit_r(B);
+  Mat Cp[2][2], Ap[2][2], Bp[2][2];
+  int cr, cc, ar, ac, br, bc;
+  partition(C, rs, cs, Cp, cr, cc);
+  partition(A, rs, ks, Ap, ar, ac);
+  partition(B, ks, cs, Bp, br, bc);
+  for (int i = 0; i < cr; ++i)
+    for (int j = 0; j < cc; ++j)
+      for (int k = 0; k < ac; ++k) gemm(Cp[i][j], Ap[i][k], Bp[k][j], alpha);
+}
+
+// alpha * A * B as x y^T * sign, with the sign folded into a zero-filled work buffer
+// whenever one is needed anyway.
+Generator::LRP Generator::lr_product(const Mat& A, const Mat& B, int alpha) {
+  if (A.kind == Mat::LR && B.kind == Mat::LR) {
+    View S = tmp(A.k, B.k);  // alpha Va^T Ub
+    gemm_tiles(S, A.v.T(), B.u, alpha);
+    if (A.k <= B.k) {
+      View Y = tmp(B.n, A.k);  // Vb S^T
+      gemm_tiles(Y, B.v, S.T(), +1);
+      return {A.u, Y, +1};
+    }
+    View X = tmp(A.m, B.k);  // Ua S
+    gemm_tiles(X, A.u, S, +1);
+    return {X, B.v, +1};
+  }
+  if (A.kind == Mat::LR) {
+    View Y = tmp(B.n, A.k);  // alpha B^T Va
+    gemm(asD(Y), transpose(B), asD(A.v), alpha);
+    return {A.u, Y, +1};
+  }
+  if (B.kind == Mat::LR) {
+    View X = tmp(A.m, B.k);  // alpha A Ub
+    gemm(asD(X), A, asD(B.u), alpha);
+    return {X, B.v, +1};
+  }
+  if (A.kind == Mat::D && B.kind == Mat::D) return {A.d, B.d.T(), alpha};
+  throw std::runtime_error("unsupported: low-rank form of a hierarchical product");
+}
+
+void Generator::lr_update(const Mat& C, const View& X, const View& Y, int sign) {
+  if (C.kind == Mat::D) { gemm_tiles(C.d, X, Y.T(), sign); return; }
+  if (C.kind == Mat::LR) { accum(C, X, Y, sign); return; }
+  const int rs = hsplit_r(C), cs = hsplit_c(C);
+  const int roff[2] = {0, rs}, coff[2] = {0, cs};
+  const int rsz[2] = {rs, C.m - rs}, csz[2] = {cs, C.n - cs};
+  for (int i = 0; i < 2; ++i)
+    for (int j = 0; j < 2; ++j)
+      lr_update(child(C, i, j), X.sub(roff[i], 0, rsz[i], X.n), Y.sub(coff[j], 0, csz[j], Y.n), sign);
+}
+
+void Generator::accum(const Mat& C, const View& X, const View& Y, int sign) {
+  if (C.kind != Mat::LR) throw std::logic_error("accum target must be low-rank");
+  const int k1 = C.k, k2 = X.n;
+  if (k1 <= 0) return;
+  HTask& t = emit(PP_OP_ACCUM);
+  bind(t, 0, C.u, true);
+  bind(t, 1, C.v, true);
+  bind(t, 2, X, false);
+  bind(t, 3, Y, false);
+  View R;
+  R.obj = rand_obj(k1);
+  R.m = C.n;
+  R.n = k1;
+  bind(t, 4, R, false);
+  t.t.m = C.m;
+  t.t.n = C.n;
+  t.t.k = k1;
+  t.t.l = k2;
+  t.t.alpha = (double)sign;
+  const int64_t ny = C.m, nx = C.n;
+  t.scratch_elems = 2 * ny * k1 + nx * k1 + (int64_t)k1 * std::max(k1, k2);
+  const int ar = P_.arena_id(inst_, AR_SCRATCH);
+  t.scratch_off = (P_.arena_elems[ar] + 3) & ~int64_t(3);
+  P_.arena_elems[ar] = t.scratch_off + t.scratch_elems;
+  const int64_t kk = k1, k22 = k2;
+  t.flops = 2 * kk * nx * kk + 2 * ny * kk * kk + 2 * kk * nx * k22 + 2 * ny * k22 * kk  // sketch
+            + 8 * ny * kk * kk                                                        // QR + Q
+            + 2 * kk * ny * kk + 2 * nx * kk * kk + 2 * kk * ny * k22 + 2 * nx * k22 * kk;  // projection
+}
+
+}  // namespace pp

@@ -1,0 +1,156 @@
+// hops.h — H-LU operation generator, task program, DAG and encoders.
+//
+// Covers the reference's missing h_ops/* (h-op tree generation, DAG flattening) and
+// instructions/* (instruction encoding) layers, whose interfaces are visible at
+// Pastel-Palettes src/launcher.cu:46-90,138-139 and rts/scheduler.cpp:73-77.
+//
+// The generator walks the block tree the way the reference's H-LU does
+// (docs: GETRF -> TRSM L / TRSM R -> GEMM -> GETRF on the trailing block, recursively)
+// and emits instructions of the reference's instruction set (getrf, trsml, trsmr with
+// and without transposed B, gemm, gemm_plus, accum), on blocks of at most `tile` rows
+// and columns for the dense parts.  Intermediate low-rank products go to zero-filled
+// work buffers, the sign folded into them exactly as a reference stream would have to
+// (gemm: M -= A B, gemm_plus: M += A B, accum: U1 V1^T += U2 V2^T), so every program
+// of a factorization is also a valid reference instruction stream.  Only the solve
+// uses one instruction the reference lacks (TRSMU: B := U^-1 B).
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "hmatrix.h"
+#include "pp_task.h"
+#include "rts.h"
+
+namespace pp {
+
+// arena kinds; arena id = instance * PP_ARENAS + kind
+enum ArenaKind { AR_MATRIX = 0, AR_WORK = 1, AR_SCRATCH = 2, AR_RHS = 3, AR_RAND = 4, PP_ARENAS = 5 };
+
+struct PObj {
+  int arena;
+  int64_t off;  // element offset of storage (0, 0) in the arena
+  int rows, cols, ld;
+  bool tracked;  // false: read-only inputs the DAG can ignore (random sketch)
+};
+
+// Dense operand: logical m x n; logical (i, j) lives at storage (r0 + i, c0 + j) of
+// object `obj`, or at storage (r0 + j, c0 + i) when `t` (transposed view).
+struct View {
+  int obj = -1;
+  int r0 = 0, c0 = 0;
+  int m = 0, n = 0;
+  bool t = false;
+  View sub(int i, int j, int mm, int nn) const;
+  View T() const;
+  int srows() const { return t ? n : m; }
+  int scols() const { return t ? m : n; }
+};
+
+// Operand of the recursive generator: dense view, low-rank pair, or H node.
+struct Mat {
+  enum Kind { D = 0, LR = 1, H = 2 } kind = D;
+  int m = 0, n = 0;
+  View d;          // D
+  View u, v;       // LR: block = u v^T, u: m x k, v: n x k
+  int k = 0;
+  int node = -1;   // H: node of the instance's tree
+  bool tr = false; // H: transposed
+};
+
+struct Region {
+  int obj;
+  int r0, c0, nr, nc;
+  bool ro;
+};
+
+struct HTask {
+  pp_task t{};           // pointers filled at encode time
+  View opnd[6];
+  bool has[6] = {false, false, false, false, false, false};
+  int64_t scratch_elems = 0, scratch_off = 0;
+  std::vector<Region> regions;
+  int64_t flops = 0;
+};
+
+class Program {
+ public:
+  int n_instances = 0;
+  std::vector<PObj> objs;
+  std::vector<HTask> tasks;
+  std::vector<int64_t> arena_elems;  // per arena id
+  // DAG over tasks (program order is topological)
+  std::vector<std::vector<int>> succ, pred;
+  dependency_table deps;
+  std::vector<int64_t> blevel;  // FLOP-weighted longest path to an exit
+  int64_t edges = 0;
+
+  int add_instance();  // returns instance id
+  int add_obj(int arena, int rows, int cols, bool tracked = true);
+  int add_obj_at(int arena, int64_t off, int rows, int cols, int ld, bool tracked);
+  int arena_id(int inst, int kind) const { return inst * PP_ARENAS + kind; }
+  int64_t total_flops() const;
+  int64_t count_op(int op) const;
+
+  void build_dag();
+  h_ops_dag to_dag() const;
+  // Pointer binding and device-table encoding.  bases[arena id] = base address.
+  void encode(const std::vector<double*>& bases, std::vector<pp_task>& out, std::vector<int32_t>& succ_out,
+              std::vector<int32_t>& indeg_out, std::vector<int32_t>& ready_out) const;
+  // Append all tasks of `other` (another instance's program); arenas are renumbered.
+  void merge(const Program& other);
+
+  // Reference-format per-worker streams (format of src/kernel.cu:1384-1522).
+  // ptr_bases: index into the reference's `void** ptrs` for each arena id.
+  bool encode_reference(int workers, std::vector<std::vector<int32_t>>& streams, std::string& err,
+                        int64_t* tmp_elems_per_worker) const;
+};
+
+class Generator {
+ public:
+  // Builds programs on one H-matrix instance.  `tile`: dense blocks larger than this
+  // are split (2 x 2) before they reach an instruction.
+  Generator(Program& P, Hierarchical& H, int tile, int max_n_rand);
+  int inst() const { return inst_; }
+  void getrf_program();            // H-LU factorization of the whole matrix
+  void solve_program(int nrhs);    // B := U^-1 L^-1 B on the RHS object (n x nrhs)
+  int rhs_obj() const { return rhs_obj_; }
+
+  // building blocks (exposed for tests)
+  Mat node(int id, bool tr = false) const;
+  void getrf(const Mat& A);
+  void trsml(const Mat& L, const Mat& B);
+  void trsmr(const Mat& U, const Mat& B);
+  void trsmrt(const Mat& U, const View& V);
+  void trsmu(const Mat& U, const Mat& B);
+  void gemm(const Mat& C, const Mat& A, const Mat& B, int alpha);
+
+ private:
+  Program& P_;
+  Hierarchical& H_;
+  int inst_;
+  int T_;
+  int rand_ld_obj_[64 + 1];
+  std::vector<int> node_obj_;  // Hierarchical obj -> program obj
+  int rhs_obj_ = -1;
+  int max_n_rand_;
+
+  struct LRP { View x, y; int sign; };  // x y^T * sign
+  LRP lr_product(const Mat& A, const Mat& B, int alpha);
+  void lr_update(const Mat& C, const View& X, const View& Y, int sign);
+  void accum(const Mat& C, const View& X, const View& Y, int sign);
+  void gemm_tiles(const View& C, const View& A, const View& B, int alpha);
+  View tmp(int rows, int cols);
+  Mat asD(const View& v) const;
+  Mat child(const Mat& X, int i, int j) const;
+  int hsplit_r(const Mat& X) const;
+  int hsplit_c(const Mat& X) const;
+  int tri_split(const Mat& X) const;
+  void partition(const Mat& X, int rs, int cs, Mat out[2][2], int& nr, int& nc) const;
+  int rand_obj(int k1);
+
+  HTask& emit(int op);
+  void bind(HTask& t, int slot, const View& v, bool write);
+};
+
+}  // namespace pp

@@ -1,0 +1,59 @@
+/* pp_task.h — one device instruction of the H-LU virtual machine.
+ *
+ * The reference encodes its block operations as variable-length int32 words
+ * (opcode, signal id, operation, pointer-table indices, int offsets, dims, lds,
+ * transpose flags; Pastel-Palettes src/kernel.cu:1404-1501).  This engine keeps
+ * the same operation set (getrf / trsm L / trsm R / gemm / gemm_3x / gemm_4x /
+ * accum) but stores each instruction as a fixed 160-byte record with absolute
+ * 64-bit device pointers, so one task table can mix operands of many H-matrices
+ * (batched launches) and no offset overflows past 2^31 elements.
+ *
+ * The record is read by the VM kernel (vm.cu), written by the host encoder
+ * (hops.cpp), and executed on the CPU by the test oracle; it is plain C.
+ */
+#ifndef PP_TASK_H
+#define PP_TASK_H
+#include <stdint.h>
+
+enum pp_op {
+  PP_OP_NOP = 0,
+  PP_OP_GETRF = 1,   /* A[m x n] := L\U in place, no pivoting (kernel.cu:104-147, 820-882)      */
+  PP_OP_TRSML = 2,   /* B[m x n] := L^-1 B, L unit lower m x m      (kernel.cu:150-182, 667-715)  */
+  PP_OP_TRSMR = 3,   /* B[m x n] := B U^-1, U upper n x n           (kernel.cu:185-226, 718-766)  */
+  PP_OP_TRSMRT = 4,  /* V[m x n] := U^-T V, U upper m x m  (trsmr on V^T, kernel.cu:229-285, 769-817) */
+  PP_OP_TRSMU = 5,   /* B[m x n] := U^-1 B, U upper m x m (solve only; no reference counterpart)  */
+  PP_OP_GEMM = 6,    /* C[m x n] := beta C + alpha op(A)[m x k] op(B)[k x n] (kernel.cu:415-664)    */
+  PP_OP_GEMM3 = 7,   /* C += alpha A B D, association by ctrl          (kernel.cu:886-904)         */
+  PP_OP_GEMM4 = 8,   /* C += alpha A B D E, association by ctrl 0..4   (kernel.cu:907-955)         */
+  PP_OP_ACCUM = 9,   /* U1 V1^T := rank-k1 range of U1 V1^T + alpha U2 V2^T (kernel.cu:1255-1280)   */
+  PP_OP_COUNT = 10
+};
+
+/* flags: bit (4+i) = operand i is stored transposed (operand 0 is the target). */
+#define PP_T(i) (1 << (4 + (i)))
+/* precision of the contraction inside GEMM-class tasks */
+#define PP_PREC_FP64 0
+#define PP_PREC_TF32 1
+
+typedef struct pp_task {
+  int32_t op;
+  int32_t flags;
+  int32_t m, n, k, l, o; /* dims; meaning per op, documented in vm.cu */
+  int32_t ctrl;          /* association order for GEMM3/GEMM4 */
+  int32_t ld[6];         /* leading dimension (elements) of each operand */
+  double *p[6];          /* operand pointers: p[0] target, p[1..5] inputs */
+  double *tmp;           /* task-private scratch (GEMM3/GEMM4/ACCUM) */
+  double alpha, beta;
+  int32_t succ_begin;    /* successors: succ[succ_begin .. succ_begin + n_succ) */
+  int32_t n_succ;
+  int32_t prec;          /* PP_PREC_* */
+  int32_t instance;      /* owning H-matrix (batched launches) */
+  int32_t aux;           /* GEMM4: element offset of the second intermediate in tmp */
+  int32_t pad[3];
+} pp_task;
+
+#ifdef __cplusplus
+static_assert(sizeof(pp_task) == 160, "pp_task layout");
+#endif
+
+#endif

@@ -1,0 +1,46 @@
+// vm.cuh — host-side interface of the H-LU virtual machine kernels (vm.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "pp_task.h"
+
+#define PP_VM_THREADS 256
+#define PP_VM_TILE 64          /* largest dense block GETRF / TRSM* keep in shared memory */
+#define PP_VM_MAX_RANK 32      /* largest k1 of ACCUM (register-resident reductions)    */
+
+enum pp_vm_error { PP_VM_OK = 0, PP_VM_TIMEOUT = 1, PP_VM_BAD_TASK = 2 };
+
+typedef struct pp_vm_state {
+  int head;      /* next ready-slot index to pop                  */
+  int tail;      /* next ready-slot index to fill                 */
+  int done;      /* tasks completed                               */
+  int error;     /* pp_vm_error                                   */
+  int err_info;  /* slot index (timeout) or task id (bad task)    */
+  int pad[3];
+} pp_vm_state;
+
+struct pp_vm_launch {
+  const pp_task* tasks;
+  int n_tasks;
+  const int32_t* succ;
+  const int32_t* indeg;
+  const int32_t* ready;
+  int n_ready;
+  int32_t* counters;
+  int32_t* slots;
+  pp_vm_state* state;
+  long long spin_limit;  /* polls of an empty ready slot before the kernel gives up */
+  int grid;              /* CTAs (persistent)                                       */
+};
+
+size_t pp_vm_smem_bytes();
+int pp_vm_blocks_per_sm();
+cudaError_t pp_vm_prepare();  /* sets the dynamic shared-memory attribute (once per device) */
+cudaError_t pp_vm_run(const pp_vm_launch& L, cudaStream_t s);
+/* dense FP64 residual r = b - A x, A row-major n x n, x/b/r n x nrhs row-major */
+cudaError_t pp_dense_residual(const double* A, int lda, int n, const double* x, const double* b, double* r, int nrhs,
+                              cudaStream_t s);
+/* matrix-free residual r = b - A x for kernel matrices on points (see kernels in vm.cu) */
+cudaError_t pp_kernel_residual(int kernel, double p0, double p1, double diag_shift, const double* pts, int dim, int n,
+                               const double* x, const double* b, double* r, int nrhs, cudaStream_t s);

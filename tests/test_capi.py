@@ -1,0 +1,67 @@
+"""C ABI: the library loads, exports what include/pastel_palettes.h declares, validates
+arguments, and never computes on the host (no CPU fallback)."""
+import ctypes as C
+import subprocess
+
+import numpy as np
+import pytest
+
+
+def test_library_exports_every_declared_symbol(pp):
+    lib = pp.lib()
+    declared = pp.exported_symbols()
+    assert len(declared) >= 30
+    missing = [s for s in declared if not hasattr(lib, s)]
+    assert not missing, missing
+    out = subprocess.run(["nm", "-D", "--defined-only", pp.LIB_PATH], capture_output=True, text=True).stdout
+    for s in declared:
+        assert f" T {s}" in out, s
+
+
+def test_host_context_refuses_compute(pp, hctx):
+    h, _ = pp.make_dense_problem(hctx, n=256, leaf=64)
+    with pytest.raises(pp.PPError) as e:
+        h.upload()
+    assert e.value.status == pp.PP_CUDA_ERROR
+    with pytest.raises(pp.PPError) as e:
+        h.factor()
+    assert e.value.status in (pp.PP_CUDA_ERROR, pp.PP_INVALID_ARG)
+
+
+def test_invalid_arguments(pp, hctx):
+    lib = pp.lib()
+    out = C.c_void_p()
+    assert lib.pp_hmatrix_create_dense(hctx.handle, 0, 64, C.byref(out)) == pp.PP_INVALID_ARG
+    pts = np.zeros((4, 2))
+    assert lib.pp_hmatrix_create_geometric(hctx.handle, 4, 2, pts.ctypes.data_as(C.POINTER(C.c_double)), 2, 0, 1.0,
+                                           0, C.byref(out)) == pp.PP_INVALID_ARG
+    with pytest.raises(pp.PPError):
+        pp.Context(device=-1, tile=4)
+    h, _ = pp.make_dense_problem(hctx, n=128, leaf=64)
+    with pytest.raises(pp.PPError):
+        h.set_lowrank(h.root, np.zeros((2, 2)), np.zeros((2, 2)))
+
+
+def test_block_tree_of_configurations(pp, hctx):
+    h, _ = pp.make_dense_problem(hctx, n=1024, leaf=256)
+    blocks = h.blocks()
+    assert sum(b["kind"] == pp.DENSE for b in blocks) == 16
+    assert h.getNy_abs() == h.getNx_abs() == 1024
+    pts = np.random.default_rng(0).uniform(0, 1, (8192, 2))
+    pts = pts[pp.morton_order(pts)]
+    hg = pp.Hierarchical.geometric(hctx, pts, 256, 0, 1.0, 16)
+    kinds = [b["kind"] for b in hg.blocks()]
+    assert kinds.count(pp.DENSE) == 32 and kinds.count(pp.LOWRANK) == 62
+
+
+def test_factor_program_flops_match_dense_count(pp, hctx):
+    h, _ = pp.make_dense_problem(hctx, n=1024, leaf=256)
+    n = 1024
+    assert h.program_info(0)["flops"] == 2 * n ** 3 // 3 - n ** 2 // 2 - n // 6 == 715303424
+
+
+def test_refstream_rejects_solve_only_instruction(pp, hctx):
+    # the factor program is expressible in the reference's instruction set
+    h, _ = pp.make_kernel_problem(hctx, 512, 2, "inv", 1e-3, 64, 8)
+    words, lengths, tmp = h.refstreams(1)
+    assert words[0] == 1 and words[-1] == 0

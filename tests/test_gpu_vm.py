@@ -1,0 +1,311 @@
+"""GPU parity of the persistent VM (sm_100a) against the oracle and the reference kernel.
+
+Bar: dense instructions bitwise equal to the oracle (= the reference's update order);
+programs containing the randomized accumulation within 1e-12 relative (Frobenius) of the
+oracle and of the reference's own kernel_dynamic on the same instruction stream.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def dev(x):
+    return torch.from_numpy(np.ascontiguousarray(x, dtype=np.float64)).cuda()
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+# ----------------------------------------------------------------------------- single tasks
+class TaskBench:
+    """Builds one-task tables twice: device operands for the VM, host operands for the oracle."""
+
+    def __init__(self, pp, seed=0):
+        self.pp = pp
+        self.rng = np.random.default_rng(seed)
+        self.host, self.devs = [], []
+
+    def operand(self, rows, cols, kind="normal", ld_pad=3):
+        ld = cols + ld_pad
+        a = self.rng.standard_normal((rows, ld)) if kind == "normal" else self.rng.uniform(-1, 1, (rows, ld))
+        if kind == "diag":
+            a[:, :cols] += np.eye(rows, cols) * (2 * max(rows, cols))
+        self.host.append(a)
+        self.devs.append(dev(a))
+        return len(self.host) - 1, ld
+
+    def run(self, gctx, oracle, fields, slots, tmp_elems=0):
+        pp = self.pp
+        t_dev = np.zeros(1, dtype=pp.TASK_DTYPE)
+        t_host = np.zeros(1, dtype=pp.TASK_DTYPE)
+        for k, v in fields.items():
+            t_dev[0][k] = v
+            t_host[0][k] = v
+        for s, (idx, ld) in slots.items():
+            t_dev[0]["p"][s] = self.devs[idx].data_ptr()
+            t_host[0]["p"][s] = self.host[idx].ctypes.data
+            t_dev[0]["ld"][s] = ld
+            t_host[0]["ld"][s] = ld
+        if tmp_elems:
+            td = torch.zeros(tmp_elems, dtype=torch.float64, device="cuda")
+            th = np.zeros(tmp_elems)
+            t_dev[0]["tmp"] = td.data_ptr()
+            t_host[0]["tmp"] = th.ctypes.data
+        gctx.vm_execute(t_dev, np.zeros(0, np.int32), np.zeros(1, np.int32))
+        rc = oracle.lib().oracle_run_program(t_host.ctypes.data, 1)
+        assert rc == 0
+        return [(d.cpu().numpy(), h) for d, h in zip(self.devs, self.host)]
+
+
+@pytest.mark.parametrize("tA,tB", [(0, 0), (1, 0), (0, 1), (1, 1)])
+@pytest.mark.parametrize("alpha,beta", [(-1.0, 1.0), (1.0, 1.0), (1.0, 0.0)])
+@pytest.mark.parametrize("m,n,k", [(64, 64, 64), (37, 91, 130), (256, 16, 16), (5, 3, 0)])
+def test_gemm_task_bitwise(pp, oracle, gctx, tA, tB, alpha, beta, m, n, k):
+    tb = TaskBench(pp, seed=m * 7 + n)
+    c = tb.operand(m, n)
+    a = tb.operand(k, m) if tA else tb.operand(m, k)
+    b = tb.operand(n, k) if tB else tb.operand(k, n)
+    flags = (tA << 5) | (tB << 6)
+    out = tb.run(gctx, oracle, dict(op=6, flags=flags, m=m, n=n, k=k, alpha=alpha, beta=beta), {0: c, 1: a, 2: b})
+    d, h = out[c[0]]
+    assert np.array_equal(d, h)
+
+
+@pytest.mark.parametrize("m,n", [(64, 64), (37, 50), (1, 1), (64, 17)])
+def test_getrf_task_bitwise(pp, oracle, gctx, m, n):
+    tb = TaskBench(pp, seed=m + n)
+    a = tb.operand(m, n, kind="diag")
+    d, h = tb.run(gctx, oracle, dict(op=1, m=m, n=n), {0: a})[a[0]]
+    assert np.array_equal(d, h)
+
+
+@pytest.mark.parametrize("op", [2, 3, 4, 5])
+@pytest.mark.parametrize("m,n", [(64, 16), (64, 64), (33, 70), (1, 5)])
+def test_triangular_tasks_bitwise(pp, oracle, gctx, op, m, n):
+    tb = TaskBench(pp, seed=op * 100 + m)
+    tri = n if op == 3 else m  # trsmr: U is n x n; others: m x m
+    if op == 3 and n > 64:
+        pytest.skip("trsmr keeps U (n x n) in shared memory: n <= 64")
+    b = tb.operand(m, n)
+    t = tb.operand(tri, tri, kind="diag")
+    d, h = tb.run(gctx, oracle, dict(op=op, m=m, n=n), {0: b, 1: t})[b[0]]
+    assert np.array_equal(d, h)
+
+
+@pytest.mark.parametrize("ctrl", [0, 1])
+def test_gemm3_task_bitwise(pp, oracle, gctx, ctrl):
+    tb = TaskBench(pp, seed=ctrl + 50)
+    m, n, k, l = 70, 40, 16, 90
+    c, a, b, d_ = tb.operand(m, n), tb.operand(m, k), tb.operand(k, l), tb.operand(l, n)
+    out = tb.run(gctx, oracle, dict(op=7, m=m, n=n, k=k, l=l, ctrl=ctrl, alpha=-1.0, beta=1.0),
+                 {0: c, 1: a, 2: b, 3: d_}, tmp_elems=max(m * l, k * n))
+    d, h = out[c[0]]
+    assert np.array_equal(d, h)
+
+
+@pytest.mark.parametrize("ctrl", [0, 1, 2, 3, 4])
+def test_gemm4_task_bitwise(pp, oracle, gctx, ctrl):
+    tb = TaskBench(pp, seed=ctrl + 60)
+    m, n, k, l, o = 48, 40, 16, 80, 12
+    c = tb.operand(m, n)
+    a, b, cc, dd = tb.operand(m, k), tb.operand(k, l), tb.operand(l, o), tb.operand(o, n)
+    big = max(m, k, l) * max(n, l, o)
+    out = tb.run(gctx, oracle, dict(op=8, m=m, n=n, k=k, l=l, o=o, ctrl=ctrl, alpha=-1.0, beta=1.0, aux=big),
+                 {0: c, 1: a, 2: b, 3: cc, 4: dd}, tmp_elems=2 * big)
+    d, h = out[c[0]]
+    assert np.array_equal(d, h)
+
+
+@pytest.mark.parametrize("ny,nx,k1,k2,sign", [(300, 260, 16, 16, 1.0), (129, 64, 8, 24, 1.0), (64, 512, 16, 16, -1.0)])
+def test_accum_task_matches_reference_algorithm(pp, oracle, gctx, ny, nx, k1, k2, sign):
+    tb = TaskBench(pp, seed=ny + nx)
+    u1, v1, u2, v2 = tb.operand(ny, k1), tb.operand(nx, k1), tb.operand(ny, k2), tb.operand(nx, k2)
+    r = tb.operand(nx, k1, kind="uniform", ld_pad=0)
+    A0 = tb.host[u1[0]][:, :k1] @ tb.host[v1[0]][:, :k1].T + sign * tb.host[u2[0]][:, :k2] @ tb.host[v2[0]][:, :k2].T
+    tmp = 2 * ny * k1 + nx * k1 + k1 * max(k1, k2)
+    out = tb.run(gctx, oracle, dict(op=9, m=ny, n=nx, k=k1, l=k2, alpha=sign), {0: u1, 1: v1, 2: u2, 3: v2, 4: r},
+                 tmp_elems=tmp)
+    Ud, Uh = out[u1[0]]
+    Vd, Vh = out[v1[0]]
+    Pd = Ud[:, :k1] @ Vd[:, :k1].T
+    Ph = Uh[:, :k1] @ Vh[:, :k1].T
+    assert rel(Pd, Ph) < 1e-12
+    Q, _ = np.linalg.qr(A0 @ tb.host[r[0]][:, :k1])
+    assert rel(Pd, Q @ (Q.T @ A0)) < 1e-12
+    assert np.allclose(Ud[:, :k1].T @ Ud[:, :k1], np.eye(k1), atol=1e-12)
+
+
+# ----------------------------------------------------------------------------- programs
+def factor_on_gpu(h, grid_blocks=0):
+    h.upload()
+    if grid_blocks:
+        import importlib
+        pp = importlib.import_module("pastel_palettes_b200")
+        pp.dev_hierarchical_GETRF(h, grid_blocks, 256, 0)
+    else:
+        h.factor()
+        h.sync()
+    h.download()
+    return h.to_dense()
+
+
+def test_dense_config1_bitwise_vs_textbook_lu(pp, oracle, gctx):
+    h, A = pp.make_dense_problem(gctx, n=1024, leaf=256)
+    assert np.array_equal(factor_on_gpu(h), oracle.dense_getrf(A))
+
+
+def test_single_cta_equals_full_grid(pp, gctx):
+    h1, _ = pp.make_kernel_problem(gctx, 1024, 2, "inv", 1e-3, 128, 16)
+    h2, _ = pp.make_kernel_problem(gctx, 1024, 2, "inv", 1e-3, 128, 16)
+    F1 = factor_on_gpu(h1)
+    F2 = factor_on_gpu(h2, grid_blocks=1)
+    assert np.array_equal(F1, F2)
+
+
+def test_hodlr_factor_matches_oracle(pp, oracle, gctx):
+    h, prob = pp.make_kernel_problem(gctx, 2048, 2, "inv", 1e-3, 256, 16)
+    ar = oracle.HostArenas(h, 0)
+    ar.run(threads=8)
+    F = factor_on_gpu(h)
+    h.host_arena()[:] = ar.matrix
+    assert rel(F, h.to_dense()) < 1e-12
+
+
+def run_reference_kernel(pp, oracle, h):
+    """The reference's kernel_dynamic (1 worker) on the reference-format stream of h."""
+    ref = oracle.ref_vm()
+    if ref is None:
+        pytest.skip("reference kernel not built")
+    words, lengths, tmp = h.refstreams(1)
+    info = h.program_info(0)
+    el = info["arena_elems"]
+    arena = dev(h.host_arena())
+    work = torch.zeros(max(el["work"], 1), dtype=torch.float64, device="cuda")
+    scratch = torch.zeros(max(el["scratch"], 1), dtype=torch.float64, device="cuda")
+    rhs = torch.zeros(max(el["rhs"], 1), dtype=torch.float64, device="cuda")
+    rnd = dev(h.rand_host() if el["rand"] else np.zeros(1))
+    import ctypes as C
+    ptrs = (C.c_void_p * 5)(*[C.c_void_p(t.data_ptr()) for t in (arena, work, scratch, rhs, rnd)])
+    words = np.ascontiguousarray(words, dtype=np.int32)
+    lengths = np.ascontiguousarray(lengths, dtype=np.int32)
+    rc = ref.ref_vm_run(1, words.ctypes.data, lengths.ctypes.data, C.cast(ptrs, C.c_void_p), 5, info["n_tasks"],
+                        rnd.data_ptr(), max(tmp, 1), 256)
+    assert rc == 0, f"reference kernel failed: cuda error {rc}"
+    out = arena.cpu().numpy()
+    saved = h.host_arena().copy()
+    h.host_arena()[:] = out
+    F = h.to_dense()
+    h.host_arena()[:] = saved
+    return F
+
+
+def test_dense_matches_reference_kernel_bitwise(pp, oracle, gctx):
+    h, A = pp.make_dense_problem(gctx, n=512, leaf=128, seed=3)
+    F_ref = run_reference_kernel(pp, oracle, h)
+    F = factor_on_gpu(h)
+    assert np.array_equal(F, F_ref)
+    assert np.array_equal(F, oracle.dense_getrf(A))
+
+
+def test_hodlr_matches_reference_kernel(pp, oracle, gctx):
+    h, _ = pp.make_kernel_problem(gctx, 1024, 2, "inv", 1e-3, 128, 16)
+    F_ref = run_reference_kernel(pp, oracle, h)
+    F = factor_on_gpu(h)
+    assert rel(F, F_ref) < 1e-12
+
+
+def test_solve_matches_oracle(pp, oracle, gctx):
+    n = 2048
+    h, prob = pp.make_kernel_problem(gctx, n, 2, "inv", 1e-3, 256, 16)
+    ar = oracle.HostArenas(h, 0)
+    ar.run(threads=8)
+    b = pp.rhs(n, 3)
+    sol = oracle.HostArenas(h, 1, 3, rhs=b)
+    sol.matrix[:] = ar.matrix
+    sol.tasks, sol.succ, sol.indeg, sol.ready = h.encode_program(1, 3, sol.bases())
+    sol.run()
+    x_or = sol.rhs[: n * 3].reshape(n, 3)
+    h.upload()
+    h.factor()
+    bd = dev(b)
+    xd = torch.empty_like(bd)
+    h.solve(bd, xd)
+    h.sync()
+    assert rel(xd.cpu().numpy(), x_or) < 1e-12
+
+
+def test_dense_solve_bitwise(pp, oracle, gctx):
+    n = 512
+    h, A = pp.make_dense_problem(gctx, n=n, leaf=128)
+    ar = oracle.HostArenas(h, 0)
+    ar.run()
+    b = pp.rhs(n, 2)
+    sol = oracle.HostArenas(h, 1, 2, rhs=b)
+    sol.matrix[:] = ar.matrix
+    sol.tasks, sol.succ, sol.indeg, sol.ready = h.encode_program(1, 2, sol.bases())
+    sol.run()
+    h.upload()
+    h.factor()
+    bd = dev(b)
+    xd = torch.empty_like(bd)
+    h.solve(bd, xd)
+    h.sync()
+    assert np.array_equal(xd.cpu().numpy(), sol.rhs[: n * 2].reshape(n, 2))
+
+
+def test_refinement_reaches_1e10(pp, gctx):
+    n = 4096
+    h, prob = pp.make_kernel_problem(gctx, n, 2, "inv", 1e-3, 256, 16)
+    h.upload()
+    h.factor()
+    b_h = pp.rhs(n)
+    ref = pp.Refiner(h, gctx, prob)
+    x, hist = ref.solve(dev(b_h), tol=1e-10)
+    assert hist[-1] <= 1e-10, hist
+    A = prob.dense()
+    xh = x.cpu().numpy()
+    assert abs(np.abs(A).sum(1).max() - prob.norm_inf) < 1e-9 * prob.norm_inf
+    berr = np.abs(b_h - A @ xh).max() / (prob.norm_inf * np.abs(xh).max() + np.abs(b_h).max())
+    assert berr <= 1e-10, berr
+
+
+def test_dense_refinement(pp, gctx):
+    n = 1024
+    h, A = pp.make_dense_problem(gctx, n=n, leaf=256)
+    h.upload()
+    h.factor()
+    b_h = pp.rhs(n)
+    x, hist = pp.Refiner(h, gctx, dense=A).solve(dev(b_h), tol=1e-12)
+    assert hist[-1] <= 1e-12
+
+
+def test_dense_residual_kernel(pp, gctx):
+    rng = np.random.default_rng(0)
+    n = 300
+    A = rng.standard_normal((n, n))
+    x = rng.standard_normal((n, 2))
+    b = rng.standard_normal((n, 2))
+    r = torch.empty((n, 2), dtype=torch.float64, device="cuda")
+    gctx.dense_residual(dev(A), dev(x), dev(b), r)
+    assert np.allclose(r.cpu().numpy(), b - A @ x, rtol=1e-12, atol=1e-12)
+
+
+def test_timeout_is_reported_not_hung(pp, gctx):
+    # host-side fault: task 1 claims two predecessors but only task 0 precedes it, so
+    # its ready slot is never filled; the VM must give up and report PP_TIMEOUT
+    t = np.zeros(2, dtype=pp.TASK_DTYPE)
+    t[0]["op"] = 0
+    t[0]["succ_begin"], t[0]["n_succ"] = 0, 1
+    t[1]["op"] = 0
+    succ = np.array([1], np.int32)
+    indeg = np.array([0, 2], np.int32)
+    with pytest.raises(pp.PPError) as e:
+        gctx.vm_execute(t, succ, indeg, spin_limit=20000)
+    assert e.value.status == pp.PP_TIMEOUT
+    # the context stays usable
+    indeg_ok = np.array([0, 1], np.int32)
+    gctx.vm_execute(t, succ, indeg_ok)
