@@ -115,6 +115,9 @@ class HostArenas:
         return [a.ctypes.data for a in (self.matrix, self.work, self.scratch, self.rhs, self.rand)]
 
     def run(self, threads=1):
+        # the programs accumulate intermediate products into zero-filled work buffers
+        # (the device launch clears them too)
+        self.work[:] = 0.0
         if threads <= 1:
             rc = lib().oracle_run_program(self.tasks.ctypes.data, len(self.tasks))
         else:
