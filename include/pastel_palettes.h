@@ -152,6 +152,31 @@ pp_status pp_hmatrix_program_edges(pp_hmatrix* h, int which, int nrhs, int64_t* 
  * Counterpart of launchKernelWithArgs (include/launcher.cuh:15-16) for decoded streams. */
 pp_status pp_vm_execute(pp_context* ctx, const void* tasks, int n_tasks, const int32_t* succ, long long n_succ,
                         const int32_t* indeg, long long spin_limit, int grid, void* stream);
+/* Low-rank accumulation without any device allocation.  No counterpart in the reference.
+ *
+ * Computes the same thing as one ACCUM task run through pp_vm_execute:
+ *   U1 V1^T := Q Q^T (U1 V1^T + sign * U2 V2^T),  Q an orthonormal basis of that sum times R,
+ * in place on U1 (ny x k1, ld_u1) and V1 (nx x k1, ld_v1); U2 (ny x k2), V2 (nx x k2) and the
+ * sketch R (nx x k1) are read.  All pointers are device pointers the caller owns.
+ *
+ * For callers that cannot call cudaMalloc: code recorded into a CUDA graph while a stream is
+ * being captured (an allocation there breaks the capture), serving loops whose device memory
+ * is fully reserved by an admission budget, and host frameworks that own the device memory
+ * pool.  Its scratch is one static device array of PP_ACCUM_NOALLOC_MAX_SCRATCH doubles
+ * (8 MiB), held by every GPU that loads the library until the process exits.  A call needs
+ * 2*ny*k1 + nx*k1 + k1*max(k1, k2) doubles of it and 1 <= k1 <= 32; larger requests return
+ * PP_INVALID_ARG without touching the device.
+ *
+ * The first call on each device looks up the array's device address (with that device
+ * current); make that first call before any stream capture.  Every call shares the array and
+ * overwrites all of it that it uses before reading it, so nothing carries over between calls;
+ * calls whose executions overlap on the GPU (different streams, or graphs replayed
+ * concurrently) race on it. */
+#define PP_ACCUM_NOALLOC_MAX_SCRATCH (1 << 20)
+pp_status pp_lowrank_accum_noalloc(pp_context* ctx, double* U1, int ld_u1, double* V1, int ld_v1, const double* U2,
+                                   int ld_u2, const double* V2, int ld_v2, const double* R, int ld_r, int ny, int nx,
+                                   int k1, int k2, double sign, void* stream);
+
 /* random sketch the accum instructions read (arena `rand`, row-major n x kmax, ld = rank) */
 pp_status pp_hmatrix_rand_host(pp_hmatrix* h, double* out, long long count);
 /* Reference-format instruction streams of the factor program (src/kernel.cu:1384-1522)

@@ -108,6 +108,7 @@ def lib():
             "pp_hmatrix_rand_host": (i, [vp, dp, ll]),
             "pp_hmatrix_program_edges": (i, [vp, i, i, vp, vp, vp]),
             "pp_vm_execute": (i, [vp, vp, i, vp, ll, vp, ll, i, vp]),
+            "pp_lowrank_accum_noalloc": (i, [vp, vp, i, vp, i, vp, i, vp, i, vp, i, i, i, i, i, d, vp]),
             "pp_refstream_encode": (i, [vp, i, vp, ll, vp, C.POINTER(ll)]),
         }
         for name, (res, args) in sig.items():

@@ -585,6 +585,41 @@ pp_status pp_vm_execute(pp_context* ctx, const void* tasks, int n, const int32_t
   return PP_OK;
 }
 
+pp_status pp_lowrank_accum_noalloc(pp_context* ctx, double* U1, int ld_u1, double* V1, int ld_v1, const double* U2,
+                                   int ld_u2, const double* V2, int ld_v2, const double* R, int ld_r, int ny, int nx,
+                                   int k1, int k2, double sign, void* stream) {
+  if (!ctx) return PP_INVALID_ARG;
+  if (!has_device(ctx)) return fail(ctx, PP_CUDA_ERROR, "no CUDA device in this context");
+  if (!U1 || !V1 || !U2 || !V2 || !R || ny < 1 || nx < 1 || k1 < 1 || k1 > PP_VM_MAX_RANK || k2 < 1 ||
+      ld_u1 < k1 || ld_v1 < k1 || ld_u2 < k2 || ld_v2 < k2 || ld_r < k1 || (sign != 1.0 && sign != -1.0))
+    return fail(ctx, PP_INVALID_ARG, "pp_lowrank_accum_noalloc: bad argument");
+  const long long need = 2LL * ny * k1 + (long long)nx * k1 + (long long)k1 * std::max(k1, k2);
+  if (need > pp_accum_noalloc_capacity())
+    return fail(ctx, PP_INVALID_ARG,
+                "pp_lowrank_accum_noalloc: needs " + std::to_string(need) + " doubles of scratch, the static array holds " +
+                    std::to_string(pp_accum_noalloc_capacity()));
+  pp_task T{};
+  T.op = PP_OP_ACCUM;
+  T.m = ny;
+  T.n = nx;
+  T.k = k1;
+  T.l = k2;
+  T.alpha = sign;
+  T.beta = 1.0;
+  T.p[0] = U1;
+  T.p[1] = V1;
+  T.p[2] = const_cast<double*>(U2);
+  T.p[3] = const_cast<double*>(V2);
+  T.p[4] = const_cast<double*>(R);
+  T.ld[0] = ld_u1;
+  T.ld[1] = ld_v1;
+  T.ld[2] = ld_u2;
+  T.ld[3] = ld_v2;
+  T.ld[4] = ld_r;
+  PP_CUDA(pp_accum_noalloc_launch(T, need, (cudaStream_t)stream));
+  return PP_OK;
+}
+
 pp_status pp_hmatrix_rand_host(pp_hmatrix* h, double* out, long long count) {
   if (!h || !out) return PP_INVALID_ARG;
   pp_status st = build_program(h, 0, 0, h->factor);

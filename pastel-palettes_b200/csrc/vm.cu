@@ -637,7 +637,43 @@ __global__ void kernel_residual_kernel(int kind, double p0, double p1, double sh
     for (int q = 0; q < nrhs; ++q) r[(size_t)i * nrhs + q] = b[(size_t)i * nrhs + q] - acc[q];
 }
 
+// One ACCUM on caller buffers; its scratch (T.tmp) is the static array below.
+__global__ void __launch_bounds__(NT) accum_noalloc_kernel(pp_task T) {
+  extern __shared__ double smem[];
+  dev_accum(T, smem);
+}
+
 }  // namespace
+
+// Scratch of pp_lowrank_accum_noalloc: a file-scope device array, so the entry point never
+// allocates.  Every device that loads the library holds it (8 MiB) until the process exits.
+// Host code may not use its name as an address: the device address is looked up once per
+// device with cudaGetSymbolAddress (below) and passed to the kernel.
+#define PP_NOALLOC_SCRATCH_DOUBLES (1 << 20)
+static __device__ __align__(256) double g_accum_noalloc_scratch[PP_NOALLOC_SCRATCH_DOUBLES];
+
+long long pp_accum_noalloc_capacity() { return PP_NOALLOC_SCRATCH_DOUBLES; }
+
+cudaError_t pp_accum_noalloc_launch(const pp_task& T, long long scratch_doubles, cudaStream_t s) {
+  if (scratch_doubles < 0 || scratch_doubles > PP_NOALLOC_SCRATCH_DOUBLES) return cudaErrorInvalidValue;
+  constexpr int kMaxDevices = 64;
+  static double* addr[kMaxDevices] = {nullptr};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  if (!addr[dev]) {  // set-up, once per device, with that device current
+    double* p = nullptr;
+    e = cudaGetSymbolAddress((void**)&p, g_accum_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    addr[dev] = p;
+  }
+  pp_task t = T;
+  t.tmp = addr[dev];
+  // shared memory: the GEMM k-chunk tiles, which also hold the QR reductions
+  accum_noalloc_kernel<<<1, NT, (size_t)2 * KC * LDS * sizeof(double), s>>>(t);
+  return cudaGetLastError();
+}
 
 size_t pp_vm_smem_bytes() { return (size_t)2 * TL * LDS * sizeof(double); }
 

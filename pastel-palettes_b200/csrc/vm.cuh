@@ -34,6 +34,11 @@ struct pp_vm_launch {
   int grid;              /* CTAs (persistent)                                       */
 };
 
+/* ACCUM on caller buffers with the library's static scratch array (no allocation);
+ * returns cudaErrorInvalidValue when `scratch_doubles` exceeds the array */
+cudaError_t pp_accum_noalloc_launch(const pp_task& T, long long scratch_doubles, cudaStream_t s);
+long long pp_accum_noalloc_capacity();
+
 size_t pp_vm_smem_bytes();
 int pp_vm_blocks_per_sm();
 cudaError_t pp_vm_prepare();  /* sets the dynamic shared-memory attribute (once per device) */
