@@ -111,6 +111,8 @@ def program_bytes(pp, h, which=0, nrhs=1):
             e = (2 if t["beta"] != 0 else 1) * m * n + m * k + k * n
         elif op == 9:
             e = 2 * (m * k + n * k) + (m + n) * l + n * k
+        elif op == 10:
+            e = (k + 2) * m * n
         else:
             e = 0
         total += 8 * e

@@ -42,6 +42,8 @@ typedef struct pp_config {
   int ctas_per_sm;       /* persistent VM CTAs per SM (0 = occupancy maximum)                        */
   long long spin_limit;  /* polls of an empty ready slot before a VM CTA reports PP_TIMEOUT            */
   unsigned long long seed;  /* seed of the random sketch used by accum                                */
+  int reference_isa;     /* 1: factor programs use only the reference's instruction set (no split-k
+                            reductions), so pp_refstream_encode can export them                         */
 } pp_config;
 
 typedef struct pp_block_info {
@@ -55,7 +57,7 @@ typedef struct pp_program_info {
   int n_tasks;
   long long n_edges;
   long long flops;                  /* algorithmic FLOPs of all instructions */
-  long long op_count[10];           /* instructions per pp_op               */
+  long long op_count[12];           /* instructions per pp_op (pp_task.h)   */
   long long arena_elems[5];         /* matrix, work, scratch, rhs, rand     */
   double host_build_ms;             /* op generation + DAG + encoding        */
 } pp_program_info;
@@ -142,6 +144,11 @@ int pp_operation_dependency(int n_from, const uint64_t* regions_from, const int*
  * tasks: n_tasks records of 160 bytes (pp_task.h); succ: n_edges; indeg: n_tasks.  */
 pp_status pp_hmatrix_encode_program(pp_hmatrix* h, int which, int nrhs, double* const* bases, void* tasks,
                                     int32_t* succ, int32_t* indeg, int32_t* order);
+/* Per-instruction trace (the reference stamps clock64 per instruction, src/kernel.cu:1389-1390,
+ * and renders it with analyzeClocks, rts/scheduler.cpp:494-544): with out == NULL, enable != 0
+ * makes later launches of the program record, per task, the globaltimer (ns) at start and end
+ * and the SM (low 32 bits) and CTA (high 32 bits); out != NULL copies 3 * n_tasks words back. */
+pp_status pp_hmatrix_trace(pp_hmatrix* h, int which, int nrhs, int enable, uint64_t* out);
 /* typed DAG of the factor / solve program: edge e runs from[e] -> to[e] with dependency_t
  * bits type[e] (1 flow, 2 anti, 4 out); the dependency_table of rts/dependency.h:24-53 */
 pp_status pp_hmatrix_program_edges(pp_hmatrix* h, int which, int nrhs, int64_t* from, int64_t* to, int32_t* type);

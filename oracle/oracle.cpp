@@ -83,11 +83,12 @@ void o_trsmrt(double* B, const double* U, int nx_b, int ny_b, int ny_u, int ld_b
   }
 }
 
-// B[m x n] := U^-1 B, U upper m x m (solve; no reference counterpart)
+// B[m x n] := U^-1 B, U upper m x m (solve; no reference counterpart): row i is scaled by
+// the reciprocal of u_ii, then eliminated from the rows above
 void o_trsmu(double* B, const double* U, int m, int n, int ld_b, int ld_u) {
   for (int i = m - 1; i >= 0; --i) {
-    const double d = at(U, ld_u, i, i);
-    for (int c = 0; c < n; ++c) at(B, ld_b, i, c) = at(B, ld_b, i, c) / d;
+    const double rd = 1. / at(U, ld_u, i, i);
+    for (int c = 0; c < n; ++c) at(B, ld_b, i, c) = at(B, ld_b, i, c) * rd;
     for (int r = 0; r < i; ++r) {
       const double left = -at(U, ld_u, r, i);
       for (int c = 0; c < n; ++c) at(B, ld_b, r, c) = std::fma(left, at(B, ld_b, i, c), at(B, ld_b, r, c));
@@ -284,6 +285,15 @@ int run_one(const pp_task& T, std::vector<double>& tmp) {
     case PP_OP_ACCUM:
       o_accum(T.p[0], T.p[1], T.p[2], T.p[3], T.n, T.m, T.k, T.l, T.ld[0], T.ld[1], T.ld[2], T.ld[3], t2, t3, T.alpha,
               T.p[4], T.ld[4]);
+      return 0;
+    case PP_OP_SUM:  // reduction of split-k partial products (engine instruction, p ascending)
+      for (int r = 0; r < T.m; ++r)
+        for (int c = 0; c < T.n; ++c) {
+          double s = 0.0;
+          for (int p = 0; p < T.k; ++p) s += T.p[1][(int64_t)(p * T.m + r) * T.ld[1] + c];
+          double& q = T.p[0][(int64_t)r * T.ld[0] + c];
+          q = T.beta != 0.0 ? q + s : s;
+        }
       return 0;
     default: return -1;
   }

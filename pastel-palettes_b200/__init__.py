@@ -28,7 +28,7 @@ LIB_PATH = os.path.join(_HERE, "libpastel_palettes.so")
 
 PP_OK, PP_INVALID_ARG, PP_OOM, PP_TIMEOUT, PP_NUMERICAL, PP_CUDA_ERROR, PP_UNSUPPORTED, PP_INTERNAL = range(8)
 STATUS_NAMES = ["OK", "INVALID_ARG", "OOM", "TIMEOUT", "NUMERICAL", "CUDA_ERROR", "UNSUPPORTED", "INTERNAL"]
-OP_NAMES = ["nop", "getrf", "trsml", "trsmr", "trsmrt", "trsmu", "gemm", "gemm3", "gemm4", "accum"]
+OP_NAMES = ["nop", "getrf", "trsml", "trsmr", "trsmrt", "trsmu", "gemm", "gemm3", "gemm4", "accum", "sum"]
 DENSE, LOWRANK, HIER = 0, 1, 2
 ARENAS = ["matrix", "work", "scratch", "rhs", "rand"]
 
@@ -48,7 +48,8 @@ class PPError(RuntimeError):
 
 
 class _Config(C.Structure):
-    _fields_ = [("tile", C.c_int), ("ctas_per_sm", C.c_int), ("spin_limit", C.c_longlong), ("seed", C.c_ulonglong)]
+    _fields_ = [("tile", C.c_int), ("ctas_per_sm", C.c_int), ("spin_limit", C.c_longlong), ("seed", C.c_ulonglong),
+                ("reference_isa", C.c_int)]
 
 
 class _BlockInfo(C.Structure):
@@ -58,7 +59,7 @@ class _BlockInfo(C.Structure):
 
 class _ProgramInfo(C.Structure):
     _fields_ = [("n_tasks", C.c_int), ("n_edges", C.c_longlong), ("flops", C.c_longlong),
-                ("op_count", C.c_longlong * 10), ("arena_elems", C.c_longlong * 5), ("host_build_ms", C.c_double)]
+                ("op_count", C.c_longlong * 12), ("arena_elems", C.c_longlong * 5), ("host_build_ms", C.c_double)]
 
 
 _lib = None
@@ -107,6 +108,7 @@ def lib():
             "pp_hmatrix_encode_program": (i, [vp, i, i, vp, vp, vp, vp, vp]),
             "pp_hmatrix_rand_host": (i, [vp, dp, ll]),
             "pp_hmatrix_program_edges": (i, [vp, i, i, vp, vp, vp]),
+            "pp_hmatrix_trace": (i, [vp, i, i, i, vp]),
             "pp_vm_execute": (i, [vp, vp, i, vp, ll, vp, ll, i, vp]),
             "pp_lowrank_accum_noalloc": (i, [vp, vp, i, vp, i, vp, i, vp, i, vp, i, i, i, i, i, d, vp]),
             "pp_refstream_encode": (i, [vp, i, vp, ll, vp, C.POINTER(ll)]),
@@ -134,14 +136,16 @@ def exported_symbols():
     hdr = os.path.join(os.path.dirname(_HERE), "include", "pastel_palettes.h")
     import re
     src = open(hdr).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    src = re.sub(r"//[^\n]*", "", src)
     return sorted(set(re.findall(r"\b(pp_[a-z0-9_]+)\s*\(", src)))
 
 
 class Context:
     """Device context (device >= 0) or host-only planning context (device = -1)."""
 
-    def __init__(self, device=0, tile=64, ctas_per_sm=0, spin_limit=1 << 24, seed=0x5EED5EED):
-        cfg = _Config(tile, ctas_per_sm, spin_limit, seed)
+    def __init__(self, device=0, tile=64, ctas_per_sm=0, spin_limit=1 << 24, seed=0x5EED5EED, reference_isa=0):
+        cfg = _Config(tile, ctas_per_sm, spin_limit, seed, reference_isa)
         h = C.c_void_p()
         st = lib().pp_context_create(device, C.byref(cfg), C.byref(h))
         if st != PP_OK:
@@ -150,8 +154,8 @@ class Context:
         self.device = device
 
     def __del__(self):
-        if getattr(self, "_h", None):
-            lib().pp_context_destroy(self._h)
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.pp_context_destroy(self._h)
             self._h = None
 
     @property
@@ -216,8 +220,8 @@ class Hierarchical:
         return cls(ctx, h)
 
     def __del__(self):
-        if getattr(self, "_h", None):
-            lib().pp_hmatrix_destroy(self._h)
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.pp_hmatrix_destroy(self._h)
             self._h = None
 
     @property
@@ -316,7 +320,7 @@ class Hierarchical:
         info = _ProgramInfo()
         self.ctx.check(lib().pp_hmatrix_program_info(self._h, which, nrhs, C.byref(info)), "program_info")
         return dict(n_tasks=info.n_tasks, n_edges=info.n_edges, flops=info.flops,
-                    op_count={OP_NAMES[i]: info.op_count[i] for i in range(10)},
+                    op_count={OP_NAMES[i]: info.op_count[i] for i in range(len(OP_NAMES))},
                     arena_elems={ARENAS[i]: info.arena_elems[i] for i in range(5)},
                     host_build_ms=info.host_build_ms)
 
@@ -345,6 +349,16 @@ class Hierarchical:
         self.ctx.check(lib().pp_hmatrix_program_edges(self._h, which, nrhs, f.ctypes.data, t.ctypes.data,
                                                       ty.ctypes.data), "program_edges")
         return f[:e], t[:e], ty[:e]
+
+    def enable_trace(self, which=0, nrhs=1, enable=True):
+        self.ctx.check(lib().pp_hmatrix_trace(self._h, which, nrhs, int(enable), None), "trace")
+
+    def read_trace(self, which=0, nrhs=1):
+        """(n_tasks, 3) uint64: start ns, end ns, sm | cta << 32 of the last traced launch."""
+        n = self.program_info(which, nrhs)["n_tasks"]
+        out = np.zeros((n, 3), dtype=np.uint64)
+        self.ctx.check(lib().pp_hmatrix_trace(self._h, which, nrhs, 1, out.ctypes.data), "trace")
+        return out
 
     def rand_host(self):
         n = self.program_info(0)["arena_elems"]["rand"]

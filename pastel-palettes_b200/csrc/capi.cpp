@@ -38,11 +38,14 @@ struct VmPlan {
   int64_t work_elems = 0, scratch_elems = 0, rhs_elems = 0;
   double build_ms = 0;
   int grid = 0;
+  unsigned long long* d_trace = nullptr;  // per-task (start, end, sm | cta << 32) when tracing
   void release() {
     cudaFree(d_tasks); cudaFree(d_succ); cudaFree(d_indeg); cudaFree(d_ready); cudaFree(d_counters);
     cudaFree(d_slots); cudaFree(d_state); cudaFree(d_work); cudaFree(d_scratch); cudaFree(d_rhs);
+    cudaFree(d_trace);
     d_tasks = nullptr; d_succ = d_indeg = d_ready = d_counters = d_slots = nullptr; d_state = nullptr;
     d_work = d_scratch = d_rhs = nullptr;
+    d_trace = nullptr;
     on_device = false;
   }
 };
@@ -116,7 +119,7 @@ pp_status build_program(pp_hmatrix* h, int which, int nrhs, VmPlan& plan) {
   if (plan.built) return PP_OK;
   auto t0 = std::chrono::steady_clock::now();
   try {
-    pp::Generator g(plan.prog, *h->H, ctx->cfg.tile, h->H->n);
+    pp::Generator g(plan.prog, *h->H, ctx->cfg.tile, h->H->n, ctx->cfg.reference_isa == 0);
     if (which == 0) g.getrf_program();
     else g.solve_program(nrhs);
     plan.prog.build_dag();
@@ -183,6 +186,7 @@ pp_status launch_plan(pp_hmatrix* h, VmPlan& plan, cudaStream_t s, int grid_cap)
   L.state = plan.d_state;
   L.spin_limit = ctx->cfg.spin_limit;
   L.grid = grid_cap > 0 ? std::min(plan.grid, grid_cap) : plan.grid;
+  L.trace = plan.d_trace;
   PP_CUDA(pp_vm_run(L, s));
   h->last = &plan;
   return PP_OK;
@@ -206,6 +210,7 @@ pp_status pp_context_create(int device, const pp_config* cfg, pp_context** out) 
     c->cfg.ctas_per_sm = cfg->ctas_per_sm;
     if (cfg->spin_limit > 0) c->cfg.spin_limit = cfg->spin_limit;
     if (cfg->seed) c->cfg.seed = cfg->seed;
+    c->cfg.reference_isa = cfg->reference_isa;
   }
   if (c->cfg.tile < 8 || c->cfg.tile > PP_VM_TILE) { delete c; return PP_INVALID_ARG; }
   c->device = device;
@@ -444,7 +449,7 @@ pp_status pp_hmatrix_program_info(pp_hmatrix* h, int which, int nrhs, pp_program
   info->n_tasks = plan->n_tasks;
   info->n_edges = plan->prog.edges;
   info->flops = plan->prog.total_flops();
-  for (int op = 0; op < 10; ++op) info->op_count[op] = plan->prog.count_op(op);
+  for (int op = 0; op < PP_OP_COUNT; ++op) info->op_count[op] = plan->prog.count_op(op);
   for (int a = 0; a < 5; ++a) info->arena_elems[a] = plan->prog.arena_elems[a];
   info->host_build_ms = plan->build_ms;
   return PP_OK;
@@ -521,6 +526,29 @@ pp_status pp_hmatrix_encode_program(pp_hmatrix* h, int which, int nrhs, double* 
   return PP_OK;
 }
 
+pp_status pp_hmatrix_trace(pp_hmatrix* h, int which, int nrhs, int enable, uint64_t* out) {
+  if (!h || (which != 0 && which != 1)) return PP_INVALID_ARG;
+  pp_context* ctx = h->ctx;
+  VmPlan* plan = which == 0 ? &h->factor : solve_plan(h, nrhs);
+  pp_status st = build_program(h, which, nrhs, *plan);
+  if (st != PP_OK) return st;
+  if (!has_device(ctx)) return fail(ctx, PP_CUDA_ERROR, "no CUDA device in this context");
+  const size_t bytes = sizeof(unsigned long long) * 3 * (size_t)std::max(plan->n_tasks, 1);
+  if (out) {
+    if (!plan->d_trace) return fail(ctx, PP_INVALID_ARG, "tracing was not enabled for this program");
+    PP_CUDA(cudaMemcpy(out, plan->d_trace, bytes, cudaMemcpyDeviceToHost));
+    return PP_OK;
+  }
+  if (enable && !plan->d_trace) {
+    PP_CUDA(cudaMalloc((void**)&plan->d_trace, bytes));
+    PP_CUDA(cudaMemset(plan->d_trace, 0, bytes));
+  } else if (!enable && plan->d_trace) {
+    cudaFree(plan->d_trace);
+    plan->d_trace = nullptr;
+  }
+  return PP_OK;
+}
+
 pp_status pp_hmatrix_program_edges(pp_hmatrix* h, int which, int nrhs, int64_t* from, int64_t* to, int32_t* type) {
   if (!h || !from || !to || !type || (which != 0 && which != 1)) return PP_INVALID_ARG;
   VmPlan* plan = which == 0 ? &h->factor : solve_plan(h, nrhs);
@@ -590,7 +618,8 @@ pp_status pp_lowrank_accum_noalloc(pp_context* ctx, double* U1, int ld_u1, doubl
                                    int k1, int k2, double sign, void* stream) {
   if (!ctx) return PP_INVALID_ARG;
   if (!has_device(ctx)) return fail(ctx, PP_CUDA_ERROR, "no CUDA device in this context");
-  if (!U1 || !V1 || !U2 || !V2 || !R || ny < 1 || nx < 1 || k1 < 1 || k1 > PP_VM_MAX_RANK || k2 < 1 ||
+  if (!U1 || !V1 || !U2 || !V2 || !R || ny < 1 || nx < 1 || k1 < 1 || k1 > PP_VM_MAX_RANK || k1 > ny || k1 > nx ||
+      k2 < 1 ||
       ld_u1 < k1 || ld_v1 < k1 || ld_u2 < k2 || ld_v2 < k2 || ld_r < k1 || (sign != 1.0 && sign != -1.0))
     return fail(ctx, PP_INVALID_ARG, "pp_lowrank_accum_noalloc: bad argument");
   const long long need = 2LL * ny * k1 + (long long)nx * k1 + (long long)k1 * std::max(k1, k2);

@@ -306,8 +306,8 @@ bool Program::encode_reference(int workers, std::vector<std::vector<int32_t>>& s
 }
 
 // ----------------------------------------------------------------------------- generator
-Generator::Generator(Program& P, Hierarchical& H, int tile, int max_n_rand)
-    : P_(P), H_(H), T_(tile), max_n_rand_(max_n_rand) {
+Generator::Generator(Program& P, Hierarchical& H, int tile, int max_n_rand, bool split_k)
+    : P_(P), H_(H), T_(tile), max_n_rand_(max_n_rand), split_k_(split_k) {
   if (tile < 8) throw std::invalid_argument("tile must be >= 8");
   inst_ = P.add_instance();
   const int ar = P.arena_id(inst_, AR_MATRIX);
@@ -590,6 +590,38 @@ void Generator::trsmu(const Mat& U, const Mat& B) {
 void Generator::gemm_tiles(const View& C, const View& A, const View& B, int alpha) {
   if (C.t) throw std::logic_error("gemm target must be untransposed");
   if (A.m != C.m || B.n != C.n || A.n != B.m) throw std::logic_error("gemm dimension mismatch");
+  const bool work_target = P_.objs[C.obj].arena == P_.arena_id(inst_, AR_WORK);
+  constexpr int kSplitK = 512;
+  if (split_k_ && work_target && (int64_t)C.m * C.n <= 256 && A.n > kSplitK) {
+    // a small product over a long k (e.g. V_a^T U_b): independent partial products over
+    // k slices on many SMs, then one reduction into C (order fixed, not ascending k)
+    const int parts = (A.n + kSplitK - 1) / kSplitK;
+    View Tp = tmp(parts * C.m, C.n);
+    for (int p = 0; p < parts; ++p) {
+      const int k0 = p * kSplitK, kk = std::min(kSplitK, A.n - k0);
+      HTask& t = emit(PP_OP_GEMM);
+      bind(t, 0, Tp.sub(p * C.m, 0, C.m, C.n), true);
+      bind(t, 1, A.sub(0, k0, C.m, kk), false);
+      bind(t, 2, B.sub(k0, 0, kk, C.n), false);
+      t.t.m = C.m;
+      t.t.n = C.n;
+      t.t.k = kk;
+      t.t.alpha = (double)alpha;
+      t.t.beta = 0.0;
+      t.t.flags |= PP_FREE_ORDER;
+      t.flops = 2LL * C.m * C.n * kk;
+    }
+    HTask& s = emit(PP_OP_SUM);
+    bind(s, 0, C, true);
+    bind(s, 1, Tp, false);
+    s.t.m = C.m;
+    s.t.n = C.n;
+    s.t.k = parts;
+    s.t.alpha = 1.0;
+    s.t.beta = 1.0;
+    s.flops = (int64_t)C.m * C.n * parts;
+    return;
+  }
   const int TN = std::min(C.n, 64);
   const int TM = std::min(C.m, std::max(64, 4096 / std::max(TN, 1)));
   for (int i = 0; i < C.m; i += TM)
@@ -604,6 +636,8 @@ void Generator::gemm_tiles(const View& C, const View& A, const View& B, int alph
       t.t.k = A.n;
       t.t.alpha = (double)alpha;
       t.t.beta = 1.0;
+      // intermediates of low-rank products (work buffers) may sum in any fixed order
+      if (P_.objs[C.obj].arena == P_.arena_id(inst_, AR_WORK)) t.t.flags |= PP_FREE_ORDER;
       t.flops = 2LL * mi * nj * A.n;
     }
 }

@@ -110,7 +110,9 @@ class Generator {
  public:
   // Builds programs on one H-matrix instance.  `tile`: dense blocks larger than this
   // are split (2 x 2) before they reach an instruction.
-  Generator(Program& P, Hierarchical& H, int tile, int max_n_rand);
+  // `split_k`: small products over a long k become partial products on many CTAs plus a
+  // SUM reduction (an engine instruction the reference's set does not have)
+  Generator(Program& P, Hierarchical& H, int tile, int max_n_rand, bool split_k = true);
   int inst() const { return inst_; }
   void getrf_program();            // H-LU factorization of the whole matrix
   void solve_program(int nrhs);    // B := U^-1 L^-1 B on the RHS object (n x nrhs)
@@ -134,6 +136,7 @@ class Generator {
   std::vector<int> node_obj_;  // Hierarchical obj -> program obj
   int rhs_obj_ = -1;
   int max_n_rand_;
+  bool split_k_;
 
   struct LRP { View x, y; int sign; };  // x y^T * sign
   LRP lr_product(const Mat& A, const Mat& B, int alpha);

@@ -21,16 +21,23 @@ enum pp_op {
   PP_OP_TRSML = 2,   /* B[m x n] := L^-1 B, L unit lower m x m      (kernel.cu:150-182, 667-715)  */
   PP_OP_TRSMR = 3,   /* B[m x n] := B U^-1, U upper n x n           (kernel.cu:185-226, 718-766)  */
   PP_OP_TRSMRT = 4,  /* V[m x n] := U^-T V, U upper m x m  (trsmr on V^T, kernel.cu:229-285, 769-817) */
-  PP_OP_TRSMU = 5,   /* B[m x n] := U^-1 B, U upper m x m (solve only; no reference counterpart)  */
+  PP_OP_TRSMU = 5,   /* B[m x n] := U^-1 B, U upper m x m (solve only; no reference counterpart;
+                        rows are scaled by the reciprocal of the diagonal)                     */
   PP_OP_GEMM = 6,    /* C[m x n] := beta C + alpha op(A)[m x k] op(B)[k x n] (kernel.cu:415-664)    */
   PP_OP_GEMM3 = 7,   /* C += alpha A B D, association by ctrl          (kernel.cu:886-904)         */
   PP_OP_GEMM4 = 8,   /* C += alpha A B D E, association by ctrl 0..4   (kernel.cu:907-955)         */
   PP_OP_ACCUM = 9,   /* U1 V1^T := rank-k1 range of U1 V1^T + alpha U2 V2^T (kernel.cu:1255-1280)   */
-  PP_OP_COUNT = 10
+  PP_OP_SUM = 10,    /* C[m x n] := beta C + sum_{p<k} T_p, T_p = p-th m x n block (ld n) of p[1]:
+                        reduction of split-k partial products (no reference counterpart)       */
+  PP_OP_COUNT = 11
 };
 
 /* flags: bit (4+i) = operand i is stored transposed (operand 0 is the target). */
 #define PP_T(i) (1 << (4 + (i)))
+/* flags bit 0: the contraction may sum its k products in any fixed order (set on
+ * products into work buffers, whose results are only compared within a tolerance);
+ * without it every element accumulates in ascending k, as the reference does. */
+#define PP_FREE_ORDER 1
 /* precision of the contraction inside GEMM-class tasks */
 #define PP_PREC_FP64 0
 #define PP_PREC_TF32 1

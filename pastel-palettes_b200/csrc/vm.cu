@@ -16,6 +16,10 @@
 //   TRSMR  kernel.cu:185-226   x_ri = b_ri / u_ii; b_rc = fma(-x_ri, u_ic, b_rc)
 //   TRSMRT kernel.cu:229-285   x_ic = v_ic * (1 / u_ii); v_rc = fma(-u_ir, x_ic, v_rc)
 //   GEMM   kernel.cu:288-664   c_ij = fma(alpha a_ik, b_kj, c_ij), k ascending from beta c_ij
+// Work distribution does not touch that order: GEMM tiles are shaped to the operands
+// (square, skinny, single column, small output with a long k), the triangular routines
+// keep each column (or row) in registers across four lanes of a warp and broadcast the
+// finished pivot entry with a shuffle, so they need no CTA barrier per step.
 // All global loads of data other CTAs may have written use ld.global.cg (L2), never L1.
 #include <cuda_runtime.h>
 #include <math.h>
@@ -25,8 +29,8 @@
 
 #define NT PP_VM_THREADS
 #define TL PP_VM_TILE
-#define LDS (PP_VM_TILE + 1)  /* padded smem row stride (doubles) */
-#define KC 16                 /* k-chunk of the GEMM tile loop   */
+#define LDS (PP_VM_TILE + 1)   /* padded smem row stride (doubles) */
+#define VM_SMEM_BYTES 40960    /* largest routine: the skinny GEMM tiles (37.4 KB) */
 
 namespace {
 
@@ -53,67 +57,188 @@ __device__ __forceinline__ int ld_relaxed(const int* p) {
 
 // ------------------------------------------------------------------------- GEMM
 // C[m x n] = beta C + alpha op(A) op(B), alpha in {+1, -1}, beta in {0, 1}.
-// 64 x 64 output tiles, 4 x 4 elements per thread, k staged through shared memory
-// in chunks of KC; each element's k loop runs in ascending order with one fma.
-__device__ void dev_gemm(double* __restrict__ C, int ldc, const double* __restrict__ A, int lda, bool tA,
-                         const double* __restrict__ B, int ldb, bool tB, int m, int n, int k, double alpha,
-                         double beta, double* smem) {
-  double* As = smem;            // [KC][LDS], element (kk, r)
-  double* Bs = smem + KC * LDS;  // [KC][LDS], element (kk, c)
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-  for (int i0 = 0; i0 < m; i0 += 64)
-    for (int j0 = 0; j0 < n; j0 += 64) {
-      double acc[4][4];
+// CTA tile TM x TN, thread micro-tile RM x RN (rows ty + TY a, columns tx + TX b), k in
+// chunks of KCH staged through shared memory; the next chunk is fetched into registers
+// while the current one is consumed.  Each element's k loop runs in ascending order.
+template <int TM, int TN, int RM, int RN, int KCH>
+__device__ __noinline__ void gemm_cfg(double* __restrict__ C, int ldc, const double* __restrict__ A, int lda,
+                                         bool tA, const double* __restrict__ B, int ldb, bool tB, int m, int n, int k,
+                                         double alpha, double beta, double* smem) {
+  constexpr int TX = TN / RN, TY = TM / RM;
+  static_assert(TX * TY == NT, "thread layout");
+  constexpr int LA = TM + 1, LB = TN + 1;
+  constexpr int AE = TM * KCH, BE = KCH * TN;
+  constexpr int AP = (AE + NT - 1) / NT, BP = (BE + NT - 1) / NT;
+  static_assert((KCH * LA + KCH * LB) * 8 <= VM_SMEM_BYTES, "smem");
+  double* As = smem;             // [KCH][LA]
+  double* Bs = smem + KCH * LA;  // [KCH][LB]
+  const int tid = threadIdx.x, tx = tid % TX, ty = tid / TX;
+  const int nch = (k + KCH - 1) / KCH;
+  for (int i0 = 0; i0 < m; i0 += TM)
+    for (int j0 = 0; j0 < n; j0 += TN) {
+      double acc[RM][RN];
 #pragma unroll
-      for (int a = 0; a < 4; ++a)
+      for (int a = 0; a < RM; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
-          const int r = i0 + ty + 16 * a, c = j0 + tx + 16 * b;
+        for (int b = 0; b < RN; ++b) {
+          const int r = i0 + ty + TY * a, c = j0 + tx + TX * b;
           acc[a][b] = (beta != 0.0 && r < m && c < n) ? ldcg(&C[(size_t)r * ldc + c]) : 0.0;
         }
-      for (int k0 = 0; k0 < k; k0 += KC) {
-        const int kc = min(KC, k - k0);
+      double ra[AP], rb[BP];
+#define PP_GEMM_FETCH(K0)                                                                                     \
+  do {                                                                                                        \
+    const int k0_ = (K0);                                                                                     \
+    _Pragma("unroll") for (int p = 0; p < AP; ++p) {                                                          \
+      const int e = tid + p * NT;                                                                             \
+      int r, kk;                                                                                              \
+      if (!tA) { r = e / KCH; kk = e % KCH; }                                                                 \
+      else { kk = e / TM; r = e % TM; }                                                                       \
+      double v = 0.0;                                                                                         \
+      if (e < AE && k0_ + kk < k && i0 + r < m)                                                               \
+        v = tA ? ldcg(&A[(size_t)(k0_ + kk) * lda + i0 + r]) : ldcg(&A[(size_t)(i0 + r) * lda + k0_ + kk]);   \
+      ra[p] = v * alpha; /* exact: alpha is +-1 */                                                            \
+    }                                                                                                         \
+    _Pragma("unroll") for (int p = 0; p < BP; ++p) {                                                          \
+      const int e = tid + p * NT;                                                                             \
+      int c, kk;                                                                                              \
+      if (!tB) { kk = e / TN; c = e % TN; }                                                                   \
+      else { c = e / KCH; kk = e % KCH; }                                                                     \
+      double v = 0.0;                                                                                         \
+      if (e < BE && k0_ + kk < k && j0 + c < n)                                                               \
+        v = tB ? ldcg(&B[(size_t)(j0 + c) * ldb + k0_ + kk]) : ldcg(&B[(size_t)(k0_ + kk) * ldb + j0 + c]);   \
+      rb[p] = v;                                                                                              \
+    }                                                                                                         \
+  } while (0)
+      if (nch > 0) PP_GEMM_FETCH(0);
+      for (int ch = 0; ch < nch; ++ch) {
         __syncthreads();
-        for (int e = tid; e < 64 * KC; e += NT) {
-          int kk, r;
-          if (!tA) { r = e / KC; kk = e % KC; }
-          else { kk = e / 64; r = e % 64; }
-          double v = 0.0;
-          if (kk < kc && i0 + r < m)
-            v = tA ? ldcg(&A[(size_t)(k0 + kk) * lda + i0 + r]) : ldcg(&A[(size_t)(i0 + r) * lda + k0 + kk]);
-          As[kk * LDS + r] = v * alpha;  // exact: alpha is +-1
+#pragma unroll
+        for (int p = 0; p < AP; ++p) {
+          const int e = tid + p * NT;
+          if (e < AE) {
+            int r, kk;
+            if (!tA) { r = e / KCH; kk = e % KCH; }
+            else { kk = e / TM; r = e % TM; }
+            As[kk * LA + r] = ra[p];
+          }
         }
-        for (int e = tid; e < 64 * KC; e += NT) {
-          int kk, c;
-          if (!tB) { kk = e / 64; c = e % 64; }
-          else { c = e / KC; kk = e % KC; }
-          double v = 0.0;
-          if (kk < kc && j0 + c < n)
-            v = tB ? ldcg(&B[(size_t)(j0 + c) * ldb + k0 + kk]) : ldcg(&B[(size_t)(k0 + kk) * ldb + j0 + c]);
-          Bs[kk * LDS + c] = v;
+#pragma unroll
+        for (int p = 0; p < BP; ++p) {
+          const int e = tid + p * NT;
+          if (e < BE) {
+            int c, kk;
+            if (!tB) { kk = e / TN; c = e % TN; }
+            else { c = e / KCH; kk = e % KCH; }
+            Bs[kk * LB + c] = rb[p];
+          }
         }
         __syncthreads();
+        if (ch + 1 < nch) PP_GEMM_FETCH((ch + 1) * KCH);
+        const int kc = min(KCH, k - ch * KCH);
         for (int kk = 0; kk < kc; ++kk) {
-          double av[4], bv[4];
+          double av[RM], bv[RN];
 #pragma unroll
-          for (int a = 0; a < 4; ++a) av[a] = As[kk * LDS + ty + 16 * a];
+          for (int a = 0; a < RM; ++a) av[a] = As[kk * LA + ty + TY * a];
 #pragma unroll
-          for (int b = 0; b < 4; ++b) bv[b] = Bs[kk * LDS + tx + 16 * b];
+          for (int b = 0; b < RN; ++b) bv[b] = Bs[kk * LB + tx + TX * b];
 #pragma unroll
-          for (int a = 0; a < 4; ++a)
+          for (int a = 0; a < RM; ++a)
 #pragma unroll
-            for (int b = 0; b < 4; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
+            for (int b = 0; b < RN; ++b) acc[a][b] = fma(av[a], bv[b], acc[a][b]);
         }
       }
 #pragma unroll
-      for (int a = 0; a < 4; ++a)
+      for (int a = 0; a < RM; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
-          const int r = i0 + ty + 16 * a, c = j0 + tx + 16 * b;
+        for (int b = 0; b < RN; ++b) {
+          const int r = i0 + ty + TY * a, c = j0 + tx + TX * b;
           if (r < m && c < n) C[(size_t)r * ldc + c] = acc[a][b];
         }
-      __syncthreads();
     }
+  __syncthreads();
+}
+
+// C[m x n] (m, n <= 16) = beta C + alpha op(A) op(B) for a long k, in free order: each warp
+// sums a contiguous k slice (ascending, 8 outputs per lane), the slices are then added in
+// warp order.  Deterministic, but not the reference's single ascending chain per element.
+__device__ __noinline__ void gemm_splitk(double* __restrict__ C, int ldc, const double* __restrict__ A, int lda,
+                                         bool tA, const double* __restrict__ B, int ldb, bool tB, int m, int n, int k,
+                                         double alpha, double beta, double* smem) {
+  constexpr int KW = 16, NW = NT / 32, LW = 17;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* As = smem + w * (2 * KW * LW);  // [KW][LW] (kk, r), this warp's
+  double* Bs = As + KW * LW;              // [KW][LW] (kk, c)
+  const int kseg = (k + NW - 1) / NW;
+  const int kb = min(k, w * kseg), ke = min(k, kb + kseg);
+  const int c_out = lane & 15;
+  double acc[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) acc[q] = 0.0;
+  double ra[8], rb[8];
+#define PP_SPLITK_FETCH(K0)                                                                                   \
+  do {                                                                                                        \
+    const int k0_ = (K0);                                                                                     \
+    _Pragma("unroll") for (int p = 0; p < 8; ++p) {                                                           \
+      const int e = lane + 32 * p;                                                                            \
+      const int kk = tA ? (e >> 4) : (e & 15), r = tA ? (e & 15) : (e >> 4);                                  \
+      double v = 0.0;                                                                                         \
+      if (r < m && k0_ + kk < ke)                                                                             \
+        v = tA ? ldcg(&A[(size_t)(k0_ + kk) * lda + r]) : ldcg(&A[(size_t)r * lda + k0_ + kk]);               \
+      ra[p] = v * alpha;                                                                                      \
+      const int kb_ = tB ? (e & 15) : (e >> 4), c = tB ? (e >> 4) : (e & 15);                                 \
+      double u = 0.0;                                                                                         \
+      if (c < n && k0_ + kb_ < ke)                                                                            \
+        u = tB ? ldcg(&B[(size_t)c * ldb + k0_ + kb_]) : ldcg(&B[(size_t)(k0_ + kb_) * ldb + c]);            \
+      rb[p] = u;                                                                                              \
+    }                                                                                                         \
+  } while (0)
+  if (kb < ke) PP_SPLITK_FETCH(kb);
+  for (int k0 = kb; k0 < ke; k0 += KW) {
+#pragma unroll
+    for (int p = 0; p < 8; ++p) {
+      const int e = lane + 32 * p;
+      As[(tA ? (e >> 4) : (e & 15)) * LW + (tA ? (e & 15) : (e >> 4))] = ra[p];
+      Bs[(tB ? (e & 15) : (e >> 4)) * LW + (tB ? (e >> 4) : (e & 15))] = rb[p];
+    }
+    __syncwarp();
+    if (k0 + KW < ke) PP_SPLITK_FETCH(k0 + KW);
+    const int kc = min(KW, ke - k0);
+    for (int kk = 0; kk < kc; ++kk) {
+      const double b = Bs[kk * LW + c_out];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) acc[q] = fma(As[kk * LW + ((lane + 32 * q) >> 4)], b, acc[q]);
+    }
+    __syncwarp();
+  }
+#undef PP_SPLITK_FETCH
+  __syncthreads();
+  double* red = smem;  // [NW][256] partial sums, output o = r * 16 + c
+#pragma unroll
+  for (int q = 0; q < 8; ++q) red[w * 256 + lane + 32 * q] = acc[q];
+  __syncthreads();
+  {
+    const int o = threadIdx.x, r = o >> 4, c = o & 15;
+    if (r < m && c < n) {
+      double s = red[o];
+      for (int ww = 1; ww < NW; ++ww) s += red[ww * 256 + o];
+      double* p = &C[(size_t)r * ldc + c];
+      *p = beta != 0.0 ? ldcg(p) + s : s;
+    }
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ void dev_gemm(double* __restrict__ C, int ldc, const double* __restrict__ A, int lda, bool tA,
+                         const double* __restrict__ B, int ldb, bool tB, int m, int n, int k, double alpha,
+                         double beta, double* smem, bool free_order = false) {
+  if (free_order && m <= 16 && n <= 16 && k >= 256)
+    gemm_splitk(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
+  else if (m <= 16 && n <= 16) gemm_cfg<16, 16, 1, 1, 128>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
+  else if (m <= 32 && n <= 32) gemm_cfg<32, 32, 2, 2, 64>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
+  else if (n == 1) gemm_cfg<256, 1, 1, 1, 16>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
+  else if (n <= 16) gemm_cfg<128, 16, 8, 1, 32>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
+  else if (m <= 16) gemm_cfg<16, 128, 1, 8, 32>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
+  else gemm_cfg<64, 64, 4, 4, 32>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
 }
 
 // ------------------------------------------------------------------------- tiles in smem
@@ -123,154 +248,320 @@ __device__ void load_tile(double* S, const double* __restrict__ G, int ld, int r
     S[r * LDS + c] = ldcg(&G[(size_t)r * ld + c]);
   }
 }
-__device__ void store_tile(double* G, int ld, const double* S, int rows, int cols) {
-  for (int e = threadIdx.x; e < rows * cols; e += NT) {
-    const int r = e / cols, c = e % cols;
-    G[(size_t)r * ld + c] = S[r * LDS + c];
-  }
-}
 
-// A[m x n] := L\U in place (m, n <= TL), a warp per row like kernel.cu:104-147
-__device__ void dev_getrf(double* A, int lda, int m, int n, double* smem) {
-  double* S = smem;
-  load_tile(S, A, lda, m, n);
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+// Register layout shared by GETRF / TRSML / TRSMRT / TRSMU: warp w, lane = 4 cc + g
+// holds column 8 w + cc (of a 64-wide chunk), rows g + 4 j for j < 16.  Row i of that
+// column lives in lane 4 cc + (i & 3), register i >> 2.
+#define COL_LAYOUT                                                      \
+  const int w_ = threadIdx.x >> 5, lane_ = threadIdx.x & 31;            \
+  const int cc_ = lane_ >> 2, g_ = lane_ & 3;                           \
+  (void)w_;
+
+// A[m x n] := L\U in place (m, n <= TL), like kernel.cu:104-147: for each i the
+// multipliers l_r = a_ri / a_ii of column i go through shared memory, the pivot row
+// entry of each column comes from a lane of the same column group.
+__device__ __noinline__ void dev_getrf(double* A, int lda, int m, int n, double* smem) {
+  double* lbuf = smem;  // [2][TL] multipliers of the current / previous step
+  COL_LAYOUT
+  const int c = 8 * w_ + cc_;
+  double x[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    const int r = g_ + 4 * j;
+    x[j] = (r < m && c < n) ? ldcg(&A[(size_t)r * lda + c]) : 0.0;
+  }
   const int mn = min(m, n);
-  for (int i = 0; i < mn; ++i) {
-    const double piv = S[i * LDS + i];
-    for (int r = i + 1 + warp; r < m; r += NT / 32) {
-      double l = 0.0;
-      if (lane == 0) {
-        l = S[r * LDS + i] / piv;
-        S[r * LDS + i] = l;
+#pragma unroll
+  for (int i = 0; i < TL; ++i) {
+    if (i >= mn) break;
+    if (w_ == (i >> 3)) {
+      // the four lanes holding column i hand it to the whole warp, which divides (two
+      // rows per lane instead of sixteen per owning lane), then take the multipliers back
+      double* cbuf = lbuf + 2 * TL;
+      if (cc_ == (i & 7)) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int r = g_ + 4 * j;
+          if (r >= i && r < m) cbuf[r] = x[j];
+        }
       }
-      l = __shfl_sync(0xffffffffu, l, 0);
-      for (int c = i + 1 + lane; c < n; c += 32) S[r * LDS + c] = fma(S[i * LDS + c], -l, S[r * LDS + c]);
+      __syncwarp();
+      const double aii = cbuf[i];
+      for (int r = i + 1 + lane_; r < m; r += 32) lbuf[(i & 1) * TL + r] = cbuf[r] / aii;
+      __syncwarp();
+      if (cc_ == (i & 7)) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int r = g_ + 4 * j;
+          if (r > i && r < m) x[j] = lbuf[(i & 1) * TL + r];
+        }
+      }
     }
     __syncthreads();
+    const double p = __shfl_sync(0xffffffffu, x[i >> 2], 4 * cc_ + (i & 3));
+    if (c > i && c < n) {
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int r = g_ + 4 * j;
+        if (r > i && r < m) x[j] = fma(p, -lbuf[(i & 1) * TL + r], x[j]);
+      }
+    }
   }
-  store_tile(A, lda, S, m, n);
+#pragma unroll
+  for (int j = 0; j < 16; ++j) {
+    const int r = g_ + 4 * j;
+    if (r < m && c < n) A[(size_t)r * lda + c] = x[j];
+  }
+  __syncthreads();
 }
 
-// B[m x n] := L^-1 B, L unit lower m x m (m <= TL); column chunks of TL
-__device__ void dev_trsml(double* B, int ldb, const double* L, int ldl, int m, int n, double* smem) {
+// B[m x n] := L^-1 B, L unit lower m x m (m <= TL); columns independent
+__device__ __noinline__ void dev_trsml(double* B, int ldb, const double* L, int ldl, int m, int n, double* smem) {
   double* Ls = smem;
-  double* Bs = smem + TL * LDS;
   load_tile(Ls, L, ldl, m, m);
-  for (int c0 = 0; c0 < n; c0 += TL) {
-    const int w = min(TL, n - c0);
-    load_tile(Bs, B + c0, ldb, m, w);
-    __syncthreads();
-    for (int i = 0; i + 1 < m; ++i) {
-      const int cnt = (m - i - 1) * w;
-      for (int e = threadIdx.x; e < cnt; e += NT) {
-        const int r = i + 1 + e / w, c = e % w;
-        Bs[r * LDS + c] = fma(Bs[i * LDS + c], -Ls[r * LDS + i], Bs[r * LDS + c]);
+  __syncthreads();
+  if (n <= 4) {
+    // few right-hand sides (solve): one warp, lane holds rows lane and lane + 32, the
+    // finished row i is broadcast by a shuffle; no CTA barrier inside the sweep
+    if (threadIdx.x < 32) {
+      const int lane = threadIdx.x;
+      double x0[4], x1[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        x0[c] = (lane < m && c < n) ? ldcg(&B[(size_t)lane * ldb + c]) : 0.0;
+        x1[c] = (lane + 32 < m && c < n) ? ldcg(&B[(size_t)(lane + 32) * ldb + c]) : 0.0;
       }
-      __syncthreads();
+#pragma unroll
+      for (int i = 0; i < TL - 1; ++i) {
+        if (i + 1 >= m) break;
+        double bi[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+          if (c < n) bi[c] = __shfl_sync(0xffffffffu, i < 32 ? x0[c] : x1[c], i & 31);
+        if (lane > i && lane < m) {
+          const double left = -Ls[lane * LDS + i];
+#pragma unroll
+          for (int c = 0; c < 4; ++c)
+            if (c < n) x0[c] = fma(bi[c], left, x0[c]);
+        }
+        if (lane + 32 > i && lane + 32 < m) {
+          const double left = -Ls[(lane + 32) * LDS + i];
+#pragma unroll
+          for (int c = 0; c < 4; ++c)
+            if (c < n) x1[c] = fma(bi[c], left, x1[c]);
+        }
+      }
+      for (int c = 0; c < n; ++c) {
+        if (lane < m) B[(size_t)lane * ldb + c] = x0[c];
+        if (lane + 32 < m) B[(size_t)(lane + 32) * ldb + c] = x1[c];
+      }
     }
-    store_tile(B + c0, ldb, Bs, m, w);
     __syncthreads();
+    return;
   }
+  COL_LAYOUT
+  for (int c0 = 0; c0 < n; c0 += TL) {
+    const int c = c0 + 8 * w_ + cc_;
+    double x[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int r = g_ + 4 * j;
+      x[j] = (r < m && c < n) ? ldcg(&B[(size_t)r * ldb + c]) : 0.0;
+    }
+#pragma unroll
+    for (int i = 0; i < TL - 1; ++i) {
+      if (i + 1 >= m) break;
+      const double v = __shfl_sync(0xffffffffu, x[i >> 2], 4 * cc_ + (i & 3));
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int r = g_ + 4 * j;
+        if (r > i && r < m) x[j] = fma(v, -Ls[r * LDS + i], x[j]);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int r = g_ + 4 * j;
+      if (r < m && c < n) B[(size_t)r * ldb + c] = x[j];
+    }
+  }
+  __syncthreads();
 }
 
-// B[m x n] := B U^-1, U upper n x n (n <= TL); rows are independent: a warp per row,
-// the row held in registers (lane owns columns lane and lane + 32)
-__device__ void dev_trsmr(double* B, int ldb, const double* U, int ldu, int m, int n, double* smem) {
+// V[m x n] := U^-T V, U upper m x m (m <= TL): the reference's trsmr on a transposed B
+// (kernel.cu:229-285) — row i is scaled by the reciprocal of u_ii, then eliminated below
+__device__ __noinline__ void dev_trsmrt(double* V, int ldv, const double* U, int ldu, int m, int n, double* smem) {
+  double* Us = smem;
+  double* rd = smem + TL * LDS;
+  load_tile(Us, U, ldu, m, m);
+  __syncthreads();
+  if (threadIdx.x < m) rd[threadIdx.x] = 1. / Us[threadIdx.x * LDS + threadIdx.x];
+  __syncthreads();
+  COL_LAYOUT
+  for (int c0 = 0; c0 < n; c0 += TL) {
+    const int c = c0 + 8 * w_ + cc_;
+    double x[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int r = g_ + 4 * j;
+      x[j] = (r < m && c < n) ? ldcg(&V[(size_t)r * ldv + c]) : 0.0;
+    }
+#pragma unroll
+    for (int i = 0; i < TL; ++i) {
+      if (i >= m) break;
+      const double v = __shfl_sync(0xffffffffu, x[i >> 2], 4 * cc_ + (i & 3));
+      const double xi = v * rd[i];
+      if (g_ == (i & 3)) x[i >> 2] = xi;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int r = g_ + 4 * j;
+        if (r > i && r < m) x[j] = fma(-Us[i * LDS + r], xi, x[j]);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int r = g_ + 4 * j;
+      if (r < m && c < n) V[(size_t)r * ldv + c] = x[j];
+    }
+  }
+  __syncthreads();
+}
+
+// B[m x n] := U^-1 B, U upper m x m (m <= TL), backward substitution (solve phase; no
+// reference counterpart): x_i = b_i * (1 / u_ii), then b_r -= u_ri x_i for r < i
+__device__ __noinline__ void dev_trsmu(double* B, int ldb, const double* U, int ldu, int m, int n, double* smem) {
+  double* Us = smem;
+  double* rd = smem + TL * LDS;
+  load_tile(Us, U, ldu, m, m);
+  __syncthreads();
+  if (threadIdx.x < m) rd[threadIdx.x] = 1. / Us[threadIdx.x * LDS + threadIdx.x];
+  __syncthreads();
+  if (n <= 4) {  // few right-hand sides: one warp, rows lane and lane + 32, shuffles only
+    if (threadIdx.x < 32) {
+      const int lane = threadIdx.x;
+      double x0[4], x1[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        x0[c] = (lane < m && c < n) ? ldcg(&B[(size_t)lane * ldb + c]) : 0.0;
+        x1[c] = (lane + 32 < m && c < n) ? ldcg(&B[(size_t)(lane + 32) * ldb + c]) : 0.0;
+      }
+#pragma unroll
+      for (int i = TL - 1; i >= 0; --i) {
+        if (i >= m) continue;
+        if (lane == (i & 31)) {
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            if (i < 32) x0[c] = x0[c] * rd[i];
+            else x1[c] = x1[c] * rd[i];
+          }
+        }
+        double bi[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+          if (c < n) bi[c] = __shfl_sync(0xffffffffu, i < 32 ? x0[c] : x1[c], i & 31);
+        if (lane < i) {
+          const double u = -Us[lane * LDS + i];
+#pragma unroll
+          for (int c = 0; c < 4; ++c)
+            if (c < n) x0[c] = fma(u, bi[c], x0[c]);
+        }
+        if (lane + 32 < i) {
+          const double u = -Us[(lane + 32) * LDS + i];
+#pragma unroll
+          for (int c = 0; c < 4; ++c)
+            if (c < n) x1[c] = fma(u, bi[c], x1[c]);
+        }
+      }
+      for (int c = 0; c < n; ++c) {
+        if (lane < m) B[(size_t)lane * ldb + c] = x0[c];
+        if (lane + 32 < m) B[(size_t)(lane + 32) * ldb + c] = x1[c];
+      }
+    }
+    __syncthreads();
+    return;
+  }
+  COL_LAYOUT
+  for (int c0 = 0; c0 < n; c0 += TL) {
+    const int c = c0 + 8 * w_ + cc_;
+    double x[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int r = g_ + 4 * j;
+      x[j] = (r < m && c < n) ? ldcg(&B[(size_t)r * ldb + c]) : 0.0;
+    }
+#pragma unroll
+    for (int i = TL - 1; i >= 0; --i) {
+      if (i >= m) continue;
+      const double v = __shfl_sync(0xffffffffu, x[i >> 2], 4 * cc_ + (i & 3));
+      const double xi = v * rd[i];
+      if (g_ == (i & 3)) x[i >> 2] = xi;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int r = g_ + 4 * j;
+        if (r < i) x[j] = fma(-Us[r * LDS + i], xi, x[j]);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int r = g_ + 4 * j;
+      if (r < m && c < n) B[(size_t)r * ldb + c] = x[j];
+    }
+  }
+  __syncthreads();
+}
+
+// B[m x n] := B U^-1, U upper n x n (n <= TL); rows independent: lane = 4 rr + g holds
+// row 8 w + rr (of a 64-row chunk), columns g + 4 j
+__device__ __noinline__ void dev_trsmr(double* B, int ldb, const double* U, int ldu, int m, int n, double* smem) {
   double* Us = smem;
   load_tile(Us, U, ldu, n, n);
   __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int r = warp; r < m; r += NT / 32) {
-    double* row = B + (size_t)r * ldb;
-    double x0 = lane < n ? ldcg(&row[lane]) : 0.0;
-    double x1 = lane + 32 < n ? ldcg(&row[lane + 32]) : 0.0;
-    for (int i = 0; i < n; ++i) {
-      const double bi = __shfl_sync(0xffffffffu, i < 32 ? x0 : x1, i & 31);
-      const double xi = bi / Us[i * LDS + i];
-      if (lane == (i & 31)) {
-        if (i < 32) x0 = xi;
-        else x1 = xi;
-      }
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, rr = lane >> 2, g = lane & 3;
+  for (int r0 = 0; r0 < m; r0 += 64) {
+    const int row = r0 + 8 * w + rr;
+    double x[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int c = g + 4 * j;
+      x[j] = (row < m && c < n) ? ldcg(&B[(size_t)row * ldb + c]) : 0.0;
+    }
+#pragma unroll
+    for (int i = 0; i < TL; ++i) {
+      if (i >= n) break;
+      const double v = __shfl_sync(0xffffffffu, x[i >> 2], 4 * rr + (i & 3));
+      const double xi = v / Us[i * LDS + i];
+      if (g == (i & 3)) x[i >> 2] = xi;
       const double left = -xi;
-      if (lane > i && lane < n) x0 = fma(left, Us[i * LDS + lane], x0);
-      if (lane + 32 > i && lane + 32 < n) x1 = fma(left, Us[i * LDS + lane + 32], x1);
-    }
-    if (lane < n) row[lane] = x0;
-    if (lane + 32 < n) row[lane + 32] = x1;
-  }
-}
-
-// V[m x n] := U^-T V, U upper m x m (m <= TL): the reference's trsmr on a transposed
-// B (kernel.cu:229-285) — row i is scaled by the reciprocal of u_ii
-__device__ void dev_trsmrt(double* V, int ldv, const double* U, int ldu, int m, int n, double* smem) {
-  double* Us = smem;
-  double* Vs = smem + TL * LDS;
-  load_tile(Us, U, ldu, m, m);
-  for (int c0 = 0; c0 < n; c0 += TL) {
-    const int w = min(TL, n - c0);
-    load_tile(Vs, V + c0, ldv, m, w);
-    __syncthreads();
-    for (int i = 0; i < m; ++i) {
-      const double rd = 1.0 / Us[i * LDS + i];
-      for (int c = threadIdx.x; c < w; c += NT) Vs[i * LDS + c] *= rd;
-      __syncthreads();
-      const int cnt = (m - i - 1) * w;
-      for (int e = threadIdx.x; e < cnt; e += NT) {
-        const int r = i + 1 + e / w, c = e % w;
-        Vs[r * LDS + c] = fma(-Us[i * LDS + r], Vs[i * LDS + c], Vs[r * LDS + c]);
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int c = g + 4 * j;
+        if (c > i && c < n) x[j] = fma(left, Us[i * LDS + c], x[j]);
       }
-      __syncthreads();
     }
-    store_tile(V + c0, ldv, Vs, m, w);
-    __syncthreads();
-  }
-}
-
-// B[m x n] := U^-1 B, U upper m x m (m <= TL), backward substitution (solve phase)
-__device__ void dev_trsmu(double* B, int ldb, const double* U, int ldu, int m, int n, double* smem) {
-  double* Us = smem;
-  double* Bs = smem + TL * LDS;
-  load_tile(Us, U, ldu, m, m);
-  for (int c0 = 0; c0 < n; c0 += TL) {
-    const int w = min(TL, n - c0);
-    load_tile(Bs, B + c0, ldb, m, w);
-    __syncthreads();
-    for (int i = m - 1; i >= 0; --i) {
-      const double d = Us[i * LDS + i];
-      for (int c = threadIdx.x; c < w; c += NT) Bs[i * LDS + c] = Bs[i * LDS + c] / d;
-      __syncthreads();
-      const int cnt = i * w;
-      for (int e = threadIdx.x; e < cnt; e += NT) {
-        const int r = e / w, c = e % w;
-        Bs[r * LDS + c] = fma(-Us[r * LDS + i], Bs[i * LDS + c], Bs[r * LDS + c]);
-      }
-      __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int c = g + 4 * j;
+      if (row < m && c < n) B[(size_t)row * ldb + c] = x[j];
     }
-    store_tile(B + c0, ldb, Bs, m, w);
-    __syncthreads();
   }
+  __syncthreads();
 }
 
 // ------------------------------------------------------------------------- GEMM3 / GEMM4
 // Reference association orders (kernel.cu:886-955), intermediates in task scratch.
-__device__ void dev_gemm3(const pp_task& T, double* smem) {
+__device__ __noinline__ void dev_gemm3(const pp_task& T, double* smem) {
   const bool tA = T.flags & PP_T(1), tB = T.flags & PP_T(2), tC = T.flags & PP_T(3);
   double* t1 = T.tmp;
   const int m = T.m, n = T.n, k = T.k, l = T.l;
   if (T.ctrl) {  // (A B) C, t1: m x l
     dev_gemm(t1, l, T.p[1], T.ld[1], tA, T.p[2], T.ld[2], tB, m, l, k, 1.0, 0.0, smem);
-    __syncthreads();
     dev_gemm(T.p[0], T.ld[0], t1, l, false, T.p[3], T.ld[3], tC, m, n, l, T.alpha, 1.0, smem);
   } else {       // A (B C), t1: k x n
     dev_gemm(t1, n, T.p[2], T.ld[2], tB, T.p[3], T.ld[3], tC, k, n, l, 1.0, 0.0, smem);
-    __syncthreads();
     dev_gemm(T.p[0], T.ld[0], T.p[1], T.ld[1], tA, t1, n, false, m, n, k, T.alpha, 1.0, smem);
   }
 }
 
-__device__ void dev_gemm4(const pp_task& T, double* smem) {
+__device__ __noinline__ void dev_gemm4(const pp_task& T, double* smem) {
   const bool tA = T.flags & PP_T(1), tB = T.flags & PP_T(2), tC = T.flags & PP_T(3), tD = T.flags & PP_T(4);
   const double *A = T.p[1], *B = T.p[2], *Cm = T.p[3], *D = T.p[4];
   const int la = T.ld[1], lb = T.ld[2], lc = T.ld[3], ld = T.ld[4];
@@ -281,192 +572,139 @@ __device__ void dev_gemm4(const pp_task& T, double* smem) {
   const int lm = T.ld[0];
   switch (T.ctrl) {
     case 0:  // ((A B) C) D; t1 m x l, t2 m x o
-      dev_gemm(t1, l, A, la, tA, B, lb, tB, m, l, k, 1.0, 0.0, smem); __syncthreads();
-      dev_gemm(t2, o, t1, l, false, Cm, lc, tC, m, o, l, 1.0, 0.0, smem); __syncthreads();
+      dev_gemm(t1, l, A, la, tA, B, lb, tB, m, l, k, 1.0, 0.0, smem);
+      dev_gemm(t2, o, t1, l, false, Cm, lc, tC, m, o, l, 1.0, 0.0, smem);
       dev_gemm(M, lm, t2, o, false, D, ld, tD, m, n, o, T.alpha, 1.0, smem);
       break;
     case 1:  // (A (B C)) D; t1 k x o, t2 m x o
-      dev_gemm(t1, o, B, lb, tB, Cm, lc, tC, k, o, l, 1.0, 0.0, smem); __syncthreads();
-      dev_gemm(t2, o, A, la, tA, t1, o, false, m, o, k, 1.0, 0.0, smem); __syncthreads();
+      dev_gemm(t1, o, B, lb, tB, Cm, lc, tC, k, o, l, 1.0, 0.0, smem);
+      dev_gemm(t2, o, A, la, tA, t1, o, false, m, o, k, 1.0, 0.0, smem);
       dev_gemm(M, lm, t2, o, false, D, ld, tD, m, n, o, T.alpha, 1.0, smem);
       break;
     case 2:  // A ((B C) D); t1 k x o, t2 k x n
-      dev_gemm(t1, o, B, lb, tB, Cm, lc, tC, k, o, l, 1.0, 0.0, smem); __syncthreads();
-      dev_gemm(t2, n, t1, o, false, D, ld, tD, k, n, o, 1.0, 0.0, smem); __syncthreads();
+      dev_gemm(t1, o, B, lb, tB, Cm, lc, tC, k, o, l, 1.0, 0.0, smem);
+      dev_gemm(t2, n, t1, o, false, D, ld, tD, k, n, o, 1.0, 0.0, smem);
       dev_gemm(M, lm, A, la, tA, t2, n, false, m, n, k, T.alpha, 1.0, smem);
       break;
     case 3:  // A (B (C D)); t1 l x n, t2 k x n
-      dev_gemm(t1, n, Cm, lc, tC, D, ld, tD, l, n, o, 1.0, 0.0, smem); __syncthreads();
-      dev_gemm(t2, n, B, lb, tB, t1, n, false, k, n, l, 1.0, 0.0, smem); __syncthreads();
+      dev_gemm(t1, n, Cm, lc, tC, D, ld, tD, l, n, o, 1.0, 0.0, smem);
+      dev_gemm(t2, n, B, lb, tB, t1, n, false, k, n, l, 1.0, 0.0, smem);
       dev_gemm(M, lm, A, la, tA, t2, n, false, m, n, k, T.alpha, 1.0, smem);
       break;
     default:  // 4: (A B) (C D); t1 m x l, t2 l x n
-      dev_gemm(t1, l, A, la, tA, B, lb, tB, m, l, k, 1.0, 0.0, smem); __syncthreads();
-      dev_gemm(t2, n, Cm, lc, tC, D, ld, tD, l, n, o, 1.0, 0.0, smem); __syncthreads();
+      dev_gemm(t1, l, A, la, tA, B, lb, tB, m, l, k, 1.0, 0.0, smem);
+      dev_gemm(t2, n, Cm, lc, tC, D, ld, tD, l, n, o, 1.0, 0.0, smem);
       dev_gemm(M, lm, t1, l, false, t2, n, false, m, n, l, T.alpha, 1.0, smem);
       break;
   }
 }
 
 // ------------------------------------------------------------------------- ACCUM
-// Deterministic CTA-wide column sums: thread t accumulates rows r0 + t, r0 + t + NT, ...
-// in ascending order; lanes combine by an xor butterfly; warps are added in order.
-template <int KM>
-__device__ __forceinline__ void cta_sum_cols(double (&v)[KM], int ncols, double* red, double* out) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-#pragma unroll
-  for (int c = 0; c < KM; ++c) {
-    if (c < ncols) {
-      double x = v[c];
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
-      if (lane == 0) red[warp * KM + c] = x;
+// One Cholesky-QR pass on Y (m x k, ld k, global scratch): G = Y^T Y (+ shift I),
+// G = R^T R, Y := Y R^-1.  A non-positive pivot marks a rank-deficient column, which is
+// zeroed.  G (k x k) goes through the global scratch `Gg`.
+__device__ __noinline__ void cholqr_pass(double* Y, int m, int k, double* Gg, bool shifted, double* smem) {
+  dev_gemm(Gg, k, Y, k, true, Y, k, false, k, k, m, 1.0, 0.0, smem, true);
+  double* G = smem;                                     // k x (PP_VM_MAX_RANK + 1)
+  double* rinv = smem + PP_VM_MAX_RANK * (PP_VM_MAX_RANK + 1);
+  constexpr int LG = PP_VM_MAX_RANK + 1;
+  for (int e = threadIdx.x; e < k * k; e += NT) G[(e / k) * LG + e % k] = ldcg(&Gg[e]);
+  __syncthreads();
+  if (threadIdx.x < 32) {  // right-looking Cholesky, one lane per column
+    const int lane = threadIdx.x;
+    double tr = 0.0;
+    for (int j = 0; j < k; ++j) tr += G[j * LG + j];
+    const double tiny = 1e-28 * tr;
+    if (shifted) {
+      // shift of shifted CholeskyQR3: 11 (m k + k (k + 1)) u ||Y||_F^2, u = 2^-53
+      const double s = 11.0 * ((double)m * k + (double)k * (k + 1)) * 1.1102230246251565e-16 * tr;
+      if (lane < k) G[lane * LG + lane] += s;
+      __syncwarp();
+    }
+    for (int j = 0; j < k; ++j) {
+      const double d = G[j * LG + j];
+      const bool live = d > tiny;
+      const double rjj = live ? sqrt(d) : 0.0;
+      __syncwarp();
+      if (lane == j) { G[j * LG + j] = rjj; rinv[j] = live ? 1.0 / rjj : 0.0; }
+      if (lane > j && lane < k) G[j * LG + lane] = live ? G[j * LG + lane] / rjj : 0.0;
+      __syncwarp();
+      if (lane > j && lane < k)
+        for (int c1 = j + 1; c1 <= lane; ++c1) G[c1 * LG + lane] -= G[j * LG + c1] * G[j * LG + lane];
+      __syncwarp();
     }
   }
   __syncthreads();
-  if (threadIdx.x < ncols) {
-    double s = red[threadIdx.x];
-    for (int w = 1; w < NT / 32; ++w) s += red[w * KM + threadIdx.x];
-    out[threadIdx.x] = s;
+  // Y := Y R^-1, a thread per row: x_j = (y_j - sum_{p<j} x_p r_pj) / r_jj
+  for (int r = threadIdx.x; r < m; r += NT) {
+    double x[PP_VM_MAX_RANK];
+#pragma unroll
+    for (int j = 0; j < PP_VM_MAX_RANK; ++j) x[j] = j < k ? ldcg(&Y[(size_t)r * k + j]) : 0.0;
+#pragma unroll
+    for (int j = 0; j < PP_VM_MAX_RANK; ++j) {
+      if (j < k) {
+        double s = x[j];
+#pragma unroll
+        for (int p = 0; p < j; ++p) s = fma(-x[p], G[p * LG + j], s);
+        x[j] = s * rinv[j];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < PP_VM_MAX_RANK; ++j)
+      if (j < k) Y[(size_t)r * k + j] = x[j];
   }
   __syncthreads();
-}
-
-// Householder QR of Y (m x k, ld k, global scratch) and explicit Q (m x k, ld k).
-// Column j: nrm = sqrt(y_jj^2 + sum_{r>j} y_rj^2), beta = -sign(y_jj) nrm,
-// v_r = y_rj / (y_jj - beta), tau = (beta - y_jj) / beta.
-__device__ void dev_householder_qr(double* Y, double* Q, int m, int k, double* smem) {
-  double* red = smem;                  // NT/32 x PP_VM_MAX_RANK
-  double* sums = red + (NT / 32) * PP_VM_MAX_RANK;  // PP_VM_MAX_RANK
-  double* tau = sums + PP_VM_MAX_RANK;  // PP_VM_MAX_RANK
-  __shared__ double s_beta;
-  for (int j = 0; j < k; ++j) {
-    double v[PP_VM_MAX_RANK];
-    // norm of the column below the diagonal
-    {
-      double s = 0.0;
-      for (int r = j + 1 + threadIdx.x; r < m; r += NT) {
-        const double y = ldcg(&Y[(size_t)r * k + j]);
-        s = fma(y, y, s);
-      }
-      double one[1] = {s};
-      cta_sum_cols<1>(one, 1, red, sums);
-    }
-    if (threadIdx.x == 0) {
-      const double a = ldcg(&Y[(size_t)j * k + j]);
-      const double nrm = sqrt(fma(a, a, sums[0]));
-      if (nrm == 0.0) { tau[j] = 0.0; s_beta = 0.0; }
-      else {
-        const double beta = a >= 0.0 ? -nrm : nrm;
-        tau[j] = (beta - a) / beta;
-        s_beta = a - beta;  // divisor of v
-        Y[(size_t)j * k + j] = beta;
-      }
-    }
-    __syncthreads();
-    const double div = s_beta;
-    if (div != 0.0)
-      for (int r = j + 1 + threadIdx.x; r < m; r += NT) Y[(size_t)r * k + j] = ldcg(&Y[(size_t)r * k + j]) / div;
-    __syncthreads();
-    const double tj = tau[j];
-    const int nc = k - j - 1;  // columns j+1 .. k-1
-    if (nc > 0 && tj != 0.0) {
-#pragma unroll
-      for (int c = 0; c < PP_VM_MAX_RANK; ++c) v[c] = 0.0;
-      for (int r = j + 1 + threadIdx.x; r < m; r += NT) {
-        const double vr = ldcg(&Y[(size_t)r * k + j]);
-#pragma unroll
-        for (int c = 0; c < PP_VM_MAX_RANK; ++c)
-          if (c < nc) v[c] = fma(vr, ldcg(&Y[(size_t)r * k + j + 1 + c]), v[c]);
-      }
-      cta_sum_cols<PP_VM_MAX_RANK>(v, nc, red, sums);
-      // w_c = y_jc + sum;  y_jc -= tau w_c;  y_rc -= tau w_c v_r
-      for (int c = threadIdx.x; c < nc; c += NT) {
-        const double w = ldcg(&Y[(size_t)j * k + j + 1 + c]) + sums[c];
-        sums[c] = tj * w;
-        Y[(size_t)j * k + j + 1 + c] = fma(-tj, w, ldcg(&Y[(size_t)j * k + j + 1 + c]));
-      }
-      __syncthreads();
-      for (int r = j + 1 + threadIdx.x; r < m; r += NT) {
-        const double vr = ldcg(&Y[(size_t)r * k + j]);
-        for (int c = 0; c < nc; ++c) {
-          double* p = &Y[(size_t)r * k + j + 1 + c];
-          *p = fma(-sums[c], vr, ldcg(p));
-        }
-      }
-      __syncthreads();
-    }
-  }
-  // Q = H_0 ... H_{k-1} [I; 0]
-  for (int e = threadIdx.x; e < m * k; e += NT) {
-    const int r = e / k, c = e % k;
-    Q[e] = (r == c) ? 1.0 : 0.0;
-  }
-  __syncthreads();
-  for (int j = k - 1; j >= 0; --j) {
-    const double tj = tau[j];
-    if (tj == 0.0) continue;
-    const int nc = k - j;  // columns j .. k-1
-    double v[PP_VM_MAX_RANK];
-#pragma unroll
-    for (int c = 0; c < PP_VM_MAX_RANK; ++c) v[c] = 0.0;
-    for (int r = j + 1 + threadIdx.x; r < m; r += NT) {
-      const double vr = ldcg(&Y[(size_t)r * k + j]);
-#pragma unroll
-      for (int c = 0; c < PP_VM_MAX_RANK; ++c)
-        if (c < nc) v[c] = fma(vr, ldcg(&Q[(size_t)r * k + j + c]), v[c]);
-    }
-    cta_sum_cols<PP_VM_MAX_RANK>(v, nc, red, sums);
-    for (int c = threadIdx.x; c < nc; c += NT) {
-      const double w = ldcg(&Q[(size_t)j * k + j + c]) + sums[c];
-      sums[c] = tj * w;
-      Q[(size_t)j * k + j + c] = fma(-tj, w, ldcg(&Q[(size_t)j * k + j + c]));
-    }
-    __syncthreads();
-    for (int r = j + 1 + threadIdx.x; r < m; r += NT) {
-      const double vr = ldcg(&Y[(size_t)r * k + j]);
-      for (int c = 0; c < nc; ++c) {
-        double* p = &Q[(size_t)r * k + j + c];
-        *p = fma(-sums[c], vr, ldcg(p));
-      }
-    }
-    __syncthreads();
-  }
 }
 
 // U1 V1^T := Q Q^T (U1 V1^T + alpha U2 V2^T), Q spanning (U1 V1^T + alpha U2 V2^T) R:
-// the reference's randomized accumulation (kernel.cu:1255-1280) with a Householder QR
-// in place of its Givens sweeps.  m = ny, n = nx, k = k1 (target rank), l = k2.
-__device__ void dev_accum(const pp_task& T, double* smem) {
+// the reference's randomized accumulation (kernel.cu:1255-1280); Q from shifted
+// CholeskyQR3 (three Gram passes) in place of the reference's Givens sweeps.
+// m = ny, n = nx, k = k1 (target rank), l = k2.
+__device__ __noinline__ void dev_accum(const pp_task& T, double* smem) {
   const int ny = T.m, nx = T.n, k1 = T.k, k2 = T.l;
   const bool tU2 = T.flags & PP_T(2), tV2 = T.flags & PP_T(3);
   double *U1 = T.p[0], *V1 = T.p[1];
   const double *U2 = T.p[2], *V2 = T.p[3], *R = T.p[4];
   const int lu1 = T.ld[0], lv1 = T.ld[1], lu2 = T.ld[2], lv2 = T.ld[3], lr = T.ld[4];
   const int kp = max(k1, k2);
-  double* Ys = T.tmp;                          // ny x k1
-  double* P = Ys + (size_t)ny * k1;            // k1 x kp
-  double* W = P + (size_t)k1 * kp;             // nx x k1
-  double* Q = W + (size_t)nx * k1;             // ny x k1
+  double* Ys = T.tmp;                // ny x k1  (becomes Q)
+  double* P = Ys + (size_t)ny * k1;  // k1 x kp
+  double* W = P + (size_t)k1 * kp;   // nx x k1
+  double* Gg = W + (size_t)nx * k1;  // k1 x k1
   const double al = T.alpha;
-  dev_gemm(P, kp, R, lr, true, V1, lv1, false, k1, k1, nx, 1.0, 0.0, smem); __syncthreads();
-  dev_gemm(Ys, k1, U1, lu1, false, P, kp, true, ny, k1, k1, 1.0, 0.0, smem); __syncthreads();
-  dev_gemm(P, kp, R, lr, true, V2, lv2, tV2, k1, k2, nx, 1.0, 0.0, smem); __syncthreads();
-  dev_gemm(Ys, k1, U2, lu2, tU2, P, kp, true, ny, k1, k2, al, 1.0, smem); __syncthreads();
-  dev_householder_qr(Ys, Q, ny, k1, smem);
-  __syncthreads();
-  dev_gemm(P, kp, Q, k1, true, U1, lu1, false, k1, k1, ny, 1.0, 0.0, smem); __syncthreads();
-  dev_gemm(W, k1, V1, lv1, false, P, kp, true, nx, k1, k1, 1.0, 0.0, smem); __syncthreads();
-  dev_gemm(P, kp, Q, k1, true, U2, lu2, tU2, k1, k2, ny, 1.0, 0.0, smem); __syncthreads();
-  dev_gemm(W, k1, V2, lv2, tV2, P, kp, true, nx, k1, k2, al, 1.0, smem); __syncthreads();
+  constexpr bool fo = true;  // every product here is an intermediate of the recompression
+  dev_gemm(P, kp, R, lr, true, V1, lv1, false, k1, k1, nx, 1.0, 0.0, smem, fo);
+  dev_gemm(Ys, k1, U1, lu1, false, P, kp, true, ny, k1, k1, 1.0, 0.0, smem, fo);
+  dev_gemm(P, kp, R, lr, true, V2, lv2, tV2, k1, k2, nx, 1.0, 0.0, smem, fo);
+  dev_gemm(Ys, k1, U2, lu2, tU2, P, kp, true, ny, k1, k2, al, 1.0, smem, fo);
+  cholqr_pass(Ys, ny, k1, Gg, true, smem);
+  cholqr_pass(Ys, ny, k1, Gg, false, smem);
+  cholqr_pass(Ys, ny, k1, Gg, false, smem);
+  dev_gemm(P, kp, Ys, k1, true, U1, lu1, false, k1, k1, ny, 1.0, 0.0, smem, fo);
+  dev_gemm(W, k1, V1, lv1, false, P, kp, true, nx, k1, k1, 1.0, 0.0, smem, fo);
+  dev_gemm(P, kp, Ys, k1, true, U2, lu2, tU2, k1, k2, ny, 1.0, 0.0, smem, fo);
+  dev_gemm(W, k1, V2, lv2, tV2, P, kp, true, nx, k1, k2, al, 1.0, smem, fo);
   for (int e = threadIdx.x; e < ny * k1; e += NT) {
     const int r = e / k1, c = e % k1;
-    U1[(size_t)r * lu1 + c] = ldcg(&Q[e]);
+    U1[(size_t)r * lu1 + c] = ldcg(&Ys[e]);
   }
   for (int e = threadIdx.x; e < nx * k1; e += NT) {
     const int r = e / k1, c = e % k1;
     V1[(size_t)r * lv1 + c] = ldcg(&W[e]);
   }
+}
+
+// C[m x n] := beta C + sum_p T_p (p ascending), T_p the p-th m x n block of T
+__device__ __noinline__ void dev_sum(double* C, int ldc, const double* T, int ldt, int m, int n, int parts,
+                                     double beta) {
+  for (int e = threadIdx.x; e < m * n; e += NT) {
+    const int r = e / n, c = e % n;
+    double s = 0.0;
+    for (int p = 0; p < parts; ++p) s += ldcg(&T[(size_t)(p * m + r) * ldt + c]);
+    double* q = &C[(size_t)r * ldc + c];
+    *q = beta != 0.0 ? ldcg(q) + s : s;
+  }
+  __syncthreads();
 }
 
 __device__ bool run_task(const pp_task& T, double* smem) {
@@ -494,13 +732,16 @@ __device__ bool run_task(const pp_task& T, double* smem) {
       return true;
     case PP_OP_GEMM:
       dev_gemm(T.p[0], T.ld[0], T.p[1], T.ld[1], T.flags & PP_T(1), T.p[2], T.ld[2], T.flags & PP_T(2), T.m, T.n,
-               T.k, T.alpha, T.beta, smem);
+               T.k, T.alpha, T.beta, smem, (T.flags & PP_FREE_ORDER) != 0);
       return true;
     case PP_OP_GEMM3: dev_gemm3(T, smem); return true;
     case PP_OP_GEMM4: dev_gemm4(T, smem); return true;
     case PP_OP_ACCUM:
       if (T.k > PP_VM_MAX_RANK || T.k < 1) return false;
       dev_accum(T, smem);
+      return true;
+    case PP_OP_SUM:
+      dev_sum(T.p[0], T.ld[0], T.p[1], T.ld[1], T.m, T.n, T.k, T.beta);
       return true;
     default: return false;
   }
@@ -522,12 +763,24 @@ __global__ void vm_init(const int32_t* __restrict__ indeg, const int32_t* __rest
   }
 }
 
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ unsigned smid() {
+  unsigned s;
+  asm volatile("mov.u32 %0, %%smid;" : "=r"(s));
+  return s;
+}
+
 __global__ void __launch_bounds__(NT, 2)
     vm_kernel(const pp_task* __restrict__ tasks, int n_tasks, const int32_t* __restrict__ succ, int32_t* counters,
-              int32_t* slots, pp_vm_state* st, long long spin_limit) {
+              int32_t* slots, pp_vm_state* st, long long spin_limit, unsigned long long* trace) {
   extern __shared__ double smem[];
   __shared__ __align__(16) pp_task s_task;
   __shared__ int s_id;
+  __shared__ unsigned long long s_t0;
   for (;;) {
     if (threadIdx.x == 0) {
       int id = -1;
@@ -543,10 +796,11 @@ __global__ void __launch_bounds__(NT, 2)
             id = -1;
             break;
           }
-          __nanosleep(64);
+          __nanosleep(32);
         }
       }
       s_id = id;
+      if (trace) s_t0 = globaltimer_ns();
     }
     __syncthreads();
     const int id = s_id;
@@ -556,19 +810,27 @@ __global__ void __launch_bounds__(NT, 2)
           __ldg(reinterpret_cast<const unsigned long long*>(&tasks[id]) + threadIdx.x);
     __syncthreads();
     const bool ok = run_task(s_task, smem);
+    __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) {
       if (!ok && atomicCAS(&st->error, 0, PP_VM_BAD_TASK) == 0) st->err_info = id;
-      __threadfence();
-      for (int q = 0; q < s_task.n_succ; ++q) {
-        const int s = succ[s_task.succ_begin + q];
-        if (atom_add_acq_rel(&counters[s], -1) == 1) {
-          const int pos = atomicAdd(&st->tail, 1);
-          st_release(&slots[pos], s);
-        }
+      if (trace) {
+        trace[3 * (size_t)id] = s_t0;
+        trace[3 * (size_t)id + 1] = globaltimer_ns();
+        trace[3 * (size_t)id + 2] = smid() | ((unsigned long long)blockIdx.x << 32);
       }
-      atomicAdd(&st->done, 1);
     }
+    // successors are released in parallel, one thread each (a serial loop costs one L2
+    // round trip per successor on the critical path)
+    const int nsucc = s_task.n_succ, sbeg = s_task.succ_begin;
+    for (int q = threadIdx.x; q < nsucc; q += NT) {
+      const int s = succ[sbeg + q];
+      if (atom_add_acq_rel(&counters[s], -1) == 1) {
+        const int pos = atomicAdd(&st->tail, 1);
+        st_release(&slots[pos], s);
+      }
+    }
+    if (threadIdx.x == 0) atomicAdd(&st->done, 1);
   }
 }
 
@@ -670,12 +932,12 @@ cudaError_t pp_accum_noalloc_launch(const pp_task& T, long long scratch_doubles,
   }
   pp_task t = T;
   t.tmp = addr[dev];
-  // shared memory: the GEMM k-chunk tiles, which also hold the QR reductions
-  accum_noalloc_kernel<<<1, NT, (size_t)2 * KC * LDS * sizeof(double), s>>>(t);
+  // shared memory: the GEMM tiles and the Cholesky-QR Gram matrix (below the 48 KB default)
+  accum_noalloc_kernel<<<1, NT, VM_SMEM_BYTES, s>>>(t);
   return cudaGetLastError();
 }
 
-size_t pp_vm_smem_bytes() { return (size_t)2 * TL * LDS * sizeof(double); }
+size_t pp_vm_smem_bytes() { return VM_SMEM_BYTES; }
 
 int pp_vm_blocks_per_sm() {
   int nb = 0;
@@ -693,7 +955,7 @@ cudaError_t pp_vm_run(const pp_vm_launch& L, cudaStream_t s) {
   vm_init<<<(L.n_tasks + ib - 1) / ib, ib, 0, s>>>(L.indeg, L.ready, L.n_ready, L.n_tasks, L.counters, L.slots,
                                                   L.state);
   vm_kernel<<<L.grid, NT, pp_vm_smem_bytes(), s>>>(L.tasks, L.n_tasks, L.succ, L.counters, L.slots, L.state,
-                                                   L.spin_limit);
+                                                   L.spin_limit, L.trace);
   return cudaGetLastError();
 }
 

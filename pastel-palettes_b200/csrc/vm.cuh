@@ -32,6 +32,7 @@ struct pp_vm_launch {
   pp_vm_state* state;
   long long spin_limit;  /* polls of an empty ready slot before the kernel gives up */
   int grid;              /* CTAs (persistent)                                       */
+  unsigned long long* trace = nullptr;  /* optional: 3 words per task (start ns, end ns, sm | cta << 32) */
 };
 
 /* ACCUM on caller buffers with the library's static scratch array (no allocation);

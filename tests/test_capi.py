@@ -60,6 +60,21 @@ def test_factor_program_flops_match_dense_count(pp, hctx):
     assert h.program_info(0)["flops"] == 2 * n ** 3 // 3 - n ** 2 // 2 - n // 6 == 715303424
 
 
+def test_reference_isa_switch(pp):
+    # split-k reductions (SUM) speed up long-k products but have no reference form
+    fast = pp.Context(device=-1)
+    h, _ = pp.make_kernel_problem(fast, 2048, 2, "inv", 1e-3, 256, 16)
+    assert h.program_info(0)["op_count"]["sum"] > 0
+    with pytest.raises(pp.PPError) as e:
+        h.refstreams(1)
+    assert e.value.status == pp.PP_UNSUPPORTED
+    ref = pp.Context(device=-1, reference_isa=1)
+    h2, _ = pp.make_kernel_problem(ref, 2048, 2, "inv", 1e-3, 256, 16)
+    assert h2.program_info(0)["op_count"]["sum"] == 0
+    words, lengths, tmp = h2.refstreams(1)
+    assert len(words) > 0
+
+
 def test_refstream_rejects_solve_only_instruction(pp, hctx):
     # the factor program is expressible in the reference's instruction set
     h, _ = pp.make_kernel_problem(hctx, 512, 2, "inv", 1e-3, 64, 8)

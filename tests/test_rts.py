@@ -122,6 +122,8 @@ def task_regions(T):
         return [reg(0, m, n, False), reg(1, m, k, True), reg(2, k, n, True)]
     if op == 9:
         return [reg(0, m, k, False), reg(1, n, k, False), reg(2, m, l, True), reg(3, n, l, True)]
+    if op == 10:
+        return [reg(0, m, n, False), reg(1, k * m, n, True)]
     raise AssertionError(f"unexpected op {op}")
 
 
