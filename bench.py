@@ -1,13 +1,15 @@
 #!/usr/bin/env python
 """bench.py — H-LU factor+solve/s at <= 1e-10 backward error (FP64 HODLR, N = 8192).
 
-Workload (one "step"): restore the H-matrix (kernel 1/(r+1e-3) on 8192 Morton-sorted points
-of U[0,1]^2, diagonal shifted by 2 * max off-diagonal row sum, weak admissibility, leaf 256,
-rank 16), H-LU factorization on the persistent VM, then solve + FP64 iterative refinement
-until ||b - Ax||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= 1e-10.  Inputs are synthetic and
-seeded.  Multi-GPU: independent replicas, one per rank (no collective on the data path).
+Workload: the H-matrix of kernel 1/(r+1e-3) on 8192 Morton-sorted points of U[0,1]^2,
+diagonal shifted by 2 * max off-diagonal row sum, weak admissibility, leaf 256, rank 16.
+One "step" processes a batch of such factor+solve jobs in merged persistent launches:
+restore every instance, batched H-LU factorization, then batched solves + FP64 iterative
+refinement until ||b - Ax||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= 1e-10 for every job;
+the step is captured once as a CUDA graph and replayed.  Inputs are synthetic and seeded.
+Multi-GPU: independent replicas, one per rank (no collective on the data path).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl ours|reference]
 """
 import argparse
 import importlib.util
@@ -145,8 +147,8 @@ def fp64_peak_tflops(torch):
 
 # ----------------------------------------------------------------------------- CPU arm
 def cpu_steps(pp, oracle, h, prob, steps, threads):
-    """Factor + solve + refinement on the host cores with the oracle (restated reference
-    routines) executed over the same DAG; returns seconds per step and refinement steps."""
+    """Factor + solve + refinement of one job on the host cores with the oracle (restated
+    reference routines) executed over the same DAG; returns seconds per step and solves."""
     n = prob.n
     b = pp.rhs(n, 1, seed=7)
     A_rows = None
@@ -193,18 +195,32 @@ def run_reference_arm(args, pp, rank, world):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD_NAME, **{k: v for k, v in WORKLOAD.items()}},
             "cpu_baseline": {"value": value, "unit": "factor+solve/s", "cores": threads, "kind": "port",
-                             "sample": f"{len(t)} full steps of the workload (oracle over the same DAG, "
-                                       f"{threads} threads; refinement {iters[-1]} solves)"},
+                             "sample": f"{len(t)} full jobs of the workload, one at a time (oracle over the "
+                                       f"same DAG, {threads} threads; refinement {iters[-1]} solves)"},
             "e2e": {"value": value, "unit": "factor+solve/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
 # ----------------------------------------------------------------------------- GPU arm
+def make_batch(pp, ctx, batch, rank):
+    """`batch` instances of the workload matrix (one seeded construction, copied into each
+    instance's own host image and device arena); distinct right-hand sides per instance."""
+    w = WORKLOAD
+    h0, prob = build_problem(pp, ctx, rank)
+    hs = [h0]
+    for _ in range(1, batch):
+        h = pp.Hierarchical.geometric(ctx, prob.points, w["leaf"], w["admissibility"], 1.0, w["rank"])
+        h.host_arena()[:] = h0.host_arena()
+        hs.append(h)
+    return hs, [prob] * batch
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--batch", type=int, default=16, help="jobs per merged launch")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -222,141 +238,174 @@ def main():
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    tol = WORKLOAD["tol"]
+    B = args.batch
     ctx = pp.Context(device=local)
-    h, prob = build_problem(pp, ctx, rank)
-    h.pin_host()
-    s = torch.cuda.current_stream()
-    h.upload(s)
-    h.keep_original(s)
-    b = torch.from_numpy(pp.rhs(prob.n, 1, seed=7)).cuda()
-    ref = pp.Refiner(h, ctx, prob, stream=s)
+    hs, probs = make_batch(pp, ctx, B, rank)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        for h in hs:
+            h.pin_host()
+            h.upload(s)
+            h.keep_original(s)
+    s.synchronize()
+    batch = pp.Batch(ctx, hs)
+    n = probs[0].n
+    b_host = [torch.from_numpy(pp.rhs(n, 1, seed=7 + i)).pin_memory() for i in range(B)]
+    bs = [x.cuda() for x in b_host]
+    ref = pp.BatchRefiner(batch, probs, stream=s)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
 
-    def step():
-        h.restore(s)
-        h.factor(s)
-        x, hist = ref.solve(b, tol=WORKLOAD["tol"])
-        return x, hist
+    # --- warm-up (eager): allocates every plan, fixes the number of refinement solves
+    with torch.cuda.stream(s):
+        for _ in range(args.warmup):
+            batch.restore(s)
+            batch.factor(s)
+            xs, hist = ref.solve(bs, tol=tol)
+    batch.sync(s)
+    if hist[-1] > tol:
+        raise SystemExit(f"refinement did not reach {tol}: {hist}")
+    iters = len(hist)
 
-    for _ in range(args.warmup):
-        x, hist = step()
-    h.sync(s)
-    if hist[-1] > WORKLOAD["tol"]:
-        raise SystemExit(f"refinement did not reach {WORKLOAD['tol']}: {hist}")
+    # --- steady state captured once: restore, batched factor, `iters` batched solves
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            batch.restore(s)
+            batch.factor(s)
+            out = ref.run(bs, iters)
+    launches_per_step = 2 + iters * (2 + B)
 
     def barrier():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
 
-    # --- device-timed steps (inputs resident in HBM), L2 flushed between steps
-    launches0 = ref.launches
-    n_iters = []
-    total = 0.0
+    total, worst = 0.0, 0.0
     with Clocks(local) as clk:
         barrier()
         for _ in range(args.steps):
             flush.zero_()
+            torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(s)
-            x, hist = step()
-            e1.record(s)
+            with torch.cuda.stream(s):  # replay on the stream the events are recorded on
+                e0.record(s)
+                g.replay()
+                e1.record(s)
             e1.synchronize()
             total += e0.elapsed_time(e1) / 1e3
-            n_iters.append(len(hist))
+            worst = max(worst, max(ref.errors(bs, *out)))
         barrier()
-    h.sync(s)
-    gpu_launches = 2 * args.steps + (ref.launches - launches0)
+    batch.sync(s)
+    if worst > tol:
+        raise SystemExit(f"a timed step ended above {tol}: {worst}")
     t = torch.tensor([total], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     total_max = t.item()
-    value = world * args.steps / total_max
+    value = world * B * args.steps / total_max
 
-    # --- end to end through the C ABI with host buffers: H2D matrix + rhs, factor,
-    #     refinement, D2H solution (and the scalar norms the refinement reads back)
-    b_host = torch.from_numpy(pp.rhs(prob.n, 1, seed=7)).pin_memory()
-    x_host = torch.empty_like(b_host).pin_memory()
+    # --- end to end through the C ABI: matrices and right-hand sides up from pinned host
+    #     memory, batched factor + refinement, solutions down
+    g2 = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g2, stream=s):
+            batch.factor(s)
+            out2 = ref.run(bs, iters)
+    x_host = [torch.empty_like(x).pin_memory() for x in b_host]
+    e2e_steps = max(3, args.steps // 2)
     e2e_total = 0.0
-    d2h_extra = 0
     barrier()
-    for _ in range(max(3, args.steps // 2)):
+    for _ in range(e2e_steps):
         flush.zero_()
+        torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(s)
-        h.upload(s)
-        bd = b_host.to("cuda", non_blocking=True)
-        h.factor(s)
-        xd, hist = ref.solve(bd, tol=WORKLOAD["tol"])
-        x_host.copy_(xd, non_blocking=True)
+        with torch.cuda.stream(s):
+            e0.record(s)
+            for h in hs:
+                h.upload(s)
+            for bd, bh in zip(bs, b_host):
+                bd.copy_(bh, non_blocking=True)
+            g2.replay()
+            for xh, xd in zip(x_host, out2[0]):
+                xh.copy_(xd, non_blocking=True)
         e1.record(s)
         e1.synchronize()
         e2e_total += e0.elapsed_time(e1) / 1e3
-        d2h_extra = 16 * len(hist)
-    e2e_steps = max(3, args.steps // 2)
+    if max(ref.errors(bs, *out2)) > tol:
+        raise SystemExit("end-to-end step ended above the tolerance")
     t = torch.tensor([e2e_total], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * e2e_steps / t.item()
-    h.restore(s)
+    e2e_value = world * B * e2e_steps / t.item()
 
-    # --- roofline of the dominant kernel (the factor VM launch), timed alone
+    # --- the dominant kernel (the batched factor launch), timed alone
     fac_ms = []
-    for _ in range(args.steps):
-        h.restore(s)
-        flush.zero_()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(s)
-        h.factor(s)
-        e1.record(s)
-        e1.synchronize()
-        fac_ms.append(e0.elapsed_time(e1))
-    h.sync(s)
-    sol_ms = []
-    r = torch.empty_like(b)
-    for _ in range(args.steps):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(s)
-        h.solve(b, r, s)
-        e1.record(s)
-        e1.synchronize()
-        sol_ms.append(e0.elapsed_time(e1))
-    fbytes, finfo = program_bytes(pp, h, 0)
+    with torch.cuda.stream(s):
+        for _ in range(args.steps):
+            batch.restore(s)
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            batch.factor(s)
+            e1.record(s)
+            e1.synchronize()
+            fac_ms.append(e0.elapsed_time(e1))
+    batch.sync(s)
+    # one job alone (latency of a single factor+solve, eager with adaptive refinement)
+    single = pp.Batch(ctx, [hs[0]])
+    ref1 = pp.BatchRefiner(single, probs[:1], stream=s)
+    lat = []
+    with torch.cuda.stream(s):
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            single.restore(s)
+            single.factor(s)
+            ref1.solve(bs[:1], tol=tol)
+            e1.record(s)
+            e1.synchronize()
+            lat.append(e0.elapsed_time(e1))
+    fbytes, finfo = program_bytes(pp, hs[0], 0)
     hbm_peak, peak_kind = peaks()
-    fac_s = float(np.mean(fac_ms)) / 1e3
+    fac_s = float(np.median(fac_ms)) / 1e3
     fp64_peak = fp64_peak_tflops(torch)
-    achieved_gbs = fbytes / fac_s / 1e9
+    achieved_gbs = B * fbytes / fac_s / 1e9
     roofline = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
                 "frac": achieved_gbs / hbm_peak, "traffic": None,
-                "kernel": "vm_kernel (factor launch)", "launch_ms": 1e3 * fac_s,
-                "algorithmic_bytes": fbytes, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                "fp64": {"achieved_tflops": finfo["flops"] / fac_s / 1e12, "peak_tflops": fp64_peak,
-                         "frac": finfo["flops"] / fac_s / 1e12 / fp64_peak,
-                         "peak_source": "measured in this run: torch float64 matmul 8192^3"},
-                "solve_launch_ms": float(np.mean(sol_ms))}
+                "kernel": f"vm_kernel (batched factor launch, {B} jobs)", "launch_ms": 1e3 * fac_s,
+                "algorithmic_bytes": B * fbytes, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "fp64": {"achieved_tflops": B * finfo["flops"] / fac_s / 1e12, "peak_tflops": fp64_peak,
+                         "frac": B * finfo["flops"] / fac_s / 1e12 / fp64_peak,
+                         "peak_source": "measured in this run: torch float64 matmul 8192^3"}}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         import oracle
         threads = os.cpu_count() or 1
         hc, pc = build_problem(pp, pp.Context(device=-1), 0)
-        times, iters = cpu_steps(pp, oracle, hc, pc, 2, threads)
+        times, its = cpu_steps(pp, oracle, hc, pc, 2, threads)
         cpu = {"value": 1.0 / times[-1], "unit": "factor+solve/s", "cores": threads, "kind": "port",
-               "sample": f"1 full step of the same workload after 1 warm-up (oracle over the same DAG, "
-                         f"{threads} threads, {iters[-1]} refinement solves)"}
+               "sample": f"1 full job of the same workload after 1 warm-up (oracle over the same DAG, "
+                         f"{threads} threads, {its[-1]} refinement solves)"}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "factor+solve/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1e3 * total_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": WORKLOAD_NAME, **WORKLOAD, "l2": "flushed between steps (256 MiB write)",
-                           "parallelism": f"replicas{world}", "factor_tasks": finfo["n_tasks"],
-                           "factor_flops": finfo["flops"], "refinement_solves": int(np.median(n_iters))},
+                "config": {"workload": WORKLOAD_NAME, **WORKLOAD, "batch": B,
+                           "batch_note": "copies of one seeded matrix, distinct right-hand sides, one merged launch",
+                           "l2": "flushed between steps (256 MiB write)", "graph": "restore+factor+solves captured",
+                           "parallelism": f"replicas{world}", "factor_tasks_per_job": finfo["n_tasks"],
+                           "factor_flops_per_job": finfo["flops"], "refinement_solves": iters,
+                           "single_job_step_ms": float(np.median(lat))},
                 "e2e": {"value": e2e_value, "unit": "factor+solve/s",
-                        "h2d_bytes_per_step": h.arena_bytes() + 8 * prob.n,
-                        "d2h_bytes_per_step": 8 * prob.n + d2h_extra},
-                "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": gpu_launches}
+                        "h2d_bytes_per_step": B * (hs[0].arena_bytes() + 8 * n),
+                        "d2h_bytes_per_step": B * 8 * n},
+                "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),
+                "gpu_launches": launches_per_step * args.steps}
         print(json.dumps(line), flush=True)
+    del g, g2
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

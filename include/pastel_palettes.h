@@ -118,12 +118,31 @@ pp_status pp_hmatrix_program_info(pp_hmatrix* h, int which, int nrhs, pp_program
  * 256 or 0; kernel_size is accepted and ignored (one launch covers the whole DAG). */
 pp_status pp_dev_hierarchical_getrf(pp_hmatrix* h, int num_blocks, int num_threads, int kernel_size);
 
+/* --- batches: many H-matrices in one persistent launch (no reference counterpart;
+ *     the reference launches one DAG at a time, src/launcher.cu:146-167) ----------- */
+typedef struct pp_batch pp_batch;
+/* merges the factor programs of n uploaded H-matrices (sizes may differ) into one task
+ * table; the instances stay owned by the caller and must outlive the batch */
+pp_status pp_batch_create(pp_context* ctx, pp_hmatrix* const* hs, int n, pp_batch** out);
+void pp_batch_destroy(pp_batch* b);
+/* factor all instances: one VM launch (plus one memset of the work buffers) */
+pp_status pp_batch_factor(pp_batch* b, void* stream);
+/* X_i := A_i^-1 B_i for every instance i, one VM launch; B[i], X[i] device n_i x nrhs */
+pp_status pp_batch_solve(pp_batch* b, const double* const* B, double* const* X, int nrhs, void* stream);
+pp_status pp_batch_restore(pp_batch* b, void* stream);  /* pp_hmatrix_restore on every instance */
+pp_status pp_batch_sync(pp_batch* b, void* stream);
+pp_status pp_batch_program_info(pp_batch* b, int which, int nrhs, pp_program_info* info);
+pp_status pp_batch_trace(pp_batch* b, int which, int nrhs, int enable, uint64_t* out);
+
 /* --- residuals (FP64 refinement) ----------------------------------------- */
 /* r := b - A x, A dense row-major (device); x, b, r device n x nrhs */
 pp_status pp_dense_residual_dev(pp_context* ctx, const double* A, int lda, int n, const double* x, const double* b,
                                 double* r, int nrhs, void* stream);
 /* r := b - A x, A_ij = K(|p_i - p_j|) + shift * (i == j) evaluated on the fly.
- * kernel: 0 = 1/(r+p0), 1 = 1/(4 pi (r+p0)), 2 = exp(-r/p0), 3 = Matern-3/2 length p0 */
+ * kernel: 0 = 1/(r+p0), 1 = 1/(4 pi (r+p0)), 2 = exp(-r/p0), 3 = Matern-3/2 length p0.
+ * Partial sums go through a context-owned buffer, grown on the first call of a larger size
+ * (make that call before capturing a CUDA graph); calls on different streams must not
+ * overlap. */
 pp_status pp_kernel_residual_dev(pp_context* ctx, int kernel, double p0, double shift, const double* pts_dev,
                                  int dim, int n, const double* x, const double* b, double* r, int nrhs,
                                  void* stream);

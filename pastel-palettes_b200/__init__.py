@@ -111,6 +111,14 @@ def lib():
             "pp_hmatrix_trace": (i, [vp, i, i, i, vp]),
             "pp_vm_execute": (i, [vp, vp, i, vp, ll, vp, ll, i, vp]),
             "pp_lowrank_accum_noalloc": (i, [vp, vp, i, vp, i, vp, i, vp, i, vp, i, i, i, i, i, d, vp]),
+            "pp_batch_create": (i, [vp, vp, i, C.POINTER(vp)]),
+            "pp_batch_destroy": (None, [vp]),
+            "pp_batch_factor": (i, [vp, vp]),
+            "pp_batch_solve": (i, [vp, vp, vp, i, vp]),
+            "pp_batch_restore": (i, [vp, vp]),
+            "pp_batch_sync": (i, [vp, vp]),
+            "pp_batch_program_info": (i, [vp, i, i, C.POINTER(_ProgramInfo)]),
+            "pp_batch_trace": (i, [vp, i, i, i, vp]),
             "pp_refstream_encode": (i, [vp, i, vp, ll, vp, C.POINTER(ll)]),
         }
         for name, (res, args) in sig.items():
@@ -376,6 +384,108 @@ class Hierarchical:
         self.ctx.check(lib().pp_refstream_encode(self._h, workers, words.ctypes.data, words.size,
                                                  lengths.ctypes.data, C.byref(tmp)), "refstream")
         return words, lengths, tmp.value
+
+
+class Batch:
+    """Several uploaded H-matrices (any sizes) factored / solved by one persistent launch
+    over their merged task tables.  Each instance's result equals its result alone."""
+
+    def __init__(self, ctx, hs):
+        arr = (C.c_void_p * len(hs))(*[h.handle for h in hs])
+        h = C.c_void_p()
+        ctx.check(lib().pp_batch_create(ctx.handle, arr, len(hs), C.byref(h)), "batch_create")
+        self.ctx, self.hs, self._h = ctx, list(hs), h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.pp_batch_destroy(self._h)
+            self._h = None
+
+    def factor(self, stream=None):
+        self.ctx.check(lib().pp_batch_factor(self._h, _stream_handle(stream)), "batch_factor")
+
+    def solve(self, Bs, Xs, stream=None):
+        nrhs = Bs[0].shape[1]
+        b = (C.c_void_p * len(Bs))(*[C.c_void_p(t.data_ptr()) for t in Bs])
+        x = (C.c_void_p * len(Xs))(*[C.c_void_p(t.data_ptr()) for t in Xs])
+        self.ctx.check(lib().pp_batch_solve(self._h, b, x, nrhs, _stream_handle(stream)), "batch_solve")
+
+    def restore(self, stream=None):
+        self.ctx.check(lib().pp_batch_restore(self._h, _stream_handle(stream)), "batch_restore")
+
+    def sync(self, stream=None):
+        self.ctx.check(lib().pp_batch_sync(self._h, _stream_handle(stream)), "batch_sync")
+
+    def program_info(self, which=0, nrhs=1):
+        info = _ProgramInfo()
+        self.ctx.check(lib().pp_batch_program_info(self._h, which, nrhs, C.byref(info)), "batch_program_info")
+        return dict(n_tasks=info.n_tasks, n_edges=info.n_edges, flops=info.flops,
+                    op_count={OP_NAMES[i]: info.op_count[i] for i in range(len(OP_NAMES))},
+                    host_build_ms=info.host_build_ms)
+
+    def enable_trace(self, which=0, nrhs=1):
+        self.ctx.check(lib().pp_batch_trace(self._h, which, nrhs, 1, None), "batch_trace")
+
+    def read_trace(self, which=0, nrhs=1):
+        n = self.program_info(which, nrhs)["n_tasks"]
+        out = np.zeros((n, 3), dtype=np.uint64)
+        self.ctx.check(lib().pp_batch_trace(self._h, which, nrhs, 1, out.ctypes.data), "batch_trace")
+        return out
+
+
+class BatchRefiner:
+    """FP64 iterative refinement for every instance of a Batch (kernel problems); one batched
+    solve launch per iteration, residuals per instance, until all backward errors <= tol."""
+
+    def __init__(self, batch, probs, stream=None):
+        import torch
+        self.batch, self.probs, self.stream = batch, probs, stream
+        self.pts = [torch.from_numpy(np.ascontiguousarray(p.points)).cuda() for p in probs]
+        self.launches = 0
+
+    def _iterate(self, xs, rs, dxs, bs):
+        ctx = self.batch.ctx
+        self.batch.solve(rs, dxs, self.stream)
+        self.launches += 2
+        for x, dx in zip(xs, dxs):
+            x += dx
+        for p, pts, x, b, r in zip(self.probs, self.pts, xs, bs, rs):
+            ctx.kernel_residual(p.kernel, p.p0, p.shift, pts, x, b, r, self.stream)
+            self.launches += 1
+
+    def errors(self, bs, xs, rs):
+        """Normwise backward error of every instance (one device-to-host read)."""
+        import torch
+        bn = torch.stack([b.abs().max() for b in bs])
+        nA = torch.tensor([p.norm_inf for p in self.probs], dtype=torch.float64, device=bs[0].device)
+        err = torch.stack([r.abs().max() for r in rs]) / (nA * torch.stack([x.abs().max() for x in xs]) + bn)
+        return err.cpu().tolist()
+
+    def run(self, bs, iters):
+        """Exactly `iters` refinement solves without host synchronization (capturable in a
+        CUDA graph); returns (xs, rs) with rs the final residuals."""
+        import torch
+        xs = [torch.zeros_like(b) for b in bs]
+        rs = [b.clone() for b in bs]
+        dxs = [torch.empty_like(b) for b in bs]
+        for _ in range(iters):
+            self._iterate(xs, rs, dxs, bs)
+        return xs, rs
+
+    def solve(self, bs, tol=1e-10, max_iter=30):
+        """Refine until every instance's backward error <= tol; bs: device n_i x nrhs."""
+        import torch
+        xs = [torch.zeros_like(b) for b in bs]
+        rs = [b.clone() for b in bs]
+        dxs = [torch.empty_like(b) for b in bs]
+        hist = []
+        for _ in range(max_iter):
+            self._iterate(xs, rs, dxs, bs)
+            e = max(self.errors(bs, xs, rs))
+            hist.append(e)
+            if e <= tol:
+                break
+        return xs, hist
 
 
 def dev_hierarchical_GETRF(h, num_blocks=0, num_threads=0, kernel_size=0):

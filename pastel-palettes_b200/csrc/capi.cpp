@@ -22,6 +22,9 @@ struct pp_context {
   int blocks_per_sm = 0;
   pp_config cfg{};
   std::string err;
+  double* d_resid = nullptr;  // partial sums of the matrix-free residual (grown on demand)
+  size_t resid_elems = 0;
+  ~pp_context() { cudaFree(d_resid); }
 };
 
 namespace {
@@ -39,6 +42,7 @@ struct VmPlan {
   double build_ms = 0;
   int grid = 0;
   unsigned long long* d_trace = nullptr;  // per-task (start, end, sm | cta << 32) when tracing
+  std::vector<int64_t> work_off, scratch_off, rhs_off;  // per instance (batched plans)
   void release() {
     cudaFree(d_tasks); cudaFree(d_succ); cudaFree(d_indeg); cudaFree(d_ready); cudaFree(d_counters);
     cudaFree(d_slots); cudaFree(d_state); cudaFree(d_work); cudaFree(d_scratch); cudaFree(d_rhs);
@@ -136,18 +140,43 @@ pp_status build_program(pp_hmatrix* h, int which, int nrhs, VmPlan& plan) {
   return PP_OK;
 }
 
-pp_status plan_to_device(pp_hmatrix* h, VmPlan& plan) {
-  pp_context* ctx = h->ctx;
+// Device copy of a program over one or more instances (a batch merges their programs):
+// one contiguous work / scratch / rhs buffer each, instance j at offsets *_off[j].
+pp_status plan_to_device_multi(pp_context* ctx, const std::vector<pp_hmatrix*>& insts, VmPlan& plan) {
   if (plan.on_device) return PP_OK;
   if (!has_device(ctx)) return fail(ctx, PP_CUDA_ERROR, "no CUDA device in this context");
-  if (!h->d_arena) return fail(ctx, PP_INVALID_ARG, "H-matrix not uploaded");
+  for (auto* h : insts)
+    if (!h->d_arena || !h->d_rand) return fail(ctx, PP_INVALID_ARG, "H-matrix not uploaded");
+  if ((int)insts.size() != plan.prog.n_instances) return fail(ctx, PP_INTERNAL, "instance count mismatch");
   auto t0 = std::chrono::steady_clock::now();
   const int n = plan.n_tasks;
   auto alloc = [&](void** p, size_t bytes) { return cudaMalloc(p, bytes ? bytes : 8); };
+  const int ni = (int)insts.size();
+  plan.work_off.assign(ni, 0);
+  plan.scratch_off.assign(ni, 0);
+  plan.rhs_off.assign(ni, 0);
+  plan.work_elems = plan.scratch_elems = plan.rhs_elems = 0;
+  for (int j = 0; j < ni; ++j) {
+    auto grow = [](int64_t& total, int64_t add) {
+      const int64_t at = (total + 31) & ~int64_t(31);
+      total = at + add;
+      return at;
+    };
+    plan.work_off[j] = grow(plan.work_elems, plan.prog.arena_elems[j * pp::PP_ARENAS + pp::AR_WORK]);
+    plan.scratch_off[j] = grow(plan.scratch_elems, plan.prog.arena_elems[j * pp::PP_ARENAS + pp::AR_SCRATCH]);
+    plan.rhs_off[j] = grow(plan.rhs_elems, plan.prog.arena_elems[j * pp::PP_ARENAS + pp::AR_RHS]);
+  }
   PP_CUDA(alloc((void**)&plan.d_work, sizeof(double) * plan.work_elems));
   PP_CUDA(alloc((void**)&plan.d_scratch, sizeof(double) * plan.scratch_elems));
   PP_CUDA(alloc((void**)&plan.d_rhs, sizeof(double) * plan.rhs_elems));
-  std::vector<double*> bases = {h->d_arena, plan.d_work, plan.d_scratch, plan.d_rhs, h->d_rand};
+  std::vector<double*> bases((size_t)ni * pp::PP_ARENAS);
+  for (int j = 0; j < ni; ++j) {
+    bases[j * pp::PP_ARENAS + pp::AR_MATRIX] = insts[j]->d_arena;
+    bases[j * pp::PP_ARENAS + pp::AR_WORK] = plan.d_work + plan.work_off[j];
+    bases[j * pp::PP_ARENAS + pp::AR_SCRATCH] = plan.d_scratch + plan.scratch_off[j];
+    bases[j * pp::PP_ARENAS + pp::AR_RHS] = plan.d_rhs + plan.rhs_off[j];
+    bases[j * pp::PP_ARENAS + pp::AR_RAND] = insts[j]->d_rand;
+  }
   std::vector<pp_task> tasks;
   std::vector<int32_t> succ, indeg, ready;
   plan.prog.encode(bases, tasks, succ, indeg, ready);
@@ -171,8 +200,9 @@ pp_status plan_to_device(pp_hmatrix* h, VmPlan& plan) {
   return PP_OK;
 }
 
-pp_status launch_plan(pp_hmatrix* h, VmPlan& plan, cudaStream_t s, int grid_cap) {
-  pp_context* ctx = h->ctx;
+pp_status plan_to_device(pp_hmatrix* h, VmPlan& plan) { return plan_to_device_multi(h->ctx, {h}, plan); }
+
+pp_status launch_plan(pp_context* ctx, VmPlan& plan, cudaStream_t s, int grid_cap) {
   if (plan.work_elems > 0) PP_CUDA(cudaMemsetAsync(plan.d_work, 0, sizeof(double) * plan.work_elems, s));
   pp_vm_launch L;
   L.tasks = plan.d_tasks;
@@ -188,7 +218,25 @@ pp_status launch_plan(pp_hmatrix* h, VmPlan& plan, cudaStream_t s, int grid_cap)
   L.grid = grid_cap > 0 ? std::min(plan.grid, grid_cap) : plan.grid;
   L.trace = plan.d_trace;
   PP_CUDA(pp_vm_run(L, s));
-  h->last = &plan;
+  return PP_OK;
+}
+
+pp_status launch_plan(pp_hmatrix* h, VmPlan& plan, cudaStream_t s, int grid_cap) {
+  pp_status st = launch_plan(h->ctx, plan, s, grid_cap);
+  if (st == PP_OK) h->last = &plan;
+  return st;
+}
+
+// status of a finished launch (after the stream was synchronized)
+pp_status plan_status(pp_context* ctx, VmPlan& plan) {
+  pp_vm_state s;
+  PP_CUDA(cudaMemcpy(&s, plan.d_state, sizeof(s), cudaMemcpyDeviceToHost));
+  if (s.error == PP_VM_TIMEOUT)
+    return fail(ctx, PP_TIMEOUT, "VM: ready-queue slot " + std::to_string(s.err_info) + " never filled");
+  if (s.error == PP_VM_BAD_TASK)
+    return fail(ctx, PP_INTERNAL, "VM: task " + std::to_string(s.err_info) + " has unsupported shape");
+  if (s.done != plan.n_tasks)
+    return fail(ctx, PP_INTERNAL, "VM: " + std::to_string(s.done) + " of " + std::to_string(plan.n_tasks) + " tasks ran");
   return PP_OK;
 }
 
@@ -429,15 +477,7 @@ pp_status pp_hmatrix_sync(pp_hmatrix* h, void* stream) {
   pp_context* ctx = h->ctx;
   PP_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
   if (!h->last) return PP_OK;
-  pp_vm_state s;
-  PP_CUDA(cudaMemcpy(&s, h->last->d_state, sizeof(s), cudaMemcpyDeviceToHost));
-  if (s.error == PP_VM_TIMEOUT)
-    return fail(ctx, PP_TIMEOUT, "VM: ready-queue slot " + std::to_string(s.err_info) + " never filled");
-  if (s.error == PP_VM_BAD_TASK)
-    return fail(ctx, PP_INTERNAL, "VM: task " + std::to_string(s.err_info) + " has unsupported shape");
-  if (s.done != h->last->n_tasks)
-    return fail(ctx, PP_INTERNAL, "VM: " + std::to_string(s.done) + " of " + std::to_string(h->last->n_tasks) + " tasks ran");
-  return PP_OK;
+  return plan_status(ctx, *h->last);
 }
 
 pp_status pp_hmatrix_program_info(pp_hmatrix* h, int which, int nrhs, pp_program_info* info) {
@@ -487,7 +527,15 @@ pp_status pp_kernel_residual_dev(pp_context* ctx, int kernel, double p0, double 
   if (!has_device(ctx)) return fail(ctx, PP_CUDA_ERROR, "no CUDA device in this context");
   if (!pts || !x || !b || !r || n <= 0 || nrhs <= 0 || nrhs > 16 || dim < 1 || dim > 3 || kernel < 0 || kernel > 3)
     return fail(ctx, PP_INVALID_ARG, "kernel residual: bad argument");
-  PP_CUDA(pp_kernel_residual(kernel, p0, 0.0, shift, pts, dim, n, x, b, r, nrhs, (cudaStream_t)stream));
+  const size_t need = pp_kernel_residual_part_elems(n, nrhs);
+  if (need > ctx->resid_elems) {  // grown before any stream capture by the first (eager) call
+    cudaFree(ctx->d_resid);
+    ctx->d_resid = nullptr;
+    ctx->resid_elems = 0;
+    PP_CUDA(cudaMalloc((void**)&ctx->d_resid, sizeof(double) * need));
+    ctx->resid_elems = need;
+  }
+  PP_CUDA(pp_kernel_residual(kernel, p0, 0.0, shift, pts, dim, n, x, b, r, nrhs, ctx->d_resid, (cudaStream_t)stream));
   return PP_OK;
 }
 
@@ -678,6 +726,154 @@ pp_status pp_refstream_encode(pp_hmatrix* h, int workers, int32_t* words, long l
   for (auto& s : streams) {
     std::memcpy(words + at, s.data(), sizeof(int32_t) * s.size());
     at += (long long)s.size();
+  }
+  return PP_OK;
+}
+
+}  // extern "C"
+
+// ----------------------------------------------------------------------------- batches
+struct pp_batch {
+  pp_context* ctx = nullptr;
+  std::vector<pp_hmatrix*> hs;
+  VmPlan factor;
+  std::map<int, std::unique_ptr<VmPlan>> solves;
+  VmPlan* last = nullptr;
+  ~pp_batch() {
+    factor.release();
+    for (auto& kv : solves) kv.second->release();
+  }
+};
+
+namespace {
+
+// merged program of all instances: instance j keeps arena ids j * PP_ARENAS + kind
+pp_status batch_program(pp_batch* b, int which, int nrhs, VmPlan& plan) {
+  if (plan.built) return PP_OK;
+  auto t0 = std::chrono::steady_clock::now();
+  for (auto* h : b->hs) {
+    VmPlan* src = which == 0 ? &h->factor : solve_plan(h, nrhs);
+    pp_status st = build_program(h, which, nrhs, *src);
+    if (st != PP_OK) return st;
+    plan.prog.merge(src->prog);
+  }
+  plan.n_tasks = (int)plan.prog.tasks.size();
+  plan.built = true;
+  plan.build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return PP_OK;
+}
+
+VmPlan* batch_solve_plan(pp_batch* b, int nrhs) {
+  auto it = b->solves.find(nrhs);
+  if (it != b->solves.end()) return it->second.get();
+  auto p = std::make_unique<VmPlan>();
+  VmPlan* raw = p.get();
+  b->solves.emplace(nrhs, std::move(p));
+  return raw;
+}
+
+}  // namespace
+
+extern "C" {
+
+pp_status pp_batch_create(pp_context* ctx, pp_hmatrix* const* hs, int n, pp_batch** out) {
+  if (!ctx || !hs || n <= 0 || !out) return fail(ctx, PP_INVALID_ARG, "pp_batch_create: bad argument");
+  *out = nullptr;
+  auto b = std::make_unique<pp_batch>();
+  b->ctx = ctx;
+  for (int i = 0; i < n; ++i) {
+    if (!hs[i] || hs[i]->ctx != ctx) return fail(ctx, PP_INVALID_ARG, "pp_batch_create: instance from another context");
+    if (!hs[i]->d_arena) return fail(ctx, PP_INVALID_ARG, "pp_batch_create: instance not uploaded");
+    b->hs.push_back(hs[i]);
+  }
+  pp_status st = batch_program(b.get(), 0, 0, b->factor);
+  if (st != PP_OK) return st;
+  *out = b.release();
+  return PP_OK;
+}
+
+void pp_batch_destroy(pp_batch* b) { delete b; }
+
+pp_status pp_batch_factor(pp_batch* b, void* stream) {
+  if (!b) return PP_INVALID_ARG;
+  pp_status st = plan_to_device_multi(b->ctx, b->hs, b->factor);
+  if (st != PP_OK) return st;
+  st = launch_plan(b->ctx, b->factor, (cudaStream_t)stream, 0);
+  if (st == PP_OK) b->last = &b->factor;
+  return st;
+}
+
+pp_status pp_batch_solve(pp_batch* b, const double* const* B, double* const* X, int nrhs, void* stream) {
+  if (!b || !B || !X || nrhs <= 0) return fail(b ? b->ctx : nullptr, PP_INVALID_ARG, "pp_batch_solve: bad argument");
+  pp_context* ctx = b->ctx;
+  VmPlan* plan = batch_solve_plan(b, nrhs);
+  pp_status st = batch_program(b, 1, nrhs, *plan);
+  if (st != PP_OK) return st;
+  st = plan_to_device_multi(ctx, b->hs, *plan);
+  if (st != PP_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  for (size_t j = 0; j < b->hs.size(); ++j) {
+    if (!B[j] || !X[j]) return fail(ctx, PP_INVALID_ARG, "pp_batch_solve: null right-hand side");
+    PP_CUDA(cudaMemcpyAsync(plan->d_rhs + plan->rhs_off[j], B[j], sizeof(double) * (size_t)b->hs[j]->H->n * nrhs,
+                            cudaMemcpyDeviceToDevice, s));
+  }
+  st = launch_plan(ctx, *plan, s, 0);
+  if (st != PP_OK) return st;
+  b->last = plan;
+  for (size_t j = 0; j < b->hs.size(); ++j)
+    PP_CUDA(cudaMemcpyAsync(X[j], plan->d_rhs + plan->rhs_off[j], sizeof(double) * (size_t)b->hs[j]->H->n * nrhs,
+                            cudaMemcpyDeviceToDevice, s));
+  return PP_OK;
+}
+
+pp_status pp_batch_restore(pp_batch* b, void* stream) {
+  if (!b) return PP_INVALID_ARG;
+  for (auto* h : b->hs) {
+    pp_status st = pp_hmatrix_restore(h, stream);
+    if (st != PP_OK) return st;
+  }
+  return PP_OK;
+}
+
+pp_status pp_batch_sync(pp_batch* b, void* stream) {
+  if (!b) return PP_INVALID_ARG;
+  pp_context* ctx = b->ctx;
+  PP_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+  if (!b->last) return PP_OK;
+  return plan_status(ctx, *b->last);
+}
+
+pp_status pp_batch_program_info(pp_batch* b, int which, int nrhs, pp_program_info* info) {
+  if (!b || !info || (which != 0 && which != 1) || (which == 1 && nrhs <= 0)) return PP_INVALID_ARG;
+  VmPlan* plan = which == 0 ? &b->factor : batch_solve_plan(b, nrhs);
+  pp_status st = batch_program(b, which, nrhs, *plan);
+  if (st != PP_OK) return st;
+  std::memset(info, 0, sizeof(*info));
+  info->n_tasks = plan->n_tasks;
+  info->n_edges = plan->prog.edges;
+  info->flops = plan->prog.total_flops();
+  for (int op = 0; op < PP_OP_COUNT; ++op) info->op_count[op] = plan->prog.count_op(op);
+  for (int a = 0; a < 5; ++a)
+    for (int j = 0; j < plan->prog.n_instances; ++j) info->arena_elems[a] += plan->prog.arena_elems[j * pp::PP_ARENAS + a];
+  info->host_build_ms = plan->build_ms;
+  return PP_OK;
+}
+
+pp_status pp_batch_trace(pp_batch* b, int which, int nrhs, int enable, uint64_t* out) {
+  if (!b || (which != 0 && which != 1)) return PP_INVALID_ARG;
+  pp_context* ctx = b->ctx;
+  VmPlan* plan = which == 0 ? &b->factor : batch_solve_plan(b, nrhs);
+  pp_status st = batch_program(b, which, nrhs, *plan);
+  if (st != PP_OK) return st;
+  const size_t bytes = sizeof(unsigned long long) * 3 * (size_t)std::max(plan->n_tasks, 1);
+  if (out) {
+    if (!plan->d_trace) return fail(ctx, PP_INVALID_ARG, "tracing was not enabled for this program");
+    PP_CUDA(cudaMemcpy(out, plan->d_trace, bytes, cudaMemcpyDeviceToHost));
+    return PP_OK;
+  }
+  if (enable && !plan->d_trace) {
+    PP_CUDA(cudaMalloc((void**)&plan->d_trace, bytes));
+    PP_CUDA(cudaMemset(plan->d_trace, 0, bytes));
   }
   return PP_OK;
 }

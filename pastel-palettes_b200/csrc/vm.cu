@@ -864,24 +864,30 @@ __device__ __forceinline__ double kernel_eval(int kind, double d, double p0, dou
 
 #define KR_ROWS 128
 #define KR_COLS 256
-// matrix-free r = b - A x, A_ij = K(|p_i - p_j|) (+ diag_shift on i == j); each CTA owns
-// KR_ROWS rows (a thread per row) and sweeps all columns in KR_COLS tiles through smem
-__global__ void kernel_residual_kernel(int kind, double p0, double p1, double shift, const double* __restrict__ pts,
-                                       int dim, int n, const double* __restrict__ x, const double* __restrict__ b,
-                                       double* __restrict__ r, int nrhs) {
+#define KR_SEG 512   /* columns per partial sum */
+// matrix-free partial products of r = b - A x, A_ij = K(|p_i - p_j|) (+ shift on i == j):
+// CTA (row block, column segment) sums its KR_SEG columns (staged through smem in KR_COLS
+// tiles, a thread per row) into part[seg][i]; residual_reduce adds the segments in order.
+template <int NR>
+__global__ void __launch_bounds__(KR_ROWS) kernel_residual_part(int kind, double p0, double p1, double shift,
+                                                                const double* __restrict__ pts, int dim, int n,
+                                                                const double* __restrict__ x, double* __restrict__ part,
+                                                                int nrhs) {
   __shared__ double sp[KR_COLS * 3];
-  __shared__ double sx[KR_COLS * 16];
+  __shared__ double sx[KR_COLS * NR];
   const int i = blockIdx.x * KR_ROWS + threadIdx.x;
+  const int seg = blockIdx.y, jb = seg * KR_SEG, je = min(n, jb + KR_SEG);
   double pi[3] = {0, 0, 0};
   if (i < n)
     for (int d = 0; d < dim; ++d) pi[d] = pts[(size_t)i * dim + d];
-  double acc[16];
-  for (int q = 0; q < 16; ++q) acc[q] = 0.0;
-  for (int j0 = 0; j0 < n; j0 += KR_COLS) {
-    const int nj = min(KR_COLS, n - j0);
+  double acc[NR];
+#pragma unroll
+  for (int q = 0; q < NR; ++q) acc[q] = 0.0;
+  for (int j0 = jb; j0 < je; j0 += KR_COLS) {
+    const int nj = min(KR_COLS, je - j0);
     __syncthreads();
     for (int e = threadIdx.x; e < nj * dim; e += blockDim.x) sp[e] = pts[(size_t)j0 * dim + e];
-    for (int e = threadIdx.x; e < nj * nrhs; e += blockDim.x) sx[e] = x[(size_t)j0 * nrhs + e];
+    for (int e = threadIdx.x; e < nj * nrhs; e += blockDim.x) sx[(e / nrhs) * NR + e % nrhs] = x[(size_t)j0 * nrhs + e];
     __syncthreads();
     if (i < n)
       for (int j = 0; j < nj; ++j) {
@@ -892,11 +898,22 @@ __global__ void kernel_residual_kernel(int kind, double p0, double p1, double sh
         }
         double a = kernel_eval(kind, sqrt(d2), p0, p1);
         if (j0 + j == i) a += shift;
-        for (int q = 0; q < nrhs; ++q) acc[q] = fma(a, sx[j * nrhs + q], acc[q]);
+#pragma unroll
+        for (int q = 0; q < NR; ++q)
+          if (q < nrhs) acc[q] = fma(a, sx[j * NR + q], acc[q]);
       }
   }
   if (i < n)
-    for (int q = 0; q < nrhs; ++q) r[(size_t)i * nrhs + q] = b[(size_t)i * nrhs + q] - acc[q];
+    for (int q = 0; q < nrhs; ++q) part[((size_t)seg * n + i) * nrhs + q] = acc[q];
+}
+
+__global__ void residual_reduce(const double* __restrict__ part, int segs, int n, int nrhs,
+                                const double* __restrict__ b, double* __restrict__ r) {
+  const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (size_t)n * nrhs) return;
+  double s = 0.0;
+  for (int g = 0; g < segs; ++g) s += part[(size_t)g * n * nrhs + e];
+  r[e] = b[e] - s;
 }
 
 // One ACCUM on caller buffers; its scratch (T.tmp) is the static array below.
@@ -967,9 +984,20 @@ cudaError_t pp_dense_residual(const double* A, int lda, int n, const double* x, 
 }
 
 cudaError_t pp_kernel_residual(int kernel, double p0, double p1, double diag_shift, const double* pts, int dim, int n,
-                               const double* x, const double* b, double* r, int nrhs, cudaStream_t s) {
-  if (dim < 1 || dim > 3 || nrhs < 1 || nrhs > 16) return cudaErrorInvalidValue;
-  kernel_residual_kernel<<<(n + KR_ROWS - 1) / KR_ROWS, KR_ROWS, 0, s>>>(kernel, p0, p1, diag_shift, pts, dim, n, x, b,
-                                                                        r, nrhs);
+                               const double* x, const double* b, double* r, int nrhs, double* part,
+                               cudaStream_t s) {
+  if (dim < 1 || dim > 3 || nrhs < 1 || nrhs > 16 || !part) return cudaErrorInvalidValue;
+  const int segs = (n + KR_SEG - 1) / KR_SEG;
+  const dim3 grid((n + KR_ROWS - 1) / KR_ROWS, segs);
+  if (nrhs <= 4)
+    kernel_residual_part<4><<<grid, KR_ROWS, 0, s>>>(kernel, p0, p1, diag_shift, pts, dim, n, x, part, nrhs);
+  else
+    kernel_residual_part<16><<<grid, KR_ROWS, 0, s>>>(kernel, p0, p1, diag_shift, pts, dim, n, x, part, nrhs);
+  const size_t total = (size_t)n * nrhs;
+  residual_reduce<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(part, segs, n, nrhs, b, r);
   return cudaGetLastError();
+}
+
+size_t pp_kernel_residual_part_elems(int n, int nrhs) {
+  return (size_t)((n + KR_SEG - 1) / KR_SEG) * n * nrhs;
 }

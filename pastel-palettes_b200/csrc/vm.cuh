@@ -47,6 +47,9 @@ cudaError_t pp_vm_run(const pp_vm_launch& L, cudaStream_t s);
 /* dense FP64 residual r = b - A x, A row-major n x n, x/b/r n x nrhs row-major */
 cudaError_t pp_dense_residual(const double* A, int lda, int n, const double* x, const double* b, double* r, int nrhs,
                               cudaStream_t s);
-/* matrix-free residual r = b - A x for kernel matrices on points (see kernels in vm.cu) */
+/* matrix-free residual r = b - A x for kernel matrices on points (see kernels in vm.cu);
+ * `part` is caller scratch of pp_kernel_residual_part_elems(n, nrhs) doubles */
 cudaError_t pp_kernel_residual(int kernel, double p0, double p1, double diag_shift, const double* pts, int dim, int n,
-                               const double* x, const double* b, double* r, int nrhs, cudaStream_t s);
+                               const double* x, const double* b, double* r, int nrhs, double* part,
+                               cudaStream_t s);
+size_t pp_kernel_residual_part_elems(int n, int nrhs);
