@@ -85,7 +85,7 @@ void o_trsmrt(double* B, const double* U, int nx_b, int ny_b, int ny_u, int ld_b
 
 // B[m x n] := U^-1 B, U upper m x m (solve; no reference counterpart): row i is scaled by
 // the reciprocal of u_ii, then eliminated from the rows above
-void o_trsmu(double* B, const double* U, int m, int n, int ld_b, int ld_u) {
+void o_trsmu64(double* B, const double* U, int m, int n, int ld_b, int ld_u) {
   for (int i = m - 1; i >= 0; --i) {
     const double rd = 1. / at(U, ld_u, i, i);
     for (int c = 0; c < n; ++c) at(B, ld_b, i, c) = at(B, ld_b, i, c) * rd;
@@ -120,6 +120,17 @@ void o_gemm(double alpha, double beta, double* M, const double* A, const double*
   if (alpha != 1.) {
     for (int r = 0; r < m; ++r)
       for (int c = 0; c < n; ++c) at(M, ld_m, r, c) *= alpha;
+  }
+}
+
+// TRSMU on up to 256 rows: 64-row blocks from the bottom, each solved as above, the rows
+// above a block updated by one ascending-k product per block (the engine's definition)
+void o_trsmu(double* B, const double* U, int m, int n, int ld_b, int ld_u) {
+  const int nb = (m + 63) / 64;
+  for (int bi = nb - 1; bi >= 0; --bi) {
+    const int d = bi * 64, md = std::min(64, m - d);
+    o_trsmu64(B + (int64_t)d * ld_b, U + (int64_t)d * ld_u + d, md, n, ld_b, ld_u);
+    if (d > 0) o_gemm(-1., 1., B, U + d, B + (int64_t)d * ld_b, d, n, md, ld_b, ld_u, ld_b, false, false);
   }
 }
 

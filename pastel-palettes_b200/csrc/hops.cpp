@@ -307,7 +307,7 @@ bool Program::encode_reference(int workers, std::vector<std::vector<int32_t>>& s
 
 // ----------------------------------------------------------------------------- generator
 Generator::Generator(Program& P, Hierarchical& H, int tile, int max_n_rand, bool split_k)
-    : P_(P), H_(H), T_(tile), max_n_rand_(max_n_rand), split_k_(split_k) {
+    : P_(P), H_(H), T_(tile), max_n_rand_(max_n_rand), split_k_(split_k), Ttri_(tile) {
   if (tile < 8) throw std::invalid_argument("tile must be >= 8");
   inst_ = P.add_instance();
   const int ar = P.arena_id(inst_, AR_MATRIX);
@@ -378,9 +378,11 @@ Mat Generator::child(const Mat& X, int i, int j) const {
 int Generator::hsplit_r(const Mat& X) const { return X.kind == Mat::H ? child(X, 0, 0).m : -1; }
 int Generator::hsplit_c(const Mat& X) const { return X.kind == Mat::H ? child(X, 0, 0).n : -1; }
 
-int Generator::tri_split(const Mat& X) const {
+// Split point of a diagonal block: H blocks by their children; dense blocks in halves while
+// larger than `limit` (T_ for GETRF; the triangular solves take blocks up to Ttri_ whole).
+int Generator::tri_split(const Mat& X, int limit) const {
   if (X.kind == Mat::H) return hsplit_r(X);
-  if (X.kind == Mat::D && X.m > T_) {
+  if (X.kind == Mat::D && X.m > limit) {
     int s = X.m / 2;
     if (X.m >= 32) s = (s + 7) & ~7;
     return s;
@@ -462,7 +464,7 @@ void Generator::solve_program(int nrhs) {
 
 void Generator::getrf(const Mat& A) {
   if (A.kind == Mat::LR) throw std::logic_error("getrf on a low-rank block");
-  const int s = tri_split(A);
+  const int s = tri_split(A, T_);
   if (s < 0) {
     HTask& t = emit(PP_OP_GETRF);
     bind(t, 0, A.d, true);
@@ -483,7 +485,7 @@ void Generator::getrf(const Mat& A) {
 
 void Generator::trsml(const Mat& L, const Mat& B) {
   if (B.kind == Mat::LR) { trsml(L, asD(B.u)); return; }
-  const int s = tri_split(L);
+  const int s = tri_split(L, Ttri_);
   if (s < 0) {
     if (B.kind != Mat::D || B.d.t) throw std::logic_error("trsml: target must be a dense untransposed block");
     for (int c = 0; c < B.n; c += T_) {
@@ -510,7 +512,7 @@ void Generator::trsml(const Mat& L, const Mat& B) {
 
 void Generator::trsmr(const Mat& U, const Mat& B) {
   if (B.kind == Mat::LR) { trsmrt(U, B.v); return; }
-  const int s = tri_split(U);
+  const int s = tri_split(U, Ttri_);
   if (s < 0) {
     if (B.kind != Mat::D || B.d.t) throw std::logic_error("trsmr: target must be a dense untransposed block");
     const int rows = std::max(T_, 4096 / std::max(1, B.n));
@@ -538,7 +540,7 @@ void Generator::trsmr(const Mat& U, const Mat& B) {
 
 void Generator::trsmrt(const Mat& U, const View& V) {
   if (V.t) throw std::logic_error("trsmrt: V must be untransposed");
-  const int s = tri_split(U);
+  const int s = tri_split(U, Ttri_);
   if (s < 0) {
     for (int c = 0; c < V.n; c += T_) {
       const int w = std::min(T_, V.n - c);
@@ -562,7 +564,7 @@ void Generator::trsmrt(const Mat& U, const View& V) {
 
 void Generator::trsmu(const Mat& U, const Mat& B) {
   if (B.kind == Mat::LR) { trsmu(U, asD(B.u)); return; }
-  const int s = tri_split(U);
+  const int s = tri_split(U, Ttri_);
   if (s < 0) {
     if (B.kind != Mat::D || B.d.t) throw std::logic_error("trsmu: target must be a dense untransposed block");
     for (int c = 0; c < B.n; c += T_) {

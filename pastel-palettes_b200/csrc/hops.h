@@ -148,7 +148,11 @@ class Generator {
   Mat child(const Mat& X, int i, int j) const;
   int hsplit_r(const Mat& X) const;
   int hsplit_c(const Mat& X) const;
-  int tri_split(const Mat& X) const;
+  int tri_split(const Mat& X, int limit) const;
+  // largest triangle of one TRSM* instruction the generator emits: T_ (measured: 256-row
+  // blocked solves lengthen the factor's critical path; the device accepts up to 256 rows,
+  // which reference-format streams need)
+  int Ttri_;
   void partition(const Mat& X, int rs, int cs, Mat out[2][2], int& nr, int& nc) const;
   int rand_obj(int k1);
 

@@ -546,6 +546,49 @@ __device__ __noinline__ void dev_trsmr(double* B, int ldb, const double* U, int 
   __syncthreads();
 }
 
+// Triangular solves on blocks up to 4 x TL rows, inside one CTA: diagonal TL-blocks by the
+// routines above, the coupling between blocks by ordered GEMMs.  Every element gets the same
+// update sequence as the tiled DAG would apply (i ascending), so results are identical.
+__device__ __noinline__ void dev_trsml_big(double* B, int ldb, const double* L, int ldl, int m, int n, double* smem) {
+  for (int d = 0; d < m; d += TL) {
+    const int md = min(TL, m - d);
+    dev_trsml(B + (size_t)d * ldb, ldb, L + (size_t)d * ldl + d, ldl, md, n, smem);
+    if (d + md < m)  // B_below -= L(below, d) B_d
+      dev_gemm(B + (size_t)(d + md) * ldb, ldb, L + (size_t)(d + md) * ldl + d, ldl, false, B + (size_t)d * ldb, ldb,
+               false, m - d - md, n, md, -1.0, 1.0, smem);
+  }
+}
+
+__device__ __noinline__ void dev_trsmu_big(double* B, int ldb, const double* U, int ldu, int m, int n, double* smem) {
+  const int nb = (m + TL - 1) / TL;
+  for (int bi = nb - 1; bi >= 0; --bi) {
+    const int d = bi * TL, md = min(TL, m - d);
+    dev_trsmu(B + (size_t)d * ldb, ldb, U + (size_t)d * ldu + d, ldu, md, n, smem);
+    if (d > 0)  // B_above -= U(above, d) B_d
+      dev_gemm(B, ldb, U + d, ldu, false, B + (size_t)d * ldb, ldb, false, d, n, md, -1.0, 1.0, smem);
+  }
+}
+
+__device__ __noinline__ void dev_trsmr_big(double* B, int ldb, const double* U, int ldu, int m, int n, double* smem) {
+  for (int d = 0; d < n; d += TL) {
+    const int nd = min(TL, n - d);
+    dev_trsmr(B + d, ldb, U + (size_t)d * ldu + d, ldu, m, nd, smem);
+    if (d + nd < n)  // B(:, right) -= B_d U(d, right)
+      dev_gemm(B + d + nd, ldb, B + d, ldb, false, U + (size_t)d * ldu + d + nd, ldu, false, m, n - d - nd, nd, -1.0,
+               1.0, smem);
+  }
+}
+
+__device__ __noinline__ void dev_trsmrt_big(double* V, int ldv, const double* U, int ldu, int m, int n, double* smem) {
+  for (int d = 0; d < m; d += TL) {
+    const int md = min(TL, m - d);
+    dev_trsmrt(V + (size_t)d * ldv, ldv, U + (size_t)d * ldu + d, ldu, md, n, smem);
+    if (d + md < m)  // V_below -= U(d, below)^T V_d
+      dev_gemm(V + (size_t)(d + md) * ldv, ldv, U + (size_t)d * ldu + d + md, ldu, true, V + (size_t)d * ldv, ldv,
+               false, m - d - md, n, md, -1.0, 1.0, smem);
+  }
+}
+
 // ------------------------------------------------------------------------- GEMM3 / GEMM4
 // Reference association orders (kernel.cu:886-955), intermediates in task scratch.
 __device__ __noinline__ void dev_gemm3(const pp_task& T, double* smem) {
@@ -715,20 +758,24 @@ __device__ bool run_task(const pp_task& T, double* smem) {
       dev_getrf(T.p[0], T.ld[0], T.m, T.n, smem);
       return true;
     case PP_OP_TRSML:
-      if (T.m > TL) return false;
-      dev_trsml(T.p[0], T.ld[0], T.p[1], T.ld[1], T.m, T.n, smem);
+      if (T.m > PP_VM_TRI) return false;
+      if (T.m > TL) dev_trsml_big(T.p[0], T.ld[0], T.p[1], T.ld[1], T.m, T.n, smem);
+      else dev_trsml(T.p[0], T.ld[0], T.p[1], T.ld[1], T.m, T.n, smem);
       return true;
     case PP_OP_TRSMR:
-      if (T.n > TL) return false;
-      dev_trsmr(T.p[0], T.ld[0], T.p[1], T.ld[1], T.m, T.n, smem);
+      if (T.n > PP_VM_TRI) return false;
+      if (T.n > TL) dev_trsmr_big(T.p[0], T.ld[0], T.p[1], T.ld[1], T.m, T.n, smem);
+      else dev_trsmr(T.p[0], T.ld[0], T.p[1], T.ld[1], T.m, T.n, smem);
       return true;
     case PP_OP_TRSMRT:
-      if (T.m > TL) return false;
-      dev_trsmrt(T.p[0], T.ld[0], T.p[1], T.ld[1], T.m, T.n, smem);
+      if (T.m > PP_VM_TRI) return false;
+      if (T.m > TL) dev_trsmrt_big(T.p[0], T.ld[0], T.p[1], T.ld[1], T.m, T.n, smem);
+      else dev_trsmrt(T.p[0], T.ld[0], T.p[1], T.ld[1], T.m, T.n, smem);
       return true;
     case PP_OP_TRSMU:
-      if (T.m > TL) return false;
-      dev_trsmu(T.p[0], T.ld[0], T.p[1], T.ld[1], T.m, T.n, smem);
+      if (T.m > PP_VM_TRI) return false;
+      if (T.m > TL) dev_trsmu_big(T.p[0], T.ld[0], T.p[1], T.ld[1], T.m, T.n, smem);
+      else dev_trsmu(T.p[0], T.ld[0], T.p[1], T.ld[1], T.m, T.n, smem);
       return true;
     case PP_OP_GEMM:
       dev_gemm(T.p[0], T.ld[0], T.p[1], T.ld[1], T.flags & PP_T(1), T.p[2], T.ld[2], T.flags & PP_T(2), T.m, T.n,
@@ -850,13 +897,33 @@ __global__ void dense_residual_kernel(const double* __restrict__ A, int lda, int
   }
 }
 
-__device__ __forceinline__ double kernel_eval(int kind, double d, double p0, double p1) {
+// Reciprocal and reciprocal square root by two Newton-Raphson steps from the single-precision
+// estimate (quadratic convergence: 24 -> 48 -> ~96 bits, i.e. a few ulps of double): the
+// residual needs entries accurate to ~1e-15, not correctly rounded ones.
+__device__ __forceinline__ double rcp_nr(double x) {
+  double y = (double)__frcp_rn((float)x);
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  return fma(y, e, y);
+}
+__device__ __forceinline__ double sqrt_nr(double d2) {
+  if (!(d2 > 1e-30)) return sqrt(d2);  // outside the float range of the estimate
+  double y = (double)rsqrtf((float)d2);
+  double e = fma(-d2 * y, y, 1.0);
+  y = fma(0.5 * y, e, y);
+  e = fma(-d2 * y, y, 1.0);
+  y = fma(0.5 * y, e, y);
+  return d2 * y;
+}
+__device__ __forceinline__ double kernel_eval_nr(int kind, double d2, double p0, double inv_p0) {
+  const double d = sqrt_nr(d2);
   switch (kind) {
-    case 0: return 1.0 / (d + p0);                                  // 1 / (r + eps)
-    case 1: return 1.0 / (4.0 * 3.14159265358979323846 * (d + p0)); // Laplace 3-D
-    case 2: return exp(-d / p0);                                     // exponential
-    default: {                                                      // Matern 3/2
-      const double s = 1.7320508075688772 * d / p0;
+    case 0: return rcp_nr(d + p0);
+    case 1: return rcp_nr(4.0 * 3.14159265358979323846 * (d + p0));
+    case 2: return exp(-d * inv_p0);
+    default: {
+      const double s = 1.7320508075688772 * d * inv_p0;
       return (1.0 + s) * exp(-s);
     }
   }
@@ -877,6 +944,7 @@ __global__ void __launch_bounds__(KR_ROWS) kernel_residual_part(int kind, double
   __shared__ double sx[KR_COLS * NR];
   const int i = blockIdx.x * KR_ROWS + threadIdx.x;
   const int seg = blockIdx.y, jb = seg * KR_SEG, je = min(n, jb + KR_SEG);
+  const double inv_p0 = 1.0 / p0;
   double pi[3] = {0, 0, 0};
   if (i < n)
     for (int d = 0; d < dim; ++d) pi[d] = pts[(size_t)i * dim + d];
@@ -896,7 +964,7 @@ __global__ void __launch_bounds__(KR_ROWS) kernel_residual_part(int kind, double
           const double t = pi[d] - sp[j * dim + d];
           d2 = fma(t, t, d2);
         }
-        double a = kernel_eval(kind, sqrt(d2), p0, p1);
+        double a = kernel_eval_nr(kind, d2, p0, inv_p0);
         if (j0 + j == i) a += shift;
 #pragma unroll
         for (int q = 0; q < NR; ++q)

@@ -283,6 +283,25 @@ def test_dense_refinement(pp, gctx):
     assert hist[-1] <= 1e-12
 
 
+@pytest.mark.parametrize("kernel,p0,dim", [("inv", 1e-3, 2), ("laplace", 1e-3, 3), ("exp", 0.1, 2),
+                                           ("matern32", 0.2, 3)])
+@pytest.mark.parametrize("nrhs", [1, 3, 8])
+def test_kernel_residual_matches_dense_fp64(pp, gctx, kernel, p0, dim, nrhs):
+    n = 1500
+    rng = np.random.default_rng(5)
+    pts = rng.uniform(0, 1, (n, dim))
+    kid = pp.KERNELS[kernel]
+    prob = pp.KernelProblem(n, dim, kid, p0, 3.0, pts)
+    A = prob.dense()
+    x = rng.standard_normal((n, nrhs))
+    b = rng.standard_normal((n, nrhs))
+    r = torch.empty((n, nrhs), dtype=torch.float64, device="cuda")
+    gctx.kernel_residual(kid, p0, 3.0, dev(pts), dev(x), dev(b), r)
+    want = b - A @ x
+    scale = np.abs(A).sum(1).max() * np.abs(x).max()
+    assert np.abs(r.cpu().numpy() - want).max() <= 1e-14 * scale
+
+
 def test_dense_residual_kernel(pp, gctx):
     rng = np.random.default_rng(0)
     n = 300
