@@ -223,6 +223,9 @@ def main():
     ap.add_argument("--batch", type=int, default=16, help="jobs per merged launch")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "tf32"],
+                    help="factor GEMM precision of the headline form (tf32: tensor cores + FP64 refinement)")
+    ap.add_argument("--compare", type=int, default=1, help="also time the other precision form")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -249,40 +252,40 @@ def main():
             h.upload(s)
             h.keep_original(s)
     s.synchronize()
-    batch = pp.Batch(ctx, hs)
     n = probs[0].n
     b_host = [torch.from_numpy(pp.rhs(n, 1, seed=7 + i)).pin_memory() for i in range(B)]
     bs = [x.cuda() for x in b_host]
-    ref = pp.BatchRefiner(batch, probs, stream=s)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
-
-    # --- warm-up (eager): allocates every plan, fixes the number of refinement solves
-    with torch.cuda.stream(s):
-        for _ in range(args.warmup):
-            batch.restore(s)
-            batch.factor(s)
-            xs, hist = ref.solve(bs, tol=tol)
-    batch.sync(s)
-    if hist[-1] > tol:
-        raise SystemExit(f"refinement did not reach {tol}: {hist}")
-    iters = len(hist)
-
-    # --- steady state captured once: restore, batched factor, `iters` batched solves
-    g = torch.cuda.CUDAGraph()
-    with torch.cuda.stream(s):
-        with torch.cuda.graph(g, stream=s):
-            batch.restore(s)
-            batch.factor(s)
-            out = ref.run(bs, iters)
-    launches_per_step = 2 + iters * (2 + B)
 
     def barrier():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
 
-    total, worst = 0.0, 0.0
-    with Clocks(local) as clk:
+    def run_form(prec, clk=None):
+        """Device-timed steps of one precision form: batched restore + factor + refinement
+        solves captured as one CUDA graph.  Returns (batch, refiner, graph, outputs, stats)."""
+        for h in hs:
+            h.set_precision(prec)
+        batch = pp.Batch(ctx, hs)
+        ref = pp.BatchRefiner(batch, probs, stream=s)
+        # warm-up (eager): allocates every plan, fixes the number of refinement solves
+        with torch.cuda.stream(s):
+            for _ in range(args.warmup):
+                batch.restore(s)
+                batch.factor(s)
+                xs, hist = ref.solve(bs, tol=tol)
+        batch.sync(s)
+        if hist[-1] > tol:
+            raise SystemExit(f"refinement did not reach {tol}: {hist}")
+        iters = len(hist)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(s):
+            with torch.cuda.graph(g, stream=s):
+                batch.restore(s)
+                batch.factor(s)
+                out = ref.run(bs, iters)
+        total, worst = 0.0, 0.0
         barrier()
         for _ in range(args.steps):
             flush.zero_()
@@ -296,14 +299,30 @@ def main():
             total += e0.elapsed_time(e1) / 1e3
             worst = max(worst, max(ref.errors(bs, *out)))
         barrier()
-    batch.sync(s)
-    if worst > tol:
-        raise SystemExit(f"a timed step ended above {tol}: {worst}")
-    t = torch.tensor([total], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_max = t.item()
-    value = world * B * args.steps / total_max
+        batch.sync(s)
+        if worst > tol:
+            raise SystemExit(f"a timed step ended above {tol}: {worst}")
+        t = torch.tensor([total], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_max = t.item()
+        stats = {"value": world * B * args.steps / total_max, "ms_per_step": 1e3 * total_max / args.steps,
+                 "refinement_solves": iters, "worst_backward_error": worst, "total_s": total_max}
+        return batch, ref, g, out, stats
+
+    forms = {"fp64": pp.FP64, "tf32": pp.TF32}
+    other = "fp64" if args.precision == "tf32" else "tf32"
+    # the comparison form first, then the headline form (whose plans the rest reuses)
+    cmp_stats = None
+    if args.compare:
+        bt, _, gc, _, cmp_stats = run_form(forms[other])
+        del gc, bt
+    with Clocks(local) as clk:
+        batch, ref, g, out, main_stats = run_form(forms[args.precision])
+    iters = main_stats["refinement_solves"]
+    total_max = main_stats["total_s"]
+    value = main_stats["value"]
+    launches_per_step = 2 + iters * (2 + B)
 
     # --- end to end through the C ABI: matrices and right-hand sides up from pinned host
     #     memory, batched factor + refinement, solutions down
@@ -392,8 +411,11 @@ def main():
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "factor+solve/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1e3 * total_max / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": WORKLOAD_NAME, **WORKLOAD, "batch": B,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64" if args.precision == "fp64" else "tf32 gemm + f64", "data": "synthetic",
+                "forms": {args.precision: {k: v for k, v in main_stats.items() if k != "total_s"},
+                          **({other: {k: v for k, v in cmp_stats.items() if k != "total_s"}} if cmp_stats else {})},
+                "config": {"workload": WORKLOAD_NAME, **WORKLOAD, "batch": B, "precision": args.precision,
                            "batch_note": "copies of one seeded matrix, distinct right-hand sides, one merged launch",
                            "l2": "flushed between steps (256 MiB write)", "graph": "restore+factor+solves captured",
                            "parallelism": f"replicas{world}", "factor_tasks_per_job": finfo["n_tasks"],

@@ -102,6 +102,17 @@ double* pp_hmatrix_host_arena(pp_hmatrix* h, long long* elems);
 /* device base of the matrix arena (read-only view for residual / export helpers) */
 const double* pp_hmatrix_device_arena(const pp_hmatrix* h);
 
+/* contraction precision of the factor's GEMM (Schur-complement and low-rank product)
+ * instructions: PP_PRECISION_FP64 (default; matches the reference's FP64 factorization) or
+ * PP_PRECISION_TF32 (5th-generation tensor cores, TF32 operands, FP32 accumulation, FP64
+ * result; GETRF / TRSM / accumulation stay FP64 — pair it with iterative refinement).
+ * Rebuilds the factor program on the next factorization; set it before pp_batch_create.
+ * no reference counterpart (the reference is FP64 only) */
+#define PP_PRECISION_FP64 0
+#define PP_PRECISION_TF32 1
+pp_status pp_hmatrix_set_precision(pp_hmatrix* h, int precision);
+int pp_hmatrix_get_precision(const pp_hmatrix* h);
+
 /* --- factor / solve (launcher.cuh) --------------------------------------- */
 /* H-LU factorization in place on the device, stream ordered.
  * replaces dev_hierarchical_GETRF (include/launcher.cuh:18, src/launcher.cu:117-217) */

@@ -30,6 +30,7 @@ PP_OK, PP_INVALID_ARG, PP_OOM, PP_TIMEOUT, PP_NUMERICAL, PP_CUDA_ERROR, PP_UNSUP
 STATUS_NAMES = ["OK", "INVALID_ARG", "OOM", "TIMEOUT", "NUMERICAL", "CUDA_ERROR", "UNSUPPORTED", "INTERNAL"]
 OP_NAMES = ["nop", "getrf", "trsml", "trsmr", "trsmrt", "trsmu", "gemm", "gemm3", "gemm4", "accum", "sum"]
 DENSE, LOWRANK, HIER = 0, 1, 2
+FP64, TF32 = 0, 1  # contraction precision of the factor's GEMM instructions
 ARENAS = ["matrix", "work", "scratch", "rhs", "rand"]
 
 # pp_task (pastel-palettes_b200/csrc/pp_task.h), 160 bytes
@@ -120,6 +121,8 @@ def lib():
             "pp_batch_program_info": (i, [vp, i, i, C.POINTER(_ProgramInfo)]),
             "pp_batch_trace": (i, [vp, i, i, i, vp]),
             "pp_refstream_encode": (i, [vp, i, vp, ll, vp, C.POINTER(ll)]),
+            "pp_hmatrix_set_precision": (i, [vp, i]),
+            "pp_hmatrix_get_precision": (i, [vp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -312,6 +315,15 @@ class Hierarchical:
         return 8 * self.host_arena().size
 
     # --- factor / solve
+    @property
+    def precision(self):
+        return lib().pp_hmatrix_get_precision(self._h)
+
+    def set_precision(self, precision):
+        """FP64 (default) or TF32: the factor's GEMM instructions on the tensor cores with
+        FP32 accumulation; GETRF / TRSM / accumulation stay FP64."""
+        self.ctx.check(lib().pp_hmatrix_set_precision(self._h, precision), "set_precision")
+
     def factor(self, stream=None):
         self.ctx.check(lib().pp_hlu_factor(self._h, _stream_handle(stream)), "hlu_factor")
 

@@ -41,6 +41,7 @@ struct VmPlan {
   int64_t work_elems = 0, scratch_elems = 0, rhs_elems = 0;
   double build_ms = 0;
   int grid = 0;
+  int use_tc = 0;  // holds TF32 contractions (tensor memory per CTA)
   unsigned long long* d_trace = nullptr;  // per-task (start, end, sm | cta << 32) when tracing
   std::vector<int64_t> work_off, scratch_off, rhs_off;  // per instance (batched plans)
   void release() {
@@ -70,6 +71,7 @@ struct pp_hmatrix {
   double* d_orig = nullptr;
   double* d_rand = nullptr;
   bool pinned = false;
+  int precision = PP_PREC_FP64;  // contraction precision of the factor's GEMM instructions
   std::vector<double> rand_host;
   VmPlan factor;
   std::map<int, std::unique_ptr<VmPlan>> solves;
@@ -124,8 +126,12 @@ pp_status build_program(pp_hmatrix* h, int which, int nrhs, VmPlan& plan) {
   auto t0 = std::chrono::steady_clock::now();
   try {
     pp::Generator g(plan.prog, *h->H, ctx->cfg.tile, h->H->n, ctx->cfg.reference_isa == 0);
-    if (which == 0) g.getrf_program();
-    else g.solve_program(nrhs);
+    if (which == 0) {
+      g.getrf_program();
+      if (h->precision != PP_PREC_FP64) plan.prog.set_gemm_precision(h->precision);
+    } else {
+      g.solve_program(nrhs);
+    }
     plan.prog.build_dag();
   } catch (const std::exception& e) {
     plan.prog = pp::Program();
@@ -181,6 +187,9 @@ pp_status plan_to_device_multi(pp_context* ctx, const std::vector<pp_hmatrix*>& 
   std::vector<int32_t> succ, indeg, ready;
   plan.prog.encode(bases, tasks, succ, indeg, ready);
   plan.n_ready = (int)ready.size();
+  plan.use_tc = 0;
+  for (const auto& t : tasks)
+    if (t.prec == PP_PREC_TF32) plan.use_tc = 1;
   PP_CUDA(alloc((void**)&plan.d_tasks, sizeof(pp_task) * n));
   PP_CUDA(alloc((void**)&plan.d_succ, sizeof(int32_t) * succ.size()));
   PP_CUDA(alloc((void**)&plan.d_indeg, sizeof(int32_t) * n));
@@ -217,6 +226,7 @@ pp_status launch_plan(pp_context* ctx, VmPlan& plan, cudaStream_t s, int grid_ca
   L.spin_limit = ctx->cfg.spin_limit;
   L.grid = grid_cap > 0 ? std::min(plan.grid, grid_cap) : plan.grid;
   L.trace = plan.d_trace;
+  L.use_tc = plan.use_tc;
   PP_CUDA(pp_vm_run(L, s));
   return PP_OK;
 }
@@ -227,17 +237,24 @@ pp_status launch_plan(pp_hmatrix* h, VmPlan& plan, cudaStream_t s, int grid_cap)
   return st;
 }
 
+// error record of a finished VM launch -> status and message
+pp_status vm_state_status(pp_context* ctx, const pp_vm_state& s, int n_tasks) {
+  if (s.error == PP_VM_TIMEOUT)
+    return fail(ctx, PP_TIMEOUT, "VM: ready-queue slot " + std::to_string(s.err_info) + " never filled");
+  if (s.error == PP_VM_MMA_TIMEOUT)
+    return fail(ctx, PP_TIMEOUT, "VM: tensor-core completion of task " + std::to_string(s.err_info) + " not observed");
+  if (s.error == PP_VM_BAD_TASK)
+    return fail(ctx, PP_INTERNAL, "VM: task " + std::to_string(s.err_info) + " has unsupported shape");
+  if (s.done != n_tasks)
+    return fail(ctx, PP_INTERNAL, "VM: " + std::to_string(s.done) + " of " + std::to_string(n_tasks) + " tasks ran");
+  return PP_OK;
+}
+
 // status of a finished launch (after the stream was synchronized)
 pp_status plan_status(pp_context* ctx, VmPlan& plan) {
   pp_vm_state s;
   PP_CUDA(cudaMemcpy(&s, plan.d_state, sizeof(s), cudaMemcpyDeviceToHost));
-  if (s.error == PP_VM_TIMEOUT)
-    return fail(ctx, PP_TIMEOUT, "VM: ready-queue slot " + std::to_string(s.err_info) + " never filled");
-  if (s.error == PP_VM_BAD_TASK)
-    return fail(ctx, PP_INTERNAL, "VM: task " + std::to_string(s.err_info) + " has unsupported shape");
-  if (s.done != plan.n_tasks)
-    return fail(ctx, PP_INTERNAL, "VM: " + std::to_string(s.done) + " of " + std::to_string(plan.n_tasks) + " tasks ran");
-  return PP_OK;
+  return vm_state_status(ctx, s, plan.n_tasks);
 }
 
 }  // namespace
@@ -421,6 +438,21 @@ pp_status pp_hmatrix_restore(pp_hmatrix* h, void* stream) {
                           cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
   return PP_OK;
 }
+
+pp_status pp_hmatrix_set_precision(pp_hmatrix* h, int precision) {
+  if (!h) return PP_INVALID_ARG;
+  if (precision != PP_PREC_FP64 && precision != PP_PREC_TF32)
+    return fail(h->ctx, PP_INVALID_ARG, "pp_hmatrix_set_precision: unknown precision");
+  if (precision == h->precision) return PP_OK;
+  h->precision = precision;
+  if (h->last == &h->factor) h->last = nullptr;
+  h->factor.release();
+  h->factor.prog = pp::Program();
+  h->factor.built = false;
+  return PP_OK;
+}
+
+int pp_hmatrix_get_precision(const pp_hmatrix* h) { return h ? h->precision : -1; }
 
 pp_status pp_hmatrix_to_dense(const pp_hmatrix* h, double* out) {
   if (!h || !out) return PP_INVALID_ARG;
@@ -649,16 +681,15 @@ pp_status pp_vm_execute(pp_context* ctx, const void* tasks, int n, const int32_t
   L.n_ready = p.n_ready; L.counters = p.d_counters; L.slots = p.d_slots; L.state = p.d_state;
   L.spin_limit = spin_limit > 0 ? spin_limit : ctx->cfg.spin_limit;
   L.grid = grid > 0 ? grid : std::max(1, std::min(n, ctx->sm_count * ctx->blocks_per_sm));
+  for (int i = 0; i < n; ++i)
+    if (T[i].prec == PP_PREC_TF32) L.use_tc = 1;
   cudaStream_t s = (cudaStream_t)stream;
   PP_CUDA(pp_vm_run(L, s));
   PP_CUDA(cudaStreamSynchronize(s));
   pp_vm_state st;
   PP_CUDA(cudaMemcpy(&st, p.d_state, sizeof(st), cudaMemcpyDeviceToHost));
   p.release();
-  if (st.error == PP_VM_TIMEOUT) return fail(ctx, PP_TIMEOUT, "VM: ready-queue slot " + std::to_string(st.err_info) + " never filled");
-  if (st.error == PP_VM_BAD_TASK) return fail(ctx, PP_INTERNAL, "VM: task " + std::to_string(st.err_info) + " has unsupported shape");
-  if (st.done != n) return fail(ctx, PP_INTERNAL, "VM: " + std::to_string(st.done) + " of " + std::to_string(n) + " tasks ran");
-  return PP_OK;
+  return vm_state_status(ctx, st, n);
 }
 
 pp_status pp_lowrank_accum_noalloc(pp_context* ctx, double* U1, int ld_u1, double* V1, int ld_v1, const double* U2,

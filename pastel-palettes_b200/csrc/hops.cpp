@@ -70,6 +70,16 @@ int64_t Program::count_op(int op) const {
   return c;
 }
 
+int64_t Program::set_gemm_precision(int prec) {
+  int64_t c = 0;
+  for (auto& t : tasks)
+    if (t.t.op == PP_OP_GEMM && t.t.prec != prec) {
+      t.t.prec = prec;
+      ++c;
+    }
+  return c;
+}
+
 static inline bool rect_overlap(const Region& a, const Region& b) {
   return a.r0 < b.r0 + b.nr && b.r0 < a.r0 + a.nr && a.c0 < b.c0 + b.nc && b.c0 < a.c0 + a.nc;
 }

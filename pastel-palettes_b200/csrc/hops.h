@@ -91,6 +91,9 @@ class Program {
   int arena_id(int inst, int kind) const { return inst * PP_ARENAS + kind; }
   int64_t total_flops() const;
   int64_t count_op(int op) const;
+  // Contraction precision of every GEMM instruction (PP_PREC_TF32: tensor cores with FP32
+  // accumulation; GETRF, TRSM*, ACCUM and SUM stay FP64).  Returns the tasks changed.
+  int64_t set_gemm_precision(int prec);
 
   void build_dag();
   h_ops_dag to_dag() const;

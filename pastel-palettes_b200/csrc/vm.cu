@@ -241,6 +241,174 @@ __device__ __forceinline__ void dev_gemm(double* __restrict__ C, int ldc, const 
   else gemm_cfg<64, 64, 4, 4, 32>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
 }
 
+// ------------------------------------------------------------------------- tensor-core GEMM
+// Mixed-precision contraction on the 5th-generation tensor cores:
+//   C[m x n] (FP64) = beta C + alpha op(A) op(B),  op(A), op(B) rounded to TF32,
+//   products summed in FP32 in tensor memory (TMEM), the sum added to C in FP64.
+// Tile 128 x 64 (tcgen05.mma.cta_group::1.kind::tf32, M = 128, N = 64, K = 8 per
+// instruction), k in chunks of 32.  Operands are staged in shared memory in the canonical
+// K-major layout without swizzle: 8-row x 16-byte core matrices, core matrices 128 B apart
+// along M/N (SBO) and one k16-column of core matrices apart along K (LBO).  One thread
+// issues the MMAs and commits them to an mbarrier; the CTA waits on it (bounded) before
+// reusing the staging buffers or reading the accumulators with tcgen05.ld.
+#define TC_M 128
+#define TC_N 64
+#define TC_K 32
+#define TC_A_BYTES (TC_M * TC_K * 4)
+#define TC_B_BYTES (TC_N * TC_K * 4)
+#define TC_LBO_A (TC_M / 8 * 128)  /* bytes between k16 columns of A's core matrices */
+#define TC_LBO_B (TC_N / 8 * 128)
+#define TC_TMEM_COLS 64
+
+struct TcCtx {
+  uint32_t tmem;      // accumulator base address in tensor memory
+  uint32_t mbar;      // shared address of the MMA-completion mbarrier
+  uint32_t phase;     // parity of the next completion
+  long long limit;    // nanoseconds before a wait for the tensor core gives up
+  int pending;        // a commit whose completion was not observed (after a timeout)
+  int active;         // tensor memory and the mbarrier were set up for this CTA
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version of sm_100; layout type 0 = no swizzle
+  return d;
+}
+
+// instruction descriptor: D F32 (bits 4-5 = 1), A and B TF32 (bits 7-9, 10-12 = 2), both
+// K-major, N >> 3 at bits 17-22, M >> 4 at bits 24-28
+constexpr uint32_t kIdescTf32 = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_N >> 3) << 17) |
+                                ((uint32_t)(TC_M >> 4) << 24);
+
+__device__ __forceinline__ uint32_t to_tf32(double v) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(__double2float_rn(v)));
+  return r;
+}
+
+__device__ __forceinline__ unsigned long long gtimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// bounded wait for the completion of phase `phase` of an mbarrier: false after `limit_ns`
+__device__ __forceinline__ bool mbar_wait(uint32_t addr, uint32_t phase, long long limit_ns) {
+  const unsigned long long t0 = gtimer_ns();
+  for (;;) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(addr), "r"(phase)
+        : "memory");
+    if (done) return true;
+    if ((long long)(gtimer_ns() - t0) > limit_ns) return false;
+  }
+}
+
+__device__ __noinline__ bool dev_gemm_tc(double* __restrict__ C, int ldc, const double* __restrict__ A, int lda,
+                                         bool tA, const double* __restrict__ B, int ldb, bool tB, int m, int n, int k,
+                                         double alpha, double beta, double* smem, TcCtx& tc) {
+  uint8_t* sbase = reinterpret_cast<uint8_t*>(smem);
+  const uint32_t s0 = smem_u32(sbase);
+  const uint32_t pad = ((s0 + 1023u) & ~1023u) - s0;  // core matrices from a 1 KB boundary
+  uint32_t* As = reinterpret_cast<uint32_t*>(sbase + pad);
+  uint32_t* Bs = reinterpret_cast<uint32_t*>(sbase + pad + TC_A_BYTES);
+  const uint32_t a_addr = s0 + pad, b_addr = s0 + pad + TC_A_BYTES;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nch = (k + TC_K - 1) / TC_K;
+  bool ok = true;
+  for (int i0 = 0; i0 < m; i0 += TC_M)
+    for (int j0 = 0; j0 < n; j0 += TC_N) {
+      for (int ch = 0; ch < nch && ok; ++ch) {
+        const int k0 = ch * TC_K;
+        for (int e = tid; e < TC_M * TC_K; e += NT) {
+          int r, kk;
+          if (!tA) { r = e / TC_K; kk = e % TC_K; }
+          else { kk = e / TC_M; r = e % TC_M; }
+          double v = 0.0;
+          if (i0 + r < m && k0 + kk < k)
+            v = tA ? ldcg(&A[(size_t)(k0 + kk) * lda + i0 + r]) : ldcg(&A[(size_t)(i0 + r) * lda + k0 + kk]);
+          As[((kk >> 2) * TC_LBO_A + (r >> 3) * 128 + (r & 7) * 16 + (kk & 3) * 4) >> 2] = to_tf32(v);
+        }
+        for (int e = tid; e < TC_N * TC_K; e += NT) {
+          int c, kk;
+          if (!tB) { kk = e / TC_N; c = e % TC_N; }
+          else { c = e / TC_K; kk = e % TC_K; }
+          double v = 0.0;
+          if (j0 + c < n && k0 + kk < k)
+            v = tB ? ldcg(&B[(size_t)(j0 + c) * ldb + k0 + kk]) : ldcg(&B[(size_t)(k0 + kk) * ldb + j0 + c]);
+          Bs[((kk >> 2) * TC_LBO_B + (c >> 3) * 128 + (c & 7) * 16 + (kk & 3) * 4) >> 2] = to_tf32(v);
+        }
+        // generic-proxy smem writes become visible to the tensor core's async proxy
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+          for (int ks = 0; ks < TC_K / 8; ++ks) {
+            const uint64_t ad = umma_desc(a_addr + ks * 2 * TC_LBO_A, TC_LBO_A, 128);
+            const uint64_t bd = umma_desc(b_addr + ks * 2 * TC_LBO_B, TC_LBO_B, 128);
+            const uint32_t acc = (ch > 0 || ks > 0) ? 1u : 0u;
+            asm volatile(
+                "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+                " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(tc.tmem),
+                "l"(ad), "l"(bd), "r"(kIdescTf32), "r"(acc)
+                : "memory");
+          }
+          asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(tc.mbar)
+                       : "memory");
+        }
+        // one verdict for the whole CTA, so that every thread takes the same path below
+        ok = __syncthreads_and(mbar_wait(tc.mbar, tc.phase, tc.limit) ? 1 : 0) != 0;
+        tc.phase ^= 1u;
+        if (!ok) tc.pending = 1;
+      }
+      if (!ok) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      // accumulators: warp w reads TMEM lanes 32 (w % 4) .. + 31 (rows), columns 32 (w / 4) .. + 31
+      const int q = warp & 3, h = warp >> 2;
+      const int row = i0 + 32 * q + lane;
+      uint32_t v[32];
+      if (nch > 0) {
+        const uint32_t taddr = tc.tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(32 * h);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+            "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+              "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]),
+              "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+              "=r"(v[30]), "=r"(v[31])
+            : "r"(taddr)
+            : "memory");
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      } else {
+#pragma unroll
+        for (int c = 0; c < 32; ++c) v[c] = 0u;
+      }
+      if (row < m) {
+#pragma unroll
+        for (int c = 0; c < 32; ++c) {
+          const int col = j0 + 32 * h + c;
+          if (col < n) {
+            double* p = &C[(size_t)row * ldc + col];
+            const double s = alpha * (double)__uint_as_float(v[c]);
+            *p = beta != 0.0 ? ldcg(p) + s : s;
+          }
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncthreads();
+    }
+  return ok;
+}
+
 // ------------------------------------------------------------------------- tiles in smem
 __device__ void load_tile(double* S, const double* __restrict__ G, int ld, int rows, int cols) {
   for (int e = threadIdx.x; e < rows * cols; e += NT) {
@@ -750,7 +918,7 @@ __device__ __noinline__ void dev_sum(double* C, int ldc, const double* T, int ld
   __syncthreads();
 }
 
-__device__ bool run_task(const pp_task& T, double* smem) {
+__device__ bool run_task(const pp_task& T, double* smem, TcCtx& tc, int& err) {
   switch (T.op) {
     case PP_OP_NOP: return true;
     case PP_OP_GETRF:
@@ -778,6 +946,13 @@ __device__ bool run_task(const pp_task& T, double* smem) {
       else dev_trsmu(T.p[0], T.ld[0], T.p[1], T.ld[1], T.m, T.n, smem);
       return true;
     case PP_OP_GEMM:
+      if (T.prec == PP_PREC_TF32) {
+        if (!tc.active) return false;  // launched without tensor memory
+        if (!dev_gemm_tc(T.p[0], T.ld[0], T.p[1], T.ld[1], T.flags & PP_T(1), T.p[2], T.ld[2], T.flags & PP_T(2),
+                         T.m, T.n, T.k, T.alpha, T.beta, smem, tc))
+          err = PP_VM_MMA_TIMEOUT;
+        return true;
+      }
       dev_gemm(T.p[0], T.ld[0], T.p[1], T.ld[1], T.flags & PP_T(1), T.p[2], T.ld[2], T.flags & PP_T(2), T.m, T.n,
                T.k, T.alpha, T.beta, smem, (T.flags & PP_FREE_ORDER) != 0);
       return true;
@@ -810,11 +985,7 @@ __global__ void vm_init(const int32_t* __restrict__ indeg, const int32_t* __rest
   }
 }
 
-__device__ __forceinline__ unsigned long long globaltimer_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
+__device__ __forceinline__ unsigned long long globaltimer_ns() { return gtimer_ns(); }
 __device__ __forceinline__ unsigned smid() {
   unsigned s;
   asm volatile("mov.u32 %0, %%smid;" : "=r"(s));
@@ -823,11 +994,33 @@ __device__ __forceinline__ unsigned smid() {
 
 __global__ void __launch_bounds__(NT, 2)
     vm_kernel(const pp_task* __restrict__ tasks, int n_tasks, const int32_t* __restrict__ succ, int32_t* counters,
-              int32_t* slots, pp_vm_state* st, long long spin_limit, unsigned long long* trace) {
+              int32_t* slots, pp_vm_state* st, long long spin_limit, unsigned long long* trace, int use_tc) {
   extern __shared__ double smem[];
   __shared__ __align__(16) pp_task s_task;
   __shared__ int s_id;
   __shared__ unsigned long long s_t0;
+  __shared__ uint32_t s_tmem;
+  __shared__ __align__(8) unsigned long long s_mbar;
+  TcCtx tc{0u, 0u, 0u, spin_limit * 32, 0, 0};
+  if (use_tc) {
+    // TF32 tasks: 64 TMEM columns (128 lanes x 64 FP32 accumulators) and one mbarrier per CTA
+    if ((threadIdx.x >> 5) == 0) {
+      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                   "r"(TC_TMEM_COLS)
+                   : "memory");
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (threadIdx.x == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_mbar)) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    tc.tmem = s_tmem;
+    tc.mbar = smem_u32(&s_mbar);
+    tc.active = 1;
+  }
   for (;;) {
     if (threadIdx.x == 0) {
       int id = -1;
@@ -851,16 +1044,18 @@ __global__ void __launch_bounds__(NT, 2)
     }
     __syncthreads();
     const int id = s_id;
-    if (id < 0) return;
+    if (id < 0) break;
     if (threadIdx.x < (int)(sizeof(pp_task) / 8))
       reinterpret_cast<unsigned long long*>(&s_task)[threadIdx.x] =
           __ldg(reinterpret_cast<const unsigned long long*>(&tasks[id]) + threadIdx.x);
     __syncthreads();
-    const bool ok = run_task(s_task, smem);
+    int err = PP_VM_OK;
+    const bool ok = run_task(s_task, smem, tc, err);
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) {
       if (!ok && atomicCAS(&st->error, 0, PP_VM_BAD_TASK) == 0) st->err_info = id;
+      if (err != PP_VM_OK && atomicCAS(&st->error, 0, err) == 0) st->err_info = id;
       if (trace) {
         trace[3 * (size_t)id] = s_t0;
         trace[3 * (size_t)id + 1] = globaltimer_ns();
@@ -878,6 +1073,18 @@ __global__ void __launch_bounds__(NT, 2)
       }
     }
     if (threadIdx.x == 0) atomicAdd(&st->done, 1);
+  }
+  if (use_tc) {
+    // an MMA group whose completion was never observed still owns the accumulators:
+    // give it one more bounded wait before the columns are returned
+    if (tc.pending) mbar_wait(tc.mbar, tc.phase ^ 1u, tc.limit);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if ((threadIdx.x >> 5) == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tc.tmem), "r"(TC_TMEM_COLS)
+                   : "memory");
+    }
   }
 }
 
@@ -1040,7 +1247,7 @@ cudaError_t pp_vm_run(const pp_vm_launch& L, cudaStream_t s) {
   vm_init<<<(L.n_tasks + ib - 1) / ib, ib, 0, s>>>(L.indeg, L.ready, L.n_ready, L.n_tasks, L.counters, L.slots,
                                                   L.state);
   vm_kernel<<<L.grid, NT, pp_vm_smem_bytes(), s>>>(L.tasks, L.n_tasks, L.succ, L.counters, L.slots, L.state,
-                                                   L.spin_limit, L.trace);
+                                                   L.spin_limit, L.trace, L.use_tc);
   return cudaGetLastError();
 }
 

@@ -10,7 +10,7 @@
 #define PP_VM_TRI 256          /* largest triangle of a TRSM* task (blocked by PP_VM_TILE)   */
 #define PP_VM_MAX_RANK 32      /* largest k1 of ACCUM (register-resident reductions)    */
 
-enum pp_vm_error { PP_VM_OK = 0, PP_VM_TIMEOUT = 1, PP_VM_BAD_TASK = 2 };
+enum pp_vm_error { PP_VM_OK = 0, PP_VM_TIMEOUT = 1, PP_VM_BAD_TASK = 2, PP_VM_MMA_TIMEOUT = 3 };
 
 typedef struct pp_vm_state {
   int head;      /* next ready-slot index to pop                  */
@@ -34,6 +34,7 @@ struct pp_vm_launch {
   long long spin_limit;  /* polls of an empty ready slot before the kernel gives up */
   int grid;              /* CTAs (persistent)                                       */
   unsigned long long* trace = nullptr;  /* optional: 3 words per task (start ns, end ns, sm | cta << 32) */
+  int use_tc = 0;        /* the program holds TF32 tasks: tensor memory + an mbarrier per CTA */
 };
 
 /* ACCUM on caller buffers with the library's static scratch array (no allocation);

@@ -80,3 +80,24 @@ def test_refstream_rejects_solve_only_instruction(pp, hctx):
     h, _ = pp.make_kernel_problem(hctx, 512, 2, "inv", 1e-3, 64, 8)
     words, lengths, tmp = h.refstreams(1)
     assert words[0] == 1 and words[-1] == 0
+
+
+def test_precision_switch_marks_gemm_instructions(pp, hctx):
+    h, _ = pp.make_kernel_problem(hctx, 1024, 2, "inv", 1e-3, 128, 16)
+    bases = [0x1000000 * (i + 1) for i in range(5)]
+    t64, _, _, _ = h.encode_program(0, 1, bases)
+    assert h.precision == pp.FP64
+    assert np.all(t64["prec"] == pp.FP64)
+    h.set_precision(pp.TF32)
+    t32, s32, _, _ = h.encode_program(0, 1, bases)
+    gemm = t32["op"] == pp.OP_NAMES.index("gemm")
+    assert gemm.any()
+    assert np.all(t32["prec"][gemm] == pp.TF32)
+    assert np.all(t32["prec"][~gemm] == pp.FP64)
+    # same program otherwise; the solve program stays FP64
+    assert np.array_equal(t32["op"], t64["op"])
+    ts, _, _, _ = h.encode_program(1, 1, bases)
+    assert np.all(ts["prec"] == pp.FP64)
+    assert pp.lib().pp_hmatrix_set_precision(h.handle, 7) == pp.PP_INVALID_ARG
+    h.set_precision(pp.FP64)
+    assert np.array_equal(h.encode_program(0, 1, bases)[0], t64)
