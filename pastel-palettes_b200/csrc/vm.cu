@@ -410,307 +410,269 @@ __device__ __noinline__ bool dev_gemm_tc(double* __restrict__ C, int ldc, const 
 }
 
 // ------------------------------------------------------------------------- tiles in smem
+// rows x cols (<= TL x TL) from global (L2) into S (ld LDS); every thread issues its up to
+// sixteen loads before it stores any, so a tile costs one memory latency, not sixteen
 __device__ void load_tile(double* S, const double* __restrict__ G, int ld, int rows, int cols) {
-  for (int e = threadIdx.x; e < rows * cols; e += NT) {
-    const int r = e / cols, c = e % cols;
-    S[r * LDS + c] = ldcg(&G[(size_t)r * ld + c]);
+  const int total = rows * cols;
+  for (int e0 = 0; e0 < total; e0 += 16 * NT) {
+    double v[16];
+#pragma unroll
+    for (int p = 0; p < 16; ++p) {
+      const int e = e0 + threadIdx.x + p * NT;
+      v[p] = e < total ? ldcg(&G[(size_t)(e / cols) * ld + e % cols]) : 0.0;
+    }
+#pragma unroll
+    for (int p = 0; p < 16; ++p) {
+      const int e = e0 + threadIdx.x + p * NT;
+      if (e < total) S[(e / cols) * LDS + e % cols] = v[p];
+    }
   }
 }
 
-// Register layout shared by GETRF / TRSML / TRSMRT / TRSMU: warp w, lane = 4 cc + g
-// holds column 8 w + cc (of a 64-wide chunk), rows g + 4 j for j < 16.  Row i of that
-// column lives in lane 4 cc + (i & 3), register i >> 2.
-#define COL_LAYOUT                                                      \
-  const int w_ = threadIdx.x >> 5, lane_ = threadIdx.x & 31;            \
-  const int cc_ = lane_ >> 2, g_ = lane_ & 3;                           \
-  (void)w_;
+// ------------------------------------------------------------------------- GETRF
+// A[m x n] := L\U in place (m, n <= TL), like kernel.cu:104-147: step i divides the entries
+// below the pivot by a_ii and applies a_rc = fma(a_ic, -l_r, a_rc) to the trailing block.
+// Thread t = 16 ty + tx holds rows ty + 16 a and columns tx + 16 b (a, b < 4).  The pivot
+// row and the raw pivot column of step i are published to shared memory (double buffered)
+// by their owners at the end of step i - 1, so a step needs one CTA barrier; lanes tx < 4
+// of each half-warp form the multipliers of the half-warp's rows (one division each) and
+// share them by shuffles.  The steps run in four blocks of sixteen whose block index is a
+// compile-time constant: register selection, the shrinking trailing region and most
+// bounds tests then cost nothing at run time.
+struct GetrfState {
+  double x[4][4];
+  double* prow;  // [2][TL]
+  double* pcol;  // [2][TL]
+  int tx, ty, lane, m;
+};
 
-// A[m x n] := L\U in place (m, n <= TL), like kernel.cu:104-147: for each i the
-// multipliers l_r = a_ri / a_ii of column i go through shared memory, the pivot row
-// entry of each column comes from a lane of the same column group.
-__device__ __noinline__ void dev_getrf(double* A, int lda, int m, int n, double* smem) {
-  double* lbuf = smem;  // [2][TL] multipliers of the current / previous step
-  COL_LAYOUT
-  const int c = 8 * w_ + cc_;
-  double x[16];
+template <int JB>
+__device__ __forceinline__ void getrf_publish(GetrfState& S, int j, int buf) {
+  const int jj = j & 15;
+  if (S.ty == jj) {
 #pragma unroll
-  for (int j = 0; j < 16; ++j) {
-    const int r = g_ + 4 * j;
-    x[j] = (r < m && c < n) ? ldcg(&A[(size_t)r * lda + c]) : 0.0;
+    for (int b = JB; b < 4; ++b) S.prow[buf * TL + S.tx + 16 * b] = S.x[JB][b];
   }
-  const int mn = min(m, n);
+  if (S.tx == jj) {
 #pragma unroll
-  for (int i = 0; i < TL; ++i) {
-    if (i >= mn) break;
-    if (w_ == (i >> 3)) {
-      // the four lanes holding column i hand it to the whole warp, which divides (two
-      // rows per lane instead of sixteen per owning lane), then take the multipliers back
-      double* cbuf = lbuf + 2 * TL;
-      if (cc_ == (i & 7)) {
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int r = g_ + 4 * j;
-          if (r >= i && r < m) cbuf[r] = x[j];
-        }
-      }
-      __syncwarp();
-      const double aii = cbuf[i];
-      for (int r = i + 1 + lane_; r < m; r += 32) lbuf[(i & 1) * TL + r] = cbuf[r] / aii;
-      __syncwarp();
-      if (cc_ == (i & 7)) {
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int r = g_ + 4 * j;
-          if (r > i && r < m) x[j] = lbuf[(i & 1) * TL + r];
-        }
-      }
-    }
-    __syncthreads();
-    const double p = __shfl_sync(0xffffffffu, x[i >> 2], 4 * cc_ + (i & 3));
-    if (c > i && c < n) {
-#pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int r = g_ + 4 * j;
-        if (r > i && r < m) x[j] = fma(p, -lbuf[(i & 1) * TL + r], x[j]);
-      }
-    }
+    for (int a = JB; a < 4; ++a) S.pcol[buf * TL + S.ty + 16 * a] = S.x[a][JB];
   }
-#pragma unroll
-  for (int j = 0; j < 16; ++j) {
-    const int r = g_ + 4 * j;
-    if (r < m && c < n) A[(size_t)r * lda + c] = x[j];
-  }
+}
+
+template <int IB>
+__device__ __forceinline__ void getrf_step(GetrfState& S, int i, int i_end, int mn) {
+  const int ii = i & 15, buf = i & 1;
   __syncthreads();
+  const double piv = S.prow[buf * TL + i];
+  double lm = 0.0;
+  if (S.tx >= IB && S.tx < 4) {
+    const int r = S.ty + 16 * S.tx;
+    if (r > i && r < S.m) lm = S.pcol[buf * TL + r] / piv;
+  }
+  double l[4], u[4];
+#pragma unroll
+  for (int a = IB; a < 4; ++a) l[a] = __shfl_sync(0xffffffffu, lm, (S.lane & 16) | a);
+#pragma unroll
+  for (int b = IB; b < 4; ++b) u[b] = S.prow[buf * TL + S.tx + 16 * b];
+  const bool row_below = S.ty > ii, col_right = S.tx > ii;
+#pragma unroll
+  for (int a = IB; a < 4; ++a)
+#pragma unroll
+    for (int b = IB; b < 4; ++b) {
+      const bool live = (a > IB || row_below) && (b > IB || col_right);
+      if (live) S.x[a][b] = fma(u[b], -l[a], S.x[a][b]);
+    }
+  if (S.tx == ii) {  // column i keeps its multipliers (the L part)
+#pragma unroll
+    for (int a = IB; a < 4; ++a)
+      if (a > IB || row_below) S.x[a][IB] = l[a];
+  }
+  if (i + 1 < i_end) getrf_publish<IB>(S, i + 1, buf ^ 1);
+  else if constexpr (IB < 3) {
+    if (i + 1 < mn) getrf_publish<IB + 1>(S, i + 1, buf ^ 1);
+  }
+}
+
+template <int IB>
+__device__ __forceinline__ void getrf_block(GetrfState& S, int mn) {
+  const int i_end = min(mn, 16 * IB + 16);
+  if (i_end == 16 * IB + 16) {
+#pragma unroll
+    for (int t = 0; t < 16; ++t) getrf_step<IB>(S, 16 * IB + t, i_end, mn);
+  } else {
+#pragma unroll 1
+    for (int i = 16 * IB; i < i_end; ++i) getrf_step<IB>(S, i, i_end, mn);
+  }
+}
+
+__device__ __noinline__ void dev_getrf(double* A, int lda, int m, int n, double* smem) {
+  GetrfState S;
+  S.prow = smem;
+  S.pcol = smem + 2 * TL;
+  S.tx = threadIdx.x & 15;
+  S.ty = threadIdx.x >> 4;
+  S.lane = threadIdx.x & 31;
+  S.m = m;
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int r = S.ty + 16 * a, c = S.tx + 16 * b;
+      S.x[a][b] = (r < m && c < n) ? ldcg(&A[(size_t)r * lda + c]) : 0.0;
+    }
+  const int mn = min(m, n);
+  if (mn > 0) getrf_publish<0>(S, 0, 0);
+  getrf_block<0>(S, mn);
+  getrf_block<1>(S, mn);
+  getrf_block<2>(S, mn);
+  getrf_block<3>(S, mn);
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int r = S.ty + 16 * a, c = S.tx + 16 * b;
+      if (r < m && c < n) A[(size_t)r * lda + c] = S.x[a][b];
+    }
+  __syncthreads();
+}
+
+// ------------------------------------------------------------------------- TRSM sweeps
+// One triangular sweep over independent lines (the columns of B for TRSML / TRSMRT /
+// TRSMU, the rows of B for TRSMR) against a triangle T staged in shared memory (ld LDS).
+// Line q is held by R consecutive lanes of a warp: lane R cc + g holds positions g + R j
+// (j < TL / R); position p of step i is eliminated as x_p = fma(-coef(i, p), x_i, x_p),
+// the operand order of the reference's routines up to the commutation of the product
+// (exact inside an fma).  The finished x_i reaches the line's lanes by a shuffle; no CTA
+// barrier inside the sweep.  Steps run in TL / R blocks of R with a compile-time block
+// index (register selection and the live range of positions resolved at compile time).
+//   PIV 0: unit diagonal, x_i unchanged                     (TRSML, kernel.cu:150-182)
+//   PIV 1: x_i = x_i * rd[i], rd = 1 / diagonal              (TRSMRT kernel.cu:229-285, TRSMU)
+//   PIV 2: x_i = x_i / t_ii                                  (TRSMR, kernel.cu:185-226)
+//   CT: coef(i, p) = T[i][p] (row i of T) when true, T[p][i] (column i) when false.
+template <int R, int PIV, bool CT, bool BACK>
+struct Sweep {
+  static constexpr int NJ = TL / R;
+  double x[NJ];
+  const double* T;
+  const double* rd;
+  int g, src0, len;
+
+  template <int J>
+  __device__ __forceinline__ void step(int i) {
+    const int ii = i - R * J;
+    double v = __shfl_sync(0xffffffffu, x[J], ii, R);
+    if (PIV == 1) v = v * rd[i];
+    if (PIV == 2) v = v / T[i * LDS + i];
+    if (PIV != 0 && g == ii) x[J] = v;
+#pragma unroll
+    for (int j = 0; j < NJ; ++j) {
+      const bool live = BACK ? (j < J || (j == J && g < ii)) : (j > J || (j == J && g > ii));
+      if (live) {
+        const int p = g + R * j;
+        const double c = CT ? T[i * LDS + p] : T[p * LDS + i];
+        x[j] = fma(-c, v, x[j]);
+      }
+    }
+  }
+  template <int J>
+  __device__ __forceinline__ void block() {
+    if (R * J + R <= len) {  // a whole block: steps unrolled, coefficient loads scheduled early
+#pragma unroll
+      for (int t = 0; t < R; ++t) step<J>(BACK ? R * J + R - 1 - t : R * J + t);
+    } else {
+      const int i0 = BACK ? len - 1 : R * J;
+      const int i1 = BACK ? R * J - 1 : len;
+#pragma unroll 1
+      for (int i = i0; i != i1; i += BACK ? -1 : 1) step<J>(i);
+    }
+  }
+  template <int J>
+  __device__ __forceinline__ void run_from() {
+    if constexpr (J >= 0 && J < NJ) {
+      if (R * J < len) block<J>();
+      run_from<BACK ? J - 1 : J + 1>();
+    }
+  }
+  __device__ __forceinline__ void run() {
+    if constexpr (BACK) run_from<NJ - 1>();
+    else run_from<0>();
+  }
+};
+
+// B: lines of length len (<= TL), line q at B + q * lstride, position p at + p * pstride.
+template <int R, int PIV, bool CT, bool BACK>
+__device__ __forceinline__ void tri_sweep(double* B, size_t lstride, size_t pstride, int nlines, int len,
+                                          const double* T, const double* rd) {
+  constexpr int LPP = NT / R;  // lines per pass
+  const int lane = threadIdx.x & 31, g = lane % R;
+  const int q_in = (threadIdx.x / 32) * (32 / R) + lane / R;
+  for (int q0 = 0; q0 < nlines; q0 += LPP) {
+    if (q0 + (threadIdx.x / 32) * (32 / R) >= nlines) continue;  // warp without a live line
+    const int q = q0 + q_in;
+    Sweep<R, PIV, CT, BACK> S;
+    S.T = T;
+    S.rd = rd;
+    S.g = g;
+    S.src0 = 0;
+    S.len = len;
+#pragma unroll
+    for (int j = 0; j < Sweep<R, PIV, CT, BACK>::NJ; ++j) {
+      const int p = g + R * j;
+      S.x[j] = (q < nlines && p < len) ? ldcg(&B[q * lstride + p * pstride]) : 0.0;
+    }
+    S.run();
+#pragma unroll
+    for (int j = 0; j < Sweep<R, PIV, CT, BACK>::NJ; ++j) {
+      const int p = g + R * j;
+      if (q < nlines && p < len) B[q * lstride + p * pstride] = S.x[j];
+    }
+  }
+}
+
+template <int PIV, bool CT, bool BACK>
+__device__ __forceinline__ void tri_lines(double* B, size_t lstride, size_t pstride, int nlines, int len,
+                                          const double* T, const double* rd) {
+  if (nlines <= 16) tri_sweep<16, PIV, CT, BACK>(B, lstride, pstride, nlines, len, T, rd);
+  else tri_sweep<4, PIV, CT, BACK>(B, lstride, pstride, nlines, len, T, rd);
 }
 
 // B[m x n] := L^-1 B, L unit lower m x m (m <= TL); columns independent
 __device__ __noinline__ void dev_trsml(double* B, int ldb, const double* L, int ldl, int m, int n, double* smem) {
-  double* Ls = smem;
-  load_tile(Ls, L, ldl, m, m);
+  load_tile(smem, L, ldl, m, m);
   __syncthreads();
-  if (n <= 4) {
-    // few right-hand sides (solve): one warp, lane holds rows lane and lane + 32, the
-    // finished row i is broadcast by a shuffle; no CTA barrier inside the sweep
-    if (threadIdx.x < 32) {
-      const int lane = threadIdx.x;
-      double x0[4], x1[4];
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        x0[c] = (lane < m && c < n) ? ldcg(&B[(size_t)lane * ldb + c]) : 0.0;
-        x1[c] = (lane + 32 < m && c < n) ? ldcg(&B[(size_t)(lane + 32) * ldb + c]) : 0.0;
-      }
-#pragma unroll
-      for (int i = 0; i < TL - 1; ++i) {
-        if (i + 1 >= m) break;
-        double bi[4];
-#pragma unroll
-        for (int c = 0; c < 4; ++c)
-          if (c < n) bi[c] = __shfl_sync(0xffffffffu, i < 32 ? x0[c] : x1[c], i & 31);
-        if (lane > i && lane < m) {
-          const double left = -Ls[lane * LDS + i];
-#pragma unroll
-          for (int c = 0; c < 4; ++c)
-            if (c < n) x0[c] = fma(bi[c], left, x0[c]);
-        }
-        if (lane + 32 > i && lane + 32 < m) {
-          const double left = -Ls[(lane + 32) * LDS + i];
-#pragma unroll
-          for (int c = 0; c < 4; ++c)
-            if (c < n) x1[c] = fma(bi[c], left, x1[c]);
-        }
-      }
-      for (int c = 0; c < n; ++c) {
-        if (lane < m) B[(size_t)lane * ldb + c] = x0[c];
-        if (lane + 32 < m) B[(size_t)(lane + 32) * ldb + c] = x1[c];
-      }
-    }
-    __syncthreads();
-    return;
-  }
-  COL_LAYOUT
-  for (int c0 = 0; c0 < n; c0 += TL) {
-    const int c = c0 + 8 * w_ + cc_;
-    double x[16];
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      const int r = g_ + 4 * j;
-      x[j] = (r < m && c < n) ? ldcg(&B[(size_t)r * ldb + c]) : 0.0;
-    }
-#pragma unroll
-    for (int i = 0; i < TL - 1; ++i) {
-      if (i + 1 >= m) break;
-      const double v = __shfl_sync(0xffffffffu, x[i >> 2], 4 * cc_ + (i & 3));
-#pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int r = g_ + 4 * j;
-        if (r > i && r < m) x[j] = fma(v, -Ls[r * LDS + i], x[j]);
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      const int r = g_ + 4 * j;
-      if (r < m && c < n) B[(size_t)r * ldb + c] = x[j];
-    }
-  }
+  tri_lines<0, false, false>(B, 1, (size_t)ldb, n, m, smem, nullptr);
   __syncthreads();
 }
 
 // V[m x n] := U^-T V, U upper m x m (m <= TL): the reference's trsmr on a transposed B
 // (kernel.cu:229-285) — row i is scaled by the reciprocal of u_ii, then eliminated below
 __device__ __noinline__ void dev_trsmrt(double* V, int ldv, const double* U, int ldu, int m, int n, double* smem) {
-  double* Us = smem;
   double* rd = smem + TL * LDS;
-  load_tile(Us, U, ldu, m, m);
+  load_tile(smem, U, ldu, m, m);
   __syncthreads();
-  if (threadIdx.x < m) rd[threadIdx.x] = 1. / Us[threadIdx.x * LDS + threadIdx.x];
+  if (threadIdx.x < m) rd[threadIdx.x] = 1. / smem[threadIdx.x * LDS + threadIdx.x];
   __syncthreads();
-  COL_LAYOUT
-  for (int c0 = 0; c0 < n; c0 += TL) {
-    const int c = c0 + 8 * w_ + cc_;
-    double x[16];
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      const int r = g_ + 4 * j;
-      x[j] = (r < m && c < n) ? ldcg(&V[(size_t)r * ldv + c]) : 0.0;
-    }
-#pragma unroll
-    for (int i = 0; i < TL; ++i) {
-      if (i >= m) break;
-      const double v = __shfl_sync(0xffffffffu, x[i >> 2], 4 * cc_ + (i & 3));
-      const double xi = v * rd[i];
-      if (g_ == (i & 3)) x[i >> 2] = xi;
-#pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int r = g_ + 4 * j;
-        if (r > i && r < m) x[j] = fma(-Us[i * LDS + r], xi, x[j]);
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      const int r = g_ + 4 * j;
-      if (r < m && c < n) V[(size_t)r * ldv + c] = x[j];
-    }
-  }
+  tri_lines<1, true, false>(V, 1, (size_t)ldv, n, m, smem, rd);
   __syncthreads();
 }
 
 // B[m x n] := U^-1 B, U upper m x m (m <= TL), backward substitution (solve phase; no
 // reference counterpart): x_i = b_i * (1 / u_ii), then b_r -= u_ri x_i for r < i
 __device__ __noinline__ void dev_trsmu(double* B, int ldb, const double* U, int ldu, int m, int n, double* smem) {
-  double* Us = smem;
   double* rd = smem + TL * LDS;
-  load_tile(Us, U, ldu, m, m);
+  load_tile(smem, U, ldu, m, m);
   __syncthreads();
-  if (threadIdx.x < m) rd[threadIdx.x] = 1. / Us[threadIdx.x * LDS + threadIdx.x];
+  if (threadIdx.x < m) rd[threadIdx.x] = 1. / smem[threadIdx.x * LDS + threadIdx.x];
   __syncthreads();
-  if (n <= 4) {  // few right-hand sides: one warp, rows lane and lane + 32, shuffles only
-    if (threadIdx.x < 32) {
-      const int lane = threadIdx.x;
-      double x0[4], x1[4];
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        x0[c] = (lane < m && c < n) ? ldcg(&B[(size_t)lane * ldb + c]) : 0.0;
-        x1[c] = (lane + 32 < m && c < n) ? ldcg(&B[(size_t)(lane + 32) * ldb + c]) : 0.0;
-      }
-#pragma unroll
-      for (int i = TL - 1; i >= 0; --i) {
-        if (i >= m) continue;
-        if (lane == (i & 31)) {
-#pragma unroll
-          for (int c = 0; c < 4; ++c) {
-            if (i < 32) x0[c] = x0[c] * rd[i];
-            else x1[c] = x1[c] * rd[i];
-          }
-        }
-        double bi[4];
-#pragma unroll
-        for (int c = 0; c < 4; ++c)
-          if (c < n) bi[c] = __shfl_sync(0xffffffffu, i < 32 ? x0[c] : x1[c], i & 31);
-        if (lane < i) {
-          const double u = -Us[lane * LDS + i];
-#pragma unroll
-          for (int c = 0; c < 4; ++c)
-            if (c < n) x0[c] = fma(u, bi[c], x0[c]);
-        }
-        if (lane + 32 < i) {
-          const double u = -Us[(lane + 32) * LDS + i];
-#pragma unroll
-          for (int c = 0; c < 4; ++c)
-            if (c < n) x1[c] = fma(u, bi[c], x1[c]);
-        }
-      }
-      for (int c = 0; c < n; ++c) {
-        if (lane < m) B[(size_t)lane * ldb + c] = x0[c];
-        if (lane + 32 < m) B[(size_t)(lane + 32) * ldb + c] = x1[c];
-      }
-    }
-    __syncthreads();
-    return;
-  }
-  COL_LAYOUT
-  for (int c0 = 0; c0 < n; c0 += TL) {
-    const int c = c0 + 8 * w_ + cc_;
-    double x[16];
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      const int r = g_ + 4 * j;
-      x[j] = (r < m && c < n) ? ldcg(&B[(size_t)r * ldb + c]) : 0.0;
-    }
-#pragma unroll
-    for (int i = TL - 1; i >= 0; --i) {
-      if (i >= m) continue;
-      const double v = __shfl_sync(0xffffffffu, x[i >> 2], 4 * cc_ + (i & 3));
-      const double xi = v * rd[i];
-      if (g_ == (i & 3)) x[i >> 2] = xi;
-#pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int r = g_ + 4 * j;
-        if (r < i) x[j] = fma(-Us[r * LDS + i], xi, x[j]);
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      const int r = g_ + 4 * j;
-      if (r < m && c < n) B[(size_t)r * ldb + c] = x[j];
-    }
-  }
+  tri_lines<1, false, true>(B, 1, (size_t)ldb, n, m, smem, rd);
   __syncthreads();
 }
 
-// B[m x n] := B U^-1, U upper n x n (n <= TL); rows independent: lane = 4 rr + g holds
-// row 8 w + rr (of a 64-row chunk), columns g + 4 j
+// B[m x n] := B U^-1, U upper n x n (n <= TL); rows independent
 __device__ __noinline__ void dev_trsmr(double* B, int ldb, const double* U, int ldu, int m, int n, double* smem) {
-  double* Us = smem;
-  load_tile(Us, U, ldu, n, n);
+  load_tile(smem, U, ldu, n, n);
   __syncthreads();
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, rr = lane >> 2, g = lane & 3;
-  for (int r0 = 0; r0 < m; r0 += 64) {
-    const int row = r0 + 8 * w + rr;
-    double x[16];
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      const int c = g + 4 * j;
-      x[j] = (row < m && c < n) ? ldcg(&B[(size_t)row * ldb + c]) : 0.0;
-    }
-#pragma unroll
-    for (int i = 0; i < TL; ++i) {
-      if (i >= n) break;
-      const double v = __shfl_sync(0xffffffffu, x[i >> 2], 4 * rr + (i & 3));
-      const double xi = v / Us[i * LDS + i];
-      if (g == (i & 3)) x[i >> 2] = xi;
-      const double left = -xi;
-#pragma unroll
-      for (int j = 0; j < 16; ++j) {
-        const int c = g + 4 * j;
-        if (c > i && c < n) x[j] = fma(left, Us[i * LDS + c], x[j]);
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < 16; ++j) {
-      const int c = g + 4 * j;
-      if (row < m && c < n) B[(size_t)row * ldb + c] = x[j];
-    }
-  }
+  tri_lines<2, true, false>(B, (size_t)ldb, 1, m, n, smem, nullptr);
   __syncthreads();
 }
 
@@ -992,12 +954,13 @@ __device__ __forceinline__ unsigned smid() {
   return s;
 }
 
-__global__ void __launch_bounds__(NT, 2)
+__global__ void __launch_bounds__(NT, 1)
     vm_kernel(const pp_task* __restrict__ tasks, int n_tasks, const int32_t* __restrict__ succ, int32_t* counters,
               int32_t* slots, pp_vm_state* st, long long spin_limit, unsigned long long* trace, int use_tc) {
   extern __shared__ double smem[];
   __shared__ __align__(16) pp_task s_task;
   __shared__ int s_id;
+  __shared__ int s_keep;  // position (in the successor list) of the successor run next
   __shared__ unsigned long long s_t0;
   __shared__ uint32_t s_tmem;
   __shared__ __align__(8) unsigned long long s_mbar;
@@ -1021,22 +984,30 @@ __global__ void __launch_bounds__(NT, 2)
     tc.mbar = smem_u32(&s_mbar);
     tc.active = 1;
   }
+  // Continuation: of the successors this CTA's task makes ready, the first in the
+  // successor list (sorted by the host, longest remaining path first) is run next by the
+  // same CTA without a round trip through the queue; the others are pushed.  Queue slots
+  // therefore number fewer than tasks, so a CTA waiting on a slot also leaves once every
+  // task is done.
+  int next = -1;
   for (;;) {
     if (threadIdx.x == 0) {
-      int id = -1;
-      const int idx = atomicAdd(&st->head, 1);
-      if (idx < n_tasks) {
-        long long spins = 0;
-        for (;;) {
-          id = ld_acquire(&slots[idx]);
-          if (id >= 0) break;
-          if (ld_relaxed(&st->error)) { id = -1; break; }
-          if (++spins > spin_limit) {
-            if (atomicCAS(&st->error, 0, PP_VM_TIMEOUT) == 0) st->err_info = idx;
-            id = -1;
-            break;
+      int id = next;
+      if (id < 0) {
+        const int idx = atomicAdd(&st->head, 1);
+        if (idx < n_tasks) {
+          long long spins = 0;
+          for (;;) {
+            id = ld_acquire(&slots[idx]);
+            if (id >= 0) break;
+            if (ld_relaxed(&st->error) || ld_relaxed(&st->done) >= n_tasks) { id = -1; break; }
+            if (++spins > spin_limit) {
+              if (atomicCAS(&st->error, 0, PP_VM_TIMEOUT) == 0) st->err_info = idx;
+              id = -1;
+              break;
+            }
+            __nanosleep(32);
           }
-          __nanosleep(32);
         }
       }
       s_id = id;
@@ -1048,6 +1019,7 @@ __global__ void __launch_bounds__(NT, 2)
     if (threadIdx.x < (int)(sizeof(pp_task) / 8))
       reinterpret_cast<unsigned long long*>(&s_task)[threadIdx.x] =
           __ldg(reinterpret_cast<const unsigned long long*>(&tasks[id]) + threadIdx.x);
+    if (threadIdx.x == 0) s_keep = NT;
     __syncthreads();
     int err = PP_VM_OK;
     const bool ok = run_task(s_task, smem, tc, err);
@@ -1065,14 +1037,25 @@ __global__ void __launch_bounds__(NT, 2)
     // successors are released in parallel, one thread each (a serial loop costs one L2
     // round trip per successor on the critical path)
     const int nsucc = s_task.n_succ, sbeg = s_task.succ_begin;
+    int mine = -1;
     for (int q = threadIdx.x; q < nsucc; q += NT) {
-      const int s = succ[sbeg + q];
-      if (atom_add_acq_rel(&counters[s], -1) == 1) {
-        const int pos = atomicAdd(&st->tail, 1);
-        st_release(&slots[pos], s);
+      const int sq = succ[sbeg + q];
+      if (atom_add_acq_rel(&counters[sq], -1) == 1) {
+        if (q < NT) {
+          mine = sq;
+          atomicMin(&s_keep, q);
+        } else {
+          st_release(&slots[atomicAdd(&st->tail, 1)], sq);
+        }
       }
     }
-    if (threadIdx.x == 0) atomicAdd(&st->done, 1);
+    __syncthreads();
+    const int keep = s_keep;
+    if (mine >= 0 && (int)threadIdx.x != keep) st_release(&slots[atomicAdd(&st->tail, 1)], mine);
+    if (threadIdx.x == 0) {
+      next = keep < NT ? succ[sbeg + keep] : -1;
+      atomicAdd(&st->done, 1);
+    }
   }
   if (use_tc) {
     // an MMA group whose completion was never observed still owns the accumulators:
