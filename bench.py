@@ -115,6 +115,10 @@ def program_bytes(pp, h, which=0, nrhs=1):
             e = 2 * (m * k + n * k) + (m + n) * l + n * k
         elif op == 10:
             e = (k + 2) * m * n
+        elif op == 11:  # TRINV: leaf triangle read, an m x n column block of the inverse written
+            e = m * m // 2 + m * n
+        elif op == 12:  # TRMV: triangle read, B read and written
+            e = m * m // 2 + 2 * m * n
         else:
             e = 0
         total += 8 * e

@@ -57,7 +57,7 @@ typedef struct pp_program_info {
   int n_tasks;
   long long n_edges;
   long long flops;                  /* algorithmic FLOPs of all instructions */
-  long long op_count[12];           /* instructions per pp_op (pp_task.h)   */
+  long long op_count[16];           /* instructions per pp_op (pp_task.h)   */
   long long arena_elems[5];         /* matrix, work, scratch, rhs, rand     */
   double host_build_ms;             /* op generation + DAG + encoding        */
 } pp_program_info;
@@ -101,6 +101,11 @@ long long pp_hmatrix_storage_elems(const pp_hmatrix* h);
 double* pp_hmatrix_host_arena(pp_hmatrix* h, long long* elems);
 /* device base of the matrix arena (read-only view for residual / export helpers) */
 const double* pp_hmatrix_device_arena(const pp_hmatrix* h);
+/* elements of the arena prefix that holds the matrix blocks — what upload, download,
+ * keep_original and restore copy.  The rest of the arena holds the explicit inverses of
+ * the diagonal leaves' triangular factors, written by the factorization and read by the
+ * solves.  no reference counterpart */
+long long pp_hmatrix_block_elems(const pp_hmatrix* h);
 
 /* contraction precision of the factor's GEMM (Schur-complement and low-rank product)
  * instructions: PP_PRECISION_FP64 (default; matches the reference's FP64 factorization) or

@@ -306,6 +306,31 @@ int run_one(const pp_task& T, std::vector<double>& tmp) {
           q = T.beta != 0.0 ? q + s : s;
         }
       return 0;
+    case PP_OP_TRINV: {  // engine instruction: identity columns, then the blocked sweep
+      const int m = T.m, w = T.n, c0 = T.o, ldi = T.ld[0], lda = T.ld[1];
+      double* I = T.p[0];
+      for (int r = 0; r < m; ++r)
+        for (int j = 0; j < w; ++j) I[(int64_t)r * ldi + j] = r == c0 + j ? 1.0 : 0.0;
+      if (T.ctrl == 0)
+        o_trsml(I + (int64_t)c0 * ldi, T.p[1] + (int64_t)c0 * lda + c0, w, m - c0, m - c0, ldi, lda);
+      else
+        o_trsmu(I, T.p[1], c0 + w, w, ldi, lda);
+      return 0;
+    }
+    case PP_OP_TRMV: {  // engine instruction: B := M B, M triangular (ascending column sums)
+      const int m = T.m, n = T.n, ldb = T.ld[0], ldm = T.ld[1];
+      std::vector<double> out((size_t)m * n);
+      for (int r = 0; r < m; ++r)
+        for (int q = 0; q < n; ++q) {
+          double s = 0.0;
+          const int c_lo = T.ctrl ? r : 0, c_hi = T.ctrl ? m : r + 1;
+          for (int c = c_lo; c < c_hi; ++c) s = std::fma(T.p[1][(int64_t)r * ldm + c], T.p[0][(int64_t)c * ldb + q], s);
+          out[(size_t)r * n + q] = s;
+        }
+      for (int r = 0; r < m; ++r)
+        for (int q = 0; q < n; ++q) T.p[0][(int64_t)r * ldb + q] = out[(size_t)r * n + q];
+      return 0;
+    }
     default: return -1;
   }
 }

@@ -28,7 +28,8 @@ LIB_PATH = os.path.join(_HERE, "libpastel_palettes.so")
 
 PP_OK, PP_INVALID_ARG, PP_OOM, PP_TIMEOUT, PP_NUMERICAL, PP_CUDA_ERROR, PP_UNSUPPORTED, PP_INTERNAL = range(8)
 STATUS_NAMES = ["OK", "INVALID_ARG", "OOM", "TIMEOUT", "NUMERICAL", "CUDA_ERROR", "UNSUPPORTED", "INTERNAL"]
-OP_NAMES = ["nop", "getrf", "trsml", "trsmr", "trsmrt", "trsmu", "gemm", "gemm3", "gemm4", "accum", "sum"]
+OP_NAMES = ["nop", "getrf", "trsml", "trsmr", "trsmrt", "trsmu", "gemm", "gemm3", "gemm4", "accum", "sum", "trinv",
+            "trmv"]
 DENSE, LOWRANK, HIER = 0, 1, 2
 FP64, TF32 = 0, 1  # contraction precision of the factor's GEMM instructions
 ARENAS = ["matrix", "work", "scratch", "rhs", "rand"]
@@ -60,7 +61,7 @@ class _BlockInfo(C.Structure):
 
 class _ProgramInfo(C.Structure):
     _fields_ = [("n_tasks", C.c_int), ("n_edges", C.c_longlong), ("flops", C.c_longlong),
-                ("op_count", C.c_longlong * 12), ("arena_elems", C.c_longlong * 5), ("host_build_ms", C.c_double)]
+                ("op_count", C.c_longlong * 16), ("arena_elems", C.c_longlong * 5), ("host_build_ms", C.c_double)]
 
 
 _lib = None
@@ -96,6 +97,7 @@ def lib():
             "pp_hmatrix_storage_elems": (ll, [vp]),
             "pp_hmatrix_host_arena": (dp, [vp, C.POINTER(ll)]),
             "pp_hmatrix_device_arena": (vp, [vp]),
+            "pp_hmatrix_block_elems": (ll, [vp]),
             "pp_hlu_factor": (i, [vp, vp]),
             "pp_hlu_solve": (i, [vp, vp, vp, i, vp]),
             "pp_hmatrix_sync": (i, [vp, vp]),
@@ -312,7 +314,8 @@ class Hierarchical:
         self.ctx.check(lib().pp_hmatrix_restore(self._h, _stream_handle(stream)), "restore")
 
     def arena_bytes(self):
-        return 8 * self.host_arena().size
+        """Bytes of the matrix blocks: what upload, download and restore copy."""
+        return 8 * int(lib().pp_hmatrix_block_elems(self._h))
 
     # --- factor / solve
     @property

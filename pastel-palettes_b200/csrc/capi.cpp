@@ -126,6 +126,7 @@ pp_status build_program(pp_hmatrix* h, int which, int nrhs, VmPlan& plan) {
   auto t0 = std::chrono::steady_clock::now();
   try {
     pp::Generator g(plan.prog, *h->H, ctx->cfg.tile, h->H->n, ctx->cfg.reference_isa == 0);
+    g.use_inverses(ctx->cfg.reference_isa == 0);
     if (which == 0) {
       g.getrf_program();
       if (h->precision != PP_PREC_FP64) plan.prog.set_gemm_precision(h->precision);
@@ -387,7 +388,7 @@ pp_status pp_hmatrix_upload(pp_hmatrix* h, void* stream) {
   if (!has_device(ctx)) return fail(ctx, PP_CUDA_ERROR, "no CUDA device in this context");
   const size_t bytes = sizeof(double) * (size_t)std::max<int64_t>(h->H->arena_elems, 1);
   if (!h->d_arena) PP_CUDA(cudaMalloc((void**)&h->d_arena, bytes));
-  PP_CUDA(cudaMemcpyAsync(h->d_arena, h->H->host.data(), sizeof(double) * h->H->arena_elems, cudaMemcpyHostToDevice,
+  PP_CUDA(cudaMemcpyAsync(h->d_arena, h->H->host.data(), sizeof(double) * h->H->block_elems, cudaMemcpyHostToDevice,
                           (cudaStream_t)stream));
   // the random sketch depends on the factor program's arena sizes
   pp_status st = build_program(h, 0, 0, h->factor);
@@ -404,7 +405,7 @@ pp_status pp_hmatrix_download(pp_hmatrix* h, void* stream) {
   if (!h) return PP_INVALID_ARG;
   pp_context* ctx = h->ctx;
   if (!h->d_arena) return fail(ctx, PP_INVALID_ARG, "H-matrix not uploaded");
-  PP_CUDA(cudaMemcpyAsync(h->H->host.data(), h->d_arena, sizeof(double) * h->H->arena_elems, cudaMemcpyDeviceToHost,
+  PP_CUDA(cudaMemcpyAsync(h->H->host.data(), h->d_arena, sizeof(double) * h->H->block_elems, cudaMemcpyDeviceToHost,
                           (cudaStream_t)stream));
   PP_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
   return PP_OK;
@@ -424,7 +425,7 @@ pp_status pp_hmatrix_keep_original(pp_hmatrix* h, void* stream) {
   if (!h) return PP_INVALID_ARG;
   pp_context* ctx = h->ctx;
   if (!h->d_arena) return fail(ctx, PP_INVALID_ARG, "H-matrix not uploaded");
-  const size_t bytes = sizeof(double) * (size_t)h->H->arena_elems;
+  const size_t bytes = sizeof(double) * (size_t)h->H->block_elems;
   if (!h->d_orig) PP_CUDA(cudaMalloc((void**)&h->d_orig, std::max<size_t>(bytes, 8)));
   PP_CUDA(cudaMemcpyAsync(h->d_orig, h->d_arena, bytes, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
   return PP_OK;
@@ -434,7 +435,7 @@ pp_status pp_hmatrix_restore(pp_hmatrix* h, void* stream) {
   if (!h) return PP_INVALID_ARG;
   pp_context* ctx = h->ctx;
   if (!h->d_orig) return fail(ctx, PP_INVALID_ARG, "no original kept (pp_hmatrix_keep_original)");
-  PP_CUDA(cudaMemcpyAsync(h->d_arena, h->d_orig, sizeof(double) * (size_t)h->H->arena_elems,
+  PP_CUDA(cudaMemcpyAsync(h->d_arena, h->d_orig, sizeof(double) * (size_t)h->H->block_elems,
                           cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
   return PP_OK;
 }
@@ -468,6 +469,7 @@ double* pp_hmatrix_host_arena(pp_hmatrix* h, long long* elems) {
   return h->H->host.data();
 }
 const double* pp_hmatrix_device_arena(const pp_hmatrix* h) { return h ? h->d_arena : nullptr; }
+long long pp_hmatrix_block_elems(const pp_hmatrix* h) { return h ? h->H->block_elems : 0; }
 
 pp_status pp_hlu_factor(pp_hmatrix* h, void* stream) {
   if (!h) return PP_INVALID_ARG;

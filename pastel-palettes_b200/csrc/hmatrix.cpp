@@ -27,6 +27,15 @@ int Hierarchical::add_obj(int rows, int cols) {
   return (int)objs.size() - 1;
 }
 
+void Hierarchical::add_inverses() {
+  block_elems = arena_elems;
+  for (auto& nd : nodes)
+    if (nd.kind == HNode::D && nd.r0 == nd.c0 && nd.m == nd.n && nd.m <= kInvMax) {
+      nd.invL = add_obj(nd.m, nd.m);
+      nd.invU = add_obj(nd.m, nd.m);
+    }
+}
+
 Hierarchical* Hierarchical::dense_tiled(int n, int leaf) {
   if (n <= 0 || leaf <= 0) throw std::invalid_argument("dense_tiled: n and leaf must be positive");
   auto* h = new Hierarchical();
@@ -91,6 +100,7 @@ Hierarchical* Hierarchical::dense_tiled(int n, int leaf) {
     return id;
   };
   h->root = build(0, n, 0, 0);
+  h->add_inverses();
   h->host.assign((size_t)h->arena_elems, 0.0);
   return h;
 }
@@ -181,6 +191,7 @@ Hierarchical* Hierarchical::geometric(int n, int dim, const double* pts, int lea
     return id;
   };
   h->root = block(0, 0, 0);
+  h->add_inverses();
   h->host.assign((size_t)h->arena_elems, 0.0);
   return h;
 }

@@ -42,6 +42,7 @@ struct HNode {
   int rank = 0;      // LR: current rank
   int kmax = 0;      // LR: storage capacity (columns of U and V)
   int ch[4] = {-1, -1, -1, -1};  // H: children, row-major 2 x 2
+  int invL = -1, invU = -1;      // D on the diagonal: L^-1 and U^-1 of its factors (solve)
 };
 
 class Hierarchical {
@@ -51,6 +52,10 @@ class Hierarchical {
   std::vector<HNode> nodes;
   std::vector<StorageObj> objs;
   int64_t arena_elems = 0;
+  // the matrix blocks occupy the arena prefix [0, block_elems); the tail holds the explicit
+  // inverses of the diagonal leaves' triangular factors, which the factorization writes and
+  // the solves read (never uploaded, downloaded or restored)
+  int64_t block_elems = 0;
   std::vector<double> host;  // host image of the arena (filled by set_dense / set_lowrank)
 
   // All-dense 2x2 partition of an n x n matrix down to blocks of <= leaf rows.
@@ -77,6 +82,11 @@ class Hierarchical {
 
  private:
   int add_obj(int rows, int cols);
+  // appends L^-1 / U^-1 objects for every square diagonal dense leaf of at most kInvMax rows
+  void add_inverses();
 };
+
+// largest diagonal leaf whose triangular factors get explicit inverses
+constexpr int kInvMax = 256;
 
 }  // namespace pp

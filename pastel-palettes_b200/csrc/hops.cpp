@@ -59,8 +59,18 @@ int Program::add_obj(int arena, int rows, int cols, bool tracked) {
 }
 
 int64_t Program::total_flops() const {
+  // the algorithmic count of the factorization / solve; the TRINV instructions that prepare
+  // the solves' explicit inverses are accounted apart (aux_flops)
   int64_t s = 0;
-  for (auto& t : tasks) s += t.flops;
+  for (auto& t : tasks)
+    if (t.t.op != PP_OP_TRINV) s += t.flops;
+  return s;
+}
+
+int64_t Program::aux_flops() const {
+  int64_t s = 0;
+  for (auto& t : tasks)
+    if (t.t.op == PP_OP_TRINV) s += t.flops;
   return s;
 }
 
@@ -249,6 +259,9 @@ bool Program::encode_reference(int workers, std::vector<std::vector<int32_t>>& s
       }
       const HTask& h = tasks[en.inst];
       const pp_task& x = h.t;
+      // the solves' inverse preparation writes only the arena tail and nothing waits on it:
+      // the reference (which has no solve) gets the factorization proper
+      if (x.op == PP_OP_TRINV) continue;
       auto T = [&](int k) { return (x.flags & PP_T(k)) ? 1 : 0; };
       int32_t p[6] = {0}, o[6] = {0};
       for (int k = 0; k < 6; ++k)
@@ -326,6 +339,9 @@ Generator::Generator(Program& P, Hierarchical& H, int tile, int max_n_rand, bool
   for (size_t i = 0; i < H.objs.size(); ++i)
     node_obj_[i] = P.add_obj_at(ar, H.objs[i].off, H.objs[i].rows, H.objs[i].cols, H.objs[i].ld, true);
   for (auto& x : rand_ld_obj_) x = -1;
+  inv_obj_.assign(P.objs.size(), {-1, -1});
+  for (auto& nd : H.nodes)
+    if (nd.kind == HNode::D && nd.invL >= 0) inv_obj_[node_obj_[nd.obj]] = {node_obj_[nd.invL], node_obj_[nd.invU]};
   int kmax = 1;
   for (auto& nd : H.nodes)
     if (nd.kind == HNode::LR) kmax = std::max(kmax, nd.kmax);
@@ -460,9 +476,58 @@ void Generator::bind(HTask& t, int slot, const View& v, bool write) {
 }
 
 // --------------------------------------------------------------------------- H-LU
-void Generator::getrf_program() { getrf(node(H_.root)); }
+void Generator::getrf_program() {
+  getrf(node(H_.root));
+  if (inverses_) emit_inverses();
+}
+
+// A diagonal leaf used whole as the triangle of a solve step, and its inverse objects.
+bool Generator::inverse_of(const Mat& T, int& invL, int& invU) const {
+  if (!inverses_ || T.kind != Mat::D || T.d.t || T.d.r0 != 0 || T.d.c0 != 0) return false;
+  if (T.d.obj < 0 || T.d.obj >= (int)inv_obj_.size() || inv_obj_[T.d.obj].first < 0) return false;
+  const PObj& o = P_.objs[T.d.obj];
+  if (T.d.m != o.rows || T.d.n != o.cols) return false;
+  invL = inv_obj_[T.d.obj].first;
+  invU = inv_obj_[T.d.obj].second;
+  return true;
+}
+
+// TRINV tasks: after its GETRF a diagonal leaf is final; its L^-1 and U^-1 are built in
+// column blocks of T_ on idle CTAs while the factorization goes on elsewhere.
+void Generator::emit_inverses() {
+  for (const HNode& nd : H_.nodes) {
+    if (nd.kind != HNode::D || nd.invL < 0) continue;
+    View A;
+    A.obj = node_obj_[nd.obj];
+    A.m = nd.m;
+    A.n = nd.n;
+    for (int which = 0; which < 2; ++which) {
+      View I;
+      I.obj = node_obj_[which == 0 ? nd.invL : nd.invU];
+      I.m = nd.m;
+      I.n = nd.m;
+      for (int c0 = 0; c0 < nd.m; c0 += T_) {
+        const int w = std::min(T_, nd.m - c0);
+        HTask& t = emit(PP_OP_TRINV);
+        bind(t, 0, I.sub(0, c0, nd.m, w), true);
+        bind(t, 1, A, false);
+        t.t.m = nd.m;
+        t.t.n = w;
+        t.t.o = c0;
+        t.t.ctrl = which;
+        const int64_t rows = which == 0 ? nd.m - c0 : c0 + w;  // rows the sweep touches
+        t.flops = (int64_t)w * rows * rows;
+      }
+    }
+  }
+}
 
 void Generator::solve_program(int nrhs) {
+  // a solve sweeps each leaf triangle once with few right-hand sides: whole leaves (up to
+  // kSolveTri rows) go to one blocked instruction, which saves the inter-task latency of
+  // the 64-row pieces on the solve's sequential path
+  Ttri_ = std::max(Ttri_, kSolveTri);
+  solve_ = true;
   rhs_obj_ = P_.add_obj(P_.arena_id(inst_, AR_RHS), H_.n, nrhs, true);
   View b;
   b.obj = rhs_obj_;
@@ -495,6 +560,11 @@ void Generator::getrf(const Mat& A) {
 
 void Generator::trsml(const Mat& L, const Mat& B) {
   if (B.kind == Mat::LR) { trsml(L, asD(B.u)); return; }
+  int invL, invU;
+  if (solve_ && B.kind == Mat::D && !B.d.t && inverse_of(L, invL, invU)) {
+    trmv(invL, 0, L.m, B.d);
+    return;
+  }
   const int s = tri_split(L, Ttri_);
   if (s < 0) {
     if (B.kind != Mat::D || B.d.t) throw std::logic_error("trsml: target must be a dense untransposed block");
@@ -574,6 +644,11 @@ void Generator::trsmrt(const Mat& U, const View& V) {
 
 void Generator::trsmu(const Mat& U, const Mat& B) {
   if (B.kind == Mat::LR) { trsmu(U, asD(B.u)); return; }
+  int invL, invU;
+  if (solve_ && B.kind == Mat::D && !B.d.t && inverse_of(U, invL, invU)) {
+    trmv(invU, 1, U.m, B.d);
+    return;
+  }
   const int s = tri_split(U, Ttri_);
   if (s < 0) {
     if (B.kind != Mat::D || B.d.t) throw std::logic_error("trsmu: target must be a dense untransposed block");
@@ -753,6 +828,25 @@ void Generator::accum(const Mat& C, const View& X, const View& Y, int sign) {
   t.flops = 2 * kk * nx * kk + 2 * ny * kk * kk + 2 * kk * nx * k22 + 2 * ny * k22 * kk  // sketch
             + 8 * ny * kk * kk                                                        // QR + Q
             + 2 * kk * ny * kk + 2 * nx * kk * kk + 2 * kk * ny * k22 + 2 * nx * k22 * kk;  // projection
+}
+
+// B := M B with M the explicit inverse (object inv, m x m; lower = ctrl 0, upper = 1) of a
+// diagonal leaf's triangular factor; B's columns in groups of at most kTrmvCols
+void Generator::trmv(int inv, int upper, int m, const View& B) {
+  View M;
+  M.obj = inv;
+  M.m = m;
+  M.n = m;
+  for (int c = 0; c < B.n; c += kTrmvCols) {
+    const int w = std::min(kTrmvCols, B.n - c);
+    HTask& t = emit(PP_OP_TRMV);
+    bind(t, 0, B.sub(0, c, B.m, w), true);
+    bind(t, 1, M, false);
+    t.t.m = m;
+    t.t.n = w;
+    t.t.ctrl = upper;
+    t.flops = (int64_t)w * m * (m + 1);
+  }
 }
 
 }  // namespace pp

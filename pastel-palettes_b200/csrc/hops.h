@@ -90,6 +90,7 @@ class Program {
   int add_obj_at(int arena, int64_t off, int rows, int cols, int ld, bool tracked);
   int arena_id(int inst, int kind) const { return inst * PP_ARENAS + kind; }
   int64_t total_flops() const;
+  int64_t aux_flops() const;
   int64_t count_op(int op) const;
   // Contraction precision of every GEMM instruction (PP_PREC_TF32: tensor cores with FP32
   // accumulation; GETRF, TRSM*, ACCUM and SUM stay FP64).  Returns the tasks changed.
@@ -109,6 +110,12 @@ class Program {
                         int64_t* tmp_elems_per_worker) const;
 };
 
+// largest triangle of one solve-phase TRSML / TRSMU instruction (the VM's blocked
+// triangular routines take up to 256 rows)
+constexpr int kSolveTri = 256;
+// right-hand-side columns of one TRMV instruction
+constexpr int kTrmvCols = 16;
+
 class Generator {
  public:
   // Builds programs on one H-matrix instance.  `tile`: dense blocks larger than this
@@ -118,6 +125,9 @@ class Generator {
   Generator(Program& P, Hierarchical& H, int tile, int max_n_rand, bool split_k = true);
   int inst() const { return inst_; }
   void getrf_program();            // H-LU factorization of the whole matrix
+  // explicit inverses of the diagonal leaves' triangular factors (TRINV), which the solve
+  // program then applies with TRMV instead of substituting; set before building programs
+  void use_inverses(bool on) { inverses_ = on; }
   void solve_program(int nrhs);    // B := U^-1 L^-1 B on the RHS object (n x nrhs)
   int rhs_obj() const { return rhs_obj_; }
 
@@ -140,6 +150,12 @@ class Generator {
   int rhs_obj_ = -1;
   int max_n_rand_;
   bool split_k_;
+  bool inverses_ = false;
+  bool solve_ = false;  // building a solve program
+  void trmv(int inv, int upper, int m, const View& B);
+  std::vector<std::pair<int, int>> inv_obj_;  // program obj of a diagonal leaf -> (L^-1, U^-1) objs
+  bool inverse_of(const Mat& T, int& invL, int& invU) const;
+  void emit_inverses();
 
   struct LRP { View x, y; int sign; };  // x y^T * sign
   LRP lr_product(const Mat& A, const Mat& B, int alpha);

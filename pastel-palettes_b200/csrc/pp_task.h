@@ -29,7 +29,14 @@ enum pp_op {
   PP_OP_ACCUM = 9,   /* U1 V1^T := rank-k1 range of U1 V1^T + alpha U2 V2^T (kernel.cu:1255-1280)   */
   PP_OP_SUM = 10,    /* C[m x n] := beta C + sum_{p<k} T_p, T_p = p-th m x n block (ld n) of p[1]:
                         reduction of split-k partial products (no reference counterpart)       */
-  PP_OP_COUNT = 11
+  PP_OP_TRINV = 11,  /* columns [o, o + n) of the inverse of a factored diagonal leaf A = L\U
+                        (m x m, p[1]) into the m x n column block at p[0] (ld ld[0]):
+                        ctrl 0: L^-1 (unit lower), ctrl 1: U^-1 (upper).  Factor phase; no
+                        reference counterpart (it serves the solve)                             */
+  PP_OP_TRMV = 12,   /* B[m x n] := M B, M (p[1], m x m) lower (ctrl 0) or upper (ctrl 1)
+                        triangular with explicit diagonal: a solve step with a precomputed
+                        inverse; no reference counterpart                                       */
+  PP_OP_COUNT = 13
 };
 
 /* flags: bit (4+i) = operand i is stored transposed (operand 0 is the target). */

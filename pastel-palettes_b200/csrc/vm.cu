@@ -30,7 +30,7 @@
 #define NT PP_VM_THREADS
 #define TL PP_VM_TILE
 #define LDS (PP_VM_TILE + 1)   /* padded smem row stride (doubles) */
-#define VM_SMEM_BYTES 40960    /* largest routine: the skinny GEMM tiles (37.4 KB) */
+#define VM_SMEM_BYTES 163840   /* one CTA per SM: ACCUM keeps its ny x k1 sketch on chip */
 
 namespace {
 
@@ -228,10 +228,49 @@ __device__ __noinline__ void gemm_splitk(double* __restrict__ C, int ldc, const 
   __syncthreads();
 }
 
+// C[1 x n] (n <= 32) = beta C + alpha op(A)[1 x k] op(B)[k x n] in free order (a row vector
+// times a tall skinny matrix, e.g. x^T V in a solve): thread t sums k = t, t + NT, ... into
+// n partial sums, then warps and the CTA reduce them.
+__device__ __noinline__ void gemv_row(double* __restrict__ C, const double* __restrict__ A, int lda, bool tA,
+                                      const double* __restrict__ B, int ldb, bool tB, int n, int k, double alpha,
+                                      double beta, double* smem) {
+  constexpr int NC = 32;
+  double acc[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) acc[c] = 0.0;
+#pragma unroll 2
+  for (int kk = threadIdx.x; kk < k; kk += NT) {
+    const double a = tA ? ldcg(&A[(size_t)kk * lda]) : ldcg(&A[kk]);
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+      if (c < n) acc[c] = fma(a, tB ? ldcg(&B[(size_t)c * ldb + kk]) : ldcg(&B[(size_t)kk * ldb + c]), acc[c]);
+  }
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    if (c < n) {
+      double v = acc[c];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) smem[w * NC + c] = v;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < n) {
+    double v = 0.0;
+    for (int q = 0; q < NT / 32; ++q) v += smem[q * NC + threadIdx.x];
+    v *= alpha;
+    C[threadIdx.x] = beta != 0.0 ? ldcg(&C[threadIdx.x]) + v : v;
+  }
+  __syncthreads();
+}
+
 __device__ __forceinline__ void dev_gemm(double* __restrict__ C, int ldc, const double* __restrict__ A, int lda, bool tA,
                          const double* __restrict__ B, int ldb, bool tB, int m, int n, int k, double alpha,
                          double beta, double* smem, bool free_order = false) {
-  if (free_order && m <= 16 && n <= 16 && k >= 256)
+  if (free_order && m == 1 && n <= 32 && k >= 64)
+    gemv_row(C, A, lda, tA, B, ldb, tB, n, k, alpha, beta, smem);
+  else if (free_order && m <= 16 && n <= 16 && k >= 256)
     gemm_splitk(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
   else if (m <= 16 && n <= 16) gemm_cfg<16, 16, 1, 1, 128>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
   else if (m <= 32 && n <= 32) gemm_cfg<32, 32, 2, 2, 64>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
@@ -719,6 +758,88 @@ __device__ __noinline__ void dev_trsmrt_big(double* V, int ldv, const double* U,
   }
 }
 
+// ------------------------------------------------------------------------- TRINV / TRMV
+// Explicit inverses of a factored diagonal leaf (factor phase) and their application (solve
+// phase).  A solve then costs one triangular matrix-vector product per leaf, whose loads are
+// all independent, instead of a substitution whose steps form a chain.
+
+// Columns [c0, c0 + w) of L^-1 (upper = 0) or U^-1 (upper = 1), A = L\U (m x m, ld lda),
+// into I (the column block, m x w, ld ldi): identity columns, then the blocked sweep on the
+// sub-triangle the block needs (rows c0.. of L^-1 are the only nonzeros; rows ..c0+w of U^-1).
+__device__ __noinline__ void dev_trinv(double* I, int ldi, const double* A, int lda, int m, int w, int c0, int upper,
+                                       double* smem) {
+  for (int e = threadIdx.x; e < m * w; e += NT) {
+    const int r = e / w, j = e % w;
+    I[(size_t)r * ldi + j] = r == c0 + j ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  if (!upper) dev_trsml_big(I + (size_t)c0 * ldi, ldi, A + (size_t)c0 * lda + c0, lda, m - c0, w, smem);
+  else dev_trsmu_big(I, ldi, A, lda, c0 + w, w, smem);
+}
+
+// B[m x n] := M B, M (m x m, m <= PP_VM_TRI) lower or upper triangular.  B is staged in
+// shared memory first (so the product may overwrite it); warp w takes RU rows at a time,
+// lanes stride the columns, and every load of the RU rows is issued before the first
+// product; a warp reduction per row and right-hand side finishes the dot products.
+template <int NB, int RU>
+__device__ __noinline__ void trmv_impl(double* B, int ldb, const double* M, int ldm, int m, int n, int upper,
+                                       double* smem) {
+  double* Bs = smem;  // m x NB
+  for (int e = threadIdx.x; e < m * NB; e += NT) {
+    const int r = e / NB, q = e % NB;
+    Bs[e] = q < n ? ldcg(&B[(size_t)r * ldb + q]) : 0.0;
+  }
+  __syncthreads();
+  constexpr int TC = PP_VM_TRI / 32;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int r0 = w * RU; r0 < m; r0 += (NT / 32) * RU) {
+    double v[RU][TC];
+#pragma unroll
+    for (int u = 0; u < RU; ++u)
+#pragma unroll
+      for (int t = 0; t < TC; ++t) {
+        const int r = r0 + u, c = lane + 32 * t;
+        const bool in = r < m && c < m && (upper ? c >= r : c <= r);
+        v[u][t] = in ? ldcg(&M[(size_t)r * ldm + c]) : 0.0;
+      }
+#pragma unroll
+    for (int u = 0; u < RU; ++u) {
+      double acc[NB];
+#pragma unroll
+      for (int q = 0; q < NB; ++q) acc[q] = 0.0;
+#pragma unroll
+      for (int t = 0; t < TC; ++t) {
+        const int c = lane + 32 * t;
+        if (c < m) {
+#pragma unroll
+          for (int q = 0; q < NB; ++q) acc[q] = fma(v[u][t], Bs[c * NB + q], acc[q]);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < NB; ++q) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+      }
+      const int r = r0 + u;
+      if (lane == 0 && r < m) {
+#pragma unroll
+        for (int q = 0; q < NB; ++q)
+          if (q < n) B[(size_t)r * ldb + q] = acc[q];
+      }
+    }
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ bool dev_trmv(const pp_task& T, double* smem) {
+  const int m = T.m, n = T.n;
+  if (m > PP_VM_TRI || n < 1 || n > 16) return false;
+  if (n == 1) trmv_impl<1, 8>(T.p[0], T.ld[0], T.p[1], T.ld[1], m, n, T.ctrl, smem);
+  else if (n <= 4) trmv_impl<4, 4>(T.p[0], T.ld[0], T.p[1], T.ld[1], m, n, T.ctrl, smem);
+  else trmv_impl<16, 2>(T.p[0], T.ld[0], T.p[1], T.ld[1], m, n, T.ctrl, smem);
+  return true;
+}
+
 // ------------------------------------------------------------------------- GEMM3 / GEMM4
 // Reference association orders (kernel.cu:886-955), intermediates in task scratch.
 __device__ __noinline__ void dev_gemm3(const pp_task& T, double* smem) {
@@ -773,97 +894,255 @@ __device__ __noinline__ void dev_gemm4(const pp_task& T, double* smem) {
 }
 
 // ------------------------------------------------------------------------- ACCUM
-// One Cholesky-QR pass on Y (m x k, ld k, global scratch): G = Y^T Y (+ shift I),
-// G = R^T R, Y := Y R^-1.  A non-positive pivot marks a rank-deficient column, which is
-// zeroed.  G (k x k) goes through the global scratch `Gg`.
-__device__ __noinline__ void cholqr_pass(double* Y, int m, int k, double* Gg, bool shifted, double* smem) {
-  dev_gemm(Gg, k, Y, k, true, Y, k, false, k, k, m, 1.0, 0.0, smem, true);
-  double* G = smem;                                     // k x (PP_VM_MAX_RANK + 1)
-  double* rinv = smem + PP_VM_MAX_RANK * (PP_VM_MAX_RANK + 1);
-  constexpr int LG = PP_VM_MAX_RANK + 1;
-  for (int e = threadIdx.x; e < k * k; e += NT) G[(e / k) * LG + e % k] = ldcg(&Gg[e]);
+// U1 V1^T := Q Q^T (U1 V1^T + alpha U2 V2^T), Q spanning (U1 V1^T + alpha U2 V2^T) R:
+// the reference's randomized accumulation (kernel.cu:1255-1280) with Q from shifted
+// CholeskyQR3 (three Gram passes) in place of the reference's Givens sweeps.
+// m = ny, n = nx, k = k1 (target rank), l = k2; k1, k2 <= PP_VM_MAX_RANK.
+//   S  = R^T [V1 V2]                      (k1 x (k1 + k2), one pass over the nx rows)
+//   Y  = U1 S1^T + alpha U2 S2^T          (ny x k1, a thread per row)
+//   3x: G = Y^T Y (+ shift), G = C^T C, Y := Y C^-1
+//   P  = Y^T [U1 U2]                      (one pass over the ny rows)
+//   V1 := V1 P1^T + alpha V2 P2^T,  U1 := Y
+// Y stays in shared memory when it fits (ny k1 <= the Y capacity), else in the task's
+// global scratch.  The long reductions are warp-sliced (lanes own output columns, warps
+// own row slices) and the warp partials are combined in a fixed order, so results are
+// deterministic.
+#define ACC_LG (PP_VM_MAX_RANK + 1)
+
+template <int KB>
+struct AccumSmem {
+  static constexpr int RED = 4 * KB * 2 * KB;    // 4 partial slots of a KB x 2KB output
+  static constexpr int S = KB * 2 * KB;          // S (then P): k1 x (k1 + k2), ld 2 KB
+  static constexpr int G = KB * ACC_LG + KB;     // Gram / Cholesky factor + reciprocals
+  static constexpr int YCAP = VM_SMEM_BYTES / 8 - RED - S - G;
+};
+
+template <bool GLOBAL>
+__device__ __forceinline__ double ld_any(const double* p) {
+  if constexpr (GLOBAL) return ldcg(p);
+  else return *p;
+}
+
+// out1[a x b1] = X^T W1 and out2[a x b2] = X^T W2 (shared memory, ld ldo), X: L x a,
+// W*: L x b* (or stored transposed when tW*).  Warp w sums rows [w L/8, (w+1) L/8); lane j
+// owns column j of W1 and of W2; row l of X reaches the lanes by shuffles (XG: X in global
+// memory, read once per row by lanes i < a) or as shared-memory broadcasts.
+template <int KB, bool XG, bool WG>
+__device__ __noinline__ void accum_tn(const double* X, int lx, int a, const double* W1, int lw1, bool tW1, int b1,
+                                      const double* W2, int lw2, bool tW2, int b2, int L, double* out1,
+                                      double* out2, int ldo, double* red) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double acc1[KB], acc2[KB];
+#pragma unroll
+  for (int i = 0; i < KB; ++i) acc1[i] = acc2[i] = 0.0;
+  const int per = (L + 7) / 8, l0 = min(L, w * per), l1 = min(L, l0 + per);
+  // rows in groups of RG: every load of a group is issued before the first product, so a
+  // warp waits for one memory latency per group, not per row
+  constexpr int RG = 8;
+  for (int lb = l0; lb < l1; lb += RG) {
+    double w1[RG], w2[RG], xr[RG];
+#pragma unroll
+    for (int t = 0; t < RG; ++t) {
+      const int l = lb + t;
+      const bool in = l < l1;
+      w1[t] = in && lane < b1 ? ld_any<WG>(tW1 ? &W1[(size_t)lane * lw1 + l] : &W1[(size_t)l * lw1 + lane]) : 0.0;
+      w2[t] = in && lane < b2 ? ld_any<WG>(tW2 ? &W2[(size_t)lane * lw2 + l] : &W2[(size_t)l * lw2 + lane]) : 0.0;
+      xr[t] = 0.0;
+      if constexpr (XG) xr[t] = in && lane < a ? ldcg(&X[(size_t)l * lx + lane]) : 0.0;
+    }
+#pragma unroll
+    for (int t = 0; t < RG; ++t) {
+      const int l = lb + t;
+      if (l >= l1) break;
+#pragma unroll
+      for (int i = 0; i < KB; ++i) {
+        if (i < a) {
+          double xi;
+          if constexpr (XG) xi = __shfl_sync(0xffffffffu, xr[t], i);
+          else xi = X[(size_t)l * lx + i];
+          acc1[i] = fma(xi, w1[t], acc1[i]);
+          acc2[i] = fma(xi, w2[t], acc2[i]);
+        }
+      }
+    }
+  }
+  // warps 4..7 deposit, warps 0..3 add theirs, one thread per output adds the four slots
+  constexpr int SW = 2 * KB;  // slot row width
+  if (w >= 4) {
+#pragma unroll
+    for (int i = 0; i < KB; ++i)
+      if (i < a) {
+        if (lane < b1) red[((w - 4) * KB + i) * SW + lane] = acc1[i];
+        if (lane < b2) red[((w - 4) * KB + i) * SW + KB + lane] = acc2[i];
+      }
+  }
   __syncthreads();
-  if (threadIdx.x < 32) {  // right-looking Cholesky, one lane per column
+  if (w < 4) {
+#pragma unroll
+    for (int i = 0; i < KB; ++i)
+      if (i < a) {
+        if (lane < b1) red[(w * KB + i) * SW + lane] = acc1[i] + red[(w * KB + i) * SW + lane];
+        if (lane < b2) red[(w * KB + i) * SW + KB + lane] = acc2[i] + red[(w * KB + i) * SW + KB + lane];
+      }
+  }
+  __syncthreads();
+  const int bt = b1 + b2;
+  for (int e = threadIdx.x; e < a * bt; e += NT) {
+    const int i = e / bt, j = e % bt;
+    const int col = j < b1 ? j : KB + (j - b1);
+    const double v = red[(0 * KB + i) * SW + col] + red[(1 * KB + i) * SW + col] + red[(2 * KB + i) * SW + col] +
+                     red[(3 * KB + i) * SW + col];
+    if (j < b1) out1[i * ldo + j] = v;
+    else out2[i * ldo + (j - b1)] = v;
+  }
+  __syncthreads();
+}
+
+// Y[l][0..k) = A1[l] S1^T + alpha A2[l] S2^T for every row l (a thread per row), S1: k x c1,
+// S2: k x c2 in shared memory (ld lds).  Y may alias A1 (each row is read before written).
+template <int KB, bool YG>
+__device__ __noinline__ void accum_rows(double* Y, int ly, const double* A1, int la1, int c1, const double* A2,
+                                       int la2, bool tA2, int c2, double alpha, const double* S1,
+                                       const double* S2, int lds, int k, int L) {
+  for (int l = threadIdx.x; l < L; l += NT) {
+    double y[KB], u[KB];
+#pragma unroll
+    for (int j = 0; j < KB; ++j) u[j] = j < c1 ? ldcg(&A1[(size_t)l * la1 + j]) : 0.0;
+#pragma unroll
+    for (int i = 0; i < KB; ++i) {
+      double t = 0.0;
+      if (i < k) {
+#pragma unroll
+        for (int j = 0; j < KB; ++j)
+          if (j < c1) t = fma(u[j], S1[i * lds + j], t);
+      }
+      y[i] = t;
+    }
+#pragma unroll
+    for (int j = 0; j < KB; ++j)
+      u[j] = j < c2 ? ldcg(tA2 ? &A2[(size_t)j * la2 + l] : &A2[(size_t)l * la2 + j]) : 0.0;
+#pragma unroll
+    for (int i = 0; i < KB; ++i) {
+      if (i < k) {
+        double t = 0.0;
+#pragma unroll
+        for (int j = 0; j < KB; ++j)
+          if (j < c2) t = fma(u[j], S2[i * lds + j], t);
+        y[i] = fma(alpha, t, y[i]);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < KB; ++i)
+      if (i < k) Y[(size_t)l * ly + i] = y[i];
+  }
+}
+
+// One CholeskyQR pass on Y (m x k, ld k): G = Y^T Y (+ shift I), G = C^T C, Y := Y C^-1.
+// A non-positive pivot marks a rank-deficient column, which is zeroed.
+template <int KB, bool YG>
+__device__ __noinline__ void accum_cholqr(double* Y, int m, int k, bool shifted, double* G, double* red) {
+  double* rinv = G + KB * ACC_LG;
+  accum_tn<KB, YG, YG>(Y, k, k, Y, k, false, k, nullptr, 0, false, 0, m, G, nullptr, ACC_LG, red);
+  if (threadIdx.x < 32) {  // right-looking Cholesky: lane c holds column c of G in registers
     const int lane = threadIdx.x;
+    double g[KB];
+#pragma unroll
+    for (int j = 0; j < KB; ++j) g[j] = (j < k && lane < k) ? G[j * ACC_LG + lane] : 0.0;
     double tr = 0.0;
-    for (int j = 0; j < k; ++j) tr += G[j * LG + j];
+    for (int j = 0; j < k; ++j) tr += G[j * ACC_LG + j];
     const double tiny = 1e-28 * tr;
     if (shifted) {
       // shift of shifted CholeskyQR3: 11 (m k + k (k + 1)) u ||Y||_F^2, u = 2^-53
-      const double s = 11.0 * ((double)m * k + (double)k * (k + 1)) * 1.1102230246251565e-16 * tr;
-      if (lane < k) G[lane * LG + lane] += s;
-      __syncwarp();
+      const double sh = 11.0 * ((double)m * k + (double)k * (k + 1)) * 1.1102230246251565e-16 * tr;
+#pragma unroll
+      for (int j = 0; j < KB; ++j)
+        if (j == lane) g[j] += sh;
     }
-    for (int j = 0; j < k; ++j) {
-      const double d = G[j * LG + j];
-      const bool live = d > tiny;
-      const double rjj = live ? sqrt(d) : 0.0;
-      __syncwarp();
-      if (lane == j) { G[j * LG + j] = rjj; rinv[j] = live ? 1.0 / rjj : 0.0; }
-      if (lane > j && lane < k) G[j * LG + lane] = live ? G[j * LG + lane] / rjj : 0.0;
-      __syncwarp();
-      if (lane > j && lane < k)
-        for (int c1 = j + 1; c1 <= lane; ++c1) G[c1 * LG + lane] -= G[j * LG + c1] * G[j * LG + lane];
-      __syncwarp();
+#pragma unroll
+    for (int j = 0; j < KB; ++j) {
+      if (j < k) {
+        const double d = __shfl_sync(0xffffffffu, g[j], j);  // G[j][j]
+        const bool live = d > tiny;
+        const double rjj = live ? sqrt(d) : 0.0;
+        if (lane == j) g[j] = rjj;
+        if (lane > j) g[j] = live ? g[j] / rjj : 0.0;  // C[j][lane]
+        // G[c1][lane] -= C[j][c1] C[j][lane] for j < c1 <= lane
+#pragma unroll
+        for (int c1 = j + 1; c1 < KB; ++c1) {
+          const double cjc1 = __shfl_sync(0xffffffffu, g[j], c1);
+          if (c1 < k && lane >= c1) g[c1] = fma(-cjc1, g[j], g[c1]);
+        }
+        if (lane == j) G[KB * ACC_LG + j] = live ? 1.0 / rjj : 0.0;
+      }
     }
+#pragma unroll
+    for (int j = 0; j < KB; ++j)
+      if (j < k && lane < k) G[j * ACC_LG + lane] = g[j];
   }
   __syncthreads();
-  // Y := Y R^-1, a thread per row: x_j = (y_j - sum_{p<j} x_p r_pj) / r_jj
+  // Y := Y C^-1, a thread per row: x_j = (y_j - sum_{p<j} x_p c_pj) / c_jj
   for (int r = threadIdx.x; r < m; r += NT) {
-    double x[PP_VM_MAX_RANK];
+    double x[KB];
 #pragma unroll
-    for (int j = 0; j < PP_VM_MAX_RANK; ++j) x[j] = j < k ? ldcg(&Y[(size_t)r * k + j]) : 0.0;
+    for (int j = 0; j < KB; ++j) x[j] = j < k ? ld_any<YG>(&Y[(size_t)r * k + j]) : 0.0;
 #pragma unroll
-    for (int j = 0; j < PP_VM_MAX_RANK; ++j) {
+    for (int j = 0; j < KB; ++j) {
       if (j < k) {
         double s = x[j];
 #pragma unroll
-        for (int p = 0; p < j; ++p) s = fma(-x[p], G[p * LG + j], s);
+        for (int p = 0; p < j; ++p) s = fma(-x[p], G[p * ACC_LG + j], s);
         x[j] = s * rinv[j];
       }
     }
 #pragma unroll
-    for (int j = 0; j < PP_VM_MAX_RANK; ++j)
+    for (int j = 0; j < KB; ++j)
       if (j < k) Y[(size_t)r * k + j] = x[j];
   }
   __syncthreads();
 }
 
-// U1 V1^T := Q Q^T (U1 V1^T + alpha U2 V2^T), Q spanning (U1 V1^T + alpha U2 V2^T) R:
-// the reference's randomized accumulation (kernel.cu:1255-1280); Q from shifted
-// CholeskyQR3 (three Gram passes) in place of the reference's Givens sweeps.
-// m = ny, n = nx, k = k1 (target rank), l = k2.
-__device__ __noinline__ void dev_accum(const pp_task& T, double* smem) {
+template <int KB, bool YG>
+__device__ __forceinline__ void accum_impl(const pp_task& T, double* smem) {
+  using SM = AccumSmem<KB>;
   const int ny = T.m, nx = T.n, k1 = T.k, k2 = T.l;
   const bool tU2 = T.flags & PP_T(2), tV2 = T.flags & PP_T(3);
   double *U1 = T.p[0], *V1 = T.p[1];
   const double *U2 = T.p[2], *V2 = T.p[3], *R = T.p[4];
   const int lu1 = T.ld[0], lv1 = T.ld[1], lu2 = T.ld[2], lv2 = T.ld[3], lr = T.ld[4];
-  const int kp = max(k1, k2);
-  double* Ys = T.tmp;                // ny x k1  (becomes Q)
-  double* P = Ys + (size_t)ny * k1;  // k1 x kp
-  double* W = P + (size_t)k1 * kp;   // nx x k1
-  double* Gg = W + (size_t)nx * k1;  // k1 x k1
+  double* red = smem;
+  double* S = red + SM::RED;   // k1 x 2KB: S1 | S2, later P1 | P2
+  double* G = S + SM::S;
+  double* Y = YG ? T.tmp : G + SM::G;
   const double al = T.alpha;
-  constexpr bool fo = true;  // every product here is an intermediate of the recompression
-  dev_gemm(P, kp, R, lr, true, V1, lv1, false, k1, k1, nx, 1.0, 0.0, smem, fo);
-  dev_gemm(Ys, k1, U1, lu1, false, P, kp, true, ny, k1, k1, 1.0, 0.0, smem, fo);
-  dev_gemm(P, kp, R, lr, true, V2, lv2, tV2, k1, k2, nx, 1.0, 0.0, smem, fo);
-  dev_gemm(Ys, k1, U2, lu2, tU2, P, kp, true, ny, k1, k2, al, 1.0, smem, fo);
-  cholqr_pass(Ys, ny, k1, Gg, true, smem);
-  cholqr_pass(Ys, ny, k1, Gg, false, smem);
-  cholqr_pass(Ys, ny, k1, Gg, false, smem);
-  dev_gemm(P, kp, Ys, k1, true, U1, lu1, false, k1, k1, ny, 1.0, 0.0, smem, fo);
-  dev_gemm(W, k1, V1, lv1, false, P, kp, true, nx, k1, k1, 1.0, 0.0, smem, fo);
-  dev_gemm(P, kp, Ys, k1, true, U2, lu2, tU2, k1, k2, ny, 1.0, 0.0, smem, fo);
-  dev_gemm(W, k1, V2, lv2, tV2, P, kp, true, nx, k1, k2, al, 1.0, smem, fo);
+  constexpr int LS = 2 * KB;
+  // S1 = R^T V1, S2 = R^T V2
+  accum_tn<KB, true, true>(R, lr, k1, V1, lv1, false, k1, V2, lv2, tV2, k2, nx, S, S + KB, LS, red);
+  // Y = U1 S1^T + alpha U2 S2^T
+  accum_rows<KB, YG>(Y, k1, U1, lu1, k1, U2, lu2, tU2, k2, al, S, S + KB, LS, k1, ny);
+  __syncthreads();
+  accum_cholqr<KB, YG>(Y, ny, k1, true, G, red);
+  accum_cholqr<KB, YG>(Y, ny, k1, false, G, red);
+  accum_cholqr<KB, YG>(Y, ny, k1, false, G, red);
+  // P1 = Y^T U1, P2 = Y^T U2
+  accum_tn<KB, YG, true>(Y, k1, k1, U1, lu1, false, k1, U2, lu2, tU2, k2, ny, S, S + KB, LS, red);
+  // V1 := V1 P1^T + alpha V2 P2^T (rows read before written)
+  accum_rows<KB, false>(V1, lv1, V1, lv1, k1, V2, lv2, tV2, k2, al, S, S + KB, LS, k1, nx);
+  // U1 := Y
   for (int e = threadIdx.x; e < ny * k1; e += NT) {
     const int r = e / k1, c = e % k1;
-    U1[(size_t)r * lu1 + c] = ldcg(&Ys[e]);
+    U1[(size_t)r * lu1 + c] = ld_any<YG>(&Y[e]);
   }
-  for (int e = threadIdx.x; e < nx * k1; e += NT) {
-    const int r = e / k1, c = e % k1;
-    V1[(size_t)r * lv1 + c] = ldcg(&W[e]);
+  __syncthreads();
+}
+
+__device__ __noinline__ void dev_accum(const pp_task& T, double* smem) {
+  const int ny = T.m, k1 = T.k, k2 = T.l;
+  if (k1 <= 16 && k2 <= 16) {
+    if ((long long)ny * k1 <= AccumSmem<16>::YCAP) accum_impl<16, false>(T, smem);
+    else accum_impl<16, true>(T, smem);
+  } else {
+    if ((long long)ny * k1 <= AccumSmem<32>::YCAP) accum_impl<32, false>(T, smem);
+    else accum_impl<32, true>(T, smem);
   }
 }
 
@@ -921,12 +1200,17 @@ __device__ bool run_task(const pp_task& T, double* smem, TcCtx& tc, int& err) {
     case PP_OP_GEMM3: dev_gemm3(T, smem); return true;
     case PP_OP_GEMM4: dev_gemm4(T, smem); return true;
     case PP_OP_ACCUM:
-      if (T.k > PP_VM_MAX_RANK || T.k < 1) return false;
+      if (T.k > PP_VM_MAX_RANK || T.k < 1 || T.l > PP_VM_MAX_RANK || T.l < 0) return false;
       dev_accum(T, smem);
       return true;
     case PP_OP_SUM:
       dev_sum(T.p[0], T.ld[0], T.p[1], T.ld[1], T.m, T.n, T.k, T.beta);
       return true;
+    case PP_OP_TRINV:
+      if (T.m > PP_VM_TRI || T.n < 1 || T.o < 0 || T.o + T.n > T.m) return false;
+      dev_trinv(T.p[0], T.ld[0], T.p[1], T.ld[1], T.m, T.n, T.o, T.ctrl, smem);
+      return true;
+    case PP_OP_TRMV: return dev_trmv(T, smem);
     default: return false;
   }
 }
@@ -1106,63 +1390,102 @@ __device__ __forceinline__ double sqrt_nr(double d2) {
   y = fma(0.5 * y, e, y);
   return d2 * y;
 }
-__device__ __forceinline__ double kernel_eval_nr(int kind, double d2, double p0, double inv_p0) {
+template <int KIND>
+__device__ __forceinline__ double kernel_eval_nr(double d2, double p0, double inv_p0) {
   const double d = sqrt_nr(d2);
-  switch (kind) {
-    case 0: return rcp_nr(d + p0);
-    case 1: return rcp_nr(4.0 * 3.14159265358979323846 * (d + p0));
-    case 2: return exp(-d * inv_p0);
-    default: {
-      const double s = 1.7320508075688772 * d * inv_p0;
-      return (1.0 + s) * exp(-s);
-    }
-  }
+  if (KIND == 0) return rcp_nr(d + p0);
+  if (KIND == 1) return rcp_nr(4.0 * 3.14159265358979323846 * (d + p0));
+  if (KIND == 2) return exp(-d * inv_p0);
+  const double s = 1.7320508075688772 * d * inv_p0;
+  return (1.0 + s) * exp(-s);
 }
 
-#define KR_ROWS 128
+#define KR_THREADS 128
+#define KR_RPT 2                      /* rows per thread */
+#define KR_ROWS (KR_THREADS * KR_RPT)  /* rows per CTA */
 #define KR_COLS 256
 #define KR_SEG 512   /* columns per partial sum */
 // matrix-free partial products of r = b - A x, A_ij = K(|p_i - p_j|) (+ shift on i == j):
-// CTA (row block, column segment) sums its KR_SEG columns (staged through smem in KR_COLS
-// tiles, a thread per row) into part[seg][i]; residual_reduce adds the segments in order.
-template <int NR>
-__global__ void __launch_bounds__(KR_ROWS) kernel_residual_part(int kind, double p0, double p1, double shift,
-                                                                const double* __restrict__ pts, int dim, int n,
-                                                                const double* __restrict__ x, double* __restrict__ part,
-                                                                int nrhs) {
-  __shared__ double sp[KR_COLS * 3];
+// CTA (row block, column segment) sums its KR_SEG columns (points and x staged through smem
+// in KR_COLS tiles; each thread carries KR_RPT rows, so every staged column feeds
+// independent chains) into part[seg][i]; residual_reduce adds the segments in order.  The
+// kernel, the dimension and the right-hand-side count are compile-time parameters.
+template <int KIND, int DIM, int NR>
+__global__ void __launch_bounds__(KR_THREADS) kernel_residual_part(double p0, double shift,
+                                                                   const double* __restrict__ pts, int n,
+                                                                   const double* __restrict__ x,
+                                                                   double* __restrict__ part, int nrhs) {
+  __shared__ double sp[KR_COLS * DIM];
   __shared__ double sx[KR_COLS * NR];
-  const int i = blockIdx.x * KR_ROWS + threadIdx.x;
   const int seg = blockIdx.y, jb = seg * KR_SEG, je = min(n, jb + KR_SEG);
   const double inv_p0 = 1.0 / p0;
-  double pi[3] = {0, 0, 0};
-  if (i < n)
-    for (int d = 0; d < dim; ++d) pi[d] = pts[(size_t)i * dim + d];
-  double acc[NR];
+  int row[KR_RPT];
+  double pi[KR_RPT][DIM];
+  double acc[KR_RPT][NR];
 #pragma unroll
-  for (int q = 0; q < NR; ++q) acc[q] = 0.0;
+  for (int t = 0; t < KR_RPT; ++t) {
+    row[t] = blockIdx.x * KR_ROWS + t * KR_THREADS + threadIdx.x;
+    const int i = min(row[t], n - 1);
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) pi[t][d] = pts[(size_t)i * DIM + d];
+#pragma unroll
+    for (int q = 0; q < NR; ++q) acc[t][q] = 0.0;
+  }
   for (int j0 = jb; j0 < je; j0 += KR_COLS) {
     const int nj = min(KR_COLS, je - j0);
     __syncthreads();
-    for (int e = threadIdx.x; e < nj * dim; e += blockDim.x) sp[e] = pts[(size_t)j0 * dim + e];
-    for (int e = threadIdx.x; e < nj * nrhs; e += blockDim.x) sx[(e / nrhs) * NR + e % nrhs] = x[(size_t)j0 * nrhs + e];
+    for (int e = threadIdx.x; e < nj * DIM; e += KR_THREADS) sp[e] = pts[(size_t)j0 * DIM + e];
+    for (int e = threadIdx.x; e < nj * NR; e += KR_THREADS) {
+      const int jj = e / NR, q = e % NR;
+      sx[e] = q < nrhs ? x[(size_t)(j0 + jj) * nrhs + q] : 0.0;
+    }
     __syncthreads();
-    if (i < n)
-      for (int j = 0; j < nj; ++j) {
-        double d2 = 0.0;
-        for (int d = 0; d < dim; ++d) {
-          const double t = pi[d] - sp[j * dim + d];
-          d2 = fma(t, t, d2);
-        }
-        double a = kernel_eval_nr(kind, d2, p0, inv_p0);
-        if (j0 + j == i) a += shift;
+#pragma unroll 2
+    for (int j = 0; j < nj; ++j) {
+      double pj[DIM];
 #pragma unroll
-        for (int q = 0; q < NR; ++q)
-          if (q < nrhs) acc[q] = fma(a, sx[j * NR + q], acc[q]);
+      for (int d = 0; d < DIM; ++d) pj[d] = sp[j * DIM + d];
+#pragma unroll
+      for (int t = 0; t < KR_RPT; ++t) {
+        double d2 = 0.0;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+          const double u = pi[t][d] - pj[d];
+          d2 = fma(u, u, d2);
+        }
+        double a = kernel_eval_nr<KIND>(d2, p0, inv_p0);
+        if (j0 + j == row[t]) a += shift;
+#pragma unroll
+        for (int q = 0; q < NR; ++q) acc[t][q] = fma(a, sx[j * NR + q], acc[t][q]);
       }
+    }
   }
-  if (i < n)
-    for (int q = 0; q < nrhs; ++q) part[((size_t)seg * n + i) * nrhs + q] = acc[q];
+#pragma unroll
+  for (int t = 0; t < KR_RPT; ++t)
+    if (row[t] < n)
+      for (int q = 0; q < nrhs; ++q) part[((size_t)seg * n + row[t]) * nrhs + q] = acc[t][q];
+}
+
+template <int KIND, int DIM>
+cudaError_t launch_kernel_residual(dim3 grid, cudaStream_t s, double p0, double shift, const double* pts, int n,
+                                   const double* x, double* part, int nrhs) {
+  if (nrhs == 1)
+    kernel_residual_part<KIND, DIM, 1><<<grid, KR_THREADS, 0, s>>>(p0, shift, pts, n, x, part, nrhs);
+  else if (nrhs <= 4)
+    kernel_residual_part<KIND, DIM, 4><<<grid, KR_THREADS, 0, s>>>(p0, shift, pts, n, x, part, nrhs);
+  else if (nrhs <= 8)
+    kernel_residual_part<KIND, DIM, 8><<<grid, KR_THREADS, 0, s>>>(p0, shift, pts, n, x, part, nrhs);
+  else
+    kernel_residual_part<KIND, DIM, 16><<<grid, KR_THREADS, 0, s>>>(p0, shift, pts, n, x, part, nrhs);
+  return cudaGetLastError();
+}
+
+template <int KIND>
+cudaError_t launch_kernel_residual_dim(int dim, dim3 grid, cudaStream_t s, double p0, double shift, const double* pts,
+                                       int n, const double* x, double* part, int nrhs) {
+  if (dim == 1) return launch_kernel_residual<KIND, 1>(grid, s, p0, shift, pts, n, x, part, nrhs);
+  if (dim == 2) return launch_kernel_residual<KIND, 2>(grid, s, p0, shift, pts, n, x, part, nrhs);
+  return launch_kernel_residual<KIND, 3>(grid, s, p0, shift, pts, n, x, part, nrhs);
 }
 
 __global__ void residual_reduce(const double* __restrict__ part, int segs, int n, int nrhs,
@@ -1221,7 +1544,10 @@ int pp_vm_blocks_per_sm() {
 }
 
 cudaError_t pp_vm_prepare() {
-  return cudaFuncSetAttribute(vm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pp_vm_smem_bytes());
+  cudaError_t e = cudaFuncSetAttribute(vm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pp_vm_smem_bytes());
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(accum_noalloc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)pp_vm_smem_bytes());
 }
 
 cudaError_t pp_vm_run(const pp_vm_launch& L, cudaStream_t s) {
@@ -1244,13 +1570,18 @@ cudaError_t pp_dense_residual(const double* A, int lda, int n, const double* x, 
 cudaError_t pp_kernel_residual(int kernel, double p0, double p1, double diag_shift, const double* pts, int dim, int n,
                                const double* x, const double* b, double* r, int nrhs, double* part,
                                cudaStream_t s) {
-  if (dim < 1 || dim > 3 || nrhs < 1 || nrhs > 16 || !part) return cudaErrorInvalidValue;
+  (void)p1;
+  if (dim < 1 || dim > 3 || nrhs < 1 || nrhs > 16 || !part || kernel < 0 || kernel > 3) return cudaErrorInvalidValue;
   const int segs = (n + KR_SEG - 1) / KR_SEG;
   const dim3 grid((n + KR_ROWS - 1) / KR_ROWS, segs);
-  if (nrhs <= 4)
-    kernel_residual_part<4><<<grid, KR_ROWS, 0, s>>>(kernel, p0, p1, diag_shift, pts, dim, n, x, part, nrhs);
-  else
-    kernel_residual_part<16><<<grid, KR_ROWS, 0, s>>>(kernel, p0, p1, diag_shift, pts, dim, n, x, part, nrhs);
+  cudaError_t e;
+  switch (kernel) {
+    case 0: e = launch_kernel_residual_dim<0>(dim, grid, s, p0, diag_shift, pts, n, x, part, nrhs); break;
+    case 1: e = launch_kernel_residual_dim<1>(dim, grid, s, p0, diag_shift, pts, n, x, part, nrhs); break;
+    case 2: e = launch_kernel_residual_dim<2>(dim, grid, s, p0, diag_shift, pts, n, x, part, nrhs); break;
+    default: e = launch_kernel_residual_dim<3>(dim, grid, s, p0, diag_shift, pts, n, x, part, nrhs); break;
+  }
+  if (e != cudaSuccess) return e;
   const size_t total = (size_t)n * nrhs;
   residual_reduce<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(part, segs, n, nrhs, b, r);
   return cudaGetLastError();
