@@ -150,6 +150,58 @@ pp_status pp_batch_sync(pp_batch* b, void* stream);
 pp_status pp_batch_program_info(pp_batch* b, int which, int nrhs, pp_program_info* info);
 pp_status pp_batch_trace(pp_batch* b, int which, int nrhs, int enable, uint64_t* out);
 
+/* --- serving: a request loop with continuous admission (no reference counterpart; the
+ *     reference factors one matrix per launch) -------------------------------------------
+ * A server owns a worker thread.  Factor + solve requests of any size are admitted in arrival
+ * order while in-flight slots and the HBM budget allow (a smaller later request may pass a
+ * larger waiting one); each admitted request runs on its own CUDA stream with a persistent
+ * grid of a slot's share of the SMs, so requests that arrive while others are on the GPU
+ * overlap with them.  A request keeps its factors on the device for all of its right-hand-side
+ * sets (the first solve and its follow-ups), refines each set in FP64 (matrix-free kernel
+ * residual) until the normwise backward error ||r||_inf / (||A||_inf ||x||_inf + ||b||_inf)
+ * meets `tol`, writes the solutions to the caller's host buffer and frees its device memory
+ * (stream-ordered, so retiring one request never waits for the others).  While a server
+ * runs, its context is used only through the server's calls. */
+typedef struct pp_server pp_server;
+typedef struct pp_serve_config {
+  long long hbm_budget_bytes;  /* device bytes the admitted requests may hold together        */
+  int max_inflight;            /* requests on the device at once (slots)                      */
+  int grid_per_request;        /* persistent CTAs per request launch (0: SMs / slots)          */
+} pp_serve_config;
+typedef struct pp_request_desc {
+  int kernel;              /* matrix entries, as pp_kernel_residual_dev: 0 1/(r+p0), 1 Laplace,
+                              2 exp(-r/p0), 3 Matern-3/2 (length p0)                            */
+  double p0, shift;        /* kernel parameter and diagonal shift                             */
+  double norm_inf;         /* ||A||_inf (backward-error normalisation)                        */
+  int dim;                 /* point dimension (1..3)                                          */
+  const double* points;    /* n x dim host points in the H-matrix's cluster order (copied)    */
+  const double* rhs;       /* n_sets blocks of n x nrhs host right-hand sides (copied)        */
+  int nrhs, n_sets;        /* 1 <= nrhs <= 16; n_sets >= 1 (the first solve + follow-ups)      */
+  double tol;              /* backward-error target of every set                              */
+  int max_iter;            /* refinement solves per set at most                               */
+  double* x_out;           /* n_sets blocks of n x nrhs host solutions; must stay valid until
+                              the request is done or failed                                   */
+} pp_request_desc;
+typedef struct pp_request_stats {
+  int status;              /* 0 queued, 1 running, 2 done, 3 failed                            */
+  int iterations;          /* refinement solves over all sets                                 */
+  double backward_error;   /* worst final backward error over the finished sets               */
+  double t_submit_ms, t_admit_ms, t_done_ms;  /* server clock (ms); -1 until reached          */
+  long long device_bytes;  /* device memory the request holds while admitted                  */
+  char message[128];       /* why a request failed                                            */
+} pp_request_stats;
+pp_status pp_server_create(pp_context* ctx, const pp_serve_config* cfg, pp_server** out);
+/* queues a request; the server takes ownership of h (built and filled, not uploaded) and
+ * destroys it when the request retires.  Returns PP_OOM when the request alone exceeds the
+ * budget. */
+pp_status pp_server_submit(pp_server* s, pp_hmatrix* h, const pp_request_desc* d, long long* id);
+pp_status pp_server_poll(pp_server* s, long long id, pp_request_stats* st);
+/* waits until no request is queued or running (PP_TIMEOUT after timeout_ms) */
+pp_status pp_server_wait_all(pp_server* s, double timeout_ms);
+double pp_server_clock_ms(pp_server* s);
+/* lets the queued and running requests finish, then stops the worker */
+void pp_server_destroy(pp_server* s);
+
 /* --- residuals (FP64 refinement) ----------------------------------------- */
 /* r := b - A x, A dense row-major (device); x, b, r device n x nrhs */
 pp_status pp_dense_residual_dev(pp_context* ctx, const double* A, int lda, int n, const double* x, const double* b,

@@ -59,6 +59,22 @@ class _BlockInfo(C.Structure):
                 ("rank", C.c_int), ("kmax", C.c_int), ("level", C.c_int), ("children", C.c_int * 4)]
 
 
+class _ServeConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_longlong), ("max_inflight", C.c_int), ("grid_per_request", C.c_int)]
+
+
+class _RequestDesc(C.Structure):
+    _fields_ = [("kernel", C.c_int), ("p0", C.c_double), ("shift", C.c_double), ("norm_inf", C.c_double),
+                ("dim", C.c_int), ("points", C.c_void_p), ("rhs", C.c_void_p), ("nrhs", C.c_int),
+                ("n_sets", C.c_int), ("tol", C.c_double), ("max_iter", C.c_int), ("x_out", C.c_void_p)]
+
+
+class _RequestStats(C.Structure):
+    _fields_ = [("status", C.c_int), ("iterations", C.c_int), ("backward_error", C.c_double),
+                ("t_submit_ms", C.c_double), ("t_admit_ms", C.c_double), ("t_done_ms", C.c_double),
+                ("device_bytes", C.c_longlong), ("message", C.c_char * 128)]
+
+
 class _ProgramInfo(C.Structure):
     _fields_ = [("n_tasks", C.c_int), ("n_edges", C.c_longlong), ("flops", C.c_longlong),
                 ("op_count", C.c_longlong * 16), ("arena_elems", C.c_longlong * 5), ("host_build_ms", C.c_double)]
@@ -123,6 +139,12 @@ def lib():
             "pp_batch_program_info": (i, [vp, i, i, C.POINTER(_ProgramInfo)]),
             "pp_batch_trace": (i, [vp, i, i, i, vp]),
             "pp_refstream_encode": (i, [vp, i, vp, ll, vp, C.POINTER(ll)]),
+            "pp_server_create": (i, [vp, C.POINTER(_ServeConfig), C.POINTER(vp)]),
+            "pp_server_submit": (i, [vp, vp, C.POINTER(_RequestDesc), C.POINTER(ll)]),
+            "pp_server_poll": (i, [vp, ll, C.POINTER(_RequestStats)]),
+            "pp_server_wait_all": (i, [vp, d]),
+            "pp_server_clock_ms": (d, [vp]),
+            "pp_server_destroy": (None, [vp]),
             "pp_hmatrix_set_precision": (i, [vp, i]),
             "pp_hmatrix_get_precision": (i, [vp]),
         }
@@ -501,6 +523,68 @@ class BatchRefiner:
             if e <= tol:
                 break
         return xs, hist
+
+
+SERVE_STATUS = ["queued", "running", "done", "failed"]
+
+
+class Server:
+    """Request loop with continuous admission (C++ worker thread in the library; no reference
+    counterpart).  submit() hands over an H-matrix (built and filled, not uploaded) with its
+    kernel problem and one or more right-hand-side sets; the server admits requests by HBM
+    budget and free slots, runs each on its own stream (their work overlaps on the device),
+    keeps the factors resident for the request's follow-up sets and refines every set in FP64
+    to `tol`."""
+
+    def __init__(self, ctx, hbm_budget_bytes, max_inflight=4, grid_per_request=0):
+        cfg = _ServeConfig(int(hbm_budget_bytes), int(max_inflight), int(grid_per_request))
+        h = C.c_void_p()
+        ctx.check(lib().pp_server_create(ctx.handle, C.byref(cfg), C.byref(h)), "server_create")
+        self.ctx, self._h = ctx, h
+        self._bufs = {}
+
+    def __del__(self):
+        self.close()
+
+    def close(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.pp_server_destroy(self._h)
+            self._h = None
+
+    def clock_ms(self):
+        return lib().pp_server_clock_ms(self._h)
+
+    def submit(self, h, prob, rhs_sets, tol=1e-10, max_iter=30):
+        """rhs_sets: (n_sets, n, nrhs) array; returns the request id.  h is owned by the
+        server from here on."""
+        rhs_sets = np.ascontiguousarray(rhs_sets, dtype=np.float64)
+        if rhs_sets.ndim == 2:
+            rhs_sets = rhs_sets[None]
+        n_sets, n, nrhs = rhs_sets.shape
+        pts = np.ascontiguousarray(prob.points, dtype=np.float64)
+        x = np.zeros_like(rhs_sets)
+        d = _RequestDesc(int(prob.kernel), float(prob.p0), float(prob.shift), float(prob.norm_inf), int(prob.dim),
+                         pts.ctypes.data, rhs_sets.ctypes.data, int(nrhs), int(n_sets), float(tol), int(max_iter),
+                         x.ctypes.data)
+        rid = C.c_longlong()
+        self.ctx.check(lib().pp_server_submit(self._h, h.handle, C.byref(d), C.byref(rid)), "server_submit")
+        h._h = None  # ownership moved to the server
+        self._bufs[rid.value] = (x, rhs_sets, pts)
+        return rid.value
+
+    def poll(self, rid):
+        st = _RequestStats()
+        self.ctx.check(lib().pp_server_poll(self._h, int(rid), C.byref(st)), "server_poll")
+        return dict(status=SERVE_STATUS[st.status], iterations=st.iterations, backward_error=st.backward_error,
+                    t_submit_ms=st.t_submit_ms, t_admit_ms=st.t_admit_ms, t_done_ms=st.t_done_ms,
+                    device_bytes=st.device_bytes, message=st.message.decode(errors="replace"))
+
+    def result(self, rid):
+        """(n_sets, n, nrhs) solutions (valid once the request is done)."""
+        return self._bufs[rid][0]
+
+    def wait_all(self, timeout_ms=600000.0):
+        self.ctx.check(lib().pp_server_wait_all(self._h, float(timeout_ms)), "server_wait_all")
 
 
 def dev_hierarchical_GETRF(h, num_blocks=0, num_threads=0, kernel_size=0):

@@ -1,9 +1,16 @@
 // capi.cpp — extern "C" boundary of the engine (include/pastel_palettes.h).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstdio>
 #include <cstring>
+#include <deque>
 #include <map>
+#include <mutex>
+#include <thread>
 #include <memory>
 #include <new>
 #include <stdexcept>
@@ -44,10 +51,19 @@ struct VmPlan {
   int use_tc = 0;  // holds TF32 contractions (tensor memory per CTA)
   unsigned long long* d_trace = nullptr;  // per-task (start, end, sm | cta << 32) when tracing
   std::vector<int64_t> work_off, scratch_off, rhs_off;  // per instance (batched plans)
+  // stream-ordered memory (cudaMallocAsync / cudaFreeAsync on `astream`) for plans of a
+  // served request, so that allocating or freeing never waits for other streams' work
+  cudaStream_t astream = nullptr;
+  bool async_mem = false;
+  void dfree(void* p) {
+    if (!p) return;
+    if (async_mem) cudaFreeAsync(p, astream);
+    else cudaFree(p);
+  }
   void release() {
-    cudaFree(d_tasks); cudaFree(d_succ); cudaFree(d_indeg); cudaFree(d_ready); cudaFree(d_counters);
-    cudaFree(d_slots); cudaFree(d_state); cudaFree(d_work); cudaFree(d_scratch); cudaFree(d_rhs);
-    cudaFree(d_trace);
+    dfree(d_tasks); dfree(d_succ); dfree(d_indeg); dfree(d_ready); dfree(d_counters);
+    dfree(d_slots); dfree(d_state); dfree(d_work); dfree(d_scratch); dfree(d_rhs);
+    dfree(d_trace);
     d_tasks = nullptr; d_succ = d_indeg = d_ready = d_counters = d_slots = nullptr; d_state = nullptr;
     d_work = d_scratch = d_rhs = nullptr;
     d_trace = nullptr;
@@ -76,13 +92,39 @@ struct pp_hmatrix {
   VmPlan factor;
   std::map<int, std::unique_ptr<VmPlan>> solves;
   VmPlan* last = nullptr;
+  // stream-ordered memory mode (set by the server for the requests it owns)
+  cudaStream_t astream = nullptr;
+  bool async_mem = false;
+  cudaError_t dalloc(void** p, size_t bytes) {
+    bytes = bytes ? bytes : 8;
+    return async_mem ? cudaMallocAsync(p, bytes, astream) : cudaMalloc(p, bytes);
+  }
+  void dfree(void* p) {
+    if (!p) return;
+    if (async_mem) cudaFreeAsync(p, astream);
+    else cudaFree(p);
+  }
+  cudaError_t h2d(void* dst, const void* src, size_t bytes) {
+    return async_mem ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, astream)
+                     : cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+  }
+  void set_async(cudaStream_t s) {
+    async_mem = true;
+    astream = s;
+    factor.async_mem = true;
+    factor.astream = s;
+    for (auto& kv : solves) {
+      kv.second->async_mem = true;
+      kv.second->astream = s;
+    }
+  }
   ~pp_hmatrix() {
     factor.release();
     for (auto& kv : solves) kv.second->release();
     if (pinned) cudaHostUnregister(H->host.data());
-    cudaFree(d_arena);
-    cudaFree(d_orig);
-    cudaFree(d_rand);
+    dfree(d_arena);
+    dfree(d_orig);
+    dfree(d_rand);
   }
 };
 
@@ -157,7 +199,14 @@ pp_status plan_to_device_multi(pp_context* ctx, const std::vector<pp_hmatrix*>& 
   if ((int)insts.size() != plan.prog.n_instances) return fail(ctx, PP_INTERNAL, "instance count mismatch");
   auto t0 = std::chrono::steady_clock::now();
   const int n = plan.n_tasks;
-  auto alloc = [&](void** p, size_t bytes) { return cudaMalloc(p, bytes ? bytes : 8); };
+  auto alloc = [&](void** p, size_t bytes) {
+    bytes = bytes ? bytes : 8;
+    return plan.async_mem ? cudaMallocAsync(p, bytes, plan.astream) : cudaMalloc(p, bytes);
+  };
+  auto h2d = [&](void* dst, const void* src, size_t bytes) {
+    return plan.async_mem ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, plan.astream)
+                          : cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
+  };
   const int ni = (int)insts.size();
   plan.work_off.assign(ni, 0);
   plan.scratch_off.assign(ni, 0);
@@ -198,11 +247,12 @@ pp_status plan_to_device_multi(pp_context* ctx, const std::vector<pp_hmatrix*>& 
   PP_CUDA(alloc((void**)&plan.d_counters, sizeof(int32_t) * n));
   PP_CUDA(alloc((void**)&plan.d_slots, sizeof(int32_t) * n));
   PP_CUDA(alloc((void**)&plan.d_state, sizeof(pp_vm_state)));
-  PP_CUDA(cudaMemcpy(plan.d_tasks, tasks.data(), sizeof(pp_task) * n, cudaMemcpyHostToDevice));
-  if (!succ.empty()) PP_CUDA(cudaMemcpy(plan.d_succ, succ.data(), sizeof(int32_t) * succ.size(), cudaMemcpyHostToDevice));
-  PP_CUDA(cudaMemcpy(plan.d_indeg, indeg.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice));
-  if (!ready.empty()) PP_CUDA(cudaMemcpy(plan.d_ready, ready.data(), sizeof(int32_t) * ready.size(), cudaMemcpyHostToDevice));
-  PP_CUDA(cudaMemset(plan.d_state, 0, sizeof(pp_vm_state)));
+  PP_CUDA(h2d(plan.d_tasks, tasks.data(), sizeof(pp_task) * n));
+  if (!succ.empty()) PP_CUDA(h2d(plan.d_succ, succ.data(), sizeof(int32_t) * succ.size()));
+  PP_CUDA(h2d(plan.d_indeg, indeg.data(), sizeof(int32_t) * n));
+  if (!ready.empty()) PP_CUDA(h2d(plan.d_ready, ready.data(), sizeof(int32_t) * ready.size()));
+  if (plan.async_mem) PP_CUDA(cudaMemsetAsync(plan.d_state, 0, sizeof(pp_vm_state), plan.astream));
+  else PP_CUDA(cudaMemset(plan.d_state, 0, sizeof(pp_vm_state)));
   const int per_sm = ctx->cfg.ctas_per_sm > 0 ? std::min(ctx->cfg.ctas_per_sm, ctx->blocks_per_sm) : ctx->blocks_per_sm;
   plan.grid = std::max(1, std::min(n, ctx->sm_count * std::max(1, per_sm)));
   plan.on_device = true;
@@ -387,7 +437,7 @@ pp_status pp_hmatrix_upload(pp_hmatrix* h, void* stream) {
   pp_context* ctx = h->ctx;
   if (!has_device(ctx)) return fail(ctx, PP_CUDA_ERROR, "no CUDA device in this context");
   const size_t bytes = sizeof(double) * (size_t)std::max<int64_t>(h->H->arena_elems, 1);
-  if (!h->d_arena) PP_CUDA(cudaMalloc((void**)&h->d_arena, bytes));
+  if (!h->d_arena) PP_CUDA(h->dalloc((void**)&h->d_arena, bytes));
   PP_CUDA(cudaMemcpyAsync(h->d_arena, h->H->host.data(), sizeof(double) * h->H->block_elems, cudaMemcpyHostToDevice,
                           (cudaStream_t)stream));
   // the random sketch depends on the factor program's arena sizes
@@ -395,8 +445,8 @@ pp_status pp_hmatrix_upload(pp_hmatrix* h, void* stream) {
   if (st != PP_OK) return st;
   if (!h->d_rand) {
     make_rand(h);
-    PP_CUDA(cudaMalloc((void**)&h->d_rand, sizeof(double) * std::max<size_t>(h->rand_host.size(), 1)));
-    PP_CUDA(cudaMemcpy(h->d_rand, h->rand_host.data(), sizeof(double) * h->rand_host.size(), cudaMemcpyHostToDevice));
+    PP_CUDA(h->dalloc((void**)&h->d_rand, sizeof(double) * std::max<size_t>(h->rand_host.size(), 1)));
+    PP_CUDA(h->h2d(h->d_rand, h->rand_host.data(), sizeof(double) * h->rand_host.size()));
   }
   return PP_OK;
 }
@@ -426,7 +476,7 @@ pp_status pp_hmatrix_keep_original(pp_hmatrix* h, void* stream) {
   pp_context* ctx = h->ctx;
   if (!h->d_arena) return fail(ctx, PP_INVALID_ARG, "H-matrix not uploaded");
   const size_t bytes = sizeof(double) * (size_t)h->H->block_elems;
-  if (!h->d_orig) PP_CUDA(cudaMalloc((void**)&h->d_orig, std::max<size_t>(bytes, 8)));
+  if (!h->d_orig) PP_CUDA(h->dalloc((void**)&h->d_orig, std::max<size_t>(bytes, 8)));
   PP_CUDA(cudaMemcpyAsync(h->d_orig, h->d_arena, bytes, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
   return PP_OK;
 }
@@ -484,6 +534,8 @@ static VmPlan* solve_plan(pp_hmatrix* h, int nrhs) {
   auto it = h->solves.find(nrhs);
   if (it != h->solves.end()) return it->second.get();
   auto p = std::make_unique<VmPlan>();
+  p->async_mem = h->async_mem;
+  p->astream = h->astream;
   VmPlan* raw = p.get();
   h->solves.emplace(nrhs, std::move(p));
   return raw;
@@ -909,6 +961,341 @@ pp_status pp_batch_trace(pp_batch* b, int which, int nrhs, int enable, uint64_t*
     PP_CUDA(cudaMemset(plan->d_trace, 0, bytes));
   }
   return PP_OK;
+}
+
+}  // extern "C"
+
+// ----------------------------------------------------------------------------- serving
+// A request loop over one context: factor + solve jobs of different sizes are admitted in
+// arrival order as in-flight slots and the HBM budget allow (a later, smaller job may pass a
+// waiting larger one); every admitted job runs on its own stream with a persistent grid of
+// a slot's share of the SMs, so the work of several jobs overlaps on the device.  A job
+// keeps its factors resident for its follow-up right-hand-side sets and refines each set in
+// FP64 until the normwise backward error meets its tolerance.  Its memory is stream-ordered
+// (cudaMallocAsync / cudaFreeAsync), so admitting or retiring a job never waits for the
+// others.  No reference counterpart (the reference factors one matrix per launch).
+namespace {
+
+enum ServeState { SRV_QUEUED = 0, SRV_RUNNING = 1, SRV_DONE = 2, SRV_FAILED = 3 };
+
+struct ServeRequest {
+  long long id = 0;
+  pp_hmatrix* h = nullptr;  // owned from submission
+  int n = 0, dim = 0, kernel = 0, nrhs = 0, n_sets = 0, max_iter = 0;
+  double p0 = 0, shift = 0, norm_inf = 0, tol = 0;
+  std::vector<double> pts, rhs;
+  double* x_out = nullptr;  // caller's host buffer
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev = nullptr;
+  double *d_pts = nullptr, *d_b = nullptr, *d_x = nullptr, *d_r = nullptr, *d_dx = nullptr, *d_part = nullptr;
+  unsigned long long* d_norms = nullptr;
+  long long bytes = 0;
+  int state = SRV_QUEUED;
+  int set = 0, iters_set = 0, iters_total = 0;
+  double bmax = 0, worst = 0;
+  double t_submit = 0, t_admit = -1, t_done = -1;
+  std::string err;
+};
+
+}  // namespace
+
+struct pp_server {
+  pp_context* ctx = nullptr;
+  long long budget = 0;
+  int slots = 1, grid = 0;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::thread worker;
+  bool stop = false;
+  std::deque<ServeRequest*> queue;
+  std::vector<ServeRequest*> active;
+  std::map<long long, std::unique_ptr<ServeRequest>> all;
+  long long next_id = 1, used = 0;
+  std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+  double now_ms() const {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  }
+  void run();
+  bool start(ServeRequest* q);
+  bool iterate(ServeRequest* q);
+  bool start_set(ServeRequest* q);
+  bool advance(ServeRequest* q);
+  void retire(ServeRequest* q, bool ok);
+};
+
+namespace {
+
+bool srv_check(ServeRequest* q, cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return true;
+  q->err = std::string(what) + ": " + cudaGetErrorString(e);
+  return false;
+}
+
+bool srv_status(ServeRequest* q, pp_status st, pp_context* ctx, const char* what) {
+  if (st == PP_OK) return true;
+  q->err = std::string(what) + ": " + ctx->err;
+  return false;
+}
+
+}  // namespace
+
+bool pp_server::start(ServeRequest* q) {
+  pp_hmatrix* h = q->h;
+  if (!srv_check(q, cudaStreamCreateWithFlags(&q->stream, cudaStreamNonBlocking), "stream")) return false;
+  if (!srv_check(q, cudaEventCreateWithFlags(&q->ev, cudaEventDisableTiming), "event")) return false;
+  h->set_async(q->stream);
+  const size_t vec = sizeof(double) * (size_t)q->n * q->nrhs;
+  if (!srv_check(q, h->dalloc((void**)&q->d_pts, sizeof(double) * q->pts.size()), "alloc")) return false;
+  for (double** p : {&q->d_b, &q->d_x, &q->d_r, &q->d_dx})
+    if (!srv_check(q, h->dalloc((void**)p, vec), "alloc")) return false;
+  if (!srv_check(q, h->dalloc((void**)&q->d_part, sizeof(double) * pp_kernel_residual_part_elems(q->n, q->nrhs)),
+                 "alloc"))
+    return false;
+  if (!srv_check(q, h->dalloc((void**)&q->d_norms, 2 * sizeof(unsigned long long)), "alloc")) return false;
+  if (!srv_check(q, cudaMemcpyAsync(q->d_pts, q->pts.data(), sizeof(double) * q->pts.size(), cudaMemcpyHostToDevice,
+                                    q->stream), "points"))
+    return false;
+  if (!srv_status(q, pp_hmatrix_upload(h, q->stream), ctx, "upload")) return false;
+  if (!srv_status(q, plan_to_device(h, h->factor), ctx, "factor plan")) return false;
+  if (!srv_status(q, launch_plan(h, h->factor, q->stream, grid), ctx, "factor")) return false;
+  return start_set(q);
+}
+
+bool pp_server::start_set(ServeRequest* q) {
+  const size_t cnt = (size_t)q->n * q->nrhs, vec = sizeof(double) * cnt;
+  const double* b = q->rhs.data() + (size_t)q->set * cnt;
+  q->bmax = 0;
+  for (size_t e = 0; e < cnt; ++e) q->bmax = std::max(q->bmax, std::fabs(b[e]));
+  q->iters_set = 0;
+  if (!srv_check(q, cudaMemcpyAsync(q->d_b, b, vec, cudaMemcpyHostToDevice, q->stream), "rhs")) return false;
+  if (!srv_check(q, cudaMemcpyAsync(q->d_r, q->d_b, vec, cudaMemcpyDeviceToDevice, q->stream), "rhs")) return false;
+  if (!srv_check(q, cudaMemsetAsync(q->d_x, 0, vec, q->stream), "x")) return false;
+  return iterate(q);
+}
+
+// one refinement step: dx = (LU)^-1 r, x += dx, r = b - A x (FP64, matrix-free), norms
+bool pp_server::iterate(ServeRequest* q) {
+  pp_hmatrix* h = q->h;
+  const size_t cnt = (size_t)q->n * q->nrhs;
+  VmPlan* plan = solve_plan(h, q->nrhs);
+  if (!srv_status(q, build_program(h, 1, q->nrhs, *plan), ctx, "solve program")) return false;
+  if (!srv_status(q, plan_to_device(h, *plan), ctx, "solve plan")) return false;
+  if (!srv_check(q, cudaMemcpyAsync(plan->d_rhs, q->d_r, sizeof(double) * cnt, cudaMemcpyDeviceToDevice, q->stream),
+                 "solve"))
+    return false;
+  if (!srv_status(q, launch_plan(h, *plan, q->stream, grid), ctx, "solve")) return false;
+  if (!srv_check(q, pp_axpy(q->d_x, plan->d_rhs, cnt, q->stream), "update")) return false;
+  if (!srv_check(q, pp_kernel_residual(q->kernel, q->p0, 0.0, q->shift, q->d_pts, q->dim, q->n, q->d_x, q->d_b,
+                                       q->d_r, q->nrhs, q->d_part, q->stream), "residual"))
+    return false;
+  if (!srv_check(q, pp_absmax2(q->d_x, q->d_r, cnt, q->d_norms, q->stream), "norms")) return false;
+  if (!srv_check(q, cudaEventRecord(q->ev, q->stream), "event")) return false;
+  ++q->iters_set;
+  ++q->iters_total;
+  return true;
+}
+
+// returns true when the request made progress (its last step finished on the device)
+bool pp_server::advance(ServeRequest* q) {
+  if (cudaEventQuery(q->ev) != cudaSuccess) return false;
+  unsigned long long nb[2];
+  pp_vm_state vs, vf;
+  VmPlan* plan = solve_plan(q->h, q->nrhs);
+  bool ok = srv_check(q, cudaMemcpyAsync(nb, q->d_norms, sizeof(nb), cudaMemcpyDeviceToHost, q->stream), "norms") &&
+            srv_check(q, cudaMemcpyAsync(&vs, plan->d_state, sizeof(vs), cudaMemcpyDeviceToHost, q->stream), "state") &&
+            srv_check(q, cudaMemcpyAsync(&vf, q->h->factor.d_state, sizeof(vf), cudaMemcpyDeviceToHost, q->stream),
+                      "state") &&
+            srv_check(q, cudaStreamSynchronize(q->stream), "sync");
+  if (ok && (vs.error || vf.error)) {
+    q->err = "VM error " + std::to_string(vf.error ? vf.error : vs.error) + (vf.error ? " in the factorization" : " in a solve");
+    ok = false;
+  }
+  if (!ok) {
+    retire(q, false);
+    return true;
+  }
+  double xmax, rmax;
+  std::memcpy(&xmax, &nb[0], sizeof(double));
+  std::memcpy(&rmax, &nb[1], sizeof(double));
+  const double err = rmax / (q->norm_inf * xmax + q->bmax);
+  if (!(err <= q->tol) && q->iters_set < q->max_iter) {
+    if (!iterate(q)) retire(q, false);
+    return true;
+  }
+  q->worst = std::max(q->worst, err);
+  const size_t cnt = (size_t)q->n * q->nrhs;
+  ok = srv_check(q, cudaMemcpyAsync(q->x_out + (size_t)q->set * cnt, q->d_x, sizeof(double) * cnt,
+                                    cudaMemcpyDeviceToHost, q->stream), "result") &&
+       srv_check(q, cudaStreamSynchronize(q->stream), "sync");
+  if (!ok || !(err <= q->tol)) {
+    if (ok) q->err = "refinement did not reach the tolerance";
+    retire(q, false);
+    return true;
+  }
+  if (++q->set < q->n_sets) {
+    if (!start_set(q)) retire(q, false);
+    return true;
+  }
+  retire(q, true);
+  return true;
+}
+
+void pp_server::retire(ServeRequest* q, bool ok) {
+  pp_hmatrix* h = q->h;
+  for (void* p : {(void*)q->d_pts, (void*)q->d_b, (void*)q->d_x, (void*)q->d_r, (void*)q->d_dx, (void*)q->d_part,
+                  (void*)q->d_norms})
+    h->dfree(p);
+  pp_hmatrix_destroy(h);  // stream-ordered frees of the arena and the plans
+  q->h = nullptr;
+  if (q->ev) cudaEventDestroy(q->ev);
+  if (q->stream) cudaStreamDestroy(q->stream);  // resources go when the queued frees have run
+  q->ev = nullptr;
+  q->stream = nullptr;
+  q->state = ok ? SRV_DONE : SRV_FAILED;
+  q->t_done = now_ms();
+  used -= q->bytes;
+}
+
+void pp_server::run() {
+  cudaSetDevice(ctx->device);
+  std::unique_lock<std::mutex> lk(mu);
+  for (;;) {
+    if (stop && queue.empty() && active.empty()) break;
+    for (auto it = queue.begin(); it != queue.end() && (int)active.size() < slots;) {
+      ServeRequest* q = *it;
+      if (used + q->bytes > budget) {
+        ++it;
+        continue;
+      }
+      it = queue.erase(it);
+      used += q->bytes;
+      q->state = SRV_RUNNING;
+      q->t_admit = now_ms();
+      active.push_back(q);
+      if (!start(q)) retire(q, false);
+    }
+    bool progressed = false;
+    for (ServeRequest* q : active)
+      if (q->state == SRV_RUNNING) progressed |= advance(q);
+    active.erase(std::remove_if(active.begin(), active.end(), [](ServeRequest* q) { return q->state != SRV_RUNNING; }),
+                 active.end());
+    if (!progressed) cv.wait_for(lk, std::chrono::microseconds(50));
+  }
+}
+
+extern "C" {
+
+pp_status pp_server_create(pp_context* ctx, const pp_serve_config* cfg, pp_server** out) {
+  if (!ctx || !cfg || !out) return PP_INVALID_ARG;
+  if (!has_device(ctx)) return fail(ctx, PP_CUDA_ERROR, "no CUDA device in this context");
+  if (cfg->hbm_budget_bytes <= 0 || cfg->max_inflight <= 0)
+    return fail(ctx, PP_INVALID_ARG, "pp_server_create: budget and slots must be positive");
+  auto* s = new (std::nothrow) pp_server();
+  if (!s) return PP_OOM;
+  s->ctx = ctx;
+  s->budget = cfg->hbm_budget_bytes;
+  s->slots = cfg->max_inflight;
+  s->grid = cfg->grid_per_request > 0 ? cfg->grid_per_request
+                                      : std::max(8, ctx->sm_count * std::max(1, ctx->blocks_per_sm) / s->slots);
+  s->worker = std::thread([s] { s->run(); });
+  *out = s;
+  return PP_OK;
+}
+
+pp_status pp_server_submit(pp_server* s, pp_hmatrix* h, const pp_request_desc* d, long long* id) {
+  if (!s || !h || !d || !id || h->ctx != s->ctx) return PP_INVALID_ARG;
+  pp_context* ctx = s->ctx;
+  const int n = h->H->n;
+  if (!d->points || d->dim < 1 || d->dim > 3 || !d->rhs || d->nrhs < 1 || d->nrhs > 16 || d->n_sets < 1 ||
+      !d->x_out || d->max_iter < 1 || !(d->tol > 0) || !(d->norm_inf > 0) || d->kernel < 0 || d->kernel > 3)
+    return fail(ctx, PP_INVALID_ARG, "pp_server_submit: bad request");
+  auto q = std::make_unique<ServeRequest>();
+  q->h = h;
+  q->n = n;
+  q->dim = d->dim;
+  q->kernel = d->kernel;
+  q->p0 = d->p0;
+  q->shift = d->shift;
+  q->norm_inf = d->norm_inf;
+  q->nrhs = d->nrhs;
+  q->n_sets = d->n_sets;
+  q->tol = d->tol;
+  q->max_iter = d->max_iter;
+  q->x_out = d->x_out;
+  q->pts.assign(d->points, d->points + (size_t)n * d->dim);
+  q->rhs.assign(d->rhs, d->rhs + (size_t)n * d->nrhs * d->n_sets);
+  std::lock_guard<std::mutex> lk(s->mu);
+  // programs are built here (host work) so that the device bytes are known before admission
+  VmPlan* sp = solve_plan(h, d->nrhs);
+  pp_status st = build_program(h, 0, 0, h->factor);
+  if (st == PP_OK) st = build_program(h, 1, d->nrhs, *sp);
+  if (st != PP_OK) return st;
+  if (h->d_arena) return fail(ctx, PP_INVALID_ARG, "pp_server_submit: the H-matrix must not be uploaded yet");
+  auto plan_bytes = [](const VmPlan& p) {
+    const auto& a = p.prog.arena_elems;
+    return (long long)sizeof(double) * (a[pp::AR_WORK] + a[pp::AR_SCRATCH] + a[pp::AR_RHS]) +
+           (long long)p.n_tasks * (long long)(sizeof(pp_task) + 4 * sizeof(int32_t)) +
+           (long long)p.prog.edges * (long long)sizeof(int32_t) + 4096;
+  };
+  const long long vec = (long long)sizeof(double) * n * d->nrhs;
+  q->bytes = (long long)sizeof(double) * (h->H->arena_elems + h->factor.prog.arena_elems[pp::AR_RAND]) +
+             plan_bytes(h->factor) + plan_bytes(*sp) + 4 * vec +
+             (long long)sizeof(double) * ((long long)n * d->dim + (long long)pp_kernel_residual_part_elems(n, d->nrhs)) +
+             (1 << 20);
+  if (q->bytes > s->budget) return fail(ctx, PP_OOM, "pp_server_submit: request exceeds the whole HBM budget");
+  q->id = s->next_id++;
+  q->t_submit = s->now_ms();
+  *id = q->id;
+  s->queue.push_back(q.get());
+  s->all[q->id] = std::move(q);
+  s->cv.notify_all();
+  return PP_OK;
+}
+
+pp_status pp_server_poll(pp_server* s, long long id, pp_request_stats* st) {
+  if (!s || !st) return PP_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->all.find(id);
+  if (it == s->all.end()) return fail(s->ctx, PP_INVALID_ARG, "pp_server_poll: unknown request");
+  const ServeRequest* q = it->second.get();
+  std::memset(st, 0, sizeof(*st));
+  st->status = q->state;
+  st->iterations = q->iters_total;
+  st->backward_error = q->worst;
+  st->t_submit_ms = q->t_submit;
+  st->t_admit_ms = q->t_admit;
+  st->t_done_ms = q->t_done;
+  st->device_bytes = q->bytes;
+  std::snprintf(st->message, sizeof(st->message), "%s", q->err.c_str());
+  return PP_OK;
+}
+
+pp_status pp_server_wait_all(pp_server* s, double timeout_ms) {
+  if (!s) return PP_INVALID_ARG;
+  const auto until = std::chrono::steady_clock::now() + std::chrono::duration<double, std::milli>(timeout_ms);
+  for (;;) {
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      if (s->queue.empty() && s->active.empty()) return PP_OK;
+    }
+    if (std::chrono::steady_clock::now() > until) return fail(s->ctx, PP_TIMEOUT, "pp_server_wait_all: timed out");
+    std::this_thread::sleep_for(std::chrono::microseconds(200));
+  }
+}
+
+double pp_server_clock_ms(pp_server* s) { return s ? s->now_ms() : 0.0; }
+
+void pp_server_destroy(pp_server* s) {
+  if (!s) return;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+    s->cv.notify_all();
+  }
+  if (s->worker.joinable()) s->worker.join();
+  for (auto& kv : s->all)
+    if (kv.second->h) pp_hmatrix_destroy(kv.second->h);  // queued, never admitted
+  delete s;
 }
 
 }  // extern "C"

@@ -23,6 +23,8 @@
 // All global loads of data other CTAs may have written use ld.global.cg (L2), never L1.
 #include <cuda_runtime.h>
 #include <math.h>
+
+#include <algorithm>
 #include <stdint.h>
 
 #include "vm.cuh"
@@ -1497,6 +1499,33 @@ __global__ void residual_reduce(const double* __restrict__ part, int segs, int n
   r[e] = b[e] - s;
 }
 
+// x += dx over `count` elements (the refinement update of a served request)
+__global__ void axpy_kernel(double* __restrict__ x, const double* __restrict__ dx, size_t count) {
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < count; e += (size_t)gridDim.x * blockDim.x)
+    x[e] += dx[e];
+}
+
+// out[0] = max |x|, out[1] = max |r| as the bit patterns of non-negative doubles (their
+// integer order is their numeric order, so an integer atomicMax reduces them); out zeroed
+// by the caller
+__global__ void absmax2_kernel(const double* __restrict__ x, const double* __restrict__ r, size_t count,
+                               unsigned long long* out) {
+  double mx = 0.0, mr = 0.0;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < count; e += (size_t)gridDim.x * blockDim.x) {
+    mx = fmax(mx, fabs(x[e]));
+    mr = fmax(mr, fabs(r[e]));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&out[0], (unsigned long long)__double_as_longlong(mx));
+    atomicMax(&out[1], (unsigned long long)__double_as_longlong(mr));
+  }
+}
+
 // One ACCUM on caller buffers; its scratch (T.tmp) is the static array below.
 __global__ void __launch_bounds__(NT) accum_noalloc_kernel(pp_task T) {
   extern __shared__ double smem[];
@@ -1584,6 +1613,20 @@ cudaError_t pp_kernel_residual(int kernel, double p0, double p1, double diag_shi
   if (e != cudaSuccess) return e;
   const size_t total = (size_t)n * nrhs;
   residual_reduce<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(part, segs, n, nrhs, b, r);
+  return cudaGetLastError();
+}
+
+cudaError_t pp_axpy(double* x, const double* dx, size_t count, cudaStream_t s) {
+  const unsigned blocks = (unsigned)std::min<size_t>((count + 255) / 256, 1184);
+  axpy_kernel<<<blocks ? blocks : 1, 256, 0, s>>>(x, dx, count);
+  return cudaGetLastError();
+}
+
+cudaError_t pp_absmax2(const double* x, const double* r, size_t count, unsigned long long* out, cudaStream_t s) {
+  cudaError_t e = cudaMemsetAsync(out, 0, 2 * sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return e;
+  const unsigned blocks = (unsigned)std::min<size_t>((count + 255) / 256, 592);
+  absmax2_kernel<<<blocks ? blocks : 1, 256, 0, s>>>(x, r, count, out);
   return cudaGetLastError();
 }
 

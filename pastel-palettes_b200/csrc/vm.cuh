@@ -55,3 +55,7 @@ cudaError_t pp_kernel_residual(int kernel, double p0, double p1, double diag_shi
                                const double* x, const double* b, double* r, int nrhs, double* part,
                                cudaStream_t s);
 size_t pp_kernel_residual_part_elems(int n, int nrhs);
+/* x += dx (count elements) */
+cudaError_t pp_axpy(double* x, const double* dx, size_t count, cudaStream_t s);
+/* out[0] = max |x|, out[1] = max |r| (as double bit patterns; out is zeroed first) */
+cudaError_t pp_absmax2(const double* x, const double* r, size_t count, unsigned long long* out, cudaStream_t s);
