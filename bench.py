@@ -219,6 +219,52 @@ def make_batch(pp, ctx, batch, rank):
     return hs, [prob] * batch
 
 
+def serving_leg(pp, ctx, n_requests, rate, seed=2024, smin=1024, smax=3072):
+    """Poisson arrivals of factor+solve requests into the server (continuous admission).
+    Sizes log-uniform in [smin, smax], kernel uniform among Laplace 1/r, exp (length 0.1) and
+    Matern-3/2 (length 0.2) on U[0,1]^3, 1-16 right-hand sides, 0-4 follow-up sets reusing
+    the resident factors, FP64 refinement to 1e-10.  Matrices are built on the host before the
+    clock starts (construction is its own stage); latency = arrival -> solutions on the host."""
+    rng = np.random.default_rng(seed)
+    kinds = [("laplace", 1e-3), ("exp", 0.1), ("matern32", 0.2)]
+    reqs = []
+    for i in range(n_requests):
+        n = int(round(np.exp(rng.uniform(np.log(smin), np.log(smax))) / 64)) * 64
+        kern, p0 = kinds[int(rng.integers(0, 3))]
+        nrhs = int(rng.integers(1, 17))
+        sets = 1 + int(rng.integers(0, 5))
+        h, prob = pp.make_kernel_problem(ctx, n, 3, kern, p0, 128, 16, seed=seed + 17 * i)
+        rhs = rng.uniform(-1, 1, (sets, n, nrhs))
+        reqs.append((h, prob, rhs))
+    gaps = rng.exponential(1.0 / rate, n_requests)
+    srv = pp.Server(ctx, hbm_budget_bytes=64 << 30, max_inflight=4)
+    ids = []
+    t0 = time.perf_counter()
+    t_next = 0.0
+    for (h, prob, rhs), g in zip(reqs, gaps):
+        t_next += g
+        delay = t_next - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        ids.append(srv.submit(h, prob, rhs, tol=WORKLOAD["tol"]))
+    srv.wait_all()
+    st = [srv.poll(i) for i in ids]
+    srv.close()
+    if any(x["status"] != "done" for x in st):
+        raise SystemExit(f"serving: a request failed: {[x['message'] for x in st if x['status'] != 'done']}")
+    lat = np.array([x["t_done_ms"] - x["t_submit_ms"] for x in st])
+    span_s = (max(x["t_done_ms"] for x in st) - min(x["t_submit_ms"] for x in st)) / 1e3
+    vectors = sum(rhs.shape[0] * rhs.shape[2] for _, _, rhs in reqs)
+    return {"requests": n_requests, "arrival_rate_per_s": rate, "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
+            "solves_per_s": vectors / span_s, "solves_unit": "right-hand-side vectors solved to 1e-10 per second",
+            "worst_backward_error": max(x["backward_error"] for x in st),
+            "refinement_solves": int(sum(x["iterations"] for x in st)),
+            "workload": f"N log-uniform [{smin},{smax}] (multiple of 64), 3-D points, kernels laplace/exp/matern32, "
+                        f"leaf 128, rank 16, 1-16 RHS, 0-4 follow-up sets, Poisson arrivals; matrices built "
+                        f"before the clock", "slots": 4}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -230,6 +276,8 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "tf32"],
                     help="factor GEMM precision of the headline form (tf32: tensor cores + FP64 refinement)")
     ap.add_argument("--compare", type=int, default=1, help="also time the other precision form")
+    ap.add_argument("--serve-requests", type=int, default=16, help="requests of the serving leg (0: skip)")
+    ap.add_argument("--serve-rate", type=float, default=40.0, help="Poisson arrival rate of the serving leg (1/s)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -402,6 +450,10 @@ def main():
                          "frac": B * finfo["flops"] / fac_s / 1e12 / fp64_peak,
                          "peak_source": "measured in this run: torch float64 matmul 8192^3"}}
 
+    serving = None
+    if args.serve_requests > 0:
+        serving = serving_leg(pp, ctx, args.serve_requests, args.serve_rate, seed=2024 + rank)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         import oracle
@@ -428,7 +480,11 @@ def main():
                 "e2e": {"value": e2e_value, "unit": "factor+solve/s",
                         "h2d_bytes_per_step": B * (hs[0].arena_bytes() + 8 * n),
                         "d2h_bytes_per_step": B * 8 * n},
-                "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),
+                "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "serving": serving,
+                "plain_fp64_single_instance": {
+                    "value": 1e3 / float(np.median(lat)), "unit": "factor+solve/s",
+                    "note": "one job per persistent launch, FP64, refinement to the same tolerance (the "
+                            "reference's execution model: one DAG per launch)"},
                 "gpu_launches": launches_per_step * args.steps}
         print(json.dumps(line), flush=True)
     del g, g2

@@ -117,6 +117,15 @@ long long pp_hmatrix_block_elems(const pp_hmatrix* h);
 #define PP_PRECISION_TF32 1
 pp_status pp_hmatrix_set_precision(pp_hmatrix* h, int precision);
 int pp_hmatrix_get_precision(const pp_hmatrix* h);
+/* adaptive rank (tol > 0, before set_lowrank and upload): low-rank blocks keep kmax columns,
+ * zero beyond their numerical rank, and every accumulation into them truncates to the
+ * singular values above tol times the largest (Gram eigen-decomposition by Jacobi, the role of
+ * blockSingleSideJacobiSVD / blockReadRank, src/kernel.cu:1084-1157, 1282-1315); tol = 0
+ * restores the fixed-rank form (ranks as set, no truncation) */
+pp_status pp_hmatrix_set_rank_tolerance(pp_hmatrix* h, double tol);
+/* numerical rank of a low-rank block in the host image (set_lowrank; after a download, the
+ * ranks the factorization's accumulations chose); -1 for other blocks */
+int pp_hmatrix_block_rank(const pp_hmatrix* h, int block);
 
 /* --- factor / solve (launcher.cuh) --------------------------------------- */
 /* H-LU factorization in place on the device, stream ordered.

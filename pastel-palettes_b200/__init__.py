@@ -146,6 +146,8 @@ def lib():
             "pp_server_clock_ms": (d, [vp]),
             "pp_server_destroy": (None, [vp]),
             "pp_hmatrix_set_precision": (i, [vp, i]),
+            "pp_hmatrix_set_rank_tolerance": (i, [vp, d]),
+            "pp_hmatrix_block_rank": (i, [vp, i]),
             "pp_hmatrix_get_precision": (i, [vp]),
         }
         for name, (res, args) in sig.items():
@@ -348,6 +350,14 @@ class Hierarchical:
         """FP64 (default) or TF32: the factor's GEMM instructions on the tensor cores with
         FP32 accumulation; GETRF / TRSM / accumulation stay FP64."""
         self.ctx.check(lib().pp_hmatrix_set_precision(self._h, precision), "set_precision")
+
+    def set_rank_tolerance(self, tol):
+        """Adaptive rank (tol > 0): accumulations truncate to singular values > tol * largest."""
+        self.ctx.check(lib().pp_hmatrix_set_rank_tolerance(self._h, float(tol)), "set_rank_tolerance")
+
+    def ranks(self):
+        """{block id: numerical rank} of the low-rank blocks (host image)."""
+        return {b["id"]: lib().pp_hmatrix_block_rank(self._h, b["id"]) for b in self.blocks() if b["kind"] == LOWRANK}
 
     def factor(self, stream=None):
         self.ctx.check(lib().pp_hlu_factor(self._h, _stream_handle(stream)), "hlu_factor")
@@ -652,14 +662,15 @@ def morton_order(pts):
     return np.argsort(key, kind="stable")
 
 
-def truncated_svd(A, k, rng):
-    """Rank-k truncated SVD of A as (U*s, V): exact for small blocks, randomized with
+def truncated_svd(A, k, rng, with_s=False):
+    """Rank-k truncated SVD of A as (U*s, V) (and s): exact for small blocks, randomized with
     oversampling 10 and two power iterations otherwise."""
     m, n = A.shape
     k = min(k, m, n)
     if min(m, n) <= 2 * k + 16:
         u, s, vt = np.linalg.svd(A, full_matrices=False)
-        return u[:, :k] * s[:k], vt[:k].T.copy()
+        out = (u[:, :k] * s[:k], vt[:k].T.copy())
+        return out + (s[:k],) if with_s else out
     p = min(k + 10, min(m, n))
     Y = A @ rng.standard_normal((n, p))
     Q, _ = np.linalg.qr(Y)
@@ -669,7 +680,7 @@ def truncated_svd(A, k, rng):
     B = Q.T @ A
     ub, s, vt = np.linalg.svd(B, full_matrices=False)
     U = (Q @ ub[:, :k]) * s[:k]
-    return U, vt[:k].T.copy()
+    return (U, vt[:k].T.copy(), s[:k]) if with_s else (U, vt[:k].T.copy())
 
 
 class KernelProblem:
@@ -711,8 +722,9 @@ def offdiag_rowsum_max(points, kernel, p0, block=2048):
     return best
 
 
-def fill_kernel_hmatrix(h, prob, seed=7):
-    """Dense blocks evaluated exactly; low-rank blocks by truncated SVD at their kmax."""
+def fill_kernel_hmatrix(h, prob, seed=7, rank_tol=None):
+    """Dense blocks evaluated exactly; low-rank blocks by truncated SVD at their kmax, or (with
+    rank_tol) at the number of singular values above rank_tol times the largest, at most kmax."""
     rng = np.random.default_rng(seed)
     for b in h.blocks():
         if b["kind"] == DENSE:
@@ -720,7 +732,10 @@ def fill_kernel_hmatrix(h, prob, seed=7):
                                               slice(b["col0"], b["col0"] + b["n"])))
         elif b["kind"] == LOWRANK:
             A = prob.entries(slice(b["row0"], b["row0"] + b["m"]), slice(b["col0"], b["col0"] + b["n"]))
-            U, V = truncated_svd(A, b["kmax"], rng)
+            U, V, s = truncated_svd(A, b["kmax"], rng, with_s=True)
+            if rank_tol:
+                r = int(np.count_nonzero(s > rank_tol * s[0])) if s.size and s[0] > 0 else 0
+                U, V = U[:, :r], V[:, :r]
             h.set_lowrank(b["id"], U, V)
 
 
@@ -736,7 +751,7 @@ def make_dense_problem(ctx, n=1024, leaf=256, seed=1234):
 
 
 def make_kernel_problem(ctx, n, dim, kernel, p0, leaf, rank, admissibility=0, eta=1.0, shift=None,
-                        shift_factor=2.0, seed=1234):
+                        shift_factor=2.0, seed=1234, rank_tol=None):
     """Kernel-matrix configuration: points U[0,1]^dim (Morton order), A_ij = K(|x_i - x_j|),
     diagonal shifted by `shift` or by shift_factor * max off-diagonal row sum."""
     rng = np.random.default_rng(seed)
@@ -748,7 +763,9 @@ def make_kernel_problem(ctx, n, dim, kernel, p0, leaf, rank, admissibility=0, et
         shift = shift_factor * off
     prob = KernelProblem(n, dim, kid, p0, shift, pts, off)
     h = Hierarchical.geometric(ctx, pts, leaf, admissibility, eta, rank)
-    fill_kernel_hmatrix(h, prob, seed + 1)
+    if rank_tol:
+        h.set_rank_tolerance(rank_tol)
+    fill_kernel_hmatrix(h, prob, seed + 1, rank_tol=rank_tol)
     return h, prob
 
 

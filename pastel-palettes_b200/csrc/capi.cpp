@@ -505,6 +505,26 @@ pp_status pp_hmatrix_set_precision(pp_hmatrix* h, int precision) {
 
 int pp_hmatrix_get_precision(const pp_hmatrix* h) { return h ? h->precision : -1; }
 
+pp_status pp_hmatrix_set_rank_tolerance(pp_hmatrix* h, double tol) {
+  if (!h || !(tol >= 0.0) || tol >= 1.0) return PP_INVALID_ARG;
+  if (h->d_arena) return fail(h->ctx, PP_INVALID_ARG, "pp_hmatrix_set_rank_tolerance: set it before the upload");
+  h->H->set_rank_tolerance(tol);
+  h->factor.release();
+  h->factor.prog = pp::Program();
+  h->factor.built = false;
+  for (auto& kv : h->solves) {
+    kv.second->release();
+    kv.second->prog = pp::Program();
+    kv.second->built = false;
+  }
+  return PP_OK;
+}
+
+int pp_hmatrix_block_rank(const pp_hmatrix* h, int block) {
+  if (!h || block < 0 || block >= (int)h->H->nodes.size()) return -1;
+  return h->H->stored_rank(block);
+}
+
 pp_status pp_hmatrix_to_dense(const pp_hmatrix* h, double* out) {
   if (!h || !out) return PP_INVALID_ARG;
   h->H->to_dense(out);

@@ -28,6 +28,8 @@ int Hierarchical::add_obj(int rows, int cols) {
 }
 
 void Hierarchical::add_inverses() {
+  for (auto& nd : nodes)
+    if (nd.kind == HNode::LR) nd.rank_obj = add_obj(1, 1);
   block_elems = arena_elems;
   for (auto& nd : nodes)
     if (nd.kind == HNode::D && nd.r0 == nd.c0 && nd.m == nd.n && nd.m <= kInvMax) {
@@ -193,7 +195,24 @@ Hierarchical* Hierarchical::geometric(int n, int dim, const double* pts, int lea
   h->root = block(0, 0, 0);
   h->add_inverses();
   h->host.assign((size_t)h->arena_elems, 0.0);
+  for (auto& nd : h->nodes)
+    if (nd.kind == HNode::LR) h->host[h->objs[nd.rank_obj].off] = nd.rank;
   return h;
+}
+
+int Hierarchical::stored_rank(int node) const {
+  const HNode& nd = nodes.at(node);
+  if (nd.kind != HNode::LR || nd.rank_obj < 0) return -1;
+  return (int)host[objs[nd.rank_obj].off];
+}
+
+void Hierarchical::set_rank_tolerance(double tol) {
+  rank_tol = tol > 0.0 ? tol : 0.0;
+  for (auto& nd : nodes)
+    if (nd.kind == HNode::LR) {
+      if (rank_tol > 0.0) nd.rank = nd.kmax;
+      else nd.rank = std::min(nd.kmax, std::max(0, (int)host[objs[nd.rank_obj].off]));
+    }
 }
 
 int Hierarchical::count(HNode::Kind k) const {
@@ -219,7 +238,8 @@ void Hierarchical::set_lowrank(int id, const double* U, int ldu, const double* V
   HNode& nd = nodes.at(id);
   if (nd.kind != HNode::LR) throw std::invalid_argument("set_lowrank: block is not low-rank");
   if (rank < 0 || rank > nd.kmax) throw std::invalid_argument("set_lowrank: rank exceeds kmax");
-  nd.rank = rank;
+  nd.rank = rank_tol > 0.0 ? nd.kmax : rank;
+  if (nd.rank_obj >= 0 && !host.empty()) host[objs[nd.rank_obj].off] = rank;
   const StorageObj& ou = objs[nd.obj];
   const StorageObj& ov = objs[nd.objV];
   for (int i = 0; i < nd.m; ++i)

@@ -39,7 +39,8 @@ struct HNode {
   int level;
   int obj = -1;      // D: the block; LR: U
   int objV = -1;     // LR: V
-  int rank = 0;      // LR: current rank
+  int rank = 0;      // LR: columns the instructions use (kmax in the adaptive-rank mode)
+  int rank_obj = -1; // LR: one-element object holding the block's numerical rank
   int kmax = 0;      // LR: storage capacity (columns of U and V)
   int ch[4] = {-1, -1, -1, -1};  // H: children, row-major 2 x 2
   int invL = -1, invU = -1;      // D on the diagonal: L^-1 and U^-1 of its factors (solve)
@@ -52,7 +53,12 @@ class Hierarchical {
   std::vector<HNode> nodes;
   std::vector<StorageObj> objs;
   int64_t arena_elems = 0;
-  // the matrix blocks occupy the arena prefix [0, block_elems); the tail holds the explicit
+  // adaptive-rank mode (rank_tol > 0): low-rank blocks keep kmax columns, zero beyond their
+  // numerical rank; the accumulations truncate to the singular values above rank_tol times
+  // the largest and record the new rank in the block's rank object
+  double rank_tol = 0.0;
+  // the matrix blocks (and the per-block rank words) occupy the arena prefix
+  // [0, block_elems); the tail holds the explicit
   // inverses of the diagonal leaves' triangular factors, which the factorization writes and
   // the solves read (never uploaded, downloaded or restored)
   int64_t block_elems = 0;
@@ -82,8 +88,13 @@ class Hierarchical {
 
  private:
   int add_obj(int rows, int cols);
-  // appends L^-1 / U^-1 objects for every square diagonal dense leaf of at most kInvMax rows
+  // appends the rank words of the low-rank blocks (arena prefix), then the L^-1 / U^-1
+  // objects for every square diagonal dense leaf of at most kInvMax rows (arena tail)
   void add_inverses();
+ public:
+  // numerical rank of a low-rank block as stored in the host image
+  int stored_rank(int node) const;
+  void set_rank_tolerance(double tol);
 };
 
 // largest diagonal leaf whose triangular factors get explicit inverses

@@ -388,6 +388,7 @@ Mat Generator::node(int id, bool tr) const {
     M.k = nd.rank;
     M.u = tr ? v : u;
     M.v = tr ? u : v;
+    M.rank_obj = nd.rank_obj >= 0 ? node_obj_[nd.rank_obj] : -1;
   } else {
     M.kind = Mat::H;
     M.node = id;
@@ -819,6 +820,15 @@ void Generator::accum(const Mat& C, const View& X, const View& Y, int sign) {
   t.t.k = k1;
   t.t.l = k2;
   t.t.alpha = (double)sign;
+  if (H_.rank_tol > 0.0 && C.rank_obj >= 0) {  // adaptive: truncate and record the new rank
+    t.t.flags |= PP_ADAPT_RANK;
+    t.t.beta = H_.rank_tol;
+    View rv;
+    rv.obj = C.rank_obj;
+    rv.m = 1;
+    rv.n = 1;
+    bind(t, 5, rv, true);
+  }
   const int64_t ny = C.m, nx = C.n;
   t.scratch_elems = 2 * ny * k1 + nx * k1 + (int64_t)k1 * std::max(k1, k2);
   const int ar = P_.arena_id(inst_, AR_SCRATCH);

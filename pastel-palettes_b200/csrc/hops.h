@@ -51,6 +51,7 @@ struct View {
 struct Mat {
   enum Kind { D = 0, LR = 1, H = 2 } kind = D;
   int m = 0, n = 0;
+  int rank_obj = -1;  // LR: program object of the block's rank word
   View d;          // D
   View u, v;       // LR: block = u v^T, u: m x k, v: n x k
   int k = 0;

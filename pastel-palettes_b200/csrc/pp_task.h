@@ -45,6 +45,9 @@ enum pp_op {
  * products into work buffers, whose results are only compared within a tolerance);
  * without it every element accumulates in ascending k, as the reference does. */
 #define PP_FREE_ORDER 1
+/* flags bit 1 (ACCUM): adaptive rank — truncate to the singular values above beta times the
+ * largest and store the new rank (as a double) at p[5] when p[5] is set */
+#define PP_ADAPT_RANK 2
 /* precision of the contraction inside GEMM-class tasks */
 #define PP_PREC_FP64 0
 #define PP_PREC_TF32 1

@@ -1002,14 +1002,14 @@ __device__ __noinline__ void accum_tn(const double* X, int lx, int a, const doub
 
 // Y[l][0..k) = A1[l] S1^T + alpha A2[l] S2^T for every row l (a thread per row), S1: k x c1,
 // S2: k x c2 in shared memory (ld lds).  Y may alias A1 (each row is read before written).
-template <int KB, bool YG>
+template <int KB, bool A1G>
 __device__ __noinline__ void accum_rows(double* Y, int ly, const double* A1, int la1, int c1, const double* A2,
                                        int la2, bool tA2, int c2, double alpha, const double* S1,
                                        const double* S2, int lds, int k, int L) {
   for (int l = threadIdx.x; l < L; l += NT) {
     double y[KB], u[KB];
 #pragma unroll
-    for (int j = 0; j < KB; ++j) u[j] = j < c1 ? ldcg(&A1[(size_t)l * la1 + j]) : 0.0;
+    for (int j = 0; j < KB; ++j) u[j] = j < c1 ? ld_any<A1G>(&A1[(size_t)l * la1 + j]) : 0.0;
 #pragma unroll
     for (int i = 0; i < KB; ++i) {
       double t = 0.0;
@@ -1103,6 +1103,119 @@ __device__ __noinline__ void accum_cholqr(double* Y, int m, int k, bool shifted,
   __syncthreads();
 }
 
+// Symmetric eigen-decomposition G = Z diag(lambda) Z^T of a k x k matrix (k <= 32, shared
+// memory, ld ACC_LG) by cyclic Jacobi in round-robin order: every step rotates k/2 disjoint
+// index pairs at once (every pair once per sweep), all threads applying the column rotations
+// (G J, Z J) and then the row rotations (J^T G); sweeps stop when the off-diagonal mass is
+// below 1e-30 of the diagonal's (1e-15 in norm) or after 12.  The rotation of a pair is the
+// symmetric Schur decomposition of its 2 x 2 block (Golub & Van Loan, sym.schur2).
+__device__ __noinline__ void jacobi_eig(double* G, double* Z, int k, double* cs, int* pq, double* flag) {
+  const int kk = (k + 1) & ~1, np = kk / 2;  // an odd k gets a dummy index k that never rotates
+  for (int e = threadIdx.x; e < k * k; e += NT) Z[(e / k) * ACC_LG + e % k] = (e / k == e % k) ? 1.0 : 0.0;
+  __syncthreads();
+  for (int sweep = 0; sweep < 12; ++sweep) {
+    if (threadIdx.x < 32) {
+      double off = 0.0, dia = 0.0;
+      for (int e = threadIdx.x; e < k * k; e += 32) {
+        const int i = e / k, j = e % k;
+        const double v = G[i * ACC_LG + j];
+        if (i == j) dia += v * v;
+        else off += v * v;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        off += __shfl_xor_sync(0xffffffffu, off, o);
+        dia += __shfl_xor_sync(0xffffffffu, dia, o);
+      }
+      if (threadIdx.x == 0) flag[0] = off <= 1e-30 * dia ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    const bool done = flag[0] != 0.0;
+    __syncthreads();
+    if (done) break;
+    for (int r = 0; r < kk - 1; ++r) {
+      if (threadIdx.x < np) {
+        const int i = threadIdx.x;
+        const int pos_a = i, pos_b = kk - 1 - i;
+        int p = pos_a == 0 ? 0 : 1 + (pos_a - 1 + r) % (kk - 1);
+        int q = pos_b == 0 ? 0 : 1 + (pos_b - 1 + r) % (kk - 1);
+        if (p > q) { const int t = p; p = q; q = t; }
+        double c = 1.0, sn = 0.0;
+        if (q < k) {
+          const double app = G[p * ACC_LG + p], aqq = G[q * ACC_LG + q], apq = G[p * ACC_LG + q];
+          if (apq != 0.0) {
+            const double tau = (aqq - app) / (2.0 * apq);
+            const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+            c = 1.0 / sqrt(1.0 + t * t);
+            sn = t * c;
+          }
+        }
+        pq[2 * i] = p;
+        pq[2 * i + 1] = q;
+        cs[2 * i] = c;
+        cs[2 * i + 1] = sn;
+      }
+      __syncthreads();
+      for (int e = threadIdx.x; e < k * np; e += NT) {  // columns: G J, Z J
+        const int i = e / np, j = e % np, p = pq[2 * j], q = pq[2 * j + 1];
+        if (q < k) {
+          const double c = cs[2 * j], sn = cs[2 * j + 1];
+          const double gp = G[i * ACC_LG + p], gq = G[i * ACC_LG + q];
+          G[i * ACC_LG + p] = c * gp - sn * gq;
+          G[i * ACC_LG + q] = sn * gp + c * gq;
+          const double zp = Z[i * ACC_LG + p], zq = Z[i * ACC_LG + q];
+          Z[i * ACC_LG + p] = c * zp - sn * zq;
+          Z[i * ACC_LG + q] = sn * zp + c * zq;
+        }
+      }
+      __syncthreads();
+      for (int e = threadIdx.x; e < k * np; e += NT) {  // rows: J^T G
+        const int i = e / np, j = e % np, p = pq[2 * j], q = pq[2 * j + 1];
+        if (q < k) {
+          const double c = cs[2 * j], sn = cs[2 * j + 1];
+          const double gp = G[p * ACC_LG + i], gq = G[q * ACC_LG + i];
+          G[p * ACC_LG + i] = c * gp - sn * gq;
+          G[q * ACC_LG + i] = sn * gp + c * gq;
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Rank decision of the adaptive accumulation: eigenvalues (the diagonal of G) sorted in
+// decreasing order, rank r = #{ lambda_i > tol^2 lambda_0 } (singular values above tol times
+// the largest), and S[i][j] = Z[j][perm[i]] for i < r (zero rows beyond), so that a row
+// times S^T is its coordinates in the kept singular directions.  Returns r.
+template <int KB>
+__device__ __noinline__ int accum_truncate(const double* G, const double* Z, int k, double tol, double* S, int lds,
+                                           int* perm) {
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < k; ++i) perm[i] = i;
+    for (int i = 0; i < k; ++i) {
+      int best = i;
+      for (int j = i + 1; j < k; ++j)
+        if (G[perm[j] * ACC_LG + perm[j]] > G[perm[best] * ACC_LG + perm[best]]) best = j;
+      const int t = perm[i];
+      perm[i] = perm[best];
+      perm[best] = t;
+    }
+    const double l0 = G[perm[0] * ACC_LG + perm[0]];
+    int r = 0;
+    if (l0 > 0.0)
+      while (r < k && G[perm[r] * ACC_LG + perm[r]] > tol * tol * l0) ++r;
+    perm[KB] = r;
+  }
+  __syncthreads();
+  const int r = perm[KB];
+  for (int e = threadIdx.x; e < KB * KB; e += NT) {
+    const int i = e / KB, j = e % KB;
+    S[i * lds + j] = (i < r && j < k) ? Z[j * ACC_LG + perm[i]] : 0.0;
+  }
+  __syncthreads();
+  return r;
+}
+
 template <int KB, bool YG>
 __device__ __forceinline__ void accum_impl(const pp_task& T, double* smem) {
   using SM = AccumSmem<KB>;
@@ -1120,7 +1233,7 @@ __device__ __forceinline__ void accum_impl(const pp_task& T, double* smem) {
   // S1 = R^T V1, S2 = R^T V2
   accum_tn<KB, true, true>(R, lr, k1, V1, lv1, false, k1, V2, lv2, tV2, k2, nx, S, S + KB, LS, red);
   // Y = U1 S1^T + alpha U2 S2^T
-  accum_rows<KB, YG>(Y, k1, U1, lu1, k1, U2, lu2, tU2, k2, al, S, S + KB, LS, k1, ny);
+  accum_rows<KB, true>(Y, k1, U1, lu1, k1, U2, lu2, tU2, k2, al, S, S + KB, LS, k1, ny);
   __syncthreads();
   accum_cholqr<KB, YG>(Y, ny, k1, true, G, red);
   accum_cholqr<KB, YG>(Y, ny, k1, false, G, red);
@@ -1128,7 +1241,24 @@ __device__ __forceinline__ void accum_impl(const pp_task& T, double* smem) {
   // P1 = Y^T U1, P2 = Y^T U2
   accum_tn<KB, YG, true>(Y, k1, k1, U1, lu1, false, k1, U2, lu2, tU2, k2, ny, S, S + KB, LS, red);
   // V1 := V1 P1^T + alpha V2 P2^T (rows read before written)
-  accum_rows<KB, false>(V1, lv1, V1, lv1, k1, V2, lv2, tV2, k2, al, S, S + KB, LS, k1, nx);
+  accum_rows<KB, true>(V1, lv1, V1, lv1, k1, V2, lv2, tV2, k2, al, S, S + KB, LS, k1, nx);
+  __syncthreads();
+  if ((T.flags & PP_ADAPT_RANK) && T.beta > 0.0) {
+    // adaptive rank: U1 V1^T = Y V1^T with Y orthonormal, so the singular values are those of
+    // V1; rotate both factors into the eigenbasis of V1^T V1 and keep the directions whose
+    // singular value exceeds beta times the largest (zero columns beyond the new rank)
+    accum_tn<KB, true, true>(V1, lv1, k1, V1, lv1, false, k1, nullptr, 0, false, 0, nx, G, nullptr, ACC_LG, red);
+    double* Z = red;
+    double* cs = red + KB * ACC_LG;
+    double* flag = cs + 2 * KB;
+    int* pq = reinterpret_cast<int*>(flag + 2);
+    jacobi_eig(G, Z, k1, cs, pq, flag);
+    const int r = accum_truncate<KB>(G, Z, k1, T.beta, S, LS, pq);
+    accum_rows<KB, true>(V1, lv1, V1, lv1, k1, nullptr, 0, false, 0, 1.0, S, S, LS, k1, nx);
+    accum_rows<KB, YG>(Y, k1, Y, k1, k1, nullptr, 0, false, 0, 1.0, S, S, LS, k1, ny);
+    __syncthreads();
+    if (threadIdx.x == 0 && T.p[5]) T.p[5][0] = (double)r;
+  }
   // U1 := Y
   for (int e = threadIdx.x; e < ny * k1; e += NT) {
     const int r = e / k1, c = e % k1;
