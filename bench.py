@@ -26,6 +26,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 WORKLOAD = dict(n=8192, dim=2, kernel="inv", p0=1e-3, leaf=256, rank=16, admissibility=0, seed=1234, tol=1e-10)
 WORKLOAD_NAME = "hodlr-inv2d-n8192-leaf256-rank16-fp64-ir1e-10"
 METRIC = "H-LU factor+solve/s at 1e-10 residual (FP64 HODLR N=8192)"
+# DRAM bytes (read + write) of one job's factor work inside the batched factor launch, from one
+# ncu capture of the batch-4 launch (dram__bytes.sum.per_second x gpu__time_duration.sum / 4);
+# the jobs touch disjoint arenas, so the launch's traffic scales with the batch
+FACTOR_DRAM_BYTES_PER_JOB = 115.6e6
 
 
 def load_pp():
@@ -277,6 +281,7 @@ def main():
                     help="factor GEMM precision of the headline form (tf32: tensor cores + FP64 refinement)")
     ap.add_argument("--compare", type=int, default=1, help="also time the other precision form")
     ap.add_argument("--serve-requests", type=int, default=16, help="requests of the serving leg (0: skip)")
+    ap.add_argument("--autotune", type=int, default=1, help="pick tile and grid of the batch by timing")
     ap.add_argument("--serve-rate", type=float, default=40.0, help="Poisson arrival rate of the serving leg (1/s)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -320,6 +325,7 @@ def main():
         for h in hs:
             h.set_precision(prec)
         batch = pp.Batch(ctx, hs)
+        tune = batch.autotune(s) if args.autotune else None
         ref = pp.BatchRefiner(batch, probs, stream=s)
         # warm-up (eager): allocates every plan, fixes the number of refinement solves
         with torch.cuda.stream(s):
@@ -359,7 +365,8 @@ def main():
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_max = t.item()
         stats = {"value": world * B * args.steps / total_max, "ms_per_step": 1e3 * total_max / args.steps,
-                 "refinement_solves": iters, "worst_backward_error": worst, "total_s": total_max}
+                 "refinement_solves": iters, "worst_backward_error": worst, "total_s": total_max,
+                 "autotune": tune}
         return batch, ref, g, out, stats
 
     forms = {"fp64": pp.FP64, "tf32": pp.TF32}
@@ -443,7 +450,8 @@ def main():
     fp64_peak = fp64_peak_tflops(torch)
     achieved_gbs = B * fbytes / fac_s / 1e9
     roofline = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
-                "frac": achieved_gbs / hbm_peak, "traffic": None,
+                "frac": achieved_gbs / hbm_peak, "traffic": B * FACTOR_DRAM_BYTES_PER_JOB,
+                "traffic_source": "ncu capture of the batch-4 factor launch, scaled by jobs per launch",
                 "kernel": f"vm_kernel (batched factor launch, {B} jobs)", "launch_ms": 1e3 * fac_s,
                 "algorithmic_bytes": B * fbytes, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
                 "fp64": {"achieved_tflops": B * finfo["flops"] / fac_s / 1e12, "peak_tflops": fp64_peak,

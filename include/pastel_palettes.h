@@ -158,6 +158,17 @@ pp_status pp_batch_restore(pp_batch* b, void* stream);  /* pp_hmatrix_restore on
 pp_status pp_batch_sync(pp_batch* b, void* stream);
 pp_status pp_batch_program_info(pp_batch* b, int which, int nrhs, pp_program_info* info);
 pp_status pp_batch_trace(pp_batch* b, int which, int nrhs, int enable, uint64_t* out);
+/* Autotuner (no reference counterpart; the reference's tile sizes are compile-time constants
+ * of a missing header): times the batch's factor launch for every dense tile in {32, 64}
+ * (the largest block one GETRF / TRSM instruction takes) and persistent grid in {all, 3/4,
+ * 1/2 of the resident CTAs}, and keeps the fastest for this batch's later launches.  Every
+ * instance must hold an original (pp_hmatrix_keep_original): each trial restores it first, and
+ * on return the instances hold their restored, unfactored matrices. */
+typedef struct pp_tune_result {
+  int tile, grid, trials;
+  double factor_ms;
+} pp_tune_result;
+pp_status pp_batch_autotune(pp_batch* b, void* stream, pp_tune_result* out);
 
 /* --- serving: a request loop with continuous admission (no reference counterpart; the
  *     reference factors one matrix per launch) -------------------------------------------

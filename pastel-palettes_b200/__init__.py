@@ -75,6 +75,10 @@ class _RequestStats(C.Structure):
                 ("device_bytes", C.c_longlong), ("message", C.c_char * 128)]
 
 
+class _TuneResult(C.Structure):
+    _fields_ = [("tile", C.c_int), ("grid", C.c_int), ("trials", C.c_int), ("factor_ms", C.c_double)]
+
+
 class _ProgramInfo(C.Structure):
     _fields_ = [("n_tasks", C.c_int), ("n_edges", C.c_longlong), ("flops", C.c_longlong),
                 ("op_count", C.c_longlong * 16), ("arena_elems", C.c_longlong * 5), ("host_build_ms", C.c_double)]
@@ -138,6 +142,7 @@ def lib():
             "pp_batch_sync": (i, [vp, vp]),
             "pp_batch_program_info": (i, [vp, i, i, C.POINTER(_ProgramInfo)]),
             "pp_batch_trace": (i, [vp, i, i, i, vp]),
+            "pp_batch_autotune": (i, [vp, vp, C.POINTER(_TuneResult)]),
             "pp_refstream_encode": (i, [vp, i, vp, ll, vp, C.POINTER(ll)]),
             "pp_server_create": (i, [vp, C.POINTER(_ServeConfig), C.POINTER(vp)]),
             "pp_server_submit": (i, [vp, vp, C.POINTER(_RequestDesc), C.POINTER(ll)]),
@@ -469,6 +474,13 @@ class Batch:
         return dict(n_tasks=info.n_tasks, n_edges=info.n_edges, flops=info.flops,
                     op_count={OP_NAMES[i]: info.op_count[i] for i in range(len(OP_NAMES))},
                     host_build_ms=info.host_build_ms)
+
+    def autotune(self, stream=None):
+        """Picks the dense tile and persistent grid of this batch by timing its factor launch
+        (instances need keep_original); returns the choice and its time."""
+        r = _TuneResult()
+        self.ctx.check(lib().pp_batch_autotune(self._h, _stream_handle(stream), C.byref(r)), "batch_autotune")
+        return dict(tile=r.tile, grid=r.grid, trials=r.trials, factor_ms=r.factor_ms)
 
     def enable_trace(self, which=0, nrhs=1):
         self.ctx.check(lib().pp_batch_trace(self._h, which, nrhs, 1, None), "batch_trace")

@@ -88,6 +88,7 @@ struct pp_hmatrix {
   double* d_rand = nullptr;
   bool pinned = false;
   int precision = PP_PREC_FP64;  // contraction precision of the factor's GEMM instructions
+  int tile = 0;                  // dense tile of its programs (0: the context's)
   std::vector<double> rand_host;
   VmPlan factor;
   std::map<int, std::unique_ptr<VmPlan>> solves;
@@ -167,7 +168,7 @@ pp_status build_program(pp_hmatrix* h, int which, int nrhs, VmPlan& plan) {
   if (plan.built) return PP_OK;
   auto t0 = std::chrono::steady_clock::now();
   try {
-    pp::Generator g(plan.prog, *h->H, ctx->cfg.tile, h->H->n, ctx->cfg.reference_isa == 0);
+    pp::Generator g(plan.prog, *h->H, h->tile > 0 ? h->tile : ctx->cfg.tile, h->H->n, ctx->cfg.reference_isa == 0);
     g.use_inverses(ctx->cfg.reference_isa == 0);
     if (which == 0) {
       g.getrf_program();
@@ -841,6 +842,7 @@ pp_status pp_refstream_encode(pp_hmatrix* h, int workers, int32_t* words, long l
 struct pp_batch {
   pp_context* ctx = nullptr;
   std::vector<pp_hmatrix*> hs;
+  int grid_cap = 0;  // persistent CTAs of its launches (0: all); set by pp_batch_autotune
   VmPlan factor;
   std::map<int, std::unique_ptr<VmPlan>> solves;
   VmPlan* last = nullptr;
@@ -901,9 +903,11 @@ void pp_batch_destroy(pp_batch* b) { delete b; }
 
 pp_status pp_batch_factor(pp_batch* b, void* stream) {
   if (!b) return PP_INVALID_ARG;
-  pp_status st = plan_to_device_multi(b->ctx, b->hs, b->factor);
+  pp_status st = batch_program(b, 0, 0, b->factor);  // (re)built after an autotuner tile change
   if (st != PP_OK) return st;
-  st = launch_plan(b->ctx, b->factor, (cudaStream_t)stream, 0);
+  st = plan_to_device_multi(b->ctx, b->hs, b->factor);
+  if (st != PP_OK) return st;
+  st = launch_plan(b->ctx, b->factor, (cudaStream_t)stream, b->grid_cap);
   if (st == PP_OK) b->last = &b->factor;
   return st;
 }
@@ -922,7 +926,7 @@ pp_status pp_batch_solve(pp_batch* b, const double* const* B, double* const* X, 
     PP_CUDA(cudaMemcpyAsync(plan->d_rhs + plan->rhs_off[j], B[j], sizeof(double) * (size_t)b->hs[j]->H->n * nrhs,
                             cudaMemcpyDeviceToDevice, s));
   }
-  st = launch_plan(ctx, *plan, s, 0);
+  st = launch_plan(ctx, *plan, s, b->grid_cap);
   if (st != PP_OK) return st;
   b->last = plan;
   for (size_t j = 0; j < b->hs.size(); ++j)
@@ -961,6 +965,81 @@ pp_status pp_batch_program_info(pp_batch* b, int which, int nrhs, pp_program_inf
   for (int a = 0; a < 5; ++a)
     for (int j = 0; j < plan->prog.n_instances; ++j) info->arena_elems[a] += plan->prog.arena_elems[j * pp::PP_ARENAS + a];
   info->host_build_ms = plan->build_ms;
+  return PP_OK;
+}
+
+// Invalidates the programs of an instance and of the batch (a new tile rebuilds them).
+static void batch_reset_programs(pp_batch* b) {
+  auto reset = [](VmPlan& p) {
+    p.release();
+    p.prog = pp::Program();
+    p.built = false;
+  };
+  for (auto* h : b->hs) {
+    if (h->last) h->last = nullptr;
+    reset(h->factor);
+    for (auto& kv : h->solves) reset(*kv.second);
+  }
+  reset(b->factor);
+  for (auto& kv : b->solves) reset(*kv.second);
+  b->last = nullptr;
+}
+
+pp_status pp_batch_autotune(pp_batch* b, void* stream, pp_tune_result* out) {
+  if (!b) return PP_INVALID_ARG;
+  pp_context* ctx = b->ctx;
+  for (auto* h : b->hs)
+    if (!h->d_orig) return fail(ctx, PP_INVALID_ARG, "pp_batch_autotune: every instance needs pp_hmatrix_keep_original");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int full = ctx->sm_count * std::max(1, ctx->blocks_per_sm);
+  const int tiles[] = {32, 64};
+  const int grids[] = {full, (3 * full) / 4, full / 2};
+  cudaEvent_t e0, e1;
+  PP_CUDA(cudaEventCreate(&e0));
+  PP_CUDA(cudaEventCreate(&e1));
+  double best = 1e300;
+  int best_tile = 0, best_grid = 0, trials = 0;
+  pp_status st = PP_OK;
+  for (int t : tiles) {
+    if (t > PP_VM_TILE) continue;
+    for (auto* h : b->hs) h->tile = t;
+    batch_reset_programs(b);
+    for (int g : grids) {
+      b->grid_cap = g;
+      float ms = 0.f;
+      for (int rep = 0; rep < 2 && st == PP_OK; ++rep) {  // the first run builds and warms up
+        st = pp_batch_restore(b, stream);
+        if (st == PP_OK && cudaEventRecord(e0, s) != cudaSuccess) st = PP_CUDA_ERROR;
+        if (st == PP_OK) st = pp_batch_factor(b, stream);
+        if (st == PP_OK && cudaEventRecord(e1, s) != cudaSuccess) st = PP_CUDA_ERROR;
+        if (st == PP_OK && cudaEventSynchronize(e1) != cudaSuccess) st = PP_CUDA_ERROR;
+        if (st == PP_OK) st = plan_status(ctx, b->factor);
+        if (st == PP_OK) cudaEventElapsedTime(&ms, e0, e1);
+      }
+      if (st != PP_OK) break;
+      ++trials;
+      if (ms < best) {
+        best = ms;
+        best_tile = t;
+        best_grid = g;
+      }
+    }
+    if (st != PP_OK) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st != PP_OK) return st;
+  for (auto* h : b->hs) h->tile = best_tile;
+  batch_reset_programs(b);
+  b->grid_cap = best_grid;
+  st = pp_batch_restore(b, stream);
+  if (st != PP_OK) return st;
+  if (out) {
+    out->tile = best_tile;
+    out->grid = best_grid;
+    out->factor_ms = best;
+    out->trials = trials;
+  }
   return PP_OK;
 }
 

@@ -1,0 +1,155 @@
+#!/usr/bin/env python
+"""trace_tool.py — per-instruction trace of the VM and its critical-path analysis.
+
+Counterpart of the reference's clock tracing (every instruction stamps clock64 at start and
+end, src/kernel.cu:1389-1390, rendered per worker by analyzeClocks, rts/scheduler.cpp:494-544).
+Here the VM stamps the globaltimer (ns) at a task's start and end plus its SM and CTA
+(`pp_hmatrix_trace` / `pp_batch_trace`); this tool runs a HODLR workload with tracing on and
+reports, per program (factor, solve):
+
+  * makespan, CTAs used, busy time and the average parallelism (busy / makespan);
+  * busy time per instruction shape (op, m, n, k);
+  * the critical path recomputed from the measured durations over the program's DAG edges,
+    its composition by instruction shape, and the waits between consecutive path tasks;
+  * the ready-to-start latency (a task's start minus its last predecessor's end).
+
+  python pastel-palettes_b200/trace_tool.py [--n 8192] [--leaf 256] [--rank 16] [--batch 16]
+                                            [--out trace.npz]
+"""
+import argparse
+import collections
+import importlib.util
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _load():
+    if "pastel_palettes_b200" in sys.modules:
+        return sys.modules["pastel_palettes_b200"]
+    spec = importlib.util.spec_from_file_location("pastel_palettes_b200", os.path.join(HERE, "__init__.py"),
+                                                  submodule_search_locations=[HERE])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["pastel_palettes_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def critical_path(dur, start, preds):
+    """Longest path by measured durations (tasks visited in start order, a topological order
+    of an executed DAG); returns (length, path as task ids from sink to source)."""
+    fin, arg = {}, {}
+    for i in np.argsort(start, kind="stable"):
+        i = int(i)
+        best, bp = 0, -1
+        for p in preds[i]:
+            if fin.get(p, 0) > best:
+                best, bp = fin[p], p
+        fin[i] = int(dur[i]) + best
+        arg[i] = bp
+    i = max(fin, key=fin.get)
+    path = []
+    while i >= 0:
+        path.append(i)
+        i = arg[i]
+    return max(fin.values()), path
+
+
+def analyse(name, tasks, trace, ef, et, out=print):
+    ops = _load().OP_NAMES
+    st, en = trace[:, 0].astype(np.int64), trace[:, 1].astype(np.int64)
+    cta = trace[:, 2].astype(np.int64) >> 32
+    dur = en - st
+    mk = en.max() - st.min()
+    out(f"== {name}: tasks {len(tasks)} makespan {mk / 1e3:.1f} us, CTAs used {len(np.unique(cta))}")
+    out(f"   busy {dur.sum() / 1e3:.1f} us -> average parallelism {dur.sum() / mk:.1f}")
+    agg = collections.defaultdict(list)
+    for i in range(len(tasks)):
+        agg[(ops[tasks["op"][i]], int(tasks["m"][i]), int(tasks["n"][i]), int(tasks["k"][i]))].append(dur[i])
+    out(f"   {'op, m, n, k':34s} {'count':>6s} {'mean us':>8s} {'total us':>9s} {'share':>6s}")
+    for k, v in sorted(agg.items(), key=lambda x: -sum(x[1]))[:16]:
+        out(f"   {str(k):34s} {len(v):6d} {np.mean(v) / 1e3:8.2f} {sum(v) / 1e3:9.1f} {100 * sum(v) / dur.sum():5.1f}%")
+    preds = collections.defaultdict(list)
+    for a, b in zip(ef, et):
+        preds[int(b)].append(int(a))
+    cp, path = critical_path(dur, st, preds)
+    gaps = sum(max(0, st[path[j]] - en[path[j + 1]]) for j in range(len(path) - 1))
+    out(f"   critical path {cp / 1e3:.1f} us over {len(path)} tasks ({cp / mk:.2f} of the makespan), "
+        f"waits between path tasks {gaps / 1e3:.0f} us")
+    comp = collections.defaultdict(lambda: [0, 0])
+    for i in path:
+        k = (ops[tasks["op"][i]], int(tasks["m"][i]), int(tasks["n"][i]), int(tasks["k"][i]))
+        comp[k][0] += 1
+        comp[k][1] += dur[i]
+    for k, v in sorted(comp.items(), key=lambda x: -x[1][1])[:10]:
+        out(f"     on path: {str(k):34s} {v[0]:4d} tasks {v[1] / 1e3:9.1f} us")
+    lat = [st[i] - max(en[p] for p in preds[i]) for i in range(len(tasks)) if preds[i]]
+    if lat:
+        out(f"   ready->start latency: median {np.median(lat) / 1e3:.2f} us, p90 {np.percentile(lat, 90) / 1e3:.2f} us")
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--n", type=int, default=8192)
+    ap.add_argument("--leaf", type=int, default=256)
+    ap.add_argument("--rank", type=int, default=16)
+    ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--out", default=None, help="also save the raw trace (npz)")
+    args = ap.parse_args()
+    import torch
+
+    pp = _load()
+    ctx = pp.Context(device=0)
+    h, prob = pp.make_kernel_problem(ctx, args.n, 2, "inv", 1e-3, args.leaf, args.rank, seed=1234)
+    h.upload()
+    h.keep_original()
+    raw = {}
+    for which in (0, 1):
+        tasks, _, _, _ = h.encode_program(which, 1, [0] * 5)
+        ef, et, _ = h.edges(which, 1)
+        raw[f"tasks{which}"], raw[f"ef{which}"], raw[f"et{which}"] = tasks, ef, et
+    b = torch.from_numpy(pp.rhs(args.n)).cuda()
+    x = torch.empty_like(b)
+    h.enable_trace(0)
+    h.enable_trace(1, 1)
+    for _ in range(3):
+        h.restore()
+        h.factor()
+        h.solve(b, x)
+        h.sync()
+    raw["tr0"], raw["tr1"] = h.read_trace(0), h.read_trace(1, 1)
+    analyse("factor, one job", raw["tasks0"], raw["tr0"], raw["ef0"], raw["et0"])
+    analyse("solve, one job", raw["tasks1"], raw["tr1"], raw["ef1"], raw["et1"])
+    if args.batch > 1:
+        hs = [h] + [pp.Hierarchical.geometric(ctx, prob.points, args.leaf, 0, 1.0, args.rank)
+                    for _ in range(args.batch - 1)]
+        for q in hs[1:]:
+            q.host_arena()[:] = h.host_arena()
+            q.upload()
+            q.keep_original()
+        bt = pp.Batch(ctx, hs)
+        bt.enable_trace(0)
+        bt.enable_trace(1, 1)
+        bs = [torch.from_numpy(pp.rhs(args.n, 1, seed=7 + i)).cuda() for i in range(args.batch)]
+        xs = [torch.empty_like(q) for q in bs]
+        for _ in range(3):
+            bt.restore()
+            bt.factor()
+            bt.solve(bs, xs)
+            bt.sync()
+        for which, name in ((0, "factor"), (1, "solve")):
+            tr = bt.read_trace(which, 1).astype(np.int64)
+            raw[f"btr{which}"] = tr
+            dur = tr[:, 1] - tr[:, 0]
+            mk = tr[:, 1].max() - tr[:, 0].min()
+            print(f"== batched {name}, {args.batch} jobs: tasks {len(tr)} makespan {mk / 1e3:.1f} us, "
+                  f"busy {dur.sum() / 1e3:.0f} us, average parallelism {dur.sum() / mk:.1f}")
+    if args.out:
+        np.savez_compressed(args.out, **raw)
+
+
+if __name__ == "__main__":
+    main()

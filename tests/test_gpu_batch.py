@@ -14,6 +14,10 @@ def dev(x):
     return torch.from_numpy(np.ascontiguousarray(x, dtype=np.float64)).cuda()
 
 
+def rel(a, b):
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
 def mixed_instances(pp, ctx):
     probs = [
         pp.make_kernel_problem(ctx, 1024, 2, "inv", 1e-3, 128, 16, seed=1),
@@ -112,3 +116,28 @@ def test_batch_graph_capture_replays(pp, gctx):
         assert max(errs) <= 1e-10, errs
         for xe, xg in zip(xs_eager, out[0]):
             assert torch.equal(xe, xg)
+
+
+def test_batch_autotune_keeps_results(pp, gctx):
+    """The autotuner times tile x grid candidates and keeps the fastest; the factorization it
+    then runs equals the untuned one (dense blocks are blocking-invariant, the low-rank
+    work is decomposed independently of the tile)."""
+    hs = [pp.make_kernel_problem(gctx, n, 2, "inv", 1e-3, 128, 16, seed=11 + i)[0] for i, n in enumerate([1024, 1536])]
+    ref = []
+    for h in hs:
+        h.upload()
+        h.keep_original()
+    b0 = pp.Batch(gctx, hs)
+    b0.factor()
+    b0.sync()
+    for h in hs:
+        h.download()
+        ref.append(h.to_dense())
+    b = pp.Batch(gctx, hs)
+    choice = b.autotune()
+    assert choice["tile"] in (32, 64) and choice["grid"] > 0 and choice["trials"] == 6
+    b.factor()
+    b.sync()
+    for h, F in zip(hs, ref):
+        h.download()
+        assert rel(h.to_dense(), F) < 1e-12
