@@ -267,6 +267,46 @@ void o_accum(double* U1, double* VT1, const double* U2, const double* VT2, int n
     for (int c = 0; c < k1; ++c) VT1[(int64_t)r * ld_vt1 + c] = V[(int64_t)r * k1 + c];
 }
 
+// Y := Y C^-1 with G = Y^T Y (+ shift) = C^T C, three passes (the first shifted by
+// 11 (m k + k (k + 1)) u ||Y||_F^2): the range finder of the engine's sketched updates
+void o_cholqr3(double* Y, int m, int k) {
+  std::vector<double> G((size_t)k * k);
+  for (int pass = 0; pass < 3; ++pass) {
+    for (int i = 0; i < k; ++i)
+      for (int j = 0; j < k; ++j) {
+        double s = 0.0;
+        for (int r = 0; r < m; ++r) s += Y[(int64_t)r * k + i] * Y[(int64_t)r * k + j];
+        G[(size_t)i * k + j] = s;
+      }
+    double tr = 0.0;
+    for (int j = 0; j < k; ++j) tr += G[(size_t)j * k + j];
+    if (pass == 0) {
+      const double sh = 11.0 * ((double)m * k + (double)k * (k + 1)) * 1.1102230246251565e-16 * tr;
+      for (int j = 0; j < k; ++j) G[(size_t)j * k + j] += sh;
+    }
+    const double tiny = 1e-28 * tr;
+    std::vector<double> rinv(k);
+    for (int j = 0; j < k; ++j) {  // upper Cholesky factor in place (rows j, columns >= j)
+      const double d = G[(size_t)j * k + j];
+      const bool live = d > tiny;
+      const double rjj = live ? std::sqrt(d) : 0.0;
+      G[(size_t)j * k + j] = rjj;
+      rinv[j] = live ? 1.0 / rjj : 0.0;
+      for (int c = j + 1; c < k; ++c) G[(size_t)j * k + c] = live ? G[(size_t)j * k + c] / rjj : 0.0;
+      for (int c1 = j + 1; c1 < k; ++c1)
+        for (int c = c1; c < k; ++c) G[(size_t)c1 * k + c] -= G[(size_t)j * k + c1] * G[(size_t)j * k + c];
+    }
+    for (int r = 0; r < m; ++r) {
+      double* y = Y + (int64_t)r * k;
+      for (int j = 0; j < k; ++j) {
+        double s = y[j];
+        for (int p = 0; p < j; ++p) s -= y[p] * G[(size_t)p * k + j];
+        y[j] = s * rinv[j];
+      }
+    }
+  }
+}
+
 int run_one(const pp_task& T, std::vector<double>& tmp) {
   const bool t1 = T.flags & PP_T(1), t2 = T.flags & PP_T(2), t3 = T.flags & PP_T(3), t4 = T.flags & PP_T(4);
   switch (T.op) {
@@ -331,6 +371,14 @@ int run_one(const pp_task& T, std::vector<double>& tmp) {
         for (int q = 0; q < n; ++q) T.p[0][(int64_t)r * ldb + q] = out[(size_t)r * n + q];
       return 0;
     }
+    case PP_OP_ORTH: {  // engine instruction: shifted CholeskyQR3 of Y (m x k, ld k)
+      o_cholqr3(T.p[0], T.m, T.n);
+      return 0;
+    }
+    case PP_OP_COPY:
+      for (int r = 0; r < T.m; ++r)
+        for (int c = 0; c < T.n; ++c) T.p[0][(int64_t)r * T.ld[0] + c] = T.p[1][(int64_t)r * T.ld[1] + c];
+      return 0;
     default: return -1;
   }
 }

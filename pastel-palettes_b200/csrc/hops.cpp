@@ -738,8 +738,9 @@ void Generator::gemm(const Mat& C, const Mat& A, const Mat& B, int alpha) {
     return;
   }
   if (C.kind == Mat::LR) {
-    if (A.kind == Mat::D && B.kind == Mat::D) { accum(C, A.d, B.d.T(), alpha); return; }
-    throw std::runtime_error("unsupported: hierarchical product accumulated into a low-rank block");
+    if (A.kind == Mat::D && B.kind == Mat::D && A.n <= kAccumMaxK2) { accum(C, A.d, B.d.T(), alpha); return; }
+    sketch_update(C, A, B, alpha);
+    return;
   }
   if (C.kind == Mat::D && A.kind == Mat::D && B.kind == Mat::D) {
     gemm_tiles(C.d, A.d, B.d, alpha);
@@ -856,6 +857,52 @@ void Generator::trmv(int inv, int upper, int m, const View& B) {
     t.t.n = w;
     t.t.ctrl = upper;
     t.flops = (int64_t)w * m * (m + 1);
+  }
+}
+
+// C (low-rank, u v^T with k columns) := Q W^T, the rank-k recompression of C + alpha A B:
+//   T1 = B R                    (R: the k-column random sketch, n rows)
+//   Y  = u (v^T R) + alpha A T1  (ny x k)            Q = orth(Y)
+//   W  = v (u^T Q) + alpha B^T (A^T Q)               u := Q, v := W
+// The same one-pass randomized range finder as ACCUM (the reference's accum, kernel.cu:
+// 1255-1280), here over products of hierarchical or dense blocks, each product an ordinary
+// GEMM of the generator (work buffers, DAG-tracked).
+void Generator::sketch_update(const Mat& C, const Mat& A, const Mat& B, int alpha) {
+  const int k = C.k, ny = C.m, nx = C.n, nm = A.n;
+  if (k <= 0) return;
+  if (k > kAccumMaxK2) throw std::runtime_error("sketched update: rank above 32");
+  View R;
+  R.obj = rand_obj(k);
+  R.m = nx;
+  R.n = k;
+  View T1 = tmp(nm, k);
+  gemm(asD(T1), B, asD(R), +1);
+  View S = tmp(k, k);
+  gemm_tiles(S, C.v.T(), R, +1);
+  View Y = tmp(ny, k);
+  gemm_tiles(Y, C.u, S, +1);
+  gemm(asD(Y), A, asD(T1), alpha);
+  HTask& o = emit(PP_OP_ORTH);
+  bind(o, 0, Y, true);
+  o.t.m = ny;
+  o.t.n = k;
+  o.t.k = k;
+  o.flops = 3 * (2LL * ny * k * k + (int64_t)ny * k * k);
+  View P = tmp(k, k);
+  gemm_tiles(P, C.u.T(), Y, +1);
+  View W = tmp(nx, k);
+  gemm_tiles(W, C.v, P, +1);  // (Q^T u v^T)^T = v (u^T Q)
+  View T2 = tmp(nm, k);
+  gemm(asD(T2), transpose(A), asD(Y), +1);
+  gemm(asD(W), transpose(B), asD(T2), alpha);
+  for (int which = 0; which < 2; ++which) {
+    const View& dst = which == 0 ? C.u : C.v;
+    const View& src = which == 0 ? Y : W;
+    HTask& c = emit(PP_OP_COPY);
+    bind(c, 0, dst, true);
+    bind(c, 1, src, false);
+    c.t.m = dst.m;
+    c.t.n = dst.n;
   }
 }
 

@@ -116,6 +116,8 @@ class Program {
 constexpr int kSolveTri = 256;
 // right-hand-side columns of one TRMV instruction
 constexpr int kTrmvCols = 16;
+// largest rank of the added term of one ACCUM (the VM keeps it in registers)
+constexpr int kAccumMaxK2 = 32;
 
 class Generator {
  public:
@@ -162,6 +164,9 @@ class Generator {
   LRP lr_product(const Mat& A, const Mat& B, int alpha);
   void lr_update(const Mat& C, const View& X, const View& Y, int sign);
   void accum(const Mat& C, const View& X, const View& Y, int sign);
+  // C := rank-k recompression of C + alpha A B for hierarchical / dense operands whose
+  // product has no small low-rank form (standard admissibility), by a k-column sketch
+  void sketch_update(const Mat& C, const Mat& A, const Mat& B, int alpha);
   void gemm_tiles(const View& C, const View& A, const View& B, int alpha);
   View tmp(int rows, int cols);
   Mat asD(const View& v) const;

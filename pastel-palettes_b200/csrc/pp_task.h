@@ -36,7 +36,11 @@ enum pp_op {
   PP_OP_TRMV = 12,   /* B[m x n] := M B, M (p[1], m x m) lower (ctrl 0) or upper (ctrl 1)
                         triangular with explicit diagonal: a solve step with a precomputed
                         inverse; no reference counterpart                                       */
-  PP_OP_COUNT = 13
+  PP_OP_ORTH = 13,   /* Y[m x k] (ld k, k <= 32) := an orthonormal basis of its range (shifted
+                        CholeskyQR3; rank-deficient columns become zero): the range finder of
+                        a sketched low-rank update; no reference counterpart                   */
+  PP_OP_COPY = 14,   /* C[m x n] := A[m x n] (p[1]); no reference counterpart                   */
+  PP_OP_COUNT = 15
 };
 
 /* flags: bit (4+i) = operand i is stored transposed (operand 0 is the target). */

@@ -1267,6 +1267,32 @@ __device__ __forceinline__ void accum_impl(const pp_task& T, double* smem) {
   __syncthreads();
 }
 
+// Y (m x k, ld k, global) := an orthonormal basis of its range by shifted CholeskyQR3, the
+// range finder of the sketched low-rank update (same passes as inside ACCUM)
+template <int KB>
+__device__ __forceinline__ void orth_impl(double* Y, int m, int k, double* smem) {
+  using SM = AccumSmem<KB>;
+  double* red = smem;
+  double* G = red + SM::RED + SM::S;
+  accum_cholqr<KB, true>(Y, m, k, true, G, red);
+  accum_cholqr<KB, true>(Y, m, k, false, G, red);
+  accum_cholqr<KB, true>(Y, m, k, false, G, red);
+}
+
+__device__ __noinline__ void dev_orth(double* Y, int m, int k, double* smem) {
+  if (k <= 16) orth_impl<16>(Y, m, k, smem);
+  else orth_impl<32>(Y, m, k, smem);
+}
+
+// C[m x n] := A[m x n]
+__device__ __noinline__ void dev_copy(double* C, int ldc, const double* A, int lda, int m, int n) {
+  for (int e = threadIdx.x; e < m * n; e += NT) {
+    const int r = e / n, c = e % n;
+    C[(size_t)r * ldc + c] = ldcg(&A[(size_t)r * lda + c]);
+  }
+  __syncthreads();
+}
+
 __device__ __noinline__ void dev_accum(const pp_task& T, double* smem) {
   const int ny = T.m, k1 = T.k, k2 = T.l;
   if (k1 <= 16 && k2 <= 16) {
@@ -1343,6 +1369,13 @@ __device__ bool run_task(const pp_task& T, double* smem, TcCtx& tc, int& err) {
       dev_trinv(T.p[0], T.ld[0], T.p[1], T.ld[1], T.m, T.n, T.o, T.ctrl, smem);
       return true;
     case PP_OP_TRMV: return dev_trmv(T, smem);
+    case PP_OP_ORTH:
+      if (T.n < 1 || T.n > PP_VM_MAX_RANK || T.ld[0] != T.n) return false;
+      dev_orth(T.p[0], T.m, T.n, smem);
+      return true;
+    case PP_OP_COPY:
+      dev_copy(T.p[0], T.ld[0], T.p[1], T.ld[1], T.m, T.n);
+      return true;
     default: return false;
   }
 }

@@ -31,6 +31,19 @@ def test_parallel_executor_matches_sequential(pp, oracle, hctx):
     assert np.array_equal(a1.matrix, a2.matrix)
 
 
+def test_parallel_executor_matches_sequential_standard_admissibility(pp, oracle, hctx):
+    """Standard admissibility adds the sketched updates (GEMMs into work buffers, ORTH, COPY):
+    running the program over its DAG with 8 threads gives the sequential result bit for bit,
+    so every conflicting pair of tasks is ordered by an edge."""
+    h, _ = pp.make_kernel_problem(hctx, 1024, 2, "laplace", 1e-3, 32, 8, admissibility=1, eta=1.0, seed=3)
+    assert h.program_info(0)["op_count"]["orth"] > 0
+    a1 = oracle.HostArenas(h, 0)
+    a1.run(threads=1)
+    a2 = oracle.HostArenas(h, 0)
+    a2.run(threads=8)
+    assert np.array_equal(a1.matrix, a2.matrix)
+
+
 def test_dense_lu_is_an_lu(oracle):
     rng = np.random.default_rng(0)
     n = 200
@@ -117,3 +130,21 @@ def test_golden_accum_matches_reference_kernel(oracle):
     oracle.accum(U1, V1, g["U2"], g["V2"], g["R"])
     want = g["U1_out"] @ g["V1_out"].T
     assert np.linalg.norm(U1 @ V1.T - want) / np.linalg.norm(want) < 1e-12
+
+
+def test_standard_admissibility_program_solves(pp, oracle, hctx):
+    """The sketched updates of standard admissibility (products of hierarchical blocks into
+    low-rank blocks) give a factorization whose solve is accurate (oracle executor)."""
+    n = 2048
+    h, prob = pp.make_kernel_problem(hctx, n, 2, "laplace", 1e-3, 64, 16, admissibility=1, eta=1.0, seed=3)
+    assert h.program_info(0)["op_count"]["orth"] > 0
+    ar = oracle.HostArenas(h, 0)
+    ar.run(threads=4)
+    b = pp.rhs(n, 1)
+    sol = oracle.HostArenas(h, 1, 1, rhs=b)
+    sol.matrix[:] = ar.matrix
+    sol.tasks, sol.succ, sol.indeg, sol.ready = h.encode_program(1, 1, sol.bases())
+    sol.run()
+    x = sol.rhs[:n].reshape(n, 1)
+    r = b - prob.dense() @ x
+    assert np.abs(r).max() / (prob.norm_inf * np.abs(x).max() + np.abs(b).max()) < 1e-6

@@ -128,6 +128,10 @@ def task_regions(T):
         return [reg(0, m, n, False), reg(1, m, m, True)]
     if op == 12:  # TRMV: B (m x n) := M B, M m x m
         return [reg(0, m, n, False), reg(1, m, m, True)]
+    if op == 13:  # ORTH: Y (m x n) in place
+        return [reg(0, m, n, False)]
+    if op == 14:  # COPY: C (m x n) := A
+        return [reg(0, m, n, False), reg(1, m, n, True)]
     raise AssertionError(f"unexpected op {op}")
 
 
