@@ -81,12 +81,20 @@ int64_t Program::count_op(int op) const {
 }
 
 int64_t Program::set_gemm_precision(int prec) {
+  // the tensor-core form pays for staging the operands (FP64 -> TF32 in shared memory) and
+  // reading the accumulators back from tensor memory; only contractions of at least
+  // kTcMinDim in every dimension (the dense Schur updates) gain from it, the skinny low-rank
+  // products stay FP64 SIMT
   int64_t c = 0;
-  for (auto& t : tasks)
-    if (t.t.op == PP_OP_GEMM && t.t.prec != prec) {
-      t.t.prec = prec;
+  for (auto& t : tasks) {
+    if (t.t.op != PP_OP_GEMM) continue;
+    const bool big = t.t.m >= kTcMinDim && t.t.n >= kTcMinDim && t.t.k >= kTcMinDim;
+    const int want = big ? prec : PP_PREC_FP64;
+    if (t.t.prec != want) {
+      t.t.prec = want;
       ++c;
     }
+  }
   return c;
 }
 

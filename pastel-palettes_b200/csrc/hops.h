@@ -118,6 +118,8 @@ constexpr int kSolveTri = 256;
 constexpr int kTrmvCols = 16;
 // largest rank of the added term of one ACCUM (the VM keeps it in registers)
 constexpr int kAccumMaxK2 = 32;
+// smallest m, n and k of a GEMM instruction the TF32 form runs on the tensor cores
+constexpr int kTcMinDim = 64;
 
 class Generator {
  public:

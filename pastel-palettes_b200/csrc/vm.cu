@@ -1569,7 +1569,7 @@ __device__ __forceinline__ double kernel_eval_nr(double d2, double p0, double in
 #define KR_RPT 2                      /* rows per thread */
 #define KR_ROWS (KR_THREADS * KR_RPT)  /* rows per CTA */
 #define KR_COLS 256
-#define KR_SEG 512   /* columns per partial sum */
+#define KR_SEG 128   /* columns per partial sum (small: enough CTAs to fill the SMs) */
 // matrix-free partial products of r = b - A x, A_ij = K(|p_i - p_j|) (+ shift on i == j):
 // CTA (row block, column segment) sums its KR_SEG columns (points and x staged through smem
 // in KR_COLS tiles; each thread carries KR_RPT rows, so every staged column feeds
