@@ -1631,13 +1631,98 @@ __global__ void __launch_bounds__(KR_THREADS) kernel_residual_part(double p0, do
       for (int q = 0; q < nrhs; ++q) part[((size_t)seg * n + row[t]) * nrhs + q] = acc[t][q];
 }
 
+// Symmetric form of the partial products (kernel matrices are symmetric): CTA b takes the
+// tile pair (I, J), I <= J, of KR_SEG x KR_SEG tiles and evaluates each entry once.  Thread t
+// owns row I*KR_SEG + t: a_ij x_j goes to its register sums (part[J][i]); for I < J, a_ij x_i
+// goes to the column sums of row j (part[I][j]) through per-warp accumulators in shared memory,
+// walked on a skewed diagonal (lane l visits column (l + s) mod KR_SEG at step s, so the lanes
+// of a warp never touch the same column) and added in warp order at the end.  Every
+// (segment, row) partial is written once, by one CTA: deterministic, no atomics.
+template <int KIND, int DIM, int NR>
+__global__ void __launch_bounds__(KR_SEG) kernel_residual_sym(double p0, double shift,
+                                                               const double* __restrict__ pts, int n,
+                                                               const double* __restrict__ x,
+                                                               double* __restrict__ part, int nrhs, int T) {
+  constexpr int W = KR_SEG / 32;
+  __shared__ double sp[KR_SEG * DIM];
+  __shared__ double sx[KR_SEG * NR];
+  __shared__ double col[W][KR_SEG * NR];
+  // (I, J) of linear index b over the upper triangle, row by row: b = I T - I (I - 1) / 2 + (J - I)
+  const long long b = blockIdx.x;
+  const double tt = 2.0 * T + 1.0;
+  int I = (int)floor((tt - sqrt(tt * tt - 8.0 * (double)b)) * 0.5);
+  auto row_start = [&](int r) { return (long long)r * T - (long long)r * (r - 1) / 2; };
+  while (I > 0 && row_start(I) > b) --I;
+  while (row_start(I + 1) <= b) ++I;
+  const int J = I + (int)(b - row_start(I));
+  const int t = threadIdx.x, w = t >> 5, lane = t & 31;
+  const int i = I * KR_SEG + t, j0 = J * KR_SEG;
+  const double inv_p0 = 1.0 / p0;
+  for (int e = t; e < KR_SEG * DIM; e += KR_SEG) {
+    const int jj = e / DIM;
+    sp[e] = j0 + jj < n ? pts[(size_t)j0 * DIM + e] : 0.0;
+  }
+  for (int e = t; e < KR_SEG * NR; e += KR_SEG) {
+    const int jj = e / NR, q = e % NR;
+    sx[e] = (j0 + jj < n && q < nrhs) ? x[(size_t)(j0 + jj) * nrhs + q] : 0.0;
+  }
+  for (int e = t; e < W * KR_SEG * NR; e += KR_SEG) (&col[0][0])[e] = 0.0;
+  const int ir = min(i, n - 1);
+  double pi[DIM], xi[NR], acc[NR];
+#pragma unroll
+  for (int d = 0; d < DIM; ++d) pi[d] = pts[(size_t)ir * DIM + d];
+#pragma unroll
+  for (int q = 0; q < NR; ++q) {
+    xi[q] = (i < n && q < nrhs) ? x[(size_t)ir * nrhs + q] : 0.0;
+    acc[q] = 0.0;
+  }
+  __syncthreads();
+  const bool offdiag = I != J;
+  const int jn = min(KR_SEG, n - j0);
+#pragma unroll 2
+  for (int st = 0; st < KR_SEG; ++st) {
+    const int jj = (lane + st) & (KR_SEG - 1);
+    if (jj < jn && i < n) {
+      double d2 = 0.0;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        const double u = pi[d] - sp[jj * DIM + d];
+        d2 = fma(u, u, d2);
+      }
+      double a = kernel_eval_nr<KIND>(d2, p0, inv_p0);
+      if (!offdiag && j0 + jj == i) a += shift;
+#pragma unroll
+      for (int q = 0; q < NR; ++q) acc[q] = fma(a, sx[jj * NR + q], acc[q]);
+      if (offdiag) {
+#pragma unroll
+        for (int q = 0; q < NR; ++q) col[w][jj * NR + q] = fma(a, xi[q], col[w][jj * NR + q]);
+      }
+    }
+  }
+  if (i < n)
+    for (int q = 0; q < nrhs; ++q) part[((size_t)J * n + i) * nrhs + q] = acc[q];
+  if (offdiag) {
+    __syncthreads();
+    const int jrow = j0 + t;
+    if (jrow < n)
+      for (int q = 0; q < nrhs; ++q) {
+        double v = col[0][t * NR + q];
+#pragma unroll
+        for (int ww = 1; ww < W; ++ww) v += col[ww][t * NR + q];
+        part[((size_t)I * n + jrow) * nrhs + q] = v;
+      }
+  }
+}
+
 template <int KIND, int DIM>
 cudaError_t launch_kernel_residual(dim3 grid, cudaStream_t s, double p0, double shift, const double* pts, int n,
                                    const double* x, double* part, int nrhs) {
+  const int T = (n + KR_SEG - 1) / KR_SEG;
+  const unsigned pairs = (unsigned)((long long)T * (T + 1) / 2);
   if (nrhs == 1)
-    kernel_residual_part<KIND, DIM, 1><<<grid, KR_THREADS, 0, s>>>(p0, shift, pts, n, x, part, nrhs);
+    kernel_residual_sym<KIND, DIM, 1><<<pairs, KR_SEG, 0, s>>>(p0, shift, pts, n, x, part, nrhs, T);
   else if (nrhs <= 4)
-    kernel_residual_part<KIND, DIM, 4><<<grid, KR_THREADS, 0, s>>>(p0, shift, pts, n, x, part, nrhs);
+    kernel_residual_sym<KIND, DIM, 4><<<pairs, KR_SEG, 0, s>>>(p0, shift, pts, n, x, part, nrhs, T);
   else if (nrhs <= 8)
     kernel_residual_part<KIND, DIM, 8><<<grid, KR_THREADS, 0, s>>>(p0, shift, pts, n, x, part, nrhs);
   else
