@@ -1000,6 +1000,104 @@ __device__ __noinline__ void accum_tn(const double* X, int lx, int a, const doub
   __syncthreads();
 }
 
+// FP64 tensor-core form of accum_tn for untransposed W (the usual case): per warp, its row
+// slice is the k dimension of out = X^T [W1 W2] computed with mma.sync.m8n8k4.f64 (FP64 has
+// no tcgen05 kind; this is the FP64 tensor path of sm_100a).  Fragment layouts of m8n8k4.f64:
+// A (8 x 4) lane l holds A[l/4][l%4]; B (4 x 8) holds B[l%4][l/4]; C (8 x 8) holds
+// C[l/4][2(l%4) + {0,1}].  Rows are taken four at a time (one k step), several k steps of
+// loads issued before their products.  Warp partials are combined as in accum_tn (fixed order).
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+template <int KB, bool XG, bool WG>
+__device__ __noinline__ void accum_tn_mma(const double* X, int lx, int a, const double* W1, int lw1, int b1,
+                                          const double* W2, int lw2, int b2, int L, double* out1, double* out2,
+                                          int ldo, double* red) {
+  constexpr int MT = KB / 8, NTL = KB / 8;  // m tiles of X^T; n tiles per W
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int qr = lane >> 2, qc = lane & 3;
+  double c1[MT][NTL][2], c2[MT][NTL][2];
+#pragma unroll
+  for (int i = 0; i < MT; ++i)
+#pragma unroll
+    for (int j = 0; j < NTL; ++j) c1[i][j][0] = c1[i][j][1] = c2[i][j][0] = c2[i][j][1] = 0.0;
+  const int per = (((L + 7) / 8) + 3) & ~3, l0 = min(L, w * per), l1 = min(L, l0 + per);
+  constexpr int KS = KB >= 32 ? 1 : 4;  // k steps (of 4 rows) whose loads go out together
+  for (int lb = l0; lb < l1; lb += 4 * KS) {
+    double fa[KS][MT], f1[KS][NTL], f2[KS][NTL];
+#pragma unroll
+    for (int s = 0; s < KS; ++s) {
+      const int l = lb + 4 * s + qc;  // the row this lane feeds (A col / B row = lane % 4)
+      const bool in = l < l1;
+#pragma unroll
+      for (int i = 0; i < MT; ++i) {
+        const int col = 8 * i + qr;
+        fa[s][i] = (in && col < a) ? ld_any<XG>(&X[(size_t)l * lx + col]) : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < NTL; ++j) {
+        const int col = 8 * j + qr;
+        f1[s][j] = (in && col < b1) ? ld_any<WG>(&W1[(size_t)l * lw1 + col]) : 0.0;
+        f2[s][j] = (in && col < b2) ? ld_any<WG>(&W2[(size_t)l * lw2 + col]) : 0.0;
+      }
+    }
+#pragma unroll
+    for (int s = 0; s < KS; ++s)
+#pragma unroll
+      for (int i = 0; i < MT; ++i)
+#pragma unroll
+        for (int j = 0; j < NTL; ++j) {
+          if (8 * j < b1) dmma(c1[i][j][0], c1[i][j][1], fa[s][i], f1[s][j]);
+          if (8 * j < b2) dmma(c2[i][j][0], c2[i][j][1], fa[s][i], f2[s][j]);
+        }
+  }
+  constexpr int SW = 2 * KB;
+  auto deposit = [&](int slot, bool add) {
+#pragma unroll
+    for (int i = 0; i < MT; ++i)
+#pragma unroll
+      for (int j = 0; j < NTL; ++j)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int r = 8 * i + qr, c = 8 * j + 2 * qc + e;
+          if (r < a && c < b1) {
+            double* p = &red[(slot * KB + r) * SW + c];
+            *p = add ? c1[i][j][e] + *p : c1[i][j][e];
+          }
+          if (r < a && c < b2) {
+            double* p = &red[(slot * KB + r) * SW + KB + c];
+            *p = add ? c2[i][j][e] + *p : c2[i][j][e];
+          }
+        }
+  };
+  if (w >= 4) deposit(w - 4, false);
+  __syncthreads();
+  if (w < 4) deposit(w, true);
+  __syncthreads();
+  const int bt = b1 + b2;
+  for (int e = threadIdx.x; e < a * bt; e += NT) {
+    const int i = e / bt, j = e % bt;
+    const int col = j < b1 ? j : KB + (j - b1);
+    const double v = red[(0 * KB + i) * SW + col] + red[(1 * KB + i) * SW + col] + red[(2 * KB + i) * SW + col] +
+                     red[(3 * KB + i) * SW + col];
+    if (j < b1) out1[i * ldo + j] = v;
+    else out2[i * ldo + (j - b1)] = v;
+  }
+  __syncthreads();
+}
+
+// out = X^T [W1 W2]: the tensor-core form when both W are untransposed, else the SIMT form
+template <int KB, bool XG, bool WG>
+__device__ __forceinline__ void accum_tn_any(const double* X, int lx, int a, const double* W1, int lw1, bool tW1,
+                                             int b1, const double* W2, int lw2, bool tW2, int b2, int L,
+                                             double* out1, double* out2, int ldo, double* red) {
+  if (!tW1 && !tW2) accum_tn_mma<KB, XG, WG>(X, lx, a, W1, lw1, b1, W2, lw2, b2, L, out1, out2, ldo, red);
+  else accum_tn<KB, XG, WG>(X, lx, a, W1, lw1, tW1, b1, W2, lw2, tW2, b2, L, out1, out2, ldo, red);
+}
+
 // Y[l][0..k) = A1[l] S1^T + alpha A2[l] S2^T for every row l (a thread per row), S1: k x c1,
 // S2: k x c2 in shared memory (ld lds).  Y may alias A1 (each row is read before written).
 template <int KB, bool A1G>
@@ -1044,7 +1142,7 @@ __device__ __noinline__ void accum_rows(double* Y, int ly, const double* A1, int
 template <int KB, bool YG>
 __device__ __noinline__ void accum_cholqr(double* Y, int m, int k, bool shifted, double* G, double* red) {
   double* rinv = G + KB * ACC_LG;
-  accum_tn<KB, YG, YG>(Y, k, k, Y, k, false, k, nullptr, 0, false, 0, m, G, nullptr, ACC_LG, red);
+  accum_tn_any<KB, YG, YG>(Y, k, k, Y, k, false, k, nullptr, 0, false, 0, m, G, nullptr, ACC_LG, red);
   if (threadIdx.x < 32) {  // right-looking Cholesky: lane c holds column c of G in registers
     const int lane = threadIdx.x;
     double g[KB];
@@ -1231,7 +1329,7 @@ __device__ __forceinline__ void accum_impl(const pp_task& T, double* smem) {
   const double al = T.alpha;
   constexpr int LS = 2 * KB;
   // S1 = R^T V1, S2 = R^T V2
-  accum_tn<KB, true, true>(R, lr, k1, V1, lv1, false, k1, V2, lv2, tV2, k2, nx, S, S + KB, LS, red);
+  accum_tn_any<KB, true, true>(R, lr, k1, V1, lv1, false, k1, V2, lv2, tV2, k2, nx, S, S + KB, LS, red);
   // Y = U1 S1^T + alpha U2 S2^T
   accum_rows<KB, true>(Y, k1, U1, lu1, k1, U2, lu2, tU2, k2, al, S, S + KB, LS, k1, ny);
   __syncthreads();
@@ -1239,7 +1337,7 @@ __device__ __forceinline__ void accum_impl(const pp_task& T, double* smem) {
   accum_cholqr<KB, YG>(Y, ny, k1, false, G, red);
   accum_cholqr<KB, YG>(Y, ny, k1, false, G, red);
   // P1 = Y^T U1, P2 = Y^T U2
-  accum_tn<KB, YG, true>(Y, k1, k1, U1, lu1, false, k1, U2, lu2, tU2, k2, ny, S, S + KB, LS, red);
+  accum_tn_any<KB, YG, true>(Y, k1, k1, U1, lu1, false, k1, U2, lu2, tU2, k2, ny, S, S + KB, LS, red);
   // V1 := V1 P1^T + alpha V2 P2^T (rows read before written)
   accum_rows<KB, true>(V1, lv1, V1, lv1, k1, V2, lv2, tV2, k2, al, S, S + KB, LS, k1, nx);
   __syncthreads();
@@ -1247,7 +1345,7 @@ __device__ __forceinline__ void accum_impl(const pp_task& T, double* smem) {
     // adaptive rank: U1 V1^T = Y V1^T with Y orthonormal, so the singular values are those of
     // V1; rotate both factors into the eigenbasis of V1^T V1 and keep the directions whose
     // singular value exceeds beta times the largest (zero columns beyond the new rank)
-    accum_tn<KB, true, true>(V1, lv1, k1, V1, lv1, false, k1, nullptr, 0, false, 0, nx, G, nullptr, ACC_LG, red);
+    accum_tn_any<KB, true, true>(V1, lv1, k1, V1, lv1, false, k1, nullptr, 0, false, 0, nx, G, nullptr, ACC_LG, red);
     double* Z = red;
     double* cs = red + KB * ACC_LG;
     double* flag = cs + 2 * KB;
