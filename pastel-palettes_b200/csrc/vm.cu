@@ -1137,6 +1137,61 @@ __device__ __noinline__ void accum_rows(double* Y, int ly, const double* A1, int
   }
 }
 
+// FP64 tensor-core form of accum_rows for an untransposed A2: warp w takes 8-row tiles
+// r0 = 8 (w + 8 t); Y tile (8 x k) = A1 tile S1^T + alpha A2 tile S2^T with mma.m8n8k4.f64
+// (A fragments from the rows, B fragments from S in shared memory).  A warp reads all of its
+// tile's rows before it stores any, so Y may alias A1.
+template <int KB, bool A1G>
+__device__ __noinline__ void accum_rows_mma(double* Y, int ly, const double* A1, int la1, int c1, const double* A2,
+                                           int la2, int c2, double alpha, const double* S1, const double* S2,
+                                           int lds, int k, int L) {
+  constexpr int NTL = KB / 8, KST = KB / 4;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int qr = lane >> 2, qc = lane & 3;
+  for (int r0 = 8 * w; r0 < L; r0 += 8 * (NT / 32)) {
+    const int row = r0 + qr;
+    const bool rin = row < L;
+    double fa1[KST], fa2[KST];
+#pragma unroll
+    for (int s = 0; s < KST; ++s) {
+      const int col = 4 * s + qc;
+      fa1[s] = (rin && col < c1) ? ld_any<A1G>(&A1[(size_t)row * la1 + col]) : 0.0;
+      fa2[s] = (rin && col < c2) ? ldcg(&A2[(size_t)row * la2 + col]) : 0.0;
+    }
+    double y1[NTL][2], y2[NTL][2];
+#pragma unroll
+    for (int j = 0; j < NTL; ++j) y1[j][0] = y1[j][1] = y2[j][0] = y2[j][1] = 0.0;
+#pragma unroll
+    for (int s = 0; s < KST; ++s) {
+      const int kk = 4 * s + qc;
+#pragma unroll
+      for (int j = 0; j < NTL; ++j) {
+        const int n = 8 * j + qr;
+        if (4 * s < c1) dmma(y1[j][0], y1[j][1], fa1[s], (n < k && kk < c1) ? S1[n * lds + kk] : 0.0);
+        if (4 * s < c2) dmma(y2[j][0], y2[j][1], fa2[s], (n < k && kk < c2) ? S2[n * lds + kk] : 0.0);
+      }
+    }
+    if (rin) {
+#pragma unroll
+      for (int j = 0; j < NTL; ++j)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int col = 8 * j + 2 * qc + e;
+          if (col < k) Y[(size_t)row * ly + col] = fma(alpha, y2[j][e], y1[j][e]);
+        }
+    }
+  }
+}
+
+// Y = A1 S1^T + alpha A2 S2^T: the tensor-core form unless A2 is stored transposed
+template <int KB, bool A1G>
+__device__ __forceinline__ void accum_rows_any(double* Y, int ly, const double* A1, int la1, int c1, const double* A2,
+                                              int la2, bool tA2, int c2, double alpha, const double* S1,
+                                              const double* S2, int lds, int k, int L) {
+  if (!tA2) accum_rows_mma<KB, A1G>(Y, ly, A1, la1, c1, A2, la2, c2, alpha, S1, S2, lds, k, L);
+  else accum_rows<KB, A1G>(Y, ly, A1, la1, c1, A2, la2, tA2, c2, alpha, S1, S2, lds, k, L);
+}
+
 // One CholeskyQR pass on Y (m x k, ld k): G = Y^T Y (+ shift I), G = C^T C, Y := Y C^-1.
 // A non-positive pivot marks a rank-deficient column, which is zeroed.
 template <int KB, bool YG>
@@ -1163,16 +1218,16 @@ __device__ __noinline__ void accum_cholqr(double* Y, int m, int k, bool shifted,
       if (j < k) {
         const double d = __shfl_sync(0xffffffffu, g[j], j);  // G[j][j]
         const bool live = d > tiny;
-        const double rjj = live ? sqrt(d) : 0.0;
-        if (lane == j) g[j] = rjj;
-        if (lane > j) g[j] = live ? g[j] / rjj : 0.0;  // C[j][lane]
+        const double ri = live ? rsqrt(d) : 0.0;  // 1 / c_jj
+        if (lane == j) g[j] = d * ri;
+        if (lane > j) g[j] = g[j] * ri;  // C[j][lane]
         // G[c1][lane] -= C[j][c1] C[j][lane] for j < c1 <= lane
 #pragma unroll
         for (int c1 = j + 1; c1 < KB; ++c1) {
           const double cjc1 = __shfl_sync(0xffffffffu, g[j], c1);
           if (c1 < k && lane >= c1) g[c1] = fma(-cjc1, g[j], g[c1]);
         }
-        if (lane == j) G[KB * ACC_LG + j] = live ? 1.0 / rjj : 0.0;
+        if (lane == j) G[KB * ACC_LG + j] = ri;
       }
     }
 #pragma unroll
@@ -1331,7 +1386,7 @@ __device__ __forceinline__ void accum_impl(const pp_task& T, double* smem) {
   // S1 = R^T V1, S2 = R^T V2
   accum_tn_any<KB, true, true>(R, lr, k1, V1, lv1, false, k1, V2, lv2, tV2, k2, nx, S, S + KB, LS, red);
   // Y = U1 S1^T + alpha U2 S2^T
-  accum_rows<KB, true>(Y, k1, U1, lu1, k1, U2, lu2, tU2, k2, al, S, S + KB, LS, k1, ny);
+  accum_rows_any<KB, true>(Y, k1, U1, lu1, k1, U2, lu2, tU2, k2, al, S, S + KB, LS, k1, ny);
   __syncthreads();
   accum_cholqr<KB, YG>(Y, ny, k1, true, G, red);
   accum_cholqr<KB, YG>(Y, ny, k1, false, G, red);
@@ -1339,7 +1394,7 @@ __device__ __forceinline__ void accum_impl(const pp_task& T, double* smem) {
   // P1 = Y^T U1, P2 = Y^T U2
   accum_tn_any<KB, YG, true>(Y, k1, k1, U1, lu1, false, k1, U2, lu2, tU2, k2, ny, S, S + KB, LS, red);
   // V1 := V1 P1^T + alpha V2 P2^T (rows read before written)
-  accum_rows<KB, true>(V1, lv1, V1, lv1, k1, V2, lv2, tV2, k2, al, S, S + KB, LS, k1, nx);
+  accum_rows_any<KB, true>(V1, lv1, V1, lv1, k1, V2, lv2, tV2, k2, al, S, S + KB, LS, k1, nx);
   __syncthreads();
   if ((T.flags & PP_ADAPT_RANK) && T.beta > 0.0) {
     // adaptive rank: U1 V1^T = Y V1^T with Y orthonormal, so the singular values are those of
@@ -1352,8 +1407,8 @@ __device__ __forceinline__ void accum_impl(const pp_task& T, double* smem) {
     int* pq = reinterpret_cast<int*>(flag + 2);
     jacobi_eig(G, Z, k1, cs, pq, flag);
     const int r = accum_truncate<KB>(G, Z, k1, T.beta, S, LS, pq);
-    accum_rows<KB, true>(V1, lv1, V1, lv1, k1, nullptr, 0, false, 0, 1.0, S, S, LS, k1, nx);
-    accum_rows<KB, YG>(Y, k1, Y, k1, k1, nullptr, 0, false, 0, 1.0, S, S, LS, k1, ny);
+    accum_rows_any<KB, true>(V1, lv1, V1, lv1, k1, nullptr, 0, false, 0, 1.0, S, S, LS, k1, nx);
+    accum_rows_any<KB, YG>(Y, k1, Y, k1, k1, nullptr, 0, false, 0, 1.0, S, S, LS, k1, ny);
     __syncthreads();
     if (threadIdx.x == 0 && T.p[5]) T.p[5][0] = (double)r;
   }
