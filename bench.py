@@ -29,7 +29,7 @@ METRIC = "H-LU factor+solve/s at 1e-10 residual (FP64 HODLR N=8192)"
 # DRAM bytes (read + write) of one job's factor work inside the batched factor launch, from one
 # ncu capture of the batch-4 launch (dram__bytes.sum.per_second x gpu__time_duration.sum / 4);
 # the jobs touch disjoint arenas, so the launch's traffic scales with the batch
-FACTOR_DRAM_BYTES_PER_JOB = 115.6e6
+FACTOR_DRAM_BYTES_PER_JOB = 110.7e6
 
 
 def load_pp():
@@ -258,15 +258,83 @@ def serving_leg(pp, ctx, n_requests, rate, seed=2024, smin=1024, smax=3072):
         raise SystemExit(f"serving: a request failed: {[x['message'] for x in st if x['status'] != 'done']}")
     lat = np.array([x["t_done_ms"] - x["t_submit_ms"] for x in st])
     span_s = (max(x["t_done_ms"] for x in st) - min(x["t_submit_ms"] for x in st)) / 1e3
+    for (h, prob, rhs), x in zip(reqs, st):  # per-request record on stderr (the JSON keeps the summary)
+        print(f"serve n={prob.n} kernel={prob.kernel} nrhs={rhs.shape[2]} sets={rhs.shape[0]} "
+              f"iterations={x['iterations']} queued_ms={x['t_admit_ms'] - x['t_submit_ms']:.1f} "
+              f"run_ms={x['t_done_ms'] - x['t_admit_ms']:.1f} enqueue_ms={x['t_enqueued_ms'] - x['t_admit_ms']:.1f} "
+              f"submit_ms={x['t_submit_ms']:.1f}", file=sys.stderr)
     vectors = sum(rhs.shape[0] * rhs.shape[2] for _, _, rhs in reqs)
     return {"requests": n_requests, "arrival_rate_per_s": rate, "p50_ms": float(np.percentile(lat, 50)),
             "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
             "solves_per_s": vectors / span_s, "solves_unit": "right-hand-side vectors solved to 1e-10 per second",
+            "max_queued_ms": max(x["t_admit_ms"] - x["t_submit_ms"] for x in st),
+            "max_run_ms": max(x["t_done_ms"] - x["t_admit_ms"] for x in st),
+            "max_enqueue_ms": max(x["t_enqueued_ms"] - x["t_admit_ms"] for x in st),
             "worst_backward_error": max(x["backward_error"] for x in st),
             "refinement_solves": int(sum(x["iterations"] for x in st)),
             "workload": f"N log-uniform [{smin},{smax}] (multiple of 64), 3-D points, kernels laplace/exp/matern32, "
                         f"leaf 128, rank 16, 1-16 RHS, 0-4 follow-up sets, Poisson arrivals; matrices built "
                         f"before the clock", "slots": 4}
+
+
+def uneven_batch_leg(pp, ctx, n_inst, steps, warmup, seed=4096, smin=1024, smax=16384):
+    """Configuration-4 style batch: n_inst H-matrices of uneven size in one merged persistent
+    launch.  N log-uniform in [smin, smax] (multiple of 64), points U[0,1]^2, kernel
+    exp(-r / 0.1) + 1e-2 I, leaf 128, adaptive rank <= 24 at 1e-7, TF32 GEMM instructions with
+    FP64 refinement to 1e-10, tile / grid autotuned, restore + factor + refinement captured as a
+    CUDA graph and replayed.  Matrices are built on the host before the clock."""
+    import torch
+    rng = np.random.default_rng(seed)
+    hs, probs = [], []
+    for i in range(n_inst):
+        n = int(round(np.exp(rng.uniform(np.log(smin), np.log(smax))) / 64)) * 64
+        h, prob = pp.make_kernel_problem(ctx, n, 2, "exp", 0.1, 128, 24, shift=1e-2, seed=seed + 31 * i, rank_tol=1e-7)
+        h.set_precision(pp.TF32)
+        hs.append(h)
+        probs.append(prob)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        for h in hs:
+            h.upload(s)
+            h.keep_original(s)
+    s.synchronize()
+    batch = pp.Batch(ctx, hs)
+    tune = batch.autotune(s)
+    ref = pp.BatchRefiner(batch, probs, stream=s)
+    bs = [torch.from_numpy(pp.rhs(p.n, 1, seed=3 + i)).cuda() for i, p in enumerate(probs)]
+    with torch.cuda.stream(s):
+        for _ in range(max(1, warmup)):
+            batch.restore(s)
+            batch.factor(s)
+            xs, hist = ref.solve(bs, tol=WORKLOAD["tol"])
+    batch.sync(s)
+    iters = len(hist)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            batch.restore(s)
+            batch.factor(s)
+            out = ref.run(bs, iters)
+    total, worst = 0.0, 0.0
+    for _ in range(steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(s):
+            e0.record(s)
+            g.replay()
+            e1.record(s)
+        e1.synchronize()
+        total += e0.elapsed_time(e1) / 1e3
+        worst = max(worst, max(ref.errors(bs, *out)))
+    batch.sync(s)
+    sizes = [p.n for p in probs]
+    flops = batch.program_info(0)["flops"]
+    del g
+    return {"instances": n_inst, "n_min": min(sizes), "n_max": max(sizes), "n_total": int(sum(sizes)),
+            "factor_solve_per_s": n_inst * steps / total, "ms_per_step": 1e3 * total / steps,
+            "refinement_solves": iters, "worst_backward_error": worst, "factor_gflop_per_step": flops / 1e9,
+            "factor_gflops": flops / (total / steps) / 1e9, "autotune": tune,
+            "workload": "config-4 style: N log-uniform [1024,16384], exp(-r/0.1)+1e-2 I on U[0,1]^2, leaf 128, "
+                        "adaptive rank <= 24 @ 1e-7, TF32 GEMMs + FP64 refinement, one merged launch, graph replay"}
 
 
 def main():
@@ -282,6 +350,8 @@ def main():
     ap.add_argument("--compare", type=int, default=1, help="also time the other precision form")
     ap.add_argument("--serve-requests", type=int, default=16, help="requests of the serving leg (0: skip)")
     ap.add_argument("--autotune", type=int, default=1, help="pick tile and grid of the batch by timing")
+    ap.add_argument("--uneven", type=int, default=0, help="instances of the configuration-4 style uneven batch "
+                                                           "leg (0: skip; host construction takes minutes)")
     ap.add_argument("--serve-rate", type=float, default=40.0, help="Poisson arrival rate of the serving leg (1/s)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -381,7 +451,10 @@ def main():
     iters = main_stats["refinement_solves"]
     total_max = main_stats["total_s"]
     value = main_stats["value"]
-    launches_per_step = 2 + iters * (2 + B)
+    # per step: the factor (init + VM), per refinement iteration one batched solve (init + VM)
+    # and the batched update / residual / reduction launches
+    launches_per_step = 2 + iters * (2 + pp.residual_batch_launches(
+        [(p.kernel, p.dim, b.shape[1], True) for p, b in zip(probs, bs)]))
 
     # --- end to end through the C ABI: matrices and right-hand sides up from pinned host
     #     memory, batched factor + refinement, solutions down
@@ -458,6 +531,7 @@ def main():
                          "frac": B * finfo["flops"] / fac_s / 1e12 / fp64_peak,
                          "peak_source": "measured in this run: torch float64 matmul 8192^3"}}
 
+    uneven = uneven_batch_leg(pp, ctx, args.uneven, max(3, args.steps // 2), args.warmup) if args.uneven > 0 else None
     serving = None
     if args.serve_requests > 0:
         serving = serving_leg(pp, ctx, args.serve_requests, args.serve_rate, seed=2024 + rank)
@@ -489,6 +563,7 @@ def main():
                         "h2d_bytes_per_step": B * (hs[0].arena_bytes() + 8 * n),
                         "d2h_bytes_per_step": B * 8 * n},
                 "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "serving": serving,
+                "uneven_batch": uneven,
                 "plain_fp64_single_instance": {
                     "value": 1e3 / float(np.median(lat)), "unit": "factor+solve/s",
                     "note": "one job per persistent launch, FP64, refinement to the same tolerance (the "

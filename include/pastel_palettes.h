@@ -207,6 +207,8 @@ typedef struct pp_request_stats {
   int iterations;          /* refinement solves over all sets                                 */
   double backward_error;   /* worst final backward error over the finished sets               */
   double t_submit_ms, t_admit_ms, t_done_ms;  /* server clock (ms); -1 until reached          */
+  double t_enqueued_ms;    /* when the upload, the factorization and the first solve were
+                              queued on the device (the host work of admission ends)          */
   long long device_bytes;  /* device memory the request holds while admitted                  */
   char message[128];       /* why a request failed                                            */
 } pp_request_stats;
@@ -234,6 +236,27 @@ pp_status pp_dense_residual_dev(pp_context* ctx, const double* A, int lda, int n
 pp_status pp_kernel_residual_dev(pp_context* ctx, int kernel, double p0, double shift, const double* pts_dev,
                                  int dim, int n, const double* x, const double* b, double* r, int nrhs,
                                  void* stream);
+/* One job of pp_kernel_residual_batch_dev (device pointers). */
+typedef struct pp_residual_job {
+  int kernel;           /* as pp_kernel_residual_dev */
+  int dim;              /* 1..3 */
+  int n;
+  int nrhs;             /* 1..16 */
+  double p0, shift;
+  const double* points; /* n x dim */
+  double* x;            /* n x nrhs; x += dx first when dx is not NULL */
+  const double* dx;     /* n x nrhs or NULL */
+  const double* b;      /* n x nrhs */
+  double* r;            /* n x nrhs */
+} pp_residual_job;
+/* The refinement update and residual of many kernel problems: for every job x += dx (when dx
+ * is set), then r = b - A x.  One update launch, one residual launch per group of jobs with the
+ * same kernel, dimension and right-hand-side width (up to 64 jobs each), one reduction launch;
+ * each job's r is bit-identical to pp_kernel_residual_dev's.  Kernels 0 and 1 need a finite
+ * p0 >= 0.  Partial sums go through the context-owned buffer, sized for the sum of the
+ * jobs' needs (grown on the first call of a larger total: make that call before capturing a
+ * CUDA graph); calls on different streams must not overlap. */
+pp_status pp_kernel_residual_batch_dev(pp_context* ctx, int njobs, const pp_residual_job* jobs, void* stream);
 
 /* --- rts (DAG primitives, rts/ops.h, rts/dependency.h) ------------------- */
 /* DataMap2D::checkOverlap (rts/ops.cpp:7-40); regions: ptr, pitch, width (bytes), height */

@@ -17,6 +17,7 @@ library or raise.
 """
 from __future__ import annotations
 
+import collections
 import ctypes as C
 import os
 import time
@@ -69,9 +70,28 @@ class _RequestDesc(C.Structure):
                 ("n_sets", C.c_int), ("tol", C.c_double), ("max_iter", C.c_int), ("x_out", C.c_void_p)]
 
 
+def residual_batch_launches(jobs, per_launch=64):
+    """Kernel launches of one pp_kernel_residual_batch_dev call; jobs: (kernel, dim, nrhs,
+    has_dx) tuples.  Update and reduction run in chunks of `per_launch` jobs, the residual once
+    per chunk of a (kernel, dim, nrhs 1 | 2-4) group and once per job of more than 4 RHS."""
+    if not jobs:
+        return 0
+    chunks = lambda c: (c + per_launch - 1) // per_launch
+    groups = collections.Counter((k, d, 1 if r == 1 else 4) for k, d, r, _ in jobs if r <= 4)
+    return (chunks(sum(1 for j in jobs if j[3])) + sum(chunks(c) for c in groups.values())
+            + sum(1 for j in jobs if j[2] > 4) + chunks(len(jobs)))
+
+
+class _ResidualJob(C.Structure):
+    _fields_ = [("kernel", C.c_int), ("dim", C.c_int), ("n", C.c_int), ("nrhs", C.c_int), ("p0", C.c_double),
+                ("shift", C.c_double), ("points", C.c_void_p), ("x", C.c_void_p), ("dx", C.c_void_p),
+                ("b", C.c_void_p), ("r", C.c_void_p)]
+
+
 class _RequestStats(C.Structure):
     _fields_ = [("status", C.c_int), ("iterations", C.c_int), ("backward_error", C.c_double),
                 ("t_submit_ms", C.c_double), ("t_admit_ms", C.c_double), ("t_done_ms", C.c_double),
+                ("t_enqueued_ms", C.c_double),
                 ("device_bytes", C.c_longlong), ("message", C.c_char * 128)]
 
 
@@ -125,6 +145,7 @@ def lib():
             "pp_dev_hierarchical_getrf": (i, [vp, i, i, i]),
             "pp_dense_residual_dev": (i, [vp, vp, i, i, vp, vp, vp, i, vp]),
             "pp_kernel_residual_dev": (i, [vp, i, d, d, vp, i, i, vp, vp, vp, i, vp]),
+            "pp_kernel_residual_batch_dev": (i, [vp, i, C.POINTER(_ResidualJob), vp]),
             "pp_datamap2d_check_overlap": (i, [C.c_uint64, C.c_size_t, C.c_size_t, C.c_size_t,
                                                C.c_uint64, C.c_size_t, C.c_size_t, C.c_size_t]),
             "pp_operation_dependency": (i, [i, vp, vp, i, vp, vp]),
@@ -237,6 +258,19 @@ class Context:
         self.check(lib().pp_kernel_residual_dev(self._h, kernel, p0, shift, pts.data_ptr(), pts.shape[1], n,
                                                 x.data_ptr(), b.data_ptr(), r.data_ptr(), nrhs,
                                                 _stream_handle(stream)), "kernel_residual")
+
+    def kernel_residual_batch(self, jobs, stream=None):
+        """jobs: (kernel, p0, shift, pts, x, dx or None, b, r) per problem (device tensors);
+        every job does x += dx (when given), then r = b - A x, in a few batched launches."""
+        arr = (_ResidualJob * max(1, len(jobs)))()
+        for q, (kernel, p0, shift, pts, x, dx, b, r) in enumerate(jobs):
+            n, nrhs = x.shape
+            arr[q] = _ResidualJob(int(kernel), int(pts.shape[1]), int(n), int(nrhs), float(p0), float(shift),
+                                  pts.data_ptr(), x.data_ptr(), None if dx is None else dx.data_ptr(),
+                                  b.data_ptr(), r.data_ptr())
+        self.check(lib().pp_kernel_residual_batch_dev(self._h, len(jobs), arr, _stream_handle(stream)),
+                   "kernel_residual_batch")
+        return residual_batch_launches([(j[0], j[3].shape[1], j[4].shape[1], j[5] is not None) for j in jobs])
 
 
 class Hierarchical:
@@ -503,14 +537,13 @@ class BatchRefiner:
         self.launches = 0
 
     def _iterate(self, xs, rs, dxs, bs):
-        ctx = self.batch.ctx
         self.batch.solve(rs, dxs, self.stream)
         self.launches += 2
-        for x, dx in zip(xs, dxs):
-            x += dx
-        for p, pts, x, b, r in zip(self.probs, self.pts, xs, bs, rs):
-            ctx.kernel_residual(p.kernel, p.p0, p.shift, pts, x, b, r, self.stream)
-            self.launches += 1
+        # x += dx and r = b - A x of every instance: update, residual (one launch per group of
+        # instances with the same kernel, dimension and RHS width) and reduction launches
+        self.launches += self.batch.ctx.kernel_residual_batch(
+            [(p.kernel, p.p0, p.shift, pts, x, dx, b, r)
+             for p, pts, x, dx, b, r in zip(self.probs, self.pts, xs, dxs, bs, rs)], self.stream)
 
     def errors(self, bs, xs, rs):
         """Normwise backward error of every instance (one device-to-host read)."""
@@ -599,6 +632,7 @@ class Server:
         self.ctx.check(lib().pp_server_poll(self._h, int(rid), C.byref(st)), "server_poll")
         return dict(status=SERVE_STATUS[st.status], iterations=st.iterations, backward_error=st.backward_error,
                     t_submit_ms=st.t_submit_ms, t_admit_ms=st.t_admit_ms, t_done_ms=st.t_done_ms,
+                    t_enqueued_ms=st.t_enqueued_ms,
                     device_bytes=st.device_bytes, message=st.message.decode(errors="replace"))
 
     def result(self, rid):
@@ -819,8 +853,12 @@ class Refiner:
         for it in range(max_iter):
             self.h.solve(r, dx, self.stream)
             self.launches += 2
-            x += dx
-            self.residual(x, b, r)
+            if self.prob is not None:  # update and residual in one batched call
+                self.launches += self.ctx.kernel_residual_batch(
+                    [(self.prob.kernel, self.prob.p0, self.prob.shift, self.pts, x, dx, b, r)], self.stream)
+            else:
+                x += dx
+                self.residual(x, b, r)
             err = r.abs().max().item() / (self.norm_inf * x.abs().max().item() + bn)
             hist.append(err)
             if err <= tol:

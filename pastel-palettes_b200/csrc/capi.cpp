@@ -51,9 +51,11 @@ struct VmPlan {
   int use_tc = 0;  // holds TF32 contractions (tensor memory per CTA)
   unsigned long long* d_trace = nullptr;  // per-task (start, end, sm | cta << 32) when tracing
   std::vector<int64_t> work_off, scratch_off, rhs_off;  // per instance (batched plans)
-  // stream-ordered memory (cudaMallocAsync / cudaFreeAsync on `astream`) for plans of a
-  // served request, so that allocating or freeing never waits for other streams' work
+  // stream-ordered memory (cudaMallocAsync / cudaFreeAsync on `astream`, from `apool` when
+  // set) for plans of a served request, so that allocating or freeing never waits for other
+  // streams' work
   cudaStream_t astream = nullptr;
+  cudaMemPool_t apool = nullptr;
   bool async_mem = false;
   void dfree(void* p) {
     if (!p) return;
@@ -95,10 +97,12 @@ struct pp_hmatrix {
   VmPlan* last = nullptr;
   // stream-ordered memory mode (set by the server for the requests it owns)
   cudaStream_t astream = nullptr;
+  cudaMemPool_t apool = nullptr;
   bool async_mem = false;
   cudaError_t dalloc(void** p, size_t bytes) {
     bytes = bytes ? bytes : 8;
-    return async_mem ? cudaMallocAsync(p, bytes, astream) : cudaMalloc(p, bytes);
+    if (!async_mem) return cudaMalloc(p, bytes);
+    return apool ? cudaMallocFromPoolAsync(p, bytes, apool, astream) : cudaMallocAsync(p, bytes, astream);
   }
   void dfree(void* p) {
     if (!p) return;
@@ -109,15 +113,20 @@ struct pp_hmatrix {
     return async_mem ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, astream)
                      : cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice);
   }
-  void set_async(cudaStream_t s) {
+  void set_async(cudaStream_t s, cudaMemPool_t pool) {
     async_mem = true;
     astream = s;
-    factor.async_mem = true;
-    factor.astream = s;
-    for (auto& kv : solves) {
-      kv.second->async_mem = true;
-      kv.second->astream = s;
+    apool = pool;
+    for (VmPlan* p : all_plans()) {
+      p->async_mem = true;
+      p->astream = s;
+      p->apool = pool;
     }
+  }
+  std::vector<VmPlan*> all_plans() {
+    std::vector<VmPlan*> v{&factor};
+    for (auto& kv : solves) v.push_back(kv.second.get());
+    return v;
   }
   ~pp_hmatrix() {
     factor.release();
@@ -202,7 +211,9 @@ pp_status plan_to_device_multi(pp_context* ctx, const std::vector<pp_hmatrix*>& 
   const int n = plan.n_tasks;
   auto alloc = [&](void** p, size_t bytes) {
     bytes = bytes ? bytes : 8;
-    return plan.async_mem ? cudaMallocAsync(p, bytes, plan.astream) : cudaMalloc(p, bytes);
+    if (!plan.async_mem) return cudaMalloc(p, bytes);
+    return plan.apool ? cudaMallocFromPoolAsync(p, bytes, plan.apool, plan.astream)
+                      : cudaMallocAsync(p, bytes, plan.astream);
   };
   auto h2d = [&](void* dst, const void* src, size_t bytes) {
     return plan.async_mem ? cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, plan.astream)
@@ -557,6 +568,7 @@ static VmPlan* solve_plan(pp_hmatrix* h, int nrhs) {
   auto p = std::make_unique<VmPlan>();
   p->async_mem = h->async_mem;
   p->astream = h->astream;
+  p->apool = h->apool;
   VmPlan* raw = p.get();
   h->solves.emplace(nrhs, std::move(p));
   return raw;
@@ -642,7 +654,54 @@ pp_status pp_kernel_residual_dev(pp_context* ctx, int kernel, double p0, double 
     PP_CUDA(cudaMalloc((void**)&ctx->d_resid, sizeof(double) * need));
     ctx->resid_elems = need;
   }
-  PP_CUDA(pp_kernel_residual(kernel, p0, 0.0, shift, pts, dim, n, x, b, r, nrhs, ctx->d_resid, (cudaStream_t)stream));
+  const cudaError_t e = pp_kernel_residual(kernel, p0, 0.0, shift, pts, dim, n, x, b, r, nrhs, ctx->d_resid,
+                                           (cudaStream_t)stream);
+  if (e == cudaErrorInvalidValue) return fail(ctx, PP_INVALID_ARG, "kernel residual: p0 negative or not finite");
+  PP_CUDA(e);
+  return PP_OK;
+}
+
+pp_status pp_kernel_residual_batch_dev(pp_context* ctx, int njobs, const pp_residual_job* jobs, void* stream) {
+  if (!has_device(ctx)) return fail(ctx, PP_CUDA_ERROR, "no CUDA device in this context");
+  if (njobs < 0 || (njobs > 0 && !jobs)) return fail(ctx, PP_INVALID_ARG, "kernel residual batch: bad argument");
+  size_t need = 0;
+  for (int q = 0; q < njobs; ++q) {
+    const pp_residual_job& j = jobs[q];
+    if (!j.points || !j.x || !j.b || !j.r || j.n <= 0 || j.nrhs <= 0 || j.nrhs > 16 || j.dim < 1 || j.dim > 3 ||
+        j.kernel < 0 || j.kernel > 3)
+      return fail(ctx, PP_INVALID_ARG, "kernel residual batch: bad job " + std::to_string(q));
+    if (j.kernel <= 1 && !(j.p0 >= 0.0 && std::isfinite(j.p0)))
+      return fail(ctx, PP_INVALID_ARG, "kernel residual batch: p0 negative or not finite in job " + std::to_string(q));
+    need += pp_kernel_residual_part_elems(j.n, j.nrhs);
+  }
+  if (njobs == 0) return PP_OK;
+  if (need > ctx->resid_elems) {  // grown before any stream capture by the first (eager) call
+    cudaFree(ctx->d_resid);
+    ctx->d_resid = nullptr;
+    ctx->resid_elems = 0;
+    PP_CUDA(cudaMalloc((void**)&ctx->d_resid, sizeof(double) * need));
+    ctx->resid_elems = need;
+  }
+  std::vector<pp_resid_job> dj(njobs);
+  size_t off = 0;
+  for (int q = 0; q < njobs; ++q) {
+    const pp_residual_job& j = jobs[q];
+    pp_resid_job& o = dj[q];
+    o.kernel = j.kernel;
+    o.dim = j.dim;
+    o.n = j.n;
+    o.nrhs = j.nrhs;
+    o.p0 = j.p0;
+    o.shift = j.shift;
+    o.pts = j.points;
+    o.x = j.x;
+    o.dx = j.dx;
+    o.b = j.b;
+    o.r = j.r;
+    o.part = ctx->d_resid + off;
+    off += pp_kernel_residual_part_elems(j.n, j.nrhs);
+  }
+  PP_CUDA(pp_kernel_residual_batch(dj.data(), njobs, (cudaStream_t)stream));
   return PP_OK;
 }
 
@@ -1092,7 +1151,7 @@ struct ServeRequest {
   int state = SRV_QUEUED;
   int set = 0, iters_set = 0, iters_total = 0;
   double bmax = 0, worst = 0;
-  double t_submit = 0, t_admit = -1, t_done = -1;
+  double t_submit = 0, t_admit = -1, t_done = -1, t_enqueued = -1;
   std::string err;
 };
 
@@ -1100,6 +1159,9 @@ struct ServeRequest {
 
 struct pp_server {
   pp_context* ctx = nullptr;
+  // the requests' device memory: a pool of its own that keeps up to the budget mapped between
+  // requests (no page mapping on the admission path, no effect on other users of the device)
+  cudaMemPool_t pool = nullptr;
   long long budget = 0;
   int slots = 1, grid = 0;
   std::mutex mu;
@@ -1142,7 +1204,7 @@ bool pp_server::start(ServeRequest* q) {
   pp_hmatrix* h = q->h;
   if (!srv_check(q, cudaStreamCreateWithFlags(&q->stream, cudaStreamNonBlocking), "stream")) return false;
   if (!srv_check(q, cudaEventCreateWithFlags(&q->ev, cudaEventDisableTiming), "event")) return false;
-  h->set_async(q->stream);
+  h->set_async(q->stream, pool);
   const size_t vec = sizeof(double) * (size_t)q->n * q->nrhs;
   if (!srv_check(q, h->dalloc((void**)&q->d_pts, sizeof(double) * q->pts.size()), "alloc")) return false;
   for (double** p : {&q->d_b, &q->d_x, &q->d_r, &q->d_dx})
@@ -1272,6 +1334,7 @@ void pp_server::run() {
       q->t_admit = now_ms();
       active.push_back(q);
       if (!start(q)) retire(q, false);
+      else q->t_enqueued = now_ms();
     }
     bool progressed = false;
     for (ServeRequest* q : active)
@@ -1296,6 +1359,18 @@ pp_status pp_server_create(pp_context* ctx, const pp_serve_config* cfg, pp_serve
   s->slots = cfg->max_inflight;
   s->grid = cfg->grid_per_request > 0 ? cfg->grid_per_request
                                       : std::max(8, ctx->sm_count * std::max(1, ctx->blocks_per_sm) / s->slots);
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = ctx->device;
+  cudaError_t e = cudaMemPoolCreate(&s->pool, &props);
+  unsigned long long keep = (unsigned long long)s->budget;
+  if (e == cudaSuccess) e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  if (e != cudaSuccess) {
+    if (s->pool) cudaMemPoolDestroy(s->pool);
+    delete s;
+    return fail(ctx, PP_CUDA_ERROR, std::string("pp_server_create: memory pool: ") + cudaGetErrorString(e));
+  }
   s->worker = std::thread([s] { s->run(); });
   *out = s;
   return PP_OK;
@@ -1363,6 +1438,7 @@ pp_status pp_server_poll(pp_server* s, long long id, pp_request_stats* st) {
   st->backward_error = q->worst;
   st->t_submit_ms = q->t_submit;
   st->t_admit_ms = q->t_admit;
+  st->t_enqueued_ms = q->t_enqueued;
   st->t_done_ms = q->t_done;
   st->device_bytes = q->bytes;
   std::snprintf(st->message, sizeof(st->message), "%s", q->err.c_str());
@@ -1394,6 +1470,7 @@ void pp_server_destroy(pp_server* s) {
   if (s->worker.joinable()) s->worker.join();
   for (auto& kv : s->all)
     if (kv.second->h) pp_hmatrix_destroy(kv.second->h);  // queued, never admitted
+  if (s->pool) cudaMemPoolDestroy(s->pool);  // released once the queued frees have run
   delete s;
 }
 

@@ -25,6 +25,8 @@
 #include <math.h>
 
 #include <algorithm>
+#include <cmath>
+#include <vector>
 #include <stdint.h>
 
 #include "vm.cuh"
@@ -1689,30 +1691,44 @@ __global__ void dense_residual_kernel(const double* __restrict__ A, int lda, int
   }
 }
 
-// Reciprocal and reciprocal square root by two Newton-Raphson steps from the single-precision
-// estimate (quadratic convergence: 24 -> 48 -> ~96 bits, i.e. a few ulps of double): the
-// residual needs entries accurate to ~1e-15, not correctly rounded ones.
-__device__ __forceinline__ double rcp_nr(double x) {
-  double y = (double)__frcp_rn((float)x);
-  double e = fma(-x, y, 1.0);
-  y = fma(y, e, y);
-  e = fma(-x, y, 1.0);
-  return fma(y, e, y);
+// Estimates from the special-function unit: PTX rsqrt.approx.ftz.f64 / rcp.approx.ftz.f64
+// (computed from the upper word of the double, about single-precision accuracy, full double
+// exponent range; zero gives infinity).
+__device__ __forceinline__ double rsqrt_est(double v) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(v));
+  return y;
 }
-__device__ __forceinline__ double sqrt_nr(double d2) {
-  if (!(d2 > 1e-30)) return sqrt(d2);  // outside the float range of the estimate
-  double y = (double)rsqrtf((float)d2);
-  double e = fma(-d2 * y, y, 1.0);
-  y = fma(0.5 * y, e, y);
-  e = fma(-d2 * y, y, 1.0);
-  y = fma(0.5 * y, e, y);
-  return d2 * y;
+__device__ __forceinline__ double rcp_est(double v) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(v));
+  return y;
 }
+// One third-order correction of an estimate y0 of a^(-1/2): with e = 1 - a y0^2,
+// a^(-1/2) = y0 (1 - e)^(-1/2) = y0 (1 + e/2 + 3e^2/8 + O(e^3)) (binomial series).  For
+// |e| < 2^-19 the truncated terms are below 2^-58 relative: the result is within a few ulps of
+// double, the accuracy of two Newton steps at 5 instead of 8 operations.
+__device__ __forceinline__ double rsqrt_refine(double a, double y0) {
+  const double e = fma(-a * y0, y0, 1.0);
+  return fma(y0 * e, fma(0.375, e, 0.5), y0);
+}
+// The same for 1/a: e = 1 - a y0, 1/a = y0 (1 - e)^-1 = y0 (1 + e + e^2 + O(e^3)).
+__device__ __forceinline__ double rcp_refine(double a, double y0) {
+  const double e = fma(-a, y0, 1.0);
+  return fma(y0, fma(e, e, e), y0);
+}
+// Entry K(d) of the kernel matrix at squared distance d2, d = d2 / sqrt(max(d2, 1e-300)):
+// exact zero on the diagonal and for coincident points, an absolute error below 1e-150 for
+// 0 < d2 < 1e-300, a few ulps elsewhere.
 template <int KIND>
 __device__ __forceinline__ double kernel_eval_nr(double d2, double p0, double inv_p0) {
-  const double d = sqrt_nr(d2);
-  if (KIND == 0) return rcp_nr(d + p0);
-  if (KIND == 1) return rcp_nr(4.0 * 3.14159265358979323846 * (d + p0));
+  constexpr double c = KIND == 1 ? 4.0 * 3.14159265358979323846 : 1.0;
+  const double d2c = fmax(d2, 1e-300);
+  const double d = d2 * rsqrt_refine(d2c, rsqrt_est(d2c));
+  if (KIND <= 1) {
+    const double x = c * (d + p0);
+    return rcp_refine(x, rcp_est(x));
+  }
   if (KIND == 2) return exp(-d * inv_p0);
   const double s = 1.7320508075688772 * d * inv_p0;
   return (1.0 + s) * exp(-s);
@@ -1784,24 +1800,85 @@ __global__ void __launch_bounds__(KR_THREADS) kernel_residual_part(double p0, do
       for (int q = 0; q < nrhs; ++q) part[((size_t)seg * n + row[t]) * nrhs + q] = acc[t][q];
 }
 
-// Symmetric form of the partial products (kernel matrices are symmetric): CTA b takes the
-// tile pair (I, J), I <= J, of KR_SEG x KR_SEG tiles and evaluates each entry once.  Thread t
-// owns row I*KR_SEG + t: a_ij x_j goes to its register sums (part[J][i]); for I < J, a_ij x_i
-// goes to the column sums of row j (part[I][j]) through per-warp accumulators in shared memory,
-// walked on a skewed diagonal (lane l visits column (l + s) mod KR_SEG at step s, so the lanes
-// of a warp never touch the same column) and added in warp order at the end.  Every
-// (segment, row) partial is written once, by one CTA: deterministic, no atomics.
+// Jobs of one batched residual launch, passed by value (kernel parameter space): job j owns
+// the launch's work items [first, next job's first) — tile pairs of the residual kernel,
+// elements of the update and reduction kernels.
+#define KR_LAUNCH_JOBS 64
+struct ResidLaunch {
+  struct Job {
+    const double* pts;
+    double* x;
+    const double* dx;
+    const double* b;
+    double* r;
+    double* part;
+    double p0, shift;
+    long long first;
+    int n, nrhs, T, pad;
+  } job[KR_LAUNCH_JOBS];
+  int njobs;
+};
+
+// the job that owns work item `key` (the last job whose first <= key)
+__device__ __forceinline__ int resid_job_of(const ResidLaunch& L, long long key) {
+  int lo = 0, hi = L.njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (L.job[mid].first <= key) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// KR_SEG steps of one warp over a tile pair: lane l takes column (l + s) mod KR_SEG at step s.
+// COL: also accumulate a_ij x_i into the warp's column sums (off-diagonal tiles); EDGE: skip
+// columns at or past jn (the caller skips rows past n).
+template <int KIND, int DIM, int NR, bool COL, bool EDGE>
+__device__ __forceinline__ void residual_steps(const double* sp, const double* sx, double* colw, const double (&pi)[DIM],
+                                               const double (&xi)[NR], double (&acc)[NR], int lane, int jn, double p0,
+                                               double inv_p0) {
+#pragma unroll 4
+  for (int st = 0; st < KR_SEG; ++st) {
+    const int jj = (lane + st) & (KR_SEG - 1);
+    if (EDGE && jj >= jn) continue;
+    double d2 = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      const double u = pi[d] - sp[jj * DIM + d];
+      d2 = fma(u, u, d2);
+    }
+    const double a = kernel_eval_nr<KIND>(d2, p0, inv_p0);
+#pragma unroll
+    for (int q = 0; q < NR; ++q) acc[q] = fma(a, sx[jj * NR + q], acc[q]);
+    if (COL) {
+#pragma unroll
+      for (int q = 0; q < NR; ++q) colw[jj * NR + q] = fma(a, xi[q], colw[jj * NR + q]);
+    }
+  }
+}
+
+// Symmetric form of the partial products (kernel matrices are symmetric): a CTA takes the
+// tile pair (I, J), I <= J, of KR_SEG x KR_SEG tiles of one job and evaluates each entry once.
+// Thread t owns row I*KR_SEG + t: a_ij x_j goes to its register sums (part[J][i]); for I < J,
+// a_ij x_i goes to the column sums of row j (part[I][j]) through per-warp accumulators in
+// shared memory, walked on a skewed diagonal (lane l visits column (l + s) mod KR_SEG at step
+// s, so the lanes of a warp never touch the same column) and added in warp order at the end.
+// Every (segment, row) partial is written once, by one CTA: deterministic, no atomics, and the
+// same bits whatever the other jobs of the launch.
 template <int KIND, int DIM, int NR>
-__global__ void __launch_bounds__(KR_SEG) kernel_residual_sym(double p0, double shift,
-                                                               const double* __restrict__ pts, int n,
-                                                               const double* __restrict__ x,
-                                                               double* __restrict__ part, int nrhs, int T) {
+__global__ void __launch_bounds__(KR_SEG) kernel_residual_sym(const __grid_constant__ ResidLaunch L) {
   constexpr int W = KR_SEG / 32;
   __shared__ double sp[KR_SEG * DIM];
   __shared__ double sx[KR_SEG * NR];
   __shared__ double col[W][KR_SEG * NR];
-  // (I, J) of linear index b over the upper triangle, row by row: b = I T - I (I - 1) / 2 + (J - I)
-  const long long b = blockIdx.x;
+  const ResidLaunch::Job& jb = L.job[resid_job_of(L, (long long)blockIdx.x)];
+  const double* __restrict__ pts = jb.pts;
+  const double* __restrict__ x = jb.x;
+  double* __restrict__ part = jb.part;
+  const int n = jb.n, nrhs = jb.nrhs, T = jb.T;
+  const double p0 = jb.p0, shift = jb.shift;
+  // (I, J) of the job's pair index b over the upper triangle, row by row:
+  // b = I T - I (I - 1) / 2 + (J - I)
+  const long long b = (long long)blockIdx.x - jb.first;
   const double tt = 2.0 * T + 1.0;
   int I = (int)floor((tt - sqrt(tt * tt - 8.0 * (double)b)) * 0.5);
   auto row_start = [&](int r) { return (long long)r * T - (long long)r * (r - 1) / 2; };
@@ -1832,25 +1909,16 @@ __global__ void __launch_bounds__(KR_SEG) kernel_residual_sym(double p0, double 
   __syncthreads();
   const bool offdiag = I != J;
   const int jn = min(KR_SEG, n - j0);
-#pragma unroll 2
-  for (int st = 0; st < KR_SEG; ++st) {
-    const int jj = (lane + st) & (KR_SEG - 1);
-    if (jj < jn && i < n) {
-      double d2 = 0.0;
+  if (jn == KR_SEG && I * KR_SEG + KR_SEG <= n) {  // full tiles: no per-entry predicates
+    if (offdiag) residual_steps<KIND, DIM, NR, true, false>(sp, sx, col[w], pi, xi, acc, lane, jn, p0, inv_p0);
+    else residual_steps<KIND, DIM, NR, false, false>(sp, sx, col[w], pi, xi, acc, lane, jn, p0, inv_p0);
+  } else if (i < n) {  // ragged edge of the matrix
+    if (offdiag) residual_steps<KIND, DIM, NR, true, true>(sp, sx, col[w], pi, xi, acc, lane, jn, p0, inv_p0);
+    else residual_steps<KIND, DIM, NR, false, true>(sp, sx, col[w], pi, xi, acc, lane, jn, p0, inv_p0);
+  }
+  if (!offdiag && i < n) {  // the diagonal entry's shift
 #pragma unroll
-      for (int d = 0; d < DIM; ++d) {
-        const double u = pi[d] - sp[jj * DIM + d];
-        d2 = fma(u, u, d2);
-      }
-      double a = kernel_eval_nr<KIND>(d2, p0, inv_p0);
-      if (!offdiag && j0 + jj == i) a += shift;
-#pragma unroll
-      for (int q = 0; q < NR; ++q) acc[q] = fma(a, sx[jj * NR + q], acc[q]);
-      if (offdiag) {
-#pragma unroll
-        for (int q = 0; q < NR; ++q) col[w][jj * NR + q] = fma(a, xi[q], col[w][jj * NR + q]);
-      }
-    }
+    for (int q = 0; q < NR; ++q) acc[q] = fma(shift, xi[q], acc[q]);
   }
   if (i < n)
     for (int q = 0; q < nrhs; ++q) part[((size_t)J * n + i) * nrhs + q] = acc[q];
@@ -1867,37 +1935,93 @@ __global__ void __launch_bounds__(KR_SEG) kernel_residual_sym(double p0, double 
   }
 }
 
+// r = b - (sum of the job's segments in order), one thread per (row, rhs) element
+__global__ void residual_reduce(const __grid_constant__ ResidLaunch L) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const ResidLaunch::Job& jb = L.job[resid_job_of(L, e)];
+  const long long k = e - jb.first, count = (long long)jb.n * jb.nrhs;
+  if (k < 0 || k >= count) return;
+  double s = 0.0;
+  for (int g = 0; g < jb.T; ++g) s += jb.part[g * count + k];
+  jb.r[k] = jb.b[k] - s;
+}
+
+// x += dx of every job, one thread per element
+__global__ void residual_update(const __grid_constant__ ResidLaunch L) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const ResidLaunch::Job& jb = L.job[resid_job_of(L, e)];
+  const long long k = e - jb.first, count = (long long)jb.n * jb.nrhs;
+  if (k < 0 || k >= count) return;
+  jb.x[k] += jb.dx[k];
+}
+
 template <int KIND, int DIM>
-cudaError_t launch_kernel_residual(dim3 grid, cudaStream_t s, double p0, double shift, const double* pts, int n,
-                                   const double* x, double* part, int nrhs) {
-  const int T = (n + KR_SEG - 1) / KR_SEG;
-  const unsigned pairs = (unsigned)((long long)T * (T + 1) / 2);
-  if (nrhs == 1)
-    kernel_residual_sym<KIND, DIM, 1><<<pairs, KR_SEG, 0, s>>>(p0, shift, pts, n, x, part, nrhs, T);
-  else if (nrhs <= 4)
-    kernel_residual_sym<KIND, DIM, 4><<<pairs, KR_SEG, 0, s>>>(p0, shift, pts, n, x, part, nrhs, T);
-  else if (nrhs <= 8)
-    kernel_residual_part<KIND, DIM, 8><<<grid, KR_THREADS, 0, s>>>(p0, shift, pts, n, x, part, nrhs);
+cudaError_t launch_residual_sym(const ResidLaunch& L, unsigned pairs, int nr, cudaStream_t s) {
+  if (nr == 1)
+    kernel_residual_sym<KIND, DIM, 1><<<pairs, KR_SEG, 0, s>>>(L);
   else
-    kernel_residual_part<KIND, DIM, 16><<<grid, KR_THREADS, 0, s>>>(p0, shift, pts, n, x, part, nrhs);
+    kernel_residual_sym<KIND, DIM, 4><<<pairs, KR_SEG, 0, s>>>(L);
   return cudaGetLastError();
 }
 
 template <int KIND>
-cudaError_t launch_kernel_residual_dim(int dim, dim3 grid, cudaStream_t s, double p0, double shift, const double* pts,
-                                       int n, const double* x, double* part, int nrhs) {
-  if (dim == 1) return launch_kernel_residual<KIND, 1>(grid, s, p0, shift, pts, n, x, part, nrhs);
-  if (dim == 2) return launch_kernel_residual<KIND, 2>(grid, s, p0, shift, pts, n, x, part, nrhs);
-  return launch_kernel_residual<KIND, 3>(grid, s, p0, shift, pts, n, x, part, nrhs);
+cudaError_t launch_residual_sym_dim(int dim, const ResidLaunch& L, unsigned pairs, int nr, cudaStream_t s) {
+  if (dim == 1) return launch_residual_sym<KIND, 1>(L, pairs, nr, s);
+  if (dim == 2) return launch_residual_sym<KIND, 2>(L, pairs, nr, s);
+  return launch_residual_sym<KIND, 3>(L, pairs, nr, s);
 }
 
-__global__ void residual_reduce(const double* __restrict__ part, int segs, int n, int nrhs,
-                                const double* __restrict__ b, double* __restrict__ r) {
-  const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= (size_t)n * nrhs) return;
-  double s = 0.0;
-  for (int g = 0; g < segs; ++g) s += part[(size_t)g * n * nrhs + e];
-  r[e] = b[e] - s;
+template <int KIND, int DIM>
+cudaError_t launch_residual_part(const pp_resid_job& j, cudaStream_t s) {
+  const int segs = (j.n + KR_SEG - 1) / KR_SEG;
+  const dim3 grid((j.n + KR_ROWS - 1) / KR_ROWS, segs);
+  if (j.nrhs <= 8)
+    kernel_residual_part<KIND, DIM, 8><<<grid, KR_THREADS, 0, s>>>(j.p0, j.shift, j.pts, j.n, j.x, j.part, j.nrhs);
+  else
+    kernel_residual_part<KIND, DIM, 16><<<grid, KR_THREADS, 0, s>>>(j.p0, j.shift, j.pts, j.n, j.x, j.part, j.nrhs);
+  return cudaGetLastError();
+}
+
+template <int KIND>
+cudaError_t launch_residual_part_dim(const pp_resid_job& j, cudaStream_t s) {
+  if (j.dim == 1) return launch_residual_part<KIND, 1>(j, s);
+  if (j.dim == 2) return launch_residual_part<KIND, 2>(j, s);
+  return launch_residual_part<KIND, 3>(j, s);
+}
+
+ResidLaunch::Job resid_job(const pp_resid_job& j) {
+  ResidLaunch::Job o{};
+  o.pts = j.pts;
+  o.x = j.x;
+  o.dx = j.dx;
+  o.b = j.b;
+  o.r = j.r;
+  o.part = j.part;
+  o.p0 = j.p0;
+  o.shift = j.shift;
+  o.n = j.n;
+  o.nrhs = j.nrhs;
+  o.T = (j.n + KR_SEG - 1) / KR_SEG;
+  return o;
+}
+
+// element-wise launch (update or reduction) over jobs[sel] in chunks of KR_LAUNCH_JOBS
+template <typename F>
+cudaError_t launch_elementwise(const pp_resid_job* jobs, const std::vector<int>& sel, F kernel, cudaStream_t s) {
+  for (size_t c = 0; c < sel.size(); c += KR_LAUNCH_JOBS) {
+    ResidLaunch L;
+    L.njobs = (int)std::min<size_t>(KR_LAUNCH_JOBS, sel.size() - c);
+    long long total = 0;
+    for (int q = 0; q < L.njobs; ++q) {
+      L.job[q] = resid_job(jobs[sel[c + q]]);
+      L.job[q].first = total;
+      total += (long long)L.job[q].n * L.job[q].nrhs;
+    }
+    kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(L);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 // x += dx over `count` elements (the refinement update of a served request)
@@ -1997,24 +2121,79 @@ cudaError_t pp_dense_residual(const double* A, int lda, int n, const double* x, 
   return cudaGetLastError();
 }
 
+cudaError_t pp_kernel_residual_batch(const pp_resid_job* jobs, int njobs, cudaStream_t s) {
+  if (njobs <= 0) return cudaSuccess;
+  if (!jobs) return cudaErrorInvalidValue;
+  std::vector<int> all, upd;
+  for (int q = 0; q < njobs; ++q) {
+    const pp_resid_job& j = jobs[q];
+    if (j.dim < 1 || j.dim > 3 || j.nrhs < 1 || j.nrhs > 16 || j.n <= 0 || j.kernel < 0 || j.kernel > 3 || !j.pts ||
+        !j.x || !j.b || !j.r || !j.part)
+      return cudaErrorInvalidValue;
+    if (j.kernel <= 1 && !(j.p0 >= 0.0 && std::isfinite(j.p0))) return cudaErrorInvalidValue;
+    all.push_back(q);
+    if (j.dx) upd.push_back(q);
+  }
+  cudaError_t e = launch_elementwise(jobs, upd, residual_update, s);
+  if (e != cudaSuccess) return e;
+  // tile-pair launches, one per (kernel, dimension, right-hand-side width) group
+  for (int kern = 0; kern < 4; ++kern)
+    for (int dim = 1; dim <= 3; ++dim)
+      for (int nr : {1, 4}) {
+        std::vector<int> sel;
+        for (int q = 0; q < njobs; ++q)
+          if (jobs[q].kernel == kern && jobs[q].dim == dim && (nr == 1 ? jobs[q].nrhs == 1 : (jobs[q].nrhs > 1 && jobs[q].nrhs <= 4)))
+            sel.push_back(q);
+        for (size_t c = 0; c < sel.size(); c += KR_LAUNCH_JOBS) {
+          ResidLaunch L;
+          L.njobs = (int)std::min<size_t>(KR_LAUNCH_JOBS, sel.size() - c);
+          long long pairs = 0;
+          for (int q = 0; q < L.njobs; ++q) {
+            L.job[q] = resid_job(jobs[sel[c + q]]);
+            L.job[q].first = pairs;
+            pairs += (long long)L.job[q].T * (L.job[q].T + 1) / 2;
+          }
+          if (pairs >= (1LL << 31)) return cudaErrorInvalidValue;
+          switch (kern) {
+            case 0: e = launch_residual_sym_dim<0>(dim, L, (unsigned)pairs, nr, s); break;
+            case 1: e = launch_residual_sym_dim<1>(dim, L, (unsigned)pairs, nr, s); break;
+            case 2: e = launch_residual_sym_dim<2>(dim, L, (unsigned)pairs, nr, s); break;
+            default: e = launch_residual_sym_dim<3>(dim, L, (unsigned)pairs, nr, s); break;
+          }
+          if (e != cudaSuccess) return e;
+        }
+      }
+  // wider right-hand-side blocks: per-job row-block partial products
+  for (int q = 0; q < njobs; ++q) {
+    if (jobs[q].nrhs <= 4) continue;
+    switch (jobs[q].kernel) {
+      case 0: e = launch_residual_part_dim<0>(jobs[q], s); break;
+      case 1: e = launch_residual_part_dim<1>(jobs[q], s); break;
+      case 2: e = launch_residual_part_dim<2>(jobs[q], s); break;
+      default: e = launch_residual_part_dim<3>(jobs[q], s); break;
+    }
+    if (e != cudaSuccess) return e;
+  }
+  return launch_elementwise(jobs, all, residual_reduce, s);
+}
+
 cudaError_t pp_kernel_residual(int kernel, double p0, double p1, double diag_shift, const double* pts, int dim, int n,
                                const double* x, const double* b, double* r, int nrhs, double* part,
                                cudaStream_t s) {
   (void)p1;
-  if (dim < 1 || dim > 3 || nrhs < 1 || nrhs > 16 || !part || kernel < 0 || kernel > 3) return cudaErrorInvalidValue;
-  const int segs = (n + KR_SEG - 1) / KR_SEG;
-  const dim3 grid((n + KR_ROWS - 1) / KR_ROWS, segs);
-  cudaError_t e;
-  switch (kernel) {
-    case 0: e = launch_kernel_residual_dim<0>(dim, grid, s, p0, diag_shift, pts, n, x, part, nrhs); break;
-    case 1: e = launch_kernel_residual_dim<1>(dim, grid, s, p0, diag_shift, pts, n, x, part, nrhs); break;
-    case 2: e = launch_kernel_residual_dim<2>(dim, grid, s, p0, diag_shift, pts, n, x, part, nrhs); break;
-    default: e = launch_kernel_residual_dim<3>(dim, grid, s, p0, diag_shift, pts, n, x, part, nrhs); break;
-  }
-  if (e != cudaSuccess) return e;
-  const size_t total = (size_t)n * nrhs;
-  residual_reduce<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(part, segs, n, nrhs, b, r);
-  return cudaGetLastError();
+  pp_resid_job j{};
+  j.kernel = kernel;
+  j.dim = dim;
+  j.n = n;
+  j.nrhs = nrhs;
+  j.p0 = p0;
+  j.shift = diag_shift;
+  j.pts = pts;
+  j.x = const_cast<double*>(x);  // read only: no update without dx
+  j.b = b;
+  j.r = r;
+  j.part = part;
+  return pp_kernel_residual_batch(&j, 1, s);
 }
 
 cudaError_t pp_axpy(double* x, const double* dx, size_t count, cudaStream_t s) {

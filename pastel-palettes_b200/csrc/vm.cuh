@@ -55,6 +55,20 @@ cudaError_t pp_kernel_residual(int kernel, double p0, double p1, double diag_shi
                                const double* x, const double* b, double* r, int nrhs, double* part,
                                cudaStream_t s);
 size_t pp_kernel_residual_part_elems(int n, int nrhs);
+/* one job of a batched matrix-free residual: x += dx first when dx is set, then r = b - A x */
+struct pp_resid_job {
+  int kernel, dim, n, nrhs;
+  double p0, shift;
+  const double* pts;
+  double* x;
+  const double* dx;
+  const double* b;
+  double* r;
+  double* part; /* pp_kernel_residual_part_elems(n, nrhs) doubles of scratch, one per job */
+};
+/* the update, residual and reduction of every job in three or more launches (jobs grouped by
+ * kernel, dimension and right-hand-side width); results equal those of one job per call */
+cudaError_t pp_kernel_residual_batch(const pp_resid_job* jobs, int njobs, cudaStream_t s);
 /* x += dx (count elements) */
 cudaError_t pp_axpy(double* x, const double* dx, size_t count, cudaStream_t s);
 /* out[0] = max |x|, out[1] = max |r| (as double bit patterns; out is zeroed first) */

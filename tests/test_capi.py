@@ -104,3 +104,17 @@ def test_precision_switch_marks_gemm_instructions(pp, hctx):
     assert pp.lib().pp_hmatrix_set_precision(h.handle, 7) == pp.PP_INVALID_ARG
     h.set_precision(pp.FP64)
     assert np.array_equal(h.encode_program(0, 1, bases)[0], t64)
+
+
+def test_residual_batch_refuses_without_device_and_counts_launches(pp, hctx):
+    """The batched residual refuses a host context, and the launch count the refiners report
+    follows the library's grouping (update and reduction per 64 jobs, residual per group of
+    kernel / dimension / RHS width per 64 jobs, one per job above 4 RHS)."""
+    job = pp._ResidualJob(0, 2, 8, 1, 1e-3, 0.0, 1, 1, None, 1, 1)
+    assert pp.lib().pp_kernel_residual_batch_dev(hctx._h, 1, C.byref(job), None) == pp.PP_CUDA_ERROR
+    count = pp.residual_batch_launches
+    assert count([]) == 0
+    assert count([(0, 2, 1, True)] * 64) == 3
+    assert count([(0, 2, 1, True)] * 65) == 6
+    assert count([(0, 2, 1, False), (0, 2, 3, False), (2, 3, 1, False)]) == 4
+    assert count([(0, 2, 8, True), (0, 2, 16, True), (1, 3, 4, True)]) == 1 + 1 + 2 + 1

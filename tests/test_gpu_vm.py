@@ -83,6 +83,22 @@ def test_getrf_task_bitwise(pp, oracle, gctx, m, n):
     assert np.array_equal(d, h)
 
 
+@pytest.mark.parametrize("tA,tB", [(0, 0), (1, 0), (0, 1), (1, 1)])
+@pytest.mark.parametrize("alpha,beta", [(-1.0, 1.0), (1.0, 0.0)])
+@pytest.mark.parametrize("m,n,k", [(64, 64, 16), (256, 16, 16), (37, 91, 130), (64, 16, 64)])
+def test_gemm_task_free_order(pp, oracle, gctx, tA, tB, alpha, beta, m, n, k):
+    """GEMM with the free-order flag (products of low-rank factors): the FP64 tensor-core path,
+    within rounding of the oracle's ascending-k sum."""
+    tb = TaskBench(pp, seed=m * 7 + n + k)
+    c = tb.operand(m, n)
+    a = tb.operand(k, m) if tA else tb.operand(m, k)
+    b = tb.operand(n, k) if tB else tb.operand(k, n)
+    flags = 1 | (16 << 1 if tA else 0) | (16 << 2 if tB else 0)
+    d, h = tb.run(gctx, oracle, dict(op=6, flags=flags, m=m, n=n, k=k, alpha=alpha, beta=beta), {0: c, 1: a, 2: b})[c[0]]
+    assert rel(d[:, :n], h[:, :n]) < 1e-14
+    assert np.array_equal(d[:, n:], h[:, n:])  # the padding columns are untouched
+
+
 @pytest.mark.parametrize("op", [2, 3, 4, 5])
 @pytest.mark.parametrize("m,n", [(64, 16), (64, 64), (33, 70), (1, 5)])
 def test_triangular_tasks_bitwise(pp, oracle, gctx, op, m, n):
@@ -334,6 +350,69 @@ def test_kernel_residual_matches_dense_fp64(pp, gctx, kernel, p0, dim, nrhs):
     want = b - A @ x
     scale = np.abs(A).sum(1).max() * np.abs(x).max()
     assert np.abs(r.cpu().numpy() - want).max() <= 1e-14 * scale
+
+
+def _resid_job(pp, rng, kernel, p0, dim, n, nrhs, dup=False):
+    pts = rng.uniform(0, 1, (n, dim))
+    if dup and n > 4:
+        pts[n // 2] = pts[1]  # coincident points: distance 0 off the diagonal
+    x, dx, b = (rng.standard_normal((n, nrhs)) for _ in range(3))
+    return (pp.KERNELS[kernel], p0, 3.0, dev(pts), dev(x), dev(dx), dev(b),
+            torch.empty((n, nrhs), dtype=torch.float64, device="cuda")), pts
+
+
+def test_kernel_residual_batch_equals_single_calls(pp, gctx):
+    """The batched update + residual gives each job the bits of its own single call on x + dx,
+    across kernels, dimensions, RHS widths (tile-pair and row-block paths), ragged sizes and
+    more jobs than one launch holds."""
+    rng = np.random.default_rng(11)
+    shapes = [("inv", 1e-3, 2, 1500, 1), ("laplace", 1e-3, 3, 300, 3), ("exp", 0.1, 2, 129, 1),
+              ("matern32", 0.2, 3, 700, 8), ("inv", 1e-3, 2, 1, 1), ("inv", 1e-3, 2, 257, 4),
+              ("exp", 0.1, 1, 64, 16)] + [("inv", 1e-3, 2, 40 + q, 1) for q in range(66)]
+    jobs = [_resid_job(pp, rng, *sh, dup=(q % 3 == 0))[0] for q, sh in enumerate(shapes)]
+    want_x = [(x + dx).clone() for (_, _, _, _, x, dx, _, _) in jobs]
+    launches = gctx.kernel_residual_batch(jobs)
+    torch.cuda.synchronize()
+    assert launches == pp.residual_batch_launches([(j[0], j[3].shape[1], j[4].shape[1], True) for j in jobs])
+    for (kid, p0, shift, pts, x, dx, b, r), wx in zip(jobs, want_x):
+        assert torch.equal(x, wx)
+        r1 = torch.empty_like(r)
+        gctx.kernel_residual(kid, p0, shift, pts, x, b, r1)
+        torch.cuda.synchronize()
+        assert torch.equal(r, r1)
+
+
+@pytest.mark.parametrize("kernel,p0,dim", [("inv", 1e-3, 2), ("laplace", 1e-3, 3), ("exp", 0.1, 2),
+                                           ("matern32", 0.2, 3)])
+def test_kernel_residual_coincident_points(pp, gctx, kernel, p0, dim):
+    """Distance 0 off the diagonal and points far apart take the exact square-root path."""
+    rng = np.random.default_rng(8)
+    n = 400
+    pts = rng.uniform(0, 1, (n, dim))
+    pts[7] = pts[300]
+    pts[9] = pts[10]
+    pts[20] = 0.0
+    pts[21] = 0.0
+    pts[21, 0] = 1e-20  # squared distance 1e-40: below the float range of the estimates
+    pts[30] = 1e19  # squared distances near 1e38: above it
+    kid = pp.KERNELS[kernel]
+    prob = pp.KernelProblem(n, dim, kid, p0, 3.0, pts)
+    A = prob.dense()
+    x = rng.standard_normal((n, 1))
+    b = rng.standard_normal((n, 1))
+    r = torch.empty((n, 1), dtype=torch.float64, device="cuda")
+    gctx.kernel_residual_batch([(kid, p0, 3.0, dev(pts), dev(x), None, dev(b), r)])
+    want = b - A @ x
+    scale = np.abs(A).sum(1).max() * np.abs(x).max()
+    assert np.abs(r.cpu().numpy() - want).max() <= 1e-14 * scale
+
+
+def test_kernel_residual_rejects_p0_out_of_range(pp, gctx):
+    rng = np.random.default_rng(2)
+    job, _ = _resid_job(pp, rng, "inv", 1e-3, 2, 64, 1)
+    bad = (job[0], -1.0) + job[2:]
+    with pytest.raises(RuntimeError, match="p0"):
+        gctx.kernel_residual_batch([bad])
 
 
 def test_dense_residual_kernel(pp, gctx):
