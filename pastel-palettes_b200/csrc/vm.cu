@@ -2097,11 +2097,41 @@ int pp_vm_blocks_per_sm() {
   return nb;
 }
 
+namespace {
+// Loads one kernel's code now (lazy module loading would otherwise do it at its first launch,
+// in the middle of a served request).
+template <typename F>
+cudaError_t preload(F f) {
+  cudaFuncAttributes a;
+  return cudaFuncGetAttributes(&a, f);
+}
+template <int KIND, int DIM>
+cudaError_t preload_residual() {
+  cudaError_t e = preload(kernel_residual_sym<KIND, DIM, 1>);
+  if (e == cudaSuccess) e = preload(kernel_residual_sym<KIND, DIM, 4>);
+  if (e == cudaSuccess) e = preload(kernel_residual_part<KIND, DIM, 8>);
+  if (e == cudaSuccess) e = preload(kernel_residual_part<KIND, DIM, 16>);
+  return e;
+}
+template <int KIND>
+cudaError_t preload_residual_dims() {
+  cudaError_t e = preload_residual<KIND, 1>();
+  if (e == cudaSuccess) e = preload_residual<KIND, 2>();
+  if (e == cudaSuccess) e = preload_residual<KIND, 3>();
+  return e;
+}
+}  // namespace
+
 cudaError_t pp_vm_prepare() {
   cudaError_t e = cudaFuncSetAttribute(vm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pp_vm_smem_bytes());
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(accum_noalloc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)pp_vm_smem_bytes());
+  e = cudaFuncSetAttribute(accum_noalloc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pp_vm_smem_bytes());
+  // every kernel of the refinement and serving paths, loaded at context creation
+  for (cudaError_t r : {preload(vm_init), preload(residual_reduce), preload(residual_update), preload(axpy_kernel),
+                        preload(absmax2_kernel), preload(dense_residual_kernel), preload_residual_dims<0>(),
+                        preload_residual_dims<1>(), preload_residual_dims<2>(), preload_residual_dims<3>()})
+    if (e == cudaSuccess) e = r;
+  return e;
 }
 
 cudaError_t pp_vm_run(const pp_vm_launch& L, cudaStream_t s) {
