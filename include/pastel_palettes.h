@@ -117,6 +117,12 @@ long long pp_hmatrix_block_elems(const pp_hmatrix* h);
 #define PP_PRECISION_TF32 1
 pp_status pp_hmatrix_set_precision(pp_hmatrix* h, int precision);
 int pp_hmatrix_get_precision(const pp_hmatrix* h);
+/* output tile edge (64, the default, or 128) that the factor's products are split into;
+ * larger tiles give fewer, longer GEMM instructions (the autotuner tries both).  Results do not
+ * depend on it: every element still accumulates its k products in ascending order.  Rebuilds
+ * the programs on the next factorization; set it before pp_batch_create.  No reference
+ * counterpart (the reference's blocking is compile-time). */
+pp_status pp_hmatrix_set_gemm_tile(pp_hmatrix* h, int edge);
 /* adaptive rank (tol > 0, before set_lowrank and upload): low-rank blocks keep kmax columns,
  * zero beyond their numerical rank, and every accumulation into them truncates to the
  * singular values above tol times the largest (Gram eigen-decomposition by Jacobi, the role of
@@ -160,13 +166,15 @@ pp_status pp_batch_program_info(pp_batch* b, int which, int nrhs, pp_program_inf
 pp_status pp_batch_trace(pp_batch* b, int which, int nrhs, int enable, uint64_t* out);
 /* Autotuner (no reference counterpart; the reference's tile sizes are compile-time constants
  * of a missing header): times the batch's factor launch for every dense tile in {32, 64}
- * (the largest block one GETRF / TRSM instruction takes) and persistent grid in {all, 3/4,
- * 1/2 of the resident CTAs}, and keeps the fastest for this batch's later launches.  Every
+ * (the largest block one GETRF / TRSM instruction takes), product tile in {64, 128}
+ * (pp_hmatrix_set_gemm_tile) and persistent grid in {all, 3/4, 1/2 of the resident CTAs}, and
+ * keeps the fastest for this batch's later launches.  Every
  * instance must hold an original (pp_hmatrix_keep_original): each trial restores it first, and
  * on return the instances hold their restored, unfactored matrices. */
 typedef struct pp_tune_result {
   int tile, grid, trials;
   double factor_ms;
+  int gemm_tile; /* output tile edge of the product tasks (64 or 128) */
 } pp_tune_result;
 pp_status pp_batch_autotune(pp_batch* b, void* stream, pp_tune_result* out);
 

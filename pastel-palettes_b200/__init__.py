@@ -96,7 +96,8 @@ class _RequestStats(C.Structure):
 
 
 class _TuneResult(C.Structure):
-    _fields_ = [("tile", C.c_int), ("grid", C.c_int), ("trials", C.c_int), ("factor_ms", C.c_double)]
+    _fields_ = [("tile", C.c_int), ("grid", C.c_int), ("trials", C.c_int), ("factor_ms", C.c_double),
+                ("gemm_tile", C.c_int)]
 
 
 class _ProgramInfo(C.Structure):
@@ -172,6 +173,7 @@ def lib():
             "pp_server_clock_ms": (d, [vp]),
             "pp_server_destroy": (None, [vp]),
             "pp_hmatrix_set_precision": (i, [vp, i]),
+            "pp_hmatrix_set_gemm_tile": (i, [vp, i]),
             "pp_hmatrix_set_rank_tolerance": (i, [vp, d]),
             "pp_hmatrix_block_rank": (i, [vp, i]),
             "pp_hmatrix_get_precision": (i, [vp]),
@@ -390,6 +392,10 @@ class Hierarchical:
         FP32 accumulation; GETRF / TRSM / accumulation stay FP64."""
         self.ctx.check(lib().pp_hmatrix_set_precision(self._h, precision), "set_precision")
 
+    def set_gemm_tile(self, edge):
+        """Output tile edge (64 or 128) of the product instructions; results do not change."""
+        self.ctx.check(lib().pp_hmatrix_set_gemm_tile(self._h, edge), "set_gemm_tile")
+
     def set_rank_tolerance(self, tol):
         """Adaptive rank (tol > 0): accumulations truncate to singular values > tol * largest."""
         self.ctx.check(lib().pp_hmatrix_set_rank_tolerance(self._h, float(tol)), "set_rank_tolerance")
@@ -514,7 +520,7 @@ class Batch:
         (instances need keep_original); returns the choice and its time."""
         r = _TuneResult()
         self.ctx.check(lib().pp_batch_autotune(self._h, _stream_handle(stream), C.byref(r)), "batch_autotune")
-        return dict(tile=r.tile, grid=r.grid, trials=r.trials, factor_ms=r.factor_ms)
+        return dict(tile=r.tile, gemm_tile=r.gemm_tile, grid=r.grid, trials=r.trials, factor_ms=r.factor_ms)
 
     def enable_trace(self, which=0, nrhs=1):
         self.ctx.check(lib().pp_batch_trace(self._h, which, nrhs, 1, None), "batch_trace")

@@ -91,6 +91,7 @@ struct pp_hmatrix {
   bool pinned = false;
   int precision = PP_PREC_FP64;  // contraction precision of the factor's GEMM instructions
   int tile = 0;                  // dense tile of its programs (0: the context's)
+  int gemm_tile = 64;            // output tile edge of its product tasks (64 or 128)
   std::vector<double> rand_host;
   VmPlan factor;
   std::map<int, std::unique_ptr<VmPlan>> solves;
@@ -179,6 +180,7 @@ pp_status build_program(pp_hmatrix* h, int which, int nrhs, VmPlan& plan) {
   try {
     pp::Generator g(plan.prog, *h->H, h->tile > 0 ? h->tile : ctx->cfg.tile, h->H->n, ctx->cfg.reference_isa == 0);
     g.use_inverses(ctx->cfg.reference_isa == 0);
+    if (which == 0) g.set_gemm_tile(h->gemm_tile);  // the solve's products keep 64
     if (which == 0) {
       g.getrf_program();
       if (h->precision != PP_PREC_FP64) plan.prog.set_gemm_precision(h->precision);
@@ -516,6 +518,18 @@ pp_status pp_hmatrix_set_precision(pp_hmatrix* h, int precision) {
 }
 
 int pp_hmatrix_get_precision(const pp_hmatrix* h) { return h ? h->precision : -1; }
+
+pp_status pp_hmatrix_set_gemm_tile(pp_hmatrix* h, int edge) {
+  if (!h) return PP_INVALID_ARG;
+  if (edge != 64 && edge != 128) return fail(h->ctx, PP_INVALID_ARG, "pp_hmatrix_set_gemm_tile: 64 or 128");
+  if (edge == h->gemm_tile) return PP_OK;
+  h->gemm_tile = edge;
+  if (h->last == &h->factor) h->last = nullptr;
+  h->factor.release();
+  h->factor.prog = pp::Program();
+  h->factor.built = false;
+  return PP_OK;
+}
 
 pp_status pp_hmatrix_set_rank_tolerance(pp_hmatrix* h, double tol) {
   if (!h || !(tol >= 0.0) || tol >= 1.0) return PP_INVALID_ARG;
@@ -1052,16 +1066,21 @@ pp_status pp_batch_autotune(pp_batch* b, void* stream, pp_tune_result* out) {
   cudaStream_t s = (cudaStream_t)stream;
   const int full = ctx->sm_count * std::max(1, ctx->blocks_per_sm);
   const int tiles[] = {32, 64};
+  const int gemm_tiles[] = {64, 128};
   const int grids[] = {full, (3 * full) / 4, full / 2};
   cudaEvent_t e0, e1;
   PP_CUDA(cudaEventCreate(&e0));
   PP_CUDA(cudaEventCreate(&e1));
   double best = 1e300;
-  int best_tile = 0, best_grid = 0, trials = 0;
+  int best_tile = 0, best_grid = 0, best_gt = 64, trials = 0;
   pp_status st = PP_OK;
-  for (int t : tiles) {
+  for (int t : tiles)
+  for (int gt : gemm_tiles) {
     if (t > PP_VM_TILE) continue;
-    for (auto* h : b->hs) h->tile = t;
+    for (auto* h : b->hs) {
+      h->tile = t;
+      h->gemm_tile = gt;
+    }
     batch_reset_programs(b);
     for (int g : grids) {
       b->grid_cap = g;
@@ -1081,6 +1100,7 @@ pp_status pp_batch_autotune(pp_batch* b, void* stream, pp_tune_result* out) {
         best = ms;
         best_tile = t;
         best_grid = g;
+        best_gt = gt;
       }
     }
     if (st != PP_OK) break;
@@ -1088,7 +1108,10 @@ pp_status pp_batch_autotune(pp_batch* b, void* stream, pp_tune_result* out) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (st != PP_OK) return st;
-  for (auto* h : b->hs) h->tile = best_tile;
+  for (auto* h : b->hs) {
+    h->tile = best_tile;
+    h->gemm_tile = best_gt;
+  }
   batch_reset_programs(b);
   b->grid_cap = best_grid;
   st = pp_batch_restore(b, stream);
@@ -1096,6 +1119,7 @@ pp_status pp_batch_autotune(pp_batch* b, void* stream, pp_tune_result* out) {
   if (out) {
     out->tile = best_tile;
     out->grid = best_grid;
+    out->gemm_tile = best_gt;
     out->factor_ms = best;
     out->trials = trials;
   }

@@ -718,8 +718,9 @@ void Generator::gemm_tiles(const View& C, const View& A, const View& B, int alph
     s.flops = (int64_t)C.m * C.n * parts;
     return;
   }
-  const int TN = std::min(C.n, 64);
-  const int TM = std::min(C.m, std::max(64, 4096 / std::max(TN, 1)));
+  const int g = gemm_tile_;
+  const int TN = std::min(C.n, g);
+  const int TM = std::min(C.m, std::max(g, g * g / std::max(TN, 1)));
   for (int i = 0; i < C.m; i += TM)
     for (int j = 0; j < C.n; j += TN) {
       const int mi = std::min(TM, C.m - i), nj = std::min(TN, C.n - j);

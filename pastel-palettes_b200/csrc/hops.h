@@ -133,6 +133,9 @@ class Generator {
   // explicit inverses of the diagonal leaves' triangular factors (TRINV), which the solve
   // program then applies with TRMV instead of substituting; set before building programs
   void use_inverses(bool on) { inverses_ = on; }
+  // edge of the output tiles products are split into (64 or 128; larger tiles: fewer, longer
+  // tasks)
+  void set_gemm_tile(int t) { gemm_tile_ = t >= 128 ? 128 : 64; }
   void solve_program(int nrhs);    // B := U^-1 L^-1 B on the RHS object (n x nrhs)
   int rhs_obj() const { return rhs_obj_; }
 
@@ -156,6 +159,7 @@ class Generator {
   int max_n_rand_;
   bool split_k_;
   bool inverses_ = false;
+  int gemm_tile_ = 64;
   bool solve_ = false;  // building a solve program
   void trmv(int inv, int upper, int m, const View& B);
   std::vector<std::pair<int, int>> inv_obj_;  // program obj of a diagonal leaf -> (L^-1, U^-1) objs

@@ -281,6 +281,7 @@ __device__ __forceinline__ void dev_gemm(double* __restrict__ C, int ldc, const 
   else if (n == 1) gemm_cfg<256, 1, 1, 1, 16>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
   else if (n <= 16) gemm_cfg<128, 16, 8, 1, 32>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
   else if (m <= 16) gemm_cfg<16, 128, 1, 8, 32>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
+  else if (m > 64 && n > 64) gemm_cfg<128, 128, 8, 8, 8>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
   else gemm_cfg<64, 64, 4, 4, 32>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
 }
 

@@ -118,3 +118,16 @@ def test_residual_batch_refuses_without_device_and_counts_launches(pp, hctx):
     assert count([(0, 2, 1, True)] * 65) == 6
     assert count([(0, 2, 1, False), (0, 2, 3, False), (2, 3, 1, False)]) == 4
     assert count([(0, 2, 8, True), (0, 2, 16, True), (1, 3, 4, True)]) == 1 + 1 + 2 + 1
+
+
+def test_gemm_tile_option_shrinks_the_factor_program(pp, hctx):
+    """128 x 128 product tiles: fewer GEMM instructions and the same flops; only 64 and 128."""
+    h1, _ = pp.make_kernel_problem(hctx, 2048, 2, "inv", 1e-3, 256, 16)
+    h2, _ = pp.make_kernel_problem(hctx, 2048, 2, "inv", 1e-3, 256, 16)
+    h2.set_gemm_tile(128)
+    with pytest.raises(pp.PPError):
+        h2.set_gemm_tile(32)
+    i1, i2 = h1.program_info(0), h2.program_info(0)
+    assert i2["op_count"]["gemm"] < i1["op_count"]["gemm"]
+    assert i2["flops"] == i1["flops"]
+    assert h2.program_info(1)["n_tasks"] == h1.program_info(1)["n_tasks"]  # the solve keeps 64

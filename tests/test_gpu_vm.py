@@ -63,7 +63,8 @@ class TaskBench:
 
 @pytest.mark.parametrize("tA,tB", [(0, 0), (1, 0), (0, 1), (1, 1)])
 @pytest.mark.parametrize("alpha,beta", [(-1.0, 1.0), (1.0, 1.0), (1.0, 0.0)])
-@pytest.mark.parametrize("m,n,k", [(64, 64, 64), (37, 91, 130), (256, 16, 16), (5, 3, 0)])
+@pytest.mark.parametrize("m,n,k", [(64, 64, 64), (37, 91, 130), (256, 16, 16), (5, 3, 0), (128, 128, 16),
+                                   (130, 140, 20), (200, 256, 9)])
 def test_gemm_task_bitwise(pp, oracle, gctx, tA, tB, alpha, beta, m, n, k):
     tb = TaskBench(pp, seed=m * 7 + n)
     c = tb.operand(m, n)
@@ -87,8 +88,8 @@ def test_getrf_task_bitwise(pp, oracle, gctx, m, n):
 @pytest.mark.parametrize("alpha,beta", [(-1.0, 1.0), (1.0, 0.0)])
 @pytest.mark.parametrize("m,n,k", [(64, 64, 16), (256, 16, 16), (37, 91, 130), (64, 16, 64)])
 def test_gemm_task_free_order(pp, oracle, gctx, tA, tB, alpha, beta, m, n, k):
-    """GEMM with the free-order flag (products of low-rank factors): the FP64 tensor-core path,
-    within rounding of the oracle's ascending-k sum."""
+    """GEMM with the free-order flag (products into work buffers): within rounding of the
+    oracle's ascending-k sum."""
     tb = TaskBench(pp, seed=m * 7 + n + k)
     c = tb.operand(m, n)
     a = tb.operand(k, m) if tA else tb.operand(m, k)
@@ -221,6 +222,20 @@ def test_hodlr_factor_matches_oracle(pp, oracle, gctx):
     F = factor_on_gpu(h)
     h.host_arena()[:] = ar.matrix
     assert rel(F, h.to_dense()) < 1e-12
+
+
+def test_gemm_tile_128_factor_bitwise(pp, gctx):
+    """Products split into 128 x 128 output tiles: fewer GEMM instructions, the same bits (each
+    element keeps its ascending-k chain and the DAG keeps the update order)."""
+    h1, _ = pp.make_kernel_problem(gctx, 2048, 2, "inv", 1e-3, 256, 16)
+    h2, _ = pp.make_kernel_problem(gctx, 2048, 2, "inv", 1e-3, 256, 16)
+    h2.set_gemm_tile(128)
+    with pytest.raises(pp.PPError):
+        h2.set_gemm_tile(96)
+    F1 = factor_on_gpu(h1)
+    F2 = factor_on_gpu(h2)
+    assert h2.program_info(0)["n_tasks"] < h1.program_info(0)["n_tasks"]
+    assert np.array_equal(F1, F2)
 
 
 def run_reference_kernel(pp, oracle, h):
