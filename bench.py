@@ -223,6 +223,80 @@ def make_batch(pp, ctx, batch, rank):
     return hs, [prob] * batch
 
 
+def pipelined_e2e(pp, ctx, torch, hs, probs, b_host, bs, x_host, g_a, out_a, ref_a, batch_a, tune, iters, steps,
+                  tol, s, barrier):
+    """End-to-end throughput with the transfers overlapped: two device-resident input sets
+    (the bench batch and a second copy) alternate; step k's matrices and right-hand sides go up
+    on an upload stream while step k - 1 computes, its solutions come down on a download stream
+    while step k + 1 computes.  Every step still moves its own inputs up from pinned host
+    memory and its solutions down inside the timed region (first upload to last download).
+    Returns (factor+solve/s of this rank, description)."""
+    w = WORKLOAD
+    hs_b = []
+    for h in hs:
+        q = pp.Hierarchical.geometric(ctx, probs[0].points, w["leaf"], w["admissibility"], 1.0, w["rank"])
+        q.host_arena()[:] = h.host_arena()
+        q.pin_host()
+        q.upload(s)
+        hs_b.append(q)
+    s.synchronize()
+    batch_b = pp.Batch(ctx, hs_b)
+    if tune:
+        batch_b.set_tuning(**tune)
+    bs_b = [b.clone() for b in bs]
+    x_host_b = [torch.empty_like(x).pin_memory() for x in x_host]
+    ref_b = pp.BatchRefiner(batch_b, probs, stream=s)
+    with torch.cuda.stream(s):
+        batch_b.factor(s)
+        ref_b.run(bs_b, iters)  # eager: allocates the plans before capture
+        for q in hs_b:
+            q.upload(s)
+        g_b = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g_b, stream=s):
+            batch_b.factor(s)
+            out_b = ref_b.run(bs_b, iters)
+    s.synchronize()
+    sets = [(hs, bs, g_a, out_a, x_host, ref_a), (hs_b, bs_b, g_b, out_b, x_host_b, ref_b)]
+    up_s, down_s = torch.cuda.Stream(), torch.cuda.Stream()
+    ev = lambda: torch.cuda.Event(enable_timing=False)
+    up, comp, down = [ev(), ev()], [ev(), ev()], [ev(), ev()]
+    n_steps = 2 * max(2, steps)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(up_s)
+    for k in range(n_steps):
+        j = k % 2
+        H, Bd, G, out, Xh, _ = sets[j]
+        with torch.cuda.stream(up_s):
+            if k >= 2:
+                up_s.wait_event(down[j])  # the set's previous step has computed and come down
+            for h in H:
+                h.upload(up_s)
+            for bd, bh in zip(Bd, b_host):
+                bd.copy_(bh, non_blocking=True)
+            up[j].record(up_s)
+        with torch.cuda.stream(s):
+            s.wait_event(up[j])
+            G.replay()
+            comp[j].record(s)
+        with torch.cuda.stream(down_s):
+            down_s.wait_event(comp[j])
+            for xh, xd in zip(Xh, out[0]):
+                xh.copy_(xd, non_blocking=True)
+            down[j].record(down_s)
+    up_s.wait_event(down[0])
+    up_s.wait_event(down[1])
+    e1.record(up_s)
+    e1.synchronize()
+    total = e0.elapsed_time(e1) / 1e3
+    for H, Bd, G, out, Xh, ref in sets:
+        if max(ref.errors(Bd, *out)) > tol:
+            raise SystemExit("pipelined end-to-end step ended above the tolerance")
+    mode = (f"{n_steps} steps over two alternating device input sets: uploads of step k overlap the "
+            f"compute of step k - 1, downloads overlap step k + 1 (separate upload / download streams)")
+    return len(hs) * n_steps / total, mode
+
+
 def serving_leg(pp, ctx, n_requests, rate, seed=2024, smin=1024, smax=3072):
     """Poisson arrivals of factor+solve requests into the server (continuous admission).
     Sizes log-uniform in [smin, smax], kernel uniform among Laplace 1/r, exp (length 0.1) and
@@ -242,6 +316,10 @@ def serving_leg(pp, ctx, n_requests, rate, seed=2024, smin=1024, smax=3072):
         reqs.append((h, prob, rhs))
     gaps = rng.exponential(1.0 / rate, n_requests)
     srv = pp.Server(ctx, hbm_budget_bytes=64 << 30, max_inflight=4)
+    # one untimed warm-up request (a server's first admission pays one-time host and driver setup)
+    hw, pw = pp.make_kernel_problem(ctx, smin, 3, "laplace", 1e-3, 128, 16, seed=seed - 1)
+    srv.submit(hw, pw, rng.uniform(-1, 1, (1, smin, 4)), tol=WORKLOAD["tol"])
+    srv.wait_all()
     ids = []
     t0 = time.perf_counter()
     t_next = 0.0
@@ -488,7 +566,13 @@ def main():
     t = torch.tensor([e2e_total], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * B * e2e_steps / t.item()
+    e2e_serial = world * B * e2e_steps / t.item()
+    e2e_value, e2e_mode = pipelined_e2e(pp, ctx, torch, hs, probs, b_host, bs, x_host, g2, out2, ref, batch,
+                                        main_stats["autotune"], iters, e2e_steps, tol, s, barrier)
+    t = torch.tensor([e2e_value], dtype=torch.float64, device="cuda")
+    if world > 1:  # the slowest rank's rate
+        dist.all_reduce(t, op=dist.ReduceOp.MIN)
+    e2e_value = world * t.item()
 
     # --- the dominant kernel (the batched factor launch), timed alone
     fac_ms = []
@@ -561,7 +645,9 @@ def main():
                            "single_job_step_ms": float(np.median(lat))},
                 "e2e": {"value": e2e_value, "unit": "factor+solve/s",
                         "h2d_bytes_per_step": B * (hs[0].arena_bytes() + 8 * n),
-                        "d2h_bytes_per_step": B * 8 * n},
+                        "d2h_bytes_per_step": B * 8 * n, "mode": e2e_mode,
+                        "serial_value": e2e_serial,
+                        "serial_mode": "one step at a time: upload, factor + refinement, download, then the next"},
                 "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "serving": serving,
                 "uneven_batch": uneven,
                 "plain_fp64_single_instance": {

@@ -177,6 +177,9 @@ typedef struct pp_tune_result {
   int gemm_tile; /* output tile edge of the product tasks (64 or 128) */
 } pp_tune_result;
 pp_status pp_batch_autotune(pp_batch* b, void* stream, pp_tune_result* out);
+/* applies a tuning (from pp_batch_autotune on a batch of the same shapes) without timing:
+ * dense tile (8..64), product tile (64 or 128) and persistent grid (0: all CTAs) */
+pp_status pp_batch_set_tuning(pp_batch* b, int tile, int gemm_tile, int grid);
 
 /* --- serving: a request loop with continuous admission (no reference counterpart; the
  *     reference factors one matrix per launch) -------------------------------------------

@@ -165,6 +165,7 @@ def lib():
             "pp_batch_program_info": (i, [vp, i, i, C.POINTER(_ProgramInfo)]),
             "pp_batch_trace": (i, [vp, i, i, i, vp]),
             "pp_batch_autotune": (i, [vp, vp, C.POINTER(_TuneResult)]),
+            "pp_batch_set_tuning": (i, [vp, i, i, i]),
             "pp_refstream_encode": (i, [vp, i, vp, ll, vp, C.POINTER(ll)]),
             "pp_server_create": (i, [vp, C.POINTER(_ServeConfig), C.POINTER(vp)]),
             "pp_server_submit": (i, [vp, vp, C.POINTER(_RequestDesc), C.POINTER(ll)]),
@@ -521,6 +522,10 @@ class Batch:
         r = _TuneResult()
         self.ctx.check(lib().pp_batch_autotune(self._h, _stream_handle(stream), C.byref(r)), "batch_autotune")
         return dict(tile=r.tile, gemm_tile=r.gemm_tile, grid=r.grid, trials=r.trials, factor_ms=r.factor_ms)
+
+    def set_tuning(self, tile, gemm_tile, grid, **_):
+        """Applies an autotune() result (of a batch of the same shapes) without timing."""
+        self.ctx.check(lib().pp_batch_set_tuning(self._h, int(tile), int(gemm_tile), int(grid)), "batch_set_tuning")
 
     def enable_trace(self, which=0, nrhs=1):
         self.ctx.check(lib().pp_batch_trace(self._h, which, nrhs, 1, None), "batch_trace")

@@ -1126,6 +1126,19 @@ pp_status pp_batch_autotune(pp_batch* b, void* stream, pp_tune_result* out) {
   return PP_OK;
 }
 
+pp_status pp_batch_set_tuning(pp_batch* b, int tile, int gemm_tile, int grid) {
+  if (!b) return PP_INVALID_ARG;
+  if (tile < 8 || tile > PP_VM_TILE || (gemm_tile != 64 && gemm_tile != 128) || grid < 0)
+    return fail(b->ctx, PP_INVALID_ARG, "pp_batch_set_tuning: tile 8..64, product tile 64 or 128, grid >= 0");
+  for (auto* h : b->hs) {
+    h->tile = tile;
+    h->gemm_tile = gemm_tile;
+  }
+  batch_reset_programs(b);
+  b->grid_cap = grid;
+  return PP_OK;
+}
+
 pp_status pp_batch_trace(pp_batch* b, int which, int nrhs, int enable, uint64_t* out) {
   if (!b || (which != 0 && which != 1)) return PP_INVALID_ARG;
   pp_context* ctx = b->ctx;
@@ -1390,6 +1403,18 @@ pp_status pp_server_create(pp_context* ctx, const pp_serve_config* cfg, pp_serve
   cudaError_t e = cudaMemPoolCreate(&s->pool, &props);
   unsigned long long keep = (unsigned long long)s->budget;
   if (e == cudaSuccess) e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  if (e == cudaSuccess) {
+    // map the first part of the budget now (one allocation, freed at once: the pool keeps it),
+    // so that admitting the first requests does not wait for the device memory to be mapped
+    const size_t warm = (size_t)std::min<long long>(s->budget, 1ll << 30);
+    cudaStream_t ws = nullptr;
+    void* p = nullptr;
+    e = cudaStreamCreateWithFlags(&ws, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&p, warm, s->pool, ws);
+    if (e == cudaSuccess) e = cudaFreeAsync(p, ws);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ws);
+    if (ws) cudaStreamDestroy(ws);
+  }
   if (e != cudaSuccess) {
     if (s->pool) cudaMemPoolDestroy(s->pool);
     delete s;

@@ -1718,14 +1718,17 @@ __device__ __forceinline__ double rcp_refine(double a, double y0) {
   const double e = fma(-a, y0, 1.0);
   return fma(y0, fma(e, e, e), y0);
 }
-// Entry K(d) of the kernel matrix at squared distance d2, d = d2 / sqrt(max(d2, 1e-300)):
-// exact zero on the diagonal and for coincident points, an absolute error below 1e-150 for
-// 0 < d2 < 1e-300, a few ulps elsewhere.
+// Entry K(d) of the kernel matrix at squared distance d2.  d = sqrt(d2) as s0 = d2 y0 with y0
+// the estimate of 1 / sqrt(max(d2, 1e-300)), corrected like rsqrt_refine: with e = 1 - s0 y0,
+// d = s0 (1 + e/2 + 3e^2/8).  Exact zero on the diagonal and for coincident points, an
+// absolute error below 1e-150 for 0 < d2 < 1e-300, a few ulps elsewhere.
 template <int KIND>
 __device__ __forceinline__ double kernel_eval_nr(double d2, double p0, double inv_p0) {
   constexpr double c = KIND == 1 ? 4.0 * 3.14159265358979323846 : 1.0;
-  const double d2c = fmax(d2, 1e-300);
-  const double d = d2 * rsqrt_refine(d2c, rsqrt_est(d2c));
+  const double y0 = rsqrt_est(fmax(d2, 1e-300));
+  const double s0 = d2 * y0;
+  const double e = fma(-s0, y0, 1.0);
+  const double d = fma(s0 * e, fma(0.375, e, 0.5), s0);
   if (KIND <= 1) {
     const double x = c * (d + p0);
     return rcp_refine(x, rcp_est(x));
@@ -1832,15 +1835,17 @@ __device__ __forceinline__ int resid_job_of(const ResidLaunch& L, long long key)
 
 // KR_SEG steps of one warp over a tile pair: lane l takes column (l + s) mod KR_SEG at step s.
 // COL: also accumulate a_ij x_i into the warp's column sums (off-diagonal tiles); EDGE: skip
-// columns at or past jn (the caller skips rows past n).
-template <int KIND, int DIM, int NR, bool COL, bool EDGE>
+// columns at or past jn (the caller skips rows past n).  DUP: the tile's points, x and column
+// sums are stored twice over (2 KR_SEG entries), so the column is addressed as l + s without
+// the wrap-around; column c's sums are then split between entries c and c + KR_SEG.
+template <int KIND, int DIM, int NR, bool COL, bool EDGE, bool DUP>
 __device__ __forceinline__ void residual_steps(const double* sp, const double* sx, double* colw, const double (&pi)[DIM],
                                                const double (&xi)[NR], double (&acc)[NR], int lane, int jn, double p0,
                                                double inv_p0) {
 #pragma unroll 4
   for (int st = 0; st < KR_SEG; ++st) {
-    const int jj = (lane + st) & (KR_SEG - 1);
-    if (EDGE && jj >= jn) continue;
+    const int jj = DUP ? lane + st : (lane + st) & (KR_SEG - 1);
+    if (EDGE && ((lane + st) & (KR_SEG - 1)) >= jn) continue;
     double d2 = 0.0;
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
@@ -1868,9 +1873,11 @@ __device__ __forceinline__ void residual_steps(const double* sp, const double* s
 template <int KIND, int DIM, int NR>
 __global__ void __launch_bounds__(KR_SEG) kernel_residual_sym(const __grid_constant__ ResidLaunch L) {
   constexpr int W = KR_SEG / 32;
-  __shared__ double sp[KR_SEG * DIM];
-  __shared__ double sx[KR_SEG * NR];
-  __shared__ double col[W][KR_SEG * NR];
+  constexpr bool DUP = NR == 1;             // one RHS: tile stored twice over (residual_steps)
+  constexpr int SW = DUP ? 2 * KR_SEG : KR_SEG;
+  __shared__ double sp[SW * DIM];
+  __shared__ double sx[SW * NR];
+  __shared__ double col[W][SW * NR];
   const ResidLaunch::Job& jb = L.job[resid_job_of(L, (long long)blockIdx.x)];
   const double* __restrict__ pts = jb.pts;
   const double* __restrict__ x = jb.x;
@@ -1889,15 +1896,15 @@ __global__ void __launch_bounds__(KR_SEG) kernel_residual_sym(const __grid_const
   const int t = threadIdx.x, w = t >> 5, lane = t & 31;
   const int i = I * KR_SEG + t, j0 = J * KR_SEG;
   const double inv_p0 = 1.0 / p0;
-  for (int e = t; e < KR_SEG * DIM; e += KR_SEG) {
-    const int jj = e / DIM;
-    sp[e] = j0 + jj < n ? pts[(size_t)j0 * DIM + e] : 0.0;
+  for (int e = t; e < SW * DIM; e += KR_SEG) {
+    const int e0 = e % (KR_SEG * DIM), jj = e0 / DIM;
+    sp[e] = j0 + jj < n ? pts[(size_t)j0 * DIM + e0] : 0.0;
   }
-  for (int e = t; e < KR_SEG * NR; e += KR_SEG) {
-    const int jj = e / NR, q = e % NR;
+  for (int e = t; e < SW * NR; e += KR_SEG) {
+    const int e0 = e % (KR_SEG * NR), jj = e0 / NR, q = e0 % NR;
     sx[e] = (j0 + jj < n && q < nrhs) ? x[(size_t)(j0 + jj) * nrhs + q] : 0.0;
   }
-  for (int e = t; e < W * KR_SEG * NR; e += KR_SEG) (&col[0][0])[e] = 0.0;
+  for (int e = t; e < W * SW * NR; e += KR_SEG) (&col[0][0])[e] = 0.0;
   const int ir = min(i, n - 1);
   double pi[DIM], xi[NR], acc[NR];
 #pragma unroll
@@ -1911,11 +1918,11 @@ __global__ void __launch_bounds__(KR_SEG) kernel_residual_sym(const __grid_const
   const bool offdiag = I != J;
   const int jn = min(KR_SEG, n - j0);
   if (jn == KR_SEG && I * KR_SEG + KR_SEG <= n) {  // full tiles: no per-entry predicates
-    if (offdiag) residual_steps<KIND, DIM, NR, true, false>(sp, sx, col[w], pi, xi, acc, lane, jn, p0, inv_p0);
-    else residual_steps<KIND, DIM, NR, false, false>(sp, sx, col[w], pi, xi, acc, lane, jn, p0, inv_p0);
+    if (offdiag) residual_steps<KIND, DIM, NR, true, false, DUP>(sp, sx, col[w], pi, xi, acc, lane, jn, p0, inv_p0);
+    else residual_steps<KIND, DIM, NR, false, false, DUP>(sp, sx, col[w], pi, xi, acc, lane, jn, p0, inv_p0);
   } else if (i < n) {  // ragged edge of the matrix
-    if (offdiag) residual_steps<KIND, DIM, NR, true, true>(sp, sx, col[w], pi, xi, acc, lane, jn, p0, inv_p0);
-    else residual_steps<KIND, DIM, NR, false, true>(sp, sx, col[w], pi, xi, acc, lane, jn, p0, inv_p0);
+    if (offdiag) residual_steps<KIND, DIM, NR, true, true, DUP>(sp, sx, col[w], pi, xi, acc, lane, jn, p0, inv_p0);
+    else residual_steps<KIND, DIM, NR, false, true, DUP>(sp, sx, col[w], pi, xi, acc, lane, jn, p0, inv_p0);
   }
   if (!offdiag && i < n) {  // the diagonal entry's shift
 #pragma unroll
@@ -1929,8 +1936,12 @@ __global__ void __launch_bounds__(KR_SEG) kernel_residual_sym(const __grid_const
     if (jrow < n)
       for (int q = 0; q < nrhs; ++q) {
         double v = col[0][t * NR + q];
+        if (DUP) v += col[0][(t + KR_SEG) * NR + q];
 #pragma unroll
-        for (int ww = 1; ww < W; ++ww) v += col[ww][t * NR + q];
+        for (int ww = 1; ww < W; ++ww) {
+          v += col[ww][t * NR + q];
+          if (DUP) v += col[ww][(t + KR_SEG) * NR + q];
+        }
         part[((size_t)I * n + jrow) * nrhs + q] = v;
       }
   }

@@ -14,7 +14,7 @@ reports, per program (factor, solve):
   * the ready-to-start latency (a task's start minus its last predecessor's end).
 
   python pastel-palettes_b200/trace_tool.py [--n 8192] [--leaf 256] [--rank 16] [--batch 16]
-                                            [--out trace.npz]
+                                            [--gemm-tile 64|128] [--out trace.npz]
 """
 import argparse
 import collections
@@ -97,6 +97,7 @@ def main():
     ap.add_argument("--leaf", type=int, default=256)
     ap.add_argument("--rank", type=int, default=16)
     ap.add_argument("--batch", type=int, default=16)
+    ap.add_argument("--gemm-tile", type=int, default=128, help="output tile edge of the factor's products")
     ap.add_argument("--out", default=None, help="also save the raw trace (npz)")
     args = ap.parse_args()
     import torch
@@ -104,6 +105,7 @@ def main():
     pp = _load()
     ctx = pp.Context(device=0)
     h, prob = pp.make_kernel_problem(ctx, args.n, 2, "inv", 1e-3, args.leaf, args.rank, seed=1234)
+    h.set_gemm_tile(args.gemm_tile)
     h.upload()
     h.keep_original()
     raw = {}
@@ -127,6 +129,7 @@ def main():
         hs = [h] + [pp.Hierarchical.geometric(ctx, prob.points, args.leaf, 0, 1.0, args.rank)
                     for _ in range(args.batch - 1)]
         for q in hs[1:]:
+            q.set_gemm_tile(args.gemm_tile)
             q.host_arena()[:] = h.host_arena()
             q.upload()
             q.keep_original()

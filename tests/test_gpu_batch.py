@@ -142,3 +142,27 @@ def test_batch_autotune_keeps_results(pp, gctx):
     for h, F in zip(hs, ref):
         h.download()
         assert rel(h.to_dense(), F) < 1e-12
+
+
+def test_batch_set_tuning_applies_a_tuning(pp, gctx):
+    """A tuning found on one batch, applied to a second batch of the same shapes, gives the
+    same factors; bad tunings are refused."""
+    hs = [pp.make_kernel_problem(gctx, 1024, 2, "inv", 1e-3, 128, 16, seed=5 + i)[0] for i in range(2)]
+    hs2 = [pp.make_kernel_problem(gctx, 1024, 2, "inv", 1e-3, 128, 16, seed=5 + i)[0] for i in range(2)]
+    for h in hs + hs2:
+        h.upload()
+        h.keep_original()
+    b = pp.Batch(gctx, hs)
+    tune = b.autotune()
+    b2 = pp.Batch(gctx, hs2)
+    b2.set_tuning(**tune)
+    with pytest.raises(pp.PPError):
+        b2.set_tuning(tile=64, gemm_tile=100, grid=0)
+    b2.set_tuning(**tune)
+    for bt in (b, b2):
+        bt.factor()
+        bt.sync()
+    for h, h2 in zip(hs, hs2):
+        h.download()
+        h2.download()
+        assert np.array_equal(h.to_dense(), h2.to_dense())
