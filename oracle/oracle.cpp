@@ -357,18 +357,23 @@ int run_one(const pp_task& T, std::vector<double>& tmp) {
         o_trsmu(I, T.p[1], c0 + w, w, ldi, lda);
       return 0;
     }
-    case PP_OP_TRMV: {  // engine instruction: B := M B, M triangular (ascending column sums)
-      const int m = T.m, n = T.n, ldb = T.ld[0], ldm = T.ld[1];
-      std::vector<double> out((size_t)m * n);
-      for (int r = 0; r < m; ++r)
+    case PP_OP_TRMV: {  // engine instruction: B := M B, M triangular (ascending column sums);
+                        // l > 0: rows [o, o + l) of M S (S at p[2]) into p[0]
+      const int m = T.m, n = T.n, ldm = T.ld[1];
+      const bool part = T.l > 0;
+      const double* S = part ? T.p[2] : T.p[0];
+      const int lds = part ? T.ld[2] : T.ld[0], r0 = part ? T.o : 0, r1 = part ? T.o + T.l : m;
+      if (r0 < 0 || r1 > m || !S) return -1;
+      std::vector<double> out((size_t)(r1 - r0) * n);
+      for (int r = r0; r < r1; ++r)
         for (int q = 0; q < n; ++q) {
           double s = 0.0;
           const int c_lo = T.ctrl ? r : 0, c_hi = T.ctrl ? m : r + 1;
-          for (int c = c_lo; c < c_hi; ++c) s = std::fma(T.p[1][(int64_t)r * ldm + c], T.p[0][(int64_t)c * ldb + q], s);
-          out[(size_t)r * n + q] = s;
+          for (int c = c_lo; c < c_hi; ++c) s = std::fma(T.p[1][(int64_t)r * ldm + c], S[(int64_t)c * lds + q], s);
+          out[(size_t)(r - r0) * n + q] = s;
         }
-      for (int r = 0; r < m; ++r)
-        for (int q = 0; q < n; ++q) T.p[0][(int64_t)r * ldb + q] = out[(size_t)r * n + q];
+      for (int r = r0; r < r1; ++r)
+        for (int q = 0; q < n; ++q) T.p[0][(int64_t)(r - r0) * T.ld[0] + q] = out[(size_t)(r - r0) * n + q];
       return 0;
     }
     case PP_OP_ORTH: {  // engine instruction: shifted CholeskyQR3 of Y (m x k, ld k)

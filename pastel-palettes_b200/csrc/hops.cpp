@@ -2,6 +2,7 @@
 #include "hops.h"
 
 #include <algorithm>
+#include <cmath>
 #include <stdexcept>
 
 namespace pp {
@@ -720,7 +721,8 @@ void Generator::gemm_tiles(const View& C, const View& A, const View& B, int alph
   }
   const int g = gemm_tile_;
   const int TN = std::min(C.n, g);
-  const int TM = std::min(C.m, std::max(g, g * g / std::max(TN, 1)));
+  int TM = std::min(C.m, std::max(g, g * g / std::max(TN, 1)));
+  if (solve_ && C.n <= 16) TM = std::min(TM, kSolveGemmRows);
   for (int i = 0; i < C.m; i += TM)
     for (int j = 0; j < C.n; j += TN) {
       const int mi = std::min(TM, C.m - i), nj = std::min(TN, C.n - j);
@@ -859,13 +861,47 @@ void Generator::trmv(int inv, int upper, int m, const View& B) {
   M.n = m;
   for (int c = 0; c < B.n; c += kTrmvCols) {
     const int w = std::min(kTrmvCols, B.n - c);
-    HTask& t = emit(PP_OP_TRMV);
-    bind(t, 0, B.sub(0, c, B.m, w), true);
-    bind(t, 1, M, false);
-    t.t.m = m;
-    t.t.n = w;
-    t.t.ctrl = upper;
-    t.flops = (int64_t)w * m * (m + 1);
+    const View Bc = B.sub(0, c, B.m, w);
+    if (m < kTrmvSplitMin) {
+      HTask& t = emit(PP_OP_TRMV);
+      bind(t, 0, Bc, true);
+      bind(t, 1, M, false);
+      t.t.m = m;
+      t.t.n = w;
+      t.t.ctrl = upper;
+      t.flops = (int64_t)w * m * (m + 1);
+      continue;
+    }
+    // row blocks of equal area: lower rows [0, b) hold b^2/2 entries, upper rows [b, m) (m-b)^2/2
+    int bound[kTrmvParts + 1];
+    for (int p = 0; p <= kTrmvParts; ++p) {
+      const double f = (double)p / kTrmvParts;
+      bound[p] = upper ? m - (int)std::lround(m * std::sqrt(1.0 - f)) : (int)std::lround(m * std::sqrt(f));
+    }
+    bound[0] = 0;
+    bound[kTrmvParts] = m;
+    const View W = tmp(m, w);
+    for (int p = 0; p < kTrmvParts; ++p) {
+      const int r0 = bound[p], r1 = bound[p + 1];
+      if (r1 <= r0) continue;
+      HTask& t = emit(PP_OP_TRMV);
+      bind(t, 0, W.sub(r0, 0, r1 - r0, w), true);
+      bind(t, 1, M, false);
+      bind(t, 2, Bc, false);
+      t.t.m = m;
+      t.t.n = w;
+      t.t.ctrl = upper;
+      t.t.o = r0;
+      t.t.l = r1 - r0;
+      int64_t e = 0;
+      for (int r = r0; r < r1; ++r) e += upper ? m - r : r + 1;
+      t.flops = 2 * (int64_t)w * e;
+    }
+    HTask& cp = emit(PP_OP_COPY);
+    bind(cp, 0, Bc, true);
+    bind(cp, 1, W, false);
+    cp.t.m = m;
+    cp.t.n = w;
   }
 }
 

@@ -116,6 +116,14 @@ class Program {
 constexpr int kSolveTri = 256;
 // right-hand-side columns of one TRMV instruction
 constexpr int kTrmvCols = 16;
+// a leaf product M B on triangles of at least kTrmvSplitMin rows is split into kTrmvParts row
+// blocks of equal triangle area (one CTA each, into a work buffer) and a copy back: the solve's
+// critical path then waits for a quarter of the triangle's loads instead of all of them
+constexpr int kTrmvSplitMin = 128;
+constexpr int kTrmvParts = 4;
+// rows of one product instruction of the solve with at most 16 columns (more CTAs on the
+// matrix-vector products of the critical path)
+constexpr int kSolveGemmRows = 256;
 // largest rank of the added term of one ACCUM (the VM keeps it in registers)
 constexpr int kAccumMaxK2 = 32;
 // smallest m, n and k of a GEMM instruction the TF32 form runs on the tensor cores

@@ -35,7 +35,10 @@ enum pp_op {
                         reference counterpart (it serves the solve)                             */
   PP_OP_TRMV = 12,   /* B[m x n] := M B, M (p[1], m x m) lower (ctrl 0) or upper (ctrl 1)
                         triangular with explicit diagonal: a solve step with a precomputed
-                        inverse; no reference counterpart                                       */
+                        inverse; no reference counterpart.  With l > 0, rows [o, o + l) of
+                        M B (B read from p[2], ld[2]) go to the l x n block at p[0]: one part
+                        of a product split over several CTAs, each row summed as in the
+                        whole product                                                          */
   PP_OP_ORTH = 13,   /* Y[m x k] (ld k, k <= 32) := an orthonormal basis of its range (shifted
                         CholeskyQR3; rank-deficient columns become zero): the range finder of
                         a sketched low-rank update; no reference counterpart                   */

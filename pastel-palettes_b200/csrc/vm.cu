@@ -782,29 +782,31 @@ __device__ __noinline__ void dev_trinv(double* I, int ldi, const double* A, int 
   else dev_trsmu_big(I, ldi, A, lda, c0 + w, w, smem);
 }
 
-// B[m x n] := M B, M (m x m, m <= PP_VM_TRI) lower or upper triangular.  B is staged in
-// shared memory first (so the product may overwrite it); warp w takes RU rows at a time,
-// lanes stride the columns, and every load of the RU rows is issued before the first
-// product; a warp reduction per row and right-hand side finishes the dot products.
+// Rows [r0, r0 + rows) of M S into O (row r at O row r - r0), M (m x m, m <= PP_VM_TRI) lower
+// or upper triangular, S (m x n).  S is staged in shared memory first (so O may be S itself);
+// warp w takes RU rows at a time, lanes stride the columns, and every load of the RU rows is
+// issued before the first product; a warp reduction per row and right-hand side finishes the
+// dot products, so a row's result does not depend on which rows the call covers.
 template <int NB, int RU>
-__device__ __noinline__ void trmv_impl(double* B, int ldb, const double* M, int ldm, int m, int n, int upper,
-                                       double* smem) {
+__device__ __noinline__ void trmv_impl(double* O, int ldo, const double* S, int lds, const double* M, int ldm, int m,
+                                       int n, int upper, int rbeg, int rows, double* smem) {
   double* Bs = smem;  // m x NB
   for (int e = threadIdx.x; e < m * NB; e += NT) {
     const int r = e / NB, q = e % NB;
-    Bs[e] = q < n ? ldcg(&B[(size_t)r * ldb + q]) : 0.0;
+    Bs[e] = q < n ? ldcg(&S[(size_t)r * lds + q]) : 0.0;
   }
   __syncthreads();
   constexpr int TC = PP_VM_TRI / 32;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int r0 = w * RU; r0 < m; r0 += (NT / 32) * RU) {
+  const int rend = rbeg + rows;
+  for (int r0 = rbeg + w * RU; r0 < rend; r0 += (NT / 32) * RU) {
     double v[RU][TC];
 #pragma unroll
     for (int u = 0; u < RU; ++u)
 #pragma unroll
       for (int t = 0; t < TC; ++t) {
         const int r = r0 + u, c = lane + 32 * t;
-        const bool in = r < m && c < m && (upper ? c >= r : c <= r);
+        const bool in = r < rend && c < m && (upper ? c >= r : c <= r);
         v[u][t] = in ? ldcg(&M[(size_t)r * ldm + c]) : 0.0;
       }
 #pragma unroll
@@ -826,22 +828,27 @@ __device__ __noinline__ void trmv_impl(double* B, int ldb, const double* M, int 
         for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
       }
       const int r = r0 + u;
-      if (lane == 0 && r < m) {
+      if (lane == 0 && r < rend) {
 #pragma unroll
         for (int q = 0; q < NB; ++q)
-          if (q < n) B[(size_t)r * ldb + q] = acc[q];
+          if (q < n) O[(size_t)(r - rbeg) * ldo + q] = acc[q];
       }
     }
   }
   __syncthreads();
 }
 
+// TRMV: the whole product in place (l == 0) or rows [o, o + l) of it out of place (l > 0)
 __device__ __forceinline__ bool dev_trmv(const pp_task& T, double* smem) {
   const int m = T.m, n = T.n;
   if (m > PP_VM_TRI || n < 1 || n > 16) return false;
-  if (n == 1) trmv_impl<1, 8>(T.p[0], T.ld[0], T.p[1], T.ld[1], m, n, T.ctrl, smem);
-  else if (n <= 4) trmv_impl<4, 4>(T.p[0], T.ld[0], T.p[1], T.ld[1], m, n, T.ctrl, smem);
-  else trmv_impl<16, 2>(T.p[0], T.ld[0], T.p[1], T.ld[1], m, n, T.ctrl, smem);
+  const bool part = T.l > 0;
+  if (part && (T.o < 0 || T.o + T.l > m || !T.p[2])) return false;
+  const double* S = part ? T.p[2] : T.p[0];
+  const int lds = part ? T.ld[2] : T.ld[0], r0 = part ? T.o : 0, rows = part ? T.l : m;
+  if (n == 1) trmv_impl<1, 8>(T.p[0], T.ld[0], S, lds, T.p[1], T.ld[1], m, n, T.ctrl, r0, rows, smem);
+  else if (n <= 4) trmv_impl<4, 4>(T.p[0], T.ld[0], S, lds, T.p[1], T.ld[1], m, n, T.ctrl, r0, rows, smem);
+  else trmv_impl<16, 2>(T.p[0], T.ld[0], S, lds, T.p[1], T.ld[1], m, n, T.ctrl, r0, rows, smem);
   return true;
 }
 

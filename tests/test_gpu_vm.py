@@ -145,6 +145,33 @@ def test_trmv_task(pp, oracle, gctx, upper, m, n):
     assert rel(d[:, :n], T @ B0) < 1e-13
 
 
+@pytest.mark.parametrize("upper", [0, 1])
+@pytest.mark.parametrize("m,n,r0,l", [(256, 1, 0, 128), (256, 1, 181, 41), (256, 3, 222, 34), (200, 16, 17, 100)])
+def test_trmv_task_row_block_bitwise(pp, oracle, gctx, upper, m, n, r0, l):
+    """TRMV rows [o, o + l) out of place (one part of a split solve step): the same bits as
+    those rows of the whole in-place product, the oracle within rounding, the source intact."""
+    rng = np.random.default_rng(m + n + r0 + upper)
+    M0, B0 = rng.standard_normal((m, m)), rng.standard_normal((m, n))
+
+    def setup(tb, pairs):
+        for (idx, _), val in pairs:
+            tb.host[idx][:, :val.shape[1]] = val
+            tb.devs[idx].copy_(torch.from_numpy(tb.host[idx]))
+
+    tb = TaskBench(pp, seed=1)
+    b, mm = tb.operand(m, n), tb.operand(m, m)
+    setup(tb, [(b, B0), (mm, M0)])
+    full, _ = tb.run(gctx, oracle, dict(op=12, m=m, n=n, ctrl=upper), {0: b, 1: mm})[b[0]]
+    tb2 = TaskBench(pp, seed=2)
+    o, s, mm2 = tb2.operand(l, n), tb2.operand(m, n), tb2.operand(m, m)
+    setup(tb2, [(s, B0), (mm2, M0)])
+    out = tb2.run(gctx, oracle, dict(op=12, m=m, n=n, ctrl=upper, o=r0, l=l), {0: o, 1: mm2, 2: s})
+    d, h = out[o[0]]
+    assert np.array_equal(d[:, :n], full[r0:r0 + l, :n])
+    assert rel(d[:, :n], h[:, :n]) < 1e-14
+    assert np.array_equal(out[s[0]][0][:, :n], B0)
+
+
 @pytest.mark.parametrize("ctrl", [0, 1])
 def test_gemm3_task_bitwise(pp, oracle, gctx, ctrl):
     tb = TaskBench(pp, seed=ctrl + 50)

@@ -126,7 +126,9 @@ def task_regions(T):
         return [reg(0, m, n, False), reg(1, k * m, n, True)]
     if op == 11:  # TRINV: an m x n column block of an inverse from the m x m leaf factors
         return [reg(0, m, n, False), reg(1, m, m, True)]
-    if op == 12:  # TRMV: B (m x n) := M B, M m x m
+    if op == 12:  # TRMV: B (m x n) := M B, M m x m; l > 0: rows [o, o + l) of M S (S at p[2])
+        if l > 0:
+            return [reg(0, l, n, False), reg(1, m, m, True), reg(2, m, n, True)]
         return [reg(0, m, n, False), reg(1, m, m, True)]
     if op == 13:  # ORTH: Y (m x n) in place
         return [reg(0, m, n, False)]
