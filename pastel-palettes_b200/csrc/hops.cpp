@@ -880,9 +880,17 @@ void Generator::trmv(int inv, int upper, int m, const View& B) {
     }
     bound[0] = 0;
     bound[kTrmvParts] = m;
+    // parts of more than kTrmvPartRows rows are cut further: the VM takes kTrmvPartRows rows
+    // per pass of loads, and a second pass costs a second round of load latency
+    std::vector<int> cuts{0};
+    for (int p = 0; p < kTrmvParts; ++p)
+      for (int r = bound[p]; r < bound[p + 1];) {
+        r = std::min(bound[p + 1], r + kTrmvPartRows);
+        cuts.push_back(r);
+      }
     const View W = tmp(m, w);
-    for (int p = 0; p < kTrmvParts; ++p) {
-      const int r0 = bound[p], r1 = bound[p + 1];
+    for (size_t p = 0; p + 1 < cuts.size(); ++p) {
+      const int r0 = cuts[p], r1 = cuts[p + 1];
       if (r1 <= r0) continue;
       HTask& t = emit(PP_OP_TRMV);
       bind(t, 0, W.sub(r0, 0, r1 - r0, w), true);

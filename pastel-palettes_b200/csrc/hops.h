@@ -121,6 +121,7 @@ constexpr int kTrmvCols = 16;
 // critical path then waits for a quarter of the triangle's loads instead of all of them
 constexpr int kTrmvSplitMin = 128;
 constexpr int kTrmvParts = 4;
+constexpr int kTrmvPartRows = 64;
 // rows of one product instruction of the solve with at most 16 columns (more CTAs on the
 // matrix-vector products of the critical path)
 constexpr int kSolveGemmRows = 256;
