@@ -29,7 +29,7 @@ METRIC = "H-LU factor+solve/s at 1e-10 residual (FP64 HODLR N=8192)"
 # DRAM bytes (read + write) of one job's factor work inside the batched factor launch, from one
 # ncu capture of the batch-4 launch (dram__bytes.sum.per_second x gpu__time_duration.sum / 4);
 # the jobs touch disjoint arenas, so the launch's traffic scales with the batch
-FACTOR_DRAM_BYTES_PER_JOB = 110.7e6
+FACTOR_DRAM_BYTES_PER_JOB = 117.5e6
 
 
 def load_pp():
@@ -428,6 +428,7 @@ def main():
     ap.add_argument("--compare", type=int, default=1, help="also time the other precision form")
     ap.add_argument("--serve-requests", type=int, default=16, help="requests of the serving leg (0: skip)")
     ap.add_argument("--autotune", type=int, default=1, help="pick tile and grid of the batch by timing")
+    ap.add_argument("--gemm-tile", type=int, default=0, help="product tile edge (64 or 128) when not autotuning")
     ap.add_argument("--uneven", type=int, default=0, help="instances of the configuration-4 style uneven batch "
                                                            "leg (0: skip; host construction takes minutes)")
     ap.add_argument("--serve-rate", type=float, default=40.0, help="Poisson arrival rate of the serving leg (1/s)")
@@ -472,6 +473,8 @@ def main():
         solves captured as one CUDA graph.  Returns (batch, refiner, graph, outputs, stats)."""
         for h in hs:
             h.set_precision(prec)
+            if args.gemm_tile and not args.autotune:
+                h.set_gemm_tile(args.gemm_tile)
         batch = pp.Batch(ctx, hs)
         tune = batch.autotune(s) if args.autotune else None
         ref = pp.BatchRefiner(batch, probs, stream=s)
