@@ -148,3 +148,36 @@ def test_standard_admissibility_program_solves(pp, oracle, hctx):
     x = sol.rhs[:n].reshape(n, 1)
     r = b - prob.dense() @ x
     assert np.abs(r).max() / (prob.norm_inf * np.abs(x).max() + np.abs(b).max()) < 1e-6
+
+
+def test_trmv_row_block_restatement(pp, oracle):
+    """The oracle's TRMV against numpy: the whole product in place, and rows [o, o + l) of it
+    out of place (the parts of a split solve step), for both triangles."""
+    rng = np.random.default_rng(3)
+    m, n = 200, 3
+    M = rng.standard_normal((m, m + 2))
+    B = rng.standard_normal((m, n + 1))
+
+    def run(**fields):
+        t = np.zeros(1, dtype=pp.TASK_DTYPE)
+        for k, v in fields.items():
+            if k in ("p", "ld"):
+                for i, x in enumerate(v):
+                    t[0][k][i] = x
+            else:
+                t[0][k] = v
+        assert oracle.lib().oracle_run_program(t.ctypes.data, 1) == 0
+
+    for upper in (0, 1):
+        T = np.triu(M[:, :m]) if upper else np.tril(M[:, :m])
+        want = T @ B[:, :n]
+        for r0, l in ((0, 64), (64, 70), (150, 50)):
+            O = np.zeros((l, n + 2))
+            run(op=12, m=m, n=n, ctrl=upper, o=r0, l=l, p=[O.ctypes.data, M.ctypes.data, B.ctypes.data],
+                ld=[n + 2, m + 2, n + 1])
+            assert np.allclose(O[:, :n], want[r0:r0 + l], rtol=1e-13, atol=1e-12)
+            assert not O[:, n:].any()
+        Bc = B.copy()
+        run(op=12, m=m, n=n, ctrl=upper, p=[Bc.ctypes.data, M.ctypes.data], ld=[n + 1, m + 2])
+        assert np.allclose(Bc[:, :n], want, rtol=1e-13, atol=1e-12)
+        assert np.array_equal(Bc[:, n:], B[:, n:])

@@ -226,3 +226,29 @@ def test_scheduler_streams_cover_every_instruction(pp, hctx):
         assert sorted(seen) == expect
         if workers == 1:
             assert len(words) > 0 and tmp > 0
+
+
+def test_solve_program_splits_leaf_products(pp, hctx):
+    """Every leaf product of the solve program on a triangle of 128 rows or more is cut into
+    out-of-place parts of at most 64 rows that cover the triangle's rows once, each followed by
+    one copy back into the right-hand side."""
+    h, _ = pp.make_kernel_problem(hctx, 2048, 2, "inv", 1e-3, 256, 16)
+    info = h.program_info(1, 1)
+    bases, at = [], 1 << 32
+    for a in pp.ARENAS:
+        bases.append(at)
+        at += 8 * (info["arena_elems"][a] + 4096) + (1 << 20)
+    tasks, succ, indeg, ready = h.encode_program(1, 1, bases)
+    parts = {}
+    for t in tasks:
+        if int(t["op"]) == 12:
+            assert int(t["l"]) > 0 and int(t["m"]) >= 128
+            parts.setdefault((int(t["p"][1]), int(t["p"][2])), []).append((int(t["o"]), int(t["l"]), int(t["m"])))
+    copies = sum(1 for t in tasks if int(t["op"]) == 14)
+    assert parts and copies == len(parts)
+    for rows in parts.values():
+        rows.sort()
+        m = rows[0][2]
+        assert all(l <= 64 for _, l, _ in rows)
+        assert rows[0][0] == 0 and all(a[0] + a[1] == b[0] for a, b in zip(rows, rows[1:]))
+        assert rows[-1][0] + rows[-1][1] == m
