@@ -1712,23 +1712,19 @@ __device__ __forceinline__ double rcp_est(double v) {
   asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(v));
   return y;
 }
-// One third-order correction of an estimate y0 of a^(-1/2): with e = 1 - a y0^2,
-// a^(-1/2) = y0 (1 - e)^(-1/2) = y0 (1 + e/2 + 3e^2/8 + O(e^3)) (binomial series).  For
-// |e| < 2^-19 the truncated terms are below 2^-58 relative: the result is within a few ulps of
-// double, the accuracy of two Newton steps at 5 instead of 8 operations.
-__device__ __forceinline__ double rsqrt_refine(double a, double y0) {
-  const double e = fma(-a * y0, y0, 1.0);
-  return fma(y0 * e, fma(0.375, e, 0.5), y0);
-}
-// The same for 1/a: e = 1 - a y0, 1/a = y0 (1 - e)^-1 = y0 (1 + e + e^2 + O(e^3)).
+// One third-order correction of an estimate y0 of 1/a: with e = 1 - a y0,
+// 1/a = y0 (1 - e)^-1 = y0 (1 + e + e^2 + O(e^3)) (geometric series).  For |e| < 2^-19 the
+// truncated terms are below 2^-57 relative: the result is within a few ulps of double, the
+// accuracy of two Newton steps at 3 instead of 4 operations.
 __device__ __forceinline__ double rcp_refine(double a, double y0) {
   const double e = fma(-a, y0, 1.0);
   return fma(y0, fma(e, e, e), y0);
 }
-// Entry K(d) of the kernel matrix at squared distance d2.  d = sqrt(d2) as s0 = d2 y0 with y0
-// the estimate of 1 / sqrt(max(d2, 1e-300)), corrected like rsqrt_refine: with e = 1 - s0 y0,
-// d = s0 (1 + e/2 + 3e^2/8).  Exact zero on the diagonal and for coincident points, an
-// absolute error below 1e-150 for 0 < d2 < 1e-300, a few ulps elsewhere.
+// Entry K(d) of the kernel matrix at squared distance d2.  The distance: y0 estimates
+// 1 / sqrt(max(d2, 1e-300)), s0 = d2 y0 and e = 1 - s0 y0 = 1 - d2 y0^2; then
+// sqrt(d2) = s0 (1 - e)^(-1/2) = s0 (1 + e/2 + 3e^2/8 + O(e^3)) (binomial series, truncated
+// terms below 2^-58 relative for |e| < 2^-19).  Exact zero on the diagonal and for coincident
+// points, an absolute error below 1e-150 for 0 < d2 < 1e-300, a few ulps elsewhere.
 template <int KIND>
 __device__ __forceinline__ double kernel_eval_nr(double d2, double p0, double inv_p0) {
   constexpr double c = KIND == 1 ? 4.0 * 3.14159265358979323846 : 1.0;
