@@ -191,8 +191,11 @@ pp_status pp_batch_set_tuning(pp_batch* b, int tile, int gemm_tile, int grid);
  * sets (the first solve and its follow-ups), refines each set in FP64 (matrix-free kernel
  * residual) until the normwise backward error ||r||_inf / (||A||_inf ||x||_inf + ||b||_inf)
  * meets `tol`, writes the solutions to the caller's host buffer and frees its device memory
- * (stream-ordered, so retiring one request never waits for the others).  While a server
- * runs, its context is used only through the server's calls. */
+ * (stream-ordered, so retiring one request never waits for the others).  The requests'
+ * device memory comes from a memory pool of the server's own that keeps up to the budget
+ * mapped between requests; pp_server_create maps its first GiB (or the whole budget, if
+ * smaller) at once.  While a server runs, its context is used only through the server's
+ * calls. */
 typedef struct pp_server pp_server;
 typedef struct pp_serve_config {
   long long hbm_budget_bytes;  /* device bytes the admitted requests may hold together        */
