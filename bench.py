@@ -129,6 +129,17 @@ def program_bytes(pp, h, which=0, nrhs=1):
     return total, info
 
 
+def whole_job_rate(dist, world, seconds, jobs_per_rank, device):
+    """Whole-job throughput of `world` independent replicas: every rank processed
+    `jobs_per_rank` jobs in `seconds` of its own device time, and the job ends with the slowest
+    rank (max over ranks; the only collective of the bench).  Returns (jobs/s, max seconds)."""
+    import torch
+    t = torch.tensor([seconds], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return world * jobs_per_rank / t.item(), t.item()
+
+
 def build_problem(pp, ctx, rank):
     w = WORKLOAD
     return pp.make_kernel_problem(ctx, w["n"], w["dim"], w["kernel"], w["p0"], w["leaf"], w["rank"],
@@ -230,7 +241,7 @@ def pipelined_e2e(pp, ctx, torch, hs, probs, b_host, bs, x_host, g_a, out_a, ref
     on an upload stream while step k - 1 computes, its solutions come down on a download stream
     while step k + 1 computes.  Every step still moves its own inputs up from pinned host
     memory and its solutions down inside the timed region (first upload to last download).
-    Returns (factor+solve/s of this rank, description)."""
+    Returns (jobs of this rank, seconds, description)."""
     w = WORKLOAD
     hs_b = []
     for h in hs:
@@ -294,7 +305,7 @@ def pipelined_e2e(pp, ctx, torch, hs, probs, b_host, bs, x_host, g_a, out_a, ref
             raise SystemExit("pipelined end-to-end step ended above the tolerance")
     mode = (f"{n_steps} steps over two alternating device input sets: uploads of step k overlap the "
             f"compute of step k - 1, downloads overlap step k + 1 (separate upload / download streams)")
-    return len(hs) * n_steps / total, mode
+    return len(hs) * n_steps, total, mode
 
 
 def serving_leg(pp, ctx, n_requests, rate, seed=2024, smin=1024, smax=3072):
@@ -511,11 +522,8 @@ def main():
         batch.sync(s)
         if worst > tol:
             raise SystemExit(f"a timed step ended above {tol}: {worst}")
-        t = torch.tensor([total], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_max = t.item()
-        stats = {"value": world * B * args.steps / total_max, "ms_per_step": 1e3 * total_max / args.steps,
+        value, total_max = whole_job_rate(dist, world, total, B * args.steps, "cuda")
+        stats = {"value": value, "ms_per_step": 1e3 * total_max / args.steps,
                  "refinement_solves": iters, "worst_backward_error": worst, "total_s": total_max,
                  "autotune": tune}
         return batch, ref, g, out, stats
@@ -566,16 +574,10 @@ def main():
         e2e_total += e0.elapsed_time(e1) / 1e3
     if max(ref.errors(bs, *out2)) > tol:
         raise SystemExit("end-to-end step ended above the tolerance")
-    t = torch.tensor([e2e_total], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_serial = world * B * e2e_steps / t.item()
-    e2e_value, e2e_mode = pipelined_e2e(pp, ctx, torch, hs, probs, b_host, bs, x_host, g2, out2, ref, batch,
-                                        main_stats["autotune"], iters, e2e_steps, tol, s, barrier)
-    t = torch.tensor([e2e_value], dtype=torch.float64, device="cuda")
-    if world > 1:  # the slowest rank's rate
-        dist.all_reduce(t, op=dist.ReduceOp.MIN)
-    e2e_value = world * t.item()
+    e2e_serial, _ = whole_job_rate(dist, world, e2e_total, B * e2e_steps, "cuda")
+    e2e_jobs, e2e_seconds, e2e_mode = pipelined_e2e(pp, ctx, torch, hs, probs, b_host, bs, x_host, g2, out2, ref,
+                                                    batch, main_stats["autotune"], iters, e2e_steps, tol, s, barrier)
+    e2e_value, _ = whole_job_rate(dist, world, e2e_seconds, e2e_jobs, "cuda")
 
     # --- the dominant kernel (the batched factor launch), timed alone
     fac_ms = []
