@@ -121,8 +121,14 @@ def program_bytes(pp, h, which=0, nrhs=1):
             e = (k + 2) * m * n
         elif op == 11:  # TRINV: leaf triangle read, an m x n column block of the inverse written
             e = m * m // 2 + m * n
+        elif op == 12 and l > 0:  # TRMV part: its rows of the triangle and B read, l x n written
+            o = int(t["o"])
+            tri = sum((m - r) if int(t["ctrl"]) else (r + 1) for r in range(o, o + l))
+            e = tri + m * n + l * n
         elif op == 12:  # TRMV: triangle read, B read and written
             e = m * m // 2 + 2 * m * n
+        elif op in (13, 14):  # ORTH (in place) / COPY: m x n read and written
+            e = 2 * m * n
         else:
             e = 0
         total += 8 * e
