@@ -250,6 +250,13 @@ pp_status pp_dense_residual_dev(pp_context* ctx, const double* A, int lda, int n
 pp_status pp_kernel_residual_dev(pp_context* ctx, int kernel, double p0, double shift, const double* pts_dev,
                                  int dim, int n, const double* x, const double* b, double* r, int nrhs,
                                  void* stream);
+/* The dense blocks of an uploaded H-matrix assembled on the device from its points (device,
+ * n x dim, in the H-matrix's cluster order): entry (i, j) = K(|p_i - p_j|) with the kernels of
+ * pp_kernel_residual_dev, plus `shift` on the matrix diagonal, with the same entry evaluation as
+ * the residual.  Low-rank blocks are left as they are.  No reference counterpart (the
+ * reference's matrices come from a separate Java compressor). */
+pp_status pp_hmatrix_assemble_dense_dev(pp_hmatrix* h, int kernel, double p0, double shift, const double* pts_dev,
+                                        int dim, void* stream);
 /* One job of pp_kernel_residual_batch_dev (device pointers). */
 typedef struct pp_residual_job {
   int kernel;           /* as pp_kernel_residual_dev */

@@ -147,6 +147,7 @@ def lib():
             "pp_dense_residual_dev": (i, [vp, vp, i, i, vp, vp, vp, i, vp]),
             "pp_kernel_residual_dev": (i, [vp, i, d, d, vp, i, i, vp, vp, vp, i, vp]),
             "pp_kernel_residual_batch_dev": (i, [vp, i, C.POINTER(_ResidualJob), vp]),
+            "pp_hmatrix_assemble_dense_dev": (i, [vp, i, d, d, vp, i, vp]),
             "pp_datamap2d_check_overlap": (i, [C.c_uint64, C.c_size_t, C.c_size_t, C.c_size_t,
                                                C.c_uint64, C.c_size_t, C.c_size_t, C.c_size_t]),
             "pp_operation_dependency": (i, [i, vp, vp, i, vp, vp]),
@@ -392,6 +393,17 @@ class Hierarchical:
         """FP64 (default) or TF32: the factor's GEMM instructions on the tensor cores with
         FP32 accumulation; GETRF / TRSM / accumulation stay FP64."""
         self.ctx.check(lib().pp_hmatrix_set_precision(self._h, precision), "set_precision")
+
+    def assemble_dense(self, prob, pts=None, stream=None):
+        """Dense blocks evaluated on the device from the kernel problem's points (after upload);
+        pts: the points as a device tensor (n x dim), made from prob when not given."""
+        import torch
+        if pts is None:
+            pts = torch.from_numpy(np.ascontiguousarray(prob.points, dtype=np.float64)).cuda()
+        self.ctx.check(lib().pp_hmatrix_assemble_dense_dev(self._h, int(prob.kernel), float(prob.p0),
+                                                           float(prob.shift), pts.data_ptr(), int(pts.shape[1]),
+                                                           _stream_handle(stream)), "assemble_dense")
+        return pts
 
     def set_gemm_tile(self, edge):
         """Output tile edge (64 or 128) of the product instructions; results do not change."""

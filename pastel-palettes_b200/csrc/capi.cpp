@@ -675,6 +675,26 @@ pp_status pp_kernel_residual_dev(pp_context* ctx, int kernel, double p0, double 
   return PP_OK;
 }
 
+pp_status pp_hmatrix_assemble_dense_dev(pp_hmatrix* h, int kernel, double p0, double shift, const double* pts,
+                                        int dim, void* stream) {
+  if (!h) return PP_INVALID_ARG;
+  pp_context* ctx = h->ctx;
+  if (!has_device(ctx)) return fail(ctx, PP_CUDA_ERROR, "no CUDA device in this context");
+  if (!pts || dim < 1 || dim > 3 || kernel < 0 || kernel > 3)
+    return fail(ctx, PP_INVALID_ARG, "pp_hmatrix_assemble_dense_dev: bad argument");
+  if (kernel <= 1 && !(p0 >= 0.0 && std::isfinite(p0)))
+    return fail(ctx, PP_INVALID_ARG, "pp_hmatrix_assemble_dense_dev: p0 negative or not finite");
+  if (!h->d_arena) return fail(ctx, PP_INVALID_ARG, "pp_hmatrix_assemble_dense_dev: upload the H-matrix first");
+  std::vector<pp_assemble_block> blocks;
+  for (const pp::HNode& nd : h->H->nodes) {
+    if (nd.kind != pp::HNode::D || nd.obj < 0) continue;
+    const pp::StorageObj& o = h->H->objs[nd.obj];
+    blocks.push_back(pp_assemble_block{h->d_arena + o.off, o.ld, nd.r0, nd.c0, nd.m, nd.n});
+  }
+  PP_CUDA(pp_assemble_dense(blocks.data(), (int)blocks.size(), kernel, dim, p0, shift, pts, (cudaStream_t)stream));
+  return PP_OK;
+}
+
 pp_status pp_kernel_residual_batch_dev(pp_context* ctx, int njobs, const pp_residual_job* jobs, void* stream) {
   if (!has_device(ctx)) return fail(ctx, PP_CUDA_ERROR, "no CUDA device in this context");
   if (njobs < 0 || (njobs > 0 && !jobs)) return fail(ctx, PP_INVALID_ARG, "kernel residual batch: bad argument");

@@ -2039,6 +2039,58 @@ cudaError_t launch_elementwise(const pp_resid_job* jobs, const std::vector<int>&
   return cudaSuccess;
 }
 
+// Dense blocks of an H-matrix assembled in place from its points (the first step of building it
+// on the device): entry (i, j) of the block at rows [r0, r0 + m), columns [c0, c0 + n) is
+// K(|p_{r0+i} - p_{c0+j}|), plus the shift on the matrix diagonal, with the residual kernel's
+// distance and entry evaluation (the same bits as the matrix the refinement applies).  One CTA
+// per AS_ROWS rows of a block; blocks passed by value, up to AS_LAUNCH_JOBS per launch.
+#define AS_LAUNCH_JOBS 64
+#define AS_ROWS 16
+struct AssembleLaunch {
+  struct Job {
+    double* a;
+    long long first;  // first CTA of the block in the launch
+    int ld, r0, c0, m, n, pad;
+  } job[AS_LAUNCH_JOBS];
+  const double* pts;
+  double p0, shift;
+  int njobs;
+};
+
+template <int KIND, int DIM>
+__global__ void __launch_bounds__(256) assemble_dense_kernel(const __grid_constant__ AssembleLaunch L) {
+  int lo = 0, hi = L.njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (L.job[mid].first <= (long long)blockIdx.x) lo = mid; else hi = mid - 1;
+  }
+  const AssembleLaunch::Job& jb = L.job[lo];
+  const int rb = (int)((long long)blockIdx.x - jb.first) * AS_ROWS;
+  const double inv_p0 = 1.0 / L.p0;
+  for (int e = threadIdx.x; e < AS_ROWS * jb.n; e += blockDim.x) {
+    const int i = rb + e / jb.n, j = e % jb.n;
+    if (i >= jb.m) break;  // e only grows: every later element is past the block too
+    const int gi = jb.r0 + i, gj = jb.c0 + j;
+    double d2 = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      const double u = L.pts[(size_t)gi * DIM + d] - L.pts[(size_t)gj * DIM + d];
+      d2 = fma(u, u, d2);
+    }
+    double a = kernel_eval_nr<KIND>(d2, L.p0, inv_p0);
+    if (gi == gj) a += L.shift;
+    jb.a[(size_t)i * jb.ld + j] = a;
+  }
+}
+
+template <int KIND>
+cudaError_t launch_assemble_dim(int dim, const AssembleLaunch& L, unsigned ctas, cudaStream_t s) {
+  if (dim == 1) assemble_dense_kernel<KIND, 1><<<ctas, 256, 0, s>>>(L);
+  else if (dim == 2) assemble_dense_kernel<KIND, 2><<<ctas, 256, 0, s>>>(L);
+  else assemble_dense_kernel<KIND, 3><<<ctas, 256, 0, s>>>(L);
+  return cudaGetLastError();
+}
+
 // x += dx over `count` elements (the refinement update of a served request)
 __global__ void axpy_kernel(double* __restrict__ x, const double* __restrict__ dx, size_t count) {
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < count; e += (size_t)gridDim.x * blockDim.x)
@@ -2133,6 +2185,9 @@ cudaError_t preload_residual_dims() {
   cudaError_t e = preload_residual<KIND, 1>();
   if (e == cudaSuccess) e = preload_residual<KIND, 2>();
   if (e == cudaSuccess) e = preload_residual<KIND, 3>();
+  if (e == cudaSuccess) e = preload(assemble_dense_kernel<KIND, 1>);
+  if (e == cudaSuccess) e = preload(assemble_dense_kernel<KIND, 2>);
+  if (e == cudaSuccess) e = preload(assemble_dense_kernel<KIND, 3>);
   return e;
 }
 }  // namespace
@@ -2239,6 +2294,37 @@ cudaError_t pp_kernel_residual(int kernel, double p0, double p1, double diag_shi
   j.r = r;
   j.part = part;
   return pp_kernel_residual_batch(&j, 1, s);
+}
+
+cudaError_t pp_assemble_dense(const pp_assemble_block* blocks, int nblocks, int kernel, int dim, double p0,
+                              double shift, const double* pts, cudaStream_t s) {
+  if (nblocks <= 0) return cudaSuccess;
+  if (!blocks || !pts || dim < 1 || dim > 3 || kernel < 0 || kernel > 3) return cudaErrorInvalidValue;
+  if (kernel <= 1 && !(p0 >= 0.0 && std::isfinite(p0))) return cudaErrorInvalidValue;
+  for (int c = 0; c < nblocks; c += AS_LAUNCH_JOBS) {
+    AssembleLaunch L;
+    L.pts = pts;
+    L.p0 = p0;
+    L.shift = shift;
+    L.njobs = std::min(AS_LAUNCH_JOBS, nblocks - c);
+    long long ctas = 0;
+    for (int q = 0; q < L.njobs; ++q) {
+      const pp_assemble_block& b = blocks[c + q];
+      if (!b.a || b.m <= 0 || b.n <= 0 || b.ld < b.n || b.r0 < 0 || b.c0 < 0) return cudaErrorInvalidValue;
+      L.job[q] = AssembleLaunch::Job{b.a, ctas, b.ld, b.r0, b.c0, b.m, b.n, 0};
+      ctas += (b.m + AS_ROWS - 1) / AS_ROWS;
+    }
+    if (ctas >= (1LL << 31)) return cudaErrorInvalidValue;
+    cudaError_t e;
+    switch (kernel) {
+      case 0: e = launch_assemble_dim<0>(dim, L, (unsigned)ctas, s); break;
+      case 1: e = launch_assemble_dim<1>(dim, L, (unsigned)ctas, s); break;
+      case 2: e = launch_assemble_dim<2>(dim, L, (unsigned)ctas, s); break;
+      default: e = launch_assemble_dim<3>(dim, L, (unsigned)ctas, s); break;
+    }
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 cudaError_t pp_axpy(double* x, const double* dx, size_t count, cudaStream_t s) {

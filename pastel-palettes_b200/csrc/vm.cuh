@@ -69,6 +69,16 @@ struct pp_resid_job {
 /* the update, residual and reduction of every job in three or more launches (jobs grouped by
  * kernel, dimension and right-hand-side width); results equal those of one job per call */
 cudaError_t pp_kernel_residual_batch(const pp_resid_job* jobs, int njobs, cudaStream_t s);
+/* one dense block of an H-matrix to assemble from points: rows [r0, r0 + m), columns
+ * [c0, c0 + n) of the matrix, stored row-major at a with leading dimension ld */
+struct pp_assemble_block {
+  double* a;
+  int ld, r0, c0, m, n;
+};
+/* entries K(|p_i - p_j|) (+ shift on the diagonal) of every listed block, evaluated as the
+ * matrix-free residual evaluates them */
+cudaError_t pp_assemble_dense(const pp_assemble_block* blocks, int nblocks, int kernel, int dim, double p0,
+                              double shift, const double* pts, cudaStream_t s);
 /* x += dx (count elements) */
 cudaError_t pp_axpy(double* x, const double* dx, size_t count, cudaStream_t s);
 /* out[0] = max |x|, out[1] = max |r| (as double bit patterns; out is zeroed first) */
