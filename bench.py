@@ -218,7 +218,9 @@ def run_reference_arm(args, pp, rank, world):
     line = {"metric": METRIC, "value": value, "unit": "factor+solve/s", "impl": "reference", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(t) / len(t),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD_NAME, **{k: v for k, v in WORKLOAD.items()}},
+            "config": {"workload": WORKLOAD_NAME, **{k: v for k, v in WORKLOAD.items()}, "batch": 1,
+                       "precision": "fp64", "parallelism": "host threads over one job's DAG",
+                       "batch_note": "one job at a time (the reference executes one DAG per launch)"},
             "cpu_baseline": {"value": value, "unit": "factor+solve/s", "cores": threads, "kind": "port",
                              "sample": f"{len(t)} full jobs of the workload, one at a time (oracle over the "
                                        f"same DAG, {threads} threads; refinement {iters[-1]} solves)"},
