@@ -131,3 +131,12 @@ def test_gemm_tile_option_shrinks_the_factor_program(pp, hctx):
     assert i2["op_count"]["gemm"] < i1["op_count"]["gemm"]
     assert i2["flops"] == i1["flops"]
     assert h2.program_info(1)["n_tasks"] == h1.program_info(1)["n_tasks"]  # the solve keeps 64
+
+
+def test_device_assembly_refuses_host_context(pp, hctx):
+    """Dense-block assembly on the device needs a device context (no host fallback)."""
+    h, prob = pp.make_kernel_problem(hctx, 512, 2, "inv", 1e-3, 128, 16)
+    pts = np.ascontiguousarray(prob.points)
+    st = pp.lib().pp_hmatrix_assemble_dense_dev(h.handle, int(prob.kernel), float(prob.p0), float(prob.shift),
+                                                pts.ctypes.data, 2, None)
+    assert st == pp.PP_CUDA_ERROR
