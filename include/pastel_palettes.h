@@ -40,7 +40,9 @@ typedef struct pp_hmatrix pp_hmatrix;
 typedef struct pp_config {
   int tile;              /* dense blocks above this are split before they reach an instruction (<= 64) */
   int ctas_per_sm;       /* persistent VM CTAs per SM (0 = occupancy maximum)                        */
-  long long spin_limit;  /* polls of an empty ready slot before a VM CTA reports PP_TIMEOUT            */
+  long long spin_limit;  /* microseconds a VM CTA waits for a ready task (or for its tensor-core
+                            work) before it reports PP_TIMEOUT; 0 = 120 s.  Timed by the GPU's
+                            global timer, so it does not depend on how fast a poll is            */
   unsigned long long seed;  /* seed of the random sketch used by accum                                */
   int reference_isa;     /* 1: factor programs use only the reference's instruction set (no split-k
                             reductions), so pp_refstream_encode can export them                         */
@@ -305,8 +307,8 @@ pp_status pp_hmatrix_trace(pp_hmatrix* h, int which, int nrhs, int enable, uint6
 pp_status pp_hmatrix_program_edges(pp_hmatrix* h, int which, int nrhs, int64_t* from, int64_t* to, int32_t* type);
 /* Runs an arbitrary task table (host array of n pp_task records with device operand
  * pointers; successor lists and in-degrees as pp_hmatrix_encode_program returns them) on
- * the VM and waits.  spin_limit <= 0 uses the context's.  Returns PP_TIMEOUT when a ready
- * slot is never filled (e.g. an in-degree that no predecessor can bring to zero).
+ * the VM and waits.  spin_limit (microseconds) <= 0 uses the context's.  Returns PP_TIMEOUT
+ * when a ready slot is never filled (e.g. an in-degree that no predecessor can bring to zero).
  * Counterpart of launchKernelWithArgs (include/launcher.cuh:15-16) for decoded streams. */
 pp_status pp_vm_execute(pp_context* ctx, const void* tasks, int n_tasks, const int32_t* succ, long long n_succ,
                         const int32_t* indeg, long long spin_limit, int grid, void* stream);
@@ -321,15 +323,17 @@ pp_status pp_vm_execute(pp_context* ctx, const void* tasks, int n_tasks, const i
  * being captured (an allocation there breaks the capture), serving loops whose device memory
  * is fully reserved by an admission budget, and host frameworks that own the device memory
  * pool.  Its scratch is one static device array of PP_ACCUM_NOALLOC_MAX_SCRATCH doubles
- * (8 MiB), held by every GPU that loads the library until the process exits.  A call needs
- * 2*ny*k1 + nx*k1 + k1*max(k1, k2) doubles of it and 1 <= k1 <= 32; larger requests return
- * PP_INVALID_ARG without touching the device.
+ * (8 MiB), held by every GPU that loads the library until the process exits.  The accumulation
+ * keeps its ny x k1 sketch in shared memory while that fits (ny * k1 up to about 9 000 - 17 000
+ * doubles, by rank); a larger sketch goes to the array, so ny * k1 <= 2^20 is the limit.
+ * 1 <= k1, k2 <= 32 and k1 <= min(ny, nx); other requests return PP_INVALID_ARG without
+ * touching the device.  The call runs on the context's device.
  *
  * The first call on each device looks up the array's device address (with that device
- * current); make that first call before any stream capture.  Every call shares the array and
- * overwrites all of it that it uses before reading it, so nothing carries over between calls;
- * calls whose executions overlap on the GPU (different streams, or graphs replayed
- * concurrently) race on it. */
+ * current, once per device even with several host threads); make that first call before any
+ * stream capture.  Every call shares the array and overwrites all of it that it uses before
+ * reading it, so nothing carries over between calls; calls whose executions overlap on the
+ * GPU (different streams, or graphs replayed concurrently) race on it. */
 #define PP_ACCUM_NOALLOC_MAX_SCRATCH (1 << 20)
 pp_status pp_lowrank_accum_noalloc(pp_context* ctx, double* U1, int ld_u1, double* V1, int ld_v1, const double* U2,
                                    int ld_u2, const double* V2, int ld_v2, const double* R, int ld_r, int ny, int nx,

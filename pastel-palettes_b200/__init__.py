@@ -211,7 +211,7 @@ def exported_symbols():
 class Context:
     """Device context (device >= 0) or host-only planning context (device = -1)."""
 
-    def __init__(self, device=0, tile=64, ctas_per_sm=0, spin_limit=1 << 24, seed=0x5EED5EED, reference_isa=0):
+    def __init__(self, device=0, tile=64, ctas_per_sm=0, spin_limit=0, seed=0x5EED5EED, reference_isa=0):
         cfg = _Config(tile, ctas_per_sm, spin_limit, seed, reference_isa)
         h = C.c_void_p()
         st = lib().pp_context_create(device, C.byref(cfg), C.byref(h))

@@ -288,7 +288,7 @@ pp_status launch_plan(pp_context* ctx, VmPlan& plan, cudaStream_t s, int grid_ca
   L.counters = plan.d_counters;
   L.slots = plan.d_slots;
   L.state = plan.d_state;
-  L.spin_limit = ctx->cfg.spin_limit;
+  L.wait_ns = ctx->cfg.spin_limit * 1000;
   L.grid = grid_cap > 0 ? std::min(plan.grid, grid_cap) : plan.grid;
   L.trace = plan.d_trace;
   L.use_tc = plan.use_tc;
@@ -333,7 +333,7 @@ pp_status pp_context_create(int device, const pp_config* cfg, pp_context** out) 
   if (!c) return PP_OOM;
   c->cfg.tile = 64;
   c->cfg.ctas_per_sm = 0;
-  c->cfg.spin_limit = 1ll << 24;
+  c->cfg.spin_limit = 120ll * 1000 * 1000;  // 120 s
   c->cfg.seed = 0x5eed5eedull;
   if (cfg) {
     if (cfg->tile > 0) c->cfg.tile = cfg->tile;
@@ -847,7 +847,7 @@ pp_status pp_vm_execute(pp_context* ctx, const void* tasks, int n, const int32_t
   pp_vm_launch L;
   L.tasks = p.d_tasks; L.n_tasks = n; L.succ = p.d_succ; L.indeg = p.d_indeg; L.ready = p.d_ready;
   L.n_ready = p.n_ready; L.counters = p.d_counters; L.slots = p.d_slots; L.state = p.d_state;
-  L.spin_limit = spin_limit > 0 ? spin_limit : ctx->cfg.spin_limit;
+  L.wait_ns = (spin_limit > 0 ? spin_limit : ctx->cfg.spin_limit) * 1000;
   L.grid = grid > 0 ? grid : std::max(1, std::min(n, ctx->sm_count * ctx->blocks_per_sm));
   for (int i = 0; i < n; ++i)
     if (T[i].prec == PP_PREC_TF32) L.use_tc = 1;
@@ -866,10 +866,10 @@ pp_status pp_lowrank_accum_noalloc(pp_context* ctx, double* U1, int ld_u1, doubl
   if (!ctx) return PP_INVALID_ARG;
   if (!has_device(ctx)) return fail(ctx, PP_CUDA_ERROR, "no CUDA device in this context");
   if (!U1 || !V1 || !U2 || !V2 || !R || ny < 1 || nx < 1 || k1 < 1 || k1 > PP_VM_MAX_RANK || k1 > ny || k1 > nx ||
-      k2 < 1 ||
-      ld_u1 < k1 || ld_v1 < k1 || ld_u2 < k2 || ld_v2 < k2 || ld_r < k1 || (sign != 1.0 && sign != -1.0))
-    return fail(ctx, PP_INVALID_ARG, "pp_lowrank_accum_noalloc: bad argument");
-  const long long need = 2LL * ny * k1 + (long long)nx * k1 + (long long)k1 * std::max(k1, k2);
+      k2 < 1 || k2 > PP_VM_MAX_RANK || ld_u1 < k1 || ld_v1 < k1 || ld_u2 < k2 || ld_v2 < k2 || ld_r < k1 ||
+      (sign != 1.0 && sign != -1.0))
+    return fail(ctx, PP_INVALID_ARG, "pp_lowrank_accum_noalloc: bad argument (1 <= k1, k2 <= 32, k1 <= ny, nx)");
+  const long long need = pp_accum_scratch_doubles(ny, k1, k2);
   if (need > pp_accum_noalloc_capacity())
     return fail(ctx, PP_INVALID_ARG,
                 "pp_lowrank_accum_noalloc: needs " + std::to_string(need) + " doubles of scratch, the static array holds " +
@@ -892,7 +892,14 @@ pp_status pp_lowrank_accum_noalloc(pp_context* ctx, double* U1, int ld_u1, doubl
   T.ld[2] = ld_u2;
   T.ld[3] = ld_v2;
   T.ld[4] = ld_r;
-  PP_CUDA(pp_accum_noalloc_launch(T, need, (cudaStream_t)stream));
+  // the context's device is current for the call (its scratch address and its launch)
+  int prev = -1;
+  if (cudaGetDevice(&prev) != cudaSuccess) return fail(ctx, PP_CUDA_ERROR, "cudaGetDevice failed");
+  if (prev != ctx->device && cudaSetDevice(ctx->device) != cudaSuccess)
+    return fail(ctx, PP_CUDA_ERROR, "cudaSetDevice failed");
+  const cudaError_t e = pp_accum_noalloc_launch(T, need, (cudaStream_t)stream);
+  if (prev != ctx->device) cudaSetDevice(prev);
+  PP_CUDA(e);
   return PP_OK;
 }
 

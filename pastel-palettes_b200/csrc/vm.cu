@@ -6,7 +6,7 @@
 // CTA of a persistent grid pops the next READY task from a device queue; finishing a
 // task decrements its successors' dependency counters (acq_rel atomics) and pushes the
 // ones that reach zero.  Waits are bounded: a CTA that polls an empty slot for
-// `spin_limit` rounds records PP_VM_TIMEOUT and every CTA returns.
+// longer than its time limit (globaltimer) records PP_VM_TIMEOUT and every CTA returns.
 //
 // Arithmetic contract (FP64 path): every matrix element receives its updates in the
 // order the reference's routines apply them, one fma per product with the same
@@ -26,6 +26,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <vector>
 #include <stdint.h>
 
@@ -1568,7 +1569,7 @@ __device__ __forceinline__ unsigned smid() {
 
 __global__ void __launch_bounds__(NT, 1)
     vm_kernel(const pp_task* __restrict__ tasks, int n_tasks, const int32_t* __restrict__ succ, int32_t* counters,
-              int32_t* slots, pp_vm_state* st, long long spin_limit, unsigned long long* trace, int use_tc) {
+              int32_t* slots, pp_vm_state* st, long long wait_ns, unsigned long long* trace, int use_tc) {
   extern __shared__ double smem[];
   __shared__ __align__(16) pp_task s_task;
   __shared__ int s_id;
@@ -1576,7 +1577,7 @@ __global__ void __launch_bounds__(NT, 1)
   __shared__ unsigned long long s_t0;
   __shared__ uint32_t s_tmem;
   __shared__ __align__(8) unsigned long long s_mbar;
-  TcCtx tc{0u, 0u, 0u, spin_limit * 32, 0, 0};
+  TcCtx tc{0u, 0u, 0u, wait_ns, 0, 0};
   if (use_tc) {
     // TF32 tasks: 64 TMEM columns (128 lanes x 64 FP32 accumulators) and one mbarrier per CTA
     if ((threadIdx.x >> 5) == 0) {
@@ -1608,12 +1609,14 @@ __global__ void __launch_bounds__(NT, 1)
       if (id < 0) {
         const int idx = atomicAdd(&st->head, 1);
         if (idx < n_tasks) {
-          long long spins = 0;
+          const unsigned long long t_wait = gtimer_ns();
           for (;;) {
             id = ld_acquire(&slots[idx]);
             if (id >= 0) break;
             if (ld_relaxed(&st->error) || ld_relaxed(&st->done) >= n_tasks) { id = -1; break; }
-            if (++spins > spin_limit) {
+            // the wait is bounded in time (globaltimer), not in polls: a poll's cost varies
+            // with the load on L2 and with other grids sharing the SMs
+            if ((long long)(gtimer_ns() - t_wait) > wait_ns) {
               if (atomicCAS(&st->error, 0, PP_VM_TIMEOUT) == 0) st->err_info = idx;
               id = -1;
               break;
@@ -2135,23 +2138,39 @@ static __device__ __align__(256) double g_accum_noalloc_scratch[PP_NOALLOC_SCRAT
 
 long long pp_accum_noalloc_capacity() { return PP_NOALLOC_SCRATCH_DOUBLES; }
 
+long long pp_accum_scratch_doubles(long long ny, int k1, int k2) {
+  // dev_accum keeps the ny x k1 sketch Y in shared memory while it fits the rest of the
+  // 160 KB; only a larger Y goes to the task's scratch, and nothing else does
+  const long long y = ny * k1;
+  const long long cap = (k1 <= 16 && k2 <= 16) ? AccumSmem<16>::YCAP : AccumSmem<32>::YCAP;
+  return y <= cap ? 0 : y;
+}
+
+namespace {
+// device address of the static scratch array, looked up once per device (std::call_once, so
+// two host threads making their first calls at once do not race on the cache)
+constexpr int kNoallocMaxDevices = 64;
+std::once_flag g_noalloc_once[kNoallocMaxDevices];
+double* g_noalloc_addr[kNoallocMaxDevices] = {nullptr};
+cudaError_t g_noalloc_err[kNoallocMaxDevices] = {cudaSuccess};
+}  // namespace
+
 cudaError_t pp_accum_noalloc_launch(const pp_task& T, long long scratch_doubles, cudaStream_t s) {
   if (scratch_doubles < 0 || scratch_doubles > PP_NOALLOC_SCRATCH_DOUBLES) return cudaErrorInvalidValue;
-  constexpr int kMaxDevices = 64;
-  static double* addr[kMaxDevices] = {nullptr};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-  if (!addr[dev]) {  // set-up, once per device, with that device current
+  if (dev < 0 || dev >= kNoallocMaxDevices) return cudaErrorInvalidDevice;
+  std::call_once(g_noalloc_once[dev], [dev] {  // set-up, once per device, with that device current
     double* p = nullptr;
-    e = cudaGetSymbolAddress((void**)&p, g_accum_noalloc_scratch);
-    if (e != cudaSuccess) return e;
-    addr[dev] = p;
-  }
+    g_noalloc_err[dev] = cudaGetSymbolAddress((void**)&p, g_accum_noalloc_scratch);
+    g_noalloc_addr[dev] = p;
+  });
+  if (g_noalloc_err[dev] != cudaSuccess) return g_noalloc_err[dev];
   pp_task t = T;
-  t.tmp = addr[dev];
-  // shared memory: the GEMM tiles and the Cholesky-QR Gram matrix (below the 48 KB default)
+  t.tmp = g_noalloc_addr[dev];
+  // 160 KB of dynamic shared memory, as the VM's ACCUM has; pp_vm_prepare (run at context
+  // creation on this device) raised the kernel's limit to that
   accum_noalloc_kernel<<<1, NT, VM_SMEM_BYTES, s>>>(t);
   return cudaGetLastError();
 }
@@ -2210,7 +2229,7 @@ cudaError_t pp_vm_run(const pp_vm_launch& L, cudaStream_t s) {
   vm_init<<<(L.n_tasks + ib - 1) / ib, ib, 0, s>>>(L.indeg, L.ready, L.n_ready, L.n_tasks, L.counters, L.slots,
                                                   L.state);
   vm_kernel<<<L.grid, NT, pp_vm_smem_bytes(), s>>>(L.tasks, L.n_tasks, L.succ, L.counters, L.slots, L.state,
-                                                   L.spin_limit, L.trace, L.use_tc);
+                                                   L.wait_ns, L.trace, L.use_tc);
   return cudaGetLastError();
 }
 

@@ -31,7 +31,8 @@ struct pp_vm_launch {
   int32_t* counters;
   int32_t* slots;
   pp_vm_state* state;
-  long long spin_limit;  /* polls of an empty ready slot before the kernel gives up */
+  long long wait_ns;     /* nanoseconds a CTA waits on an empty ready slot (or on the tensor core)
+                            before the kernel gives up */
   int grid;              /* CTAs (persistent)                                       */
   unsigned long long* trace = nullptr;  /* optional: 3 words per task (start ns, end ns, sm | cta << 32) */
   int use_tc = 0;        /* the program holds TF32 tasks: tensor memory + an mbarrier per CTA */
@@ -41,6 +42,9 @@ struct pp_vm_launch {
  * returns cudaErrorInvalidValue when `scratch_doubles` exceeds the array */
 cudaError_t pp_accum_noalloc_launch(const pp_task& T, long long scratch_doubles, cudaStream_t s);
 long long pp_accum_noalloc_capacity();
+/* scratch doubles one ACCUM of this shape needs (its ny x k1 sketch, when that does not fit the
+ * task's shared memory; 0 otherwise) */
+long long pp_accum_scratch_doubles(long long ny, int k1, int k2);
 
 size_t pp_vm_smem_bytes();
 int pp_vm_blocks_per_sm();

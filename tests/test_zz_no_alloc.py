@@ -1,11 +1,14 @@
 """pp_lowrank_accum_noalloc: the low-rank accumulation for callers that cannot allocate
 device memory (stream capture in progress, a fully reserved memory budget, a framework that
 owns the device pool).  It must give what the ACCUM instruction gives through pp_vm_execute,
-call after call, although every call reuses the same static scratch array.
+and what the reference's blockLowRankAccum (restated by the oracle) gives, call after call,
+although every call reuses the same static scratch array.
+
+The accumulation keeps its ny x k1 sketch in shared memory while it fits; the cases below are
+sized so that the sketch does not fit and goes through the static array, and they run back to
+back so that each call finds the previous call's data in it.
 
 Kept in its own file so pytest collects it last."""
-import ctypes as C
-
 import numpy as np
 import pytest
 
@@ -14,12 +17,15 @@ pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
 TOL = 1e-12  # relative Frobenius tolerance the accumulation tests use
+# sketch sizes ny * k1 that shared memory holds (dev_accum): 17376 doubles when k1, k2 <= 16,
+# 9152 otherwise
+YCAP = {16: 17376, 32: 9152}
 
 
 def _inputs(rng, ny, nx, k1, k2):
-    mk = lambda r, c: torch.from_numpy(rng.standard_normal((r, c))).cuda()
-    return dict(U1=mk(ny, k1), V1=mk(nx, k1), U2=mk(ny, k2), V2=mk(nx, k2),
-                R=torch.from_numpy(rng.uniform(-1, 1, (nx, k1))).cuda())
+    h = dict(U1=rng.standard_normal((ny, k1)), V1=rng.standard_normal((nx, k1)), U2=rng.standard_normal((ny, k2)),
+             V2=rng.standard_normal((nx, k2)), R=rng.uniform(-1, 1, (nx, k1)))
+    return h, {k: torch.from_numpy(v).cuda() for k, v in h.items()}
 
 
 def _via_vm_execute(pp, gctx, d, ny, nx, k1, k2, sign):
@@ -47,27 +53,50 @@ def _via_noalloc(pp, gctx, d, ny, nx, k1, k2, sign):
     return U1, V1
 
 
+def _via_oracle(oracle, h, sign):
+    U1, V1 = h["U1"].copy(), h["V1"].copy()
+    oracle.accum(U1, V1, h["U2"], h["V2"], np.ascontiguousarray(h["R"]), sign)
+    return U1 @ V1.T
+
+
 def _rel(a, b):
-    return (torch.linalg.norm(a - b) / torch.linalg.norm(b)).item()
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
 
 
-def test_noalloc_accum_matches_vm_accum_on_consecutive_calls(pp, gctx):
+def test_noalloc_accum_matches_vm_accum_and_oracle_on_consecutive_calls(pp, oracle, gctx):
     rng = np.random.default_rng(4242)
-    cases = [(700, 520, 16, 16, 1.0), (300, 900, 24, 8, -1.0)]
-    for ny, nx, k1, k2, sign in cases:  # two calls in a row on the shared scratch
-        d = _inputs(rng, ny, nx, k1, k2)
+    cases = [(4000, 600, 16, 16, 1.0), (2000, 500, 32, 32, -1.0), (3000, 900, 24, 8, 1.0), (700, 520, 16, 16, -1.0)]
+    # the first three keep their sketch in the static array (the last one in shared memory)
+    for ny, nx, k1, k2, _ in cases[:3]:
+        assert ny * k1 > YCAP[16 if max(k1, k2) <= 16 else 32]
+    for ny, nx, k1, k2, sign in cases:  # calls in a row on the shared scratch
+        h, d = _inputs(rng, ny, nx, k1, k2)
         U_ref, V_ref = _via_vm_execute(pp, gctx, d, ny, nx, k1, k2, sign)
         U_new, V_new = _via_noalloc(pp, gctx, d, ny, nx, k1, k2, sign)
-        assert _rel(U_new @ V_new.T, U_ref @ V_ref.T) < TOL
-        assert _rel(U_new, U_ref) < TOL and _rel(V_new, V_ref) < TOL
+        P_new = (U_new @ V_new.T).cpu().numpy()
+        assert _rel(P_new, (U_ref @ V_ref.T).cpu().numpy()) < TOL
+        assert _rel(U_new.cpu().numpy(), U_ref.cpu().numpy()) < TOL
+        assert _rel(V_new.cpu().numpy(), V_ref.cpu().numpy()) < TOL
+        # the reference's accumulation (Givens QR where the engine uses Cholesky QR): the same
+        # projection of U1 V1^T + sign U2 V2^T onto the range of its sketch
+        assert _rel(P_new, _via_oracle(oracle, h, sign)) < TOL
 
 
 def test_noalloc_accum_rejects_oversized_requests(pp, gctx):
     cap = 1 << 20
-    ny, nx, k1, k2 = 40000, 40000, 16, 16  # needs 2*ny*k1 + nx*k1 + k1*k1 > cap doubles
-    assert 2 * ny * k1 + nx * k1 + k1 * k1 > cap
+    ny, nx, k1, k2 = 40000, 1000, 32, 16  # a 40000 x 32 sketch: more than the array holds
+    assert ny * k1 > cap
     dummy = torch.zeros(1, dtype=torch.float64, device="cuda")
     p = dummy.data_ptr()
     st = pp.lib().pp_lowrank_accum_noalloc(gctx.handle, p, k1, p, k1, p, k2, p, k2, p, k1, ny, nx, k1, k2, 1.0, None)
     assert st == pp.PP_INVALID_ARG
     assert "scratch" in gctx.last_error()
+
+
+def test_noalloc_accum_rejects_ranks_above_32(pp, gctx):
+    dummy = torch.zeros(1, dtype=torch.float64, device="cuda")
+    p = dummy.data_ptr()
+    for k1, k2 in [(16, 33), (33, 16)]:
+        st = pp.lib().pp_lowrank_accum_noalloc(gctx.handle, p, k1, p, k1, p, k2, p, k2, p, k1, 500, 500, k1, k2, 1.0,
+                                               None)
+        assert st == pp.PP_INVALID_ARG
