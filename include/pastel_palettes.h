@@ -83,6 +83,13 @@ void pp_hmatrix_destroy(pp_hmatrix* h);
 int pp_hmatrix_num_blocks(const pp_hmatrix* h);
 int pp_hmatrix_root(const pp_hmatrix* h);
 pp_status pp_hmatrix_block_info(const pp_hmatrix* h, int block, pp_block_info* info);
+/* where a block lives in the arena (element offsets): a dense block at off (m x n, ld n); a
+ * low-rank block's U at off (m x kmax, ld kmax), V at off_v (n x kmax, ld kmax) and its rank word
+ * at off_rank; -1 where a block has no such part (hierarchical blocks have none).  The storage
+ * layout the reference's Dense / Hierarchical would own (matrix/Dense.h:6-18); lets a program
+ * exported with pp_hmatrix_encode_program be run on arenas filled without this library. */
+pp_status pp_hmatrix_block_storage(const pp_hmatrix* h, int block, long long* off, long long* off_v,
+                                   long long* off_rank);
 /* host data of one block (Dense(m, n, lda), matrix/Dense.h:6-18; row-major here) */
 pp_status pp_hmatrix_set_dense(pp_hmatrix* h, int block, const double* a, int lda);
 pp_status pp_hmatrix_set_lowrank(pp_hmatrix* h, int block, const double* U, int ldu, const double* V, int ldv,

@@ -127,6 +127,7 @@ def lib():
             "pp_hmatrix_num_blocks": (i, [vp]),
             "pp_hmatrix_root": (i, [vp]),
             "pp_hmatrix_block_info": (i, [vp, i, C.POINTER(_BlockInfo)]),
+            "pp_hmatrix_block_storage": (i, [vp, i, C.POINTER(ll), C.POINTER(ll), C.POINTER(ll)]),
             "pp_hmatrix_set_dense": (i, [vp, i, dp, i]),
             "pp_hmatrix_set_lowrank": (i, [vp, i, dp, i, dp, i, i]),
             "pp_hmatrix_upload": (i, [vp, vp]),
@@ -317,6 +318,13 @@ class Hierarchical:
             out.append(dict(id=b, kind=info.kind, row0=info.row0, col0=info.col0, m=info.m, n=info.n,
                             rank=info.rank, kmax=info.kmax, level=info.level, children=list(info.children)))
         return out
+
+    def block_storage(self, block):
+        """Arena element offsets of a block: dense data / U, V and the rank word (-1: none)."""
+        o, ov, orank = C.c_longlong(), C.c_longlong(), C.c_longlong()
+        self.ctx.check(lib().pp_hmatrix_block_storage(self._h, block, C.byref(o), C.byref(ov), C.byref(orank)),
+                       "block_storage")
+        return o.value, ov.value, orank.value
 
     @property
     def n(self):

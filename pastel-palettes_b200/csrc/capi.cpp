@@ -423,6 +423,16 @@ pp_status pp_hmatrix_block_info(const pp_hmatrix* h, int b, pp_block_info* info)
   return PP_OK;
 }
 
+pp_status pp_hmatrix_block_storage(const pp_hmatrix* h, int b, long long* off, long long* off_v, long long* off_rank) {
+  if (!h || b < 0 || b >= (int)h->H->nodes.size()) return PP_INVALID_ARG;
+  const pp::HNode& nd = h->H->nodes[b];
+  auto at = [&](int obj) -> long long { return obj >= 0 ? (long long)h->H->objs[obj].off : -1; };
+  if (off) *off = at(nd.obj);
+  if (off_v) *off_v = at(nd.objV);
+  if (off_rank) *off_rank = at(nd.rank_obj);
+  return PP_OK;
+}
+
 pp_status pp_hmatrix_set_dense(pp_hmatrix* h, int b, const double* a, int lda) {
   if (!h || !a) return PP_INVALID_ARG;
   try {
