@@ -124,6 +124,12 @@ long long pp_hmatrix_block_elems(const pp_hmatrix* h);
  * no reference counterpart (the reference is FP64 only) */
 #define PP_PRECISION_FP64 0
 #define PP_PRECISION_TF32 1
+/* PP_PRECISION_BF16: the Schur-complement updates of whole dense leaves of 512 or more rows and
+ * columns (multiples of 128 / 256, inner dimension of 64) run on the tensor cores from BF16
+ * shadows of their operands (written once per operand block by SHADOW instructions), FP32
+ * accumulation in tensor memory, FP64 result; the diagonal leaves' GETRF, the triangular solves,
+ * the low-rank work and every other product stay FP64.  Pair it with iterative refinement. */
+#define PP_PRECISION_BF16 2
 pp_status pp_hmatrix_set_precision(pp_hmatrix* h, int precision);
 int pp_hmatrix_get_precision(const pp_hmatrix* h);
 /* output tile edge (64, the default, or 128) that the factor's products are split into;

@@ -15,7 +15,10 @@
  *   o_gemm3/4     blockDenseGemm_3x/_4x :886-955
  *   o_accum       blockLowRankAccum     :1255-1280 with blockGivensRotation :1160-1204 and
  *                                       blockGivensRecoverQ :1206-1253
- * plus o_trsmu (B := U^-1 B), the solve step the reference does not have.
+ * plus o_trsmu (B := U^-1 B), the solve step the reference does not have, and the engine's
+ * mixed-precision pair (no reference counterpart): SHADOW (an operand rounded to BF16 in the
+ * tensor core's tiled layout) and the BF16 GEMM (products of the shadows summed in FP64 here; the
+ * tensor cores sum in FP32, so the two agree to a tolerance, not bitwise).
  * `rhypot(1, t)` of the reference is written here from its definition, 1 / hypot(1, t).
  *
  * Parity pins: dense routines must agree bitwise with the CUDA path; the Givens-based
@@ -307,6 +310,31 @@ void o_cholqr3(double* Y, int m, int k) {
   }
 }
 
+// ---------------------------------------------------------------- BF16 shadows (engine only)
+// Round to nearest even: FP64 -> FP32 (the hardware conversion), then FP32 -> BF16 by adding
+// 0x7FFF plus the lowest kept bit to the bit pattern and truncating (finite values; NaN kept
+// quiet).
+uint16_t to_bf16(double x) {
+  const float f = (float)x;
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  if ((u & 0x7F800000u) == 0x7F800000u) return (uint16_t)((u >> 16) | ((u & 0xFFFFu) ? 0x40u : 0u));
+  u += 0x7FFFu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+double from_bf16(uint16_t h) {
+  const uint32_t u = (uint32_t)h << 16;
+  float f;
+  std::memcpy(&f, &u, 4);
+  return (double)f;
+}
+// byte offset of element (r, c) of an R x K operand in the tiled layout (pp_task.h)
+inline int64_t tiled_at(int r, int c, int K) {
+  const int64_t chunk = (int64_t)(r / 128) * (K / 64) + c / 64;
+  const int rr = r % 128, cc = c % 64;
+  return chunk * 16384 + ((cc / 8) * 16 + rr / 8) * 128 + (rr % 8) * 16 + (cc % 8) * 2;
+}
+
 int run_one(const pp_task& T, std::vector<double>& tmp) {
   const bool t1 = T.flags & PP_T(1), t2 = T.flags & PP_T(2), t3 = T.flags & PP_T(3), t4 = T.flags & PP_T(4);
   switch (T.op) {
@@ -317,8 +345,37 @@ int run_one(const pp_task& T, std::vector<double>& tmp) {
     case PP_OP_TRSMRT: o_trsmrt(T.p[0], T.p[1], T.m, T.n, T.m, T.ld[0], T.ld[1]); return 0;
     case PP_OP_TRSMU: o_trsmu(T.p[0], T.p[1], T.m, T.n, T.ld[0], T.ld[1]); return 0;
     case PP_OP_GEMM:
+      if (T.prec == PP_PREC_BF16) {  // engine instruction: products of the BF16 shadows, FP64 sums
+        if (T.m % 128 || T.n % 128 || T.k % 64) return -1;
+        const uint8_t* As = reinterpret_cast<const uint8_t*>(T.p[1]);
+        const uint8_t* Bs = reinterpret_cast<const uint8_t*>(T.p[2]);
+        for (int r = 0; r < T.m; ++r)
+          for (int c = 0; c < T.n; ++c) {
+            double s = 0.0;
+            for (int q = 0; q < T.k; ++q) {
+              uint16_t a, b;
+              std::memcpy(&a, As + tiled_at(r, q, T.k), 2);
+              std::memcpy(&b, Bs + tiled_at(c, q, T.k), 2);
+              s += from_bf16(a) * from_bf16(b);
+            }
+            double& x = T.p[0][(int64_t)r * T.ld[0] + c];
+            x = (T.beta != 0.0 ? x : 0.0) + T.alpha * s;
+          }
+        return 0;
+      }
       o_gemm(T.alpha, T.beta, T.p[0], T.p[1], T.p[2], T.m, T.n, T.k, T.ld[0], T.ld[1], T.ld[2], t1, t2);
       return 0;
+    case PP_OP_SHADOW: {  // engine instruction: BF16 copy of an operand in the tiled layout
+      if (T.m % 128 || T.k % 64) return -1;
+      uint8_t* S = reinterpret_cast<uint8_t*>(T.p[0]);
+      for (int r = 0; r < T.m; ++r)
+        for (int c = 0; c < T.k; ++c) {
+          const double x = t1 ? T.p[1][(int64_t)c * T.ld[1] + r] : T.p[1][(int64_t)r * T.ld[1] + c];
+          const uint16_t h = to_bf16(x);
+          std::memcpy(S + tiled_at(r, c, T.k), &h, 2);
+        }
+      return 0;
+    }
     case PP_OP_GEMM3: {
       const int64_t need = T.ctrl ? (int64_t)T.m * T.l : (int64_t)T.k * T.n;
       if ((int64_t)tmp.size() < need) tmp.resize(need);

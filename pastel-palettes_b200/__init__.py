@@ -30,9 +30,9 @@ LIB_PATH = os.path.join(_HERE, "libpastel_palettes.so")
 PP_OK, PP_INVALID_ARG, PP_OOM, PP_TIMEOUT, PP_NUMERICAL, PP_CUDA_ERROR, PP_UNSUPPORTED, PP_INTERNAL = range(8)
 STATUS_NAMES = ["OK", "INVALID_ARG", "OOM", "TIMEOUT", "NUMERICAL", "CUDA_ERROR", "UNSUPPORTED", "INTERNAL"]
 OP_NAMES = ["nop", "getrf", "trsml", "trsmr", "trsmrt", "trsmu", "gemm", "gemm3", "gemm4", "accum", "sum", "trinv",
-            "trmv", "orth", "copy"]
+            "trmv", "orth", "copy", "shadow"]
 DENSE, LOWRANK, HIER = 0, 1, 2
-FP64, TF32 = 0, 1  # contraction precision of the factor's GEMM instructions
+FP64, TF32, BF16 = 0, 1, 2  # contraction precision of the factor's GEMM instructions
 ARENAS = ["matrix", "work", "scratch", "rhs", "rand"]
 
 # pp_task (pastel-palettes_b200/csrc/pp_task.h), 160 bytes

@@ -182,8 +182,9 @@ pp_status build_program(pp_hmatrix* h, int which, int nrhs, VmPlan& plan) {
     g.use_inverses(ctx->cfg.reference_isa == 0);
     if (which == 0) g.set_gemm_tile(h->gemm_tile);  // the solve's products keep 64
     if (which == 0) {
+      if (h->precision == PP_PREC_BF16) g.set_precision(PP_PREC_BF16);
       g.getrf_program();
-      if (h->precision != PP_PREC_FP64) plan.prog.set_gemm_precision(h->precision);
+      if (h->precision == PP_PREC_TF32) plan.prog.set_gemm_precision(h->precision);
     } else {
       g.solve_program(nrhs);
     }
@@ -253,7 +254,7 @@ pp_status plan_to_device_multi(pp_context* ctx, const std::vector<pp_hmatrix*>& 
   plan.n_ready = (int)ready.size();
   plan.use_tc = 0;
   for (const auto& t : tasks)
-    if (t.prec == PP_PREC_TF32) plan.use_tc = 1;
+    if (t.prec == PP_PREC_TF32 || t.prec == PP_PREC_BF16) plan.use_tc = 1;
   PP_CUDA(alloc((void**)&plan.d_tasks, sizeof(pp_task) * n));
   PP_CUDA(alloc((void**)&plan.d_succ, sizeof(int32_t) * succ.size()));
   PP_CUDA(alloc((void**)&plan.d_indeg, sizeof(int32_t) * n));
@@ -516,7 +517,7 @@ pp_status pp_hmatrix_restore(pp_hmatrix* h, void* stream) {
 
 pp_status pp_hmatrix_set_precision(pp_hmatrix* h, int precision) {
   if (!h) return PP_INVALID_ARG;
-  if (precision != PP_PREC_FP64 && precision != PP_PREC_TF32)
+  if (precision != PP_PREC_FP64 && precision != PP_PREC_TF32 && precision != PP_PREC_BF16)
     return fail(h->ctx, PP_INVALID_ARG, "pp_hmatrix_set_precision: unknown precision");
   if (precision == h->precision) return PP_OK;
   h->precision = precision;
@@ -860,7 +861,7 @@ pp_status pp_vm_execute(pp_context* ctx, const void* tasks, int n, const int32_t
   L.wait_ns = (spin_limit > 0 ? spin_limit : ctx->cfg.spin_limit) * 1000;
   L.grid = grid > 0 ? grid : std::max(1, std::min(n, ctx->sm_count * ctx->blocks_per_sm));
   for (int i = 0; i < n; ++i)
-    if (T[i].prec == PP_PREC_TF32) L.use_tc = 1;
+    if (T[i].prec == PP_PREC_TF32 || T[i].prec == PP_PREC_BF16) L.use_tc = 1;
   cudaStream_t s = (cudaStream_t)stream;
   PP_CUDA(pp_vm_run(L, s));
   PP_CUDA(cudaStreamSynchronize(s));

@@ -483,7 +483,52 @@ void Generator::bind(HTask& t, int slot, const View& v, bool write) {
   if (v.r0 < 0 || v.c0 < 0 || v.r0 + v.srows() > o.rows || v.c0 + v.scols() > o.cols)
     throw std::logic_error("operand view outside its storage object");
   if (o.tracked) t.regions.push_back({v.obj, v.r0, v.c0, v.srows(), v.scols(), !write});
+  if (write && v.obj < (int)shadows_.size()) shadows_[v.obj].clear();  // the shadows are stale now
 }
+
+// A view covering its whole storage object in the matrix arena (a dense leaf).
+bool Generator::whole_leaf(const View& v) const {
+  const PObj& o = P_.objs[v.obj];
+  return o.arena == P_.arena_id(inst_, AR_MATRIX) && v.r0 == 0 && v.c0 == 0 && v.srows() == o.rows &&
+         v.scols() == o.cols;
+}
+
+// Largest triangle of one TRSM* instruction: in a factorization, targets of kBigLeaf or more
+// rows (columns) take kBigTri-row triangles whole, so that a large leaf's solve is a few long
+// instructions rather than many 64-row pieces.
+int Generator::tri_limit(int target_extent) const {
+  return (!solve_ && target_extent >= kBigLeaf) ? std::max(Ttri_, kBigTri) : Ttri_;
+}
+
+// The BF16 shadow of an operand view (m x n logical, m a multiple of 128, n of 64), written by a
+// SHADOW instruction at its first use and reused until the view's object is written again.
+View Generator::shadow_of(const View& X) {
+  if ((int)shadows_.size() < (int)P_.objs.size()) shadows_.resize(P_.objs.size());
+  const ShadowKey key{X.obj, X.r0, X.c0, X.m, X.n, X.t};
+  for (auto& e : shadows_[X.obj])
+    if (e.first == key) {
+      View s;
+      s.obj = e.second;
+      s.m = P_.objs[e.second].rows;
+      s.n = P_.objs[e.second].cols;
+      return s;
+    }
+  // X.m rows of X.n BF16 values: X.n / 4 doubles per row (the tiled layout is opaque to the DAG)
+  View s;
+  s.obj = P_.add_obj(P_.arena_id(inst_, AR_SCRATCH), X.m, X.n / 4, true);
+  s.m = X.m;
+  s.n = X.n / 4;
+  HTask& t = emit(PP_OP_SHADOW);
+  bind(t, 0, s, true);
+  bind(t, 1, X, false);
+  t.t.m = X.m;
+  t.t.k = X.n;
+  t.flops = 0;
+  if ((int)shadows_.size() < (int)P_.objs.size()) shadows_.resize(P_.objs.size());
+  shadows_[X.obj].push_back({key, s.obj});
+  return s;
+}
+
 
 // --------------------------------------------------------------------------- H-LU
 void Generator::getrf_program() {
@@ -575,7 +620,7 @@ void Generator::trsml(const Mat& L, const Mat& B) {
     trmv(invL, 0, L.m, B.d);
     return;
   }
-  const int s = tri_split(L, Ttri_);
+  const int s = tri_split(L, tri_limit(B.n));
   if (s < 0) {
     if (B.kind != Mat::D || B.d.t) throw std::logic_error("trsml: target must be a dense untransposed block");
     for (int c = 0; c < B.n; c += T_) {
@@ -602,7 +647,7 @@ void Generator::trsml(const Mat& L, const Mat& B) {
 
 void Generator::trsmr(const Mat& U, const Mat& B) {
   if (B.kind == Mat::LR) { trsmrt(U, B.v); return; }
-  const int s = tri_split(U, Ttri_);
+  const int s = tri_split(U, tri_limit(B.m));
   if (s < 0) {
     if (B.kind != Mat::D || B.d.t) throw std::logic_error("trsmr: target must be a dense untransposed block");
     const int rows = std::max(T_, 4096 / std::max(1, B.n));
@@ -717,6 +762,33 @@ void Generator::gemm_tiles(const View& C, const View& A, const View& B, int alph
     s.t.alpha = 1.0;
     s.t.beta = 1.0;
     s.flops = (int64_t)C.m * C.n * parts;
+    return;
+  }
+  if (!solve_ && !work_target && C.m >= kBigLeaf && C.n >= kBigLeaf && whole_leaf(C) && whole_leaf(A) &&
+      whole_leaf(B)) {
+    // a Schur update of whole large leaves: one instruction (its CTA loops over the tile)
+    const bool bf16 = prec_ == PP_PREC_BF16 && C.m % 128 == 0 && C.n % 256 == 0 && A.n % 64 == 0;
+    View As, Bs;
+    if (bf16) {
+      As = shadow_of(A);
+      Bs = shadow_of(B.T());
+    }
+    HTask& t = emit(PP_OP_GEMM);
+    bind(t, 0, C, true);
+    if (bf16) {
+      bind(t, 1, As, false);
+      bind(t, 2, Bs, false);
+      t.t.prec = PP_PREC_BF16;
+    } else {
+      bind(t, 1, A, false);
+      bind(t, 2, B, false);
+    }
+    t.t.m = C.m;
+    t.t.n = C.n;
+    t.t.k = A.n;
+    t.t.alpha = (double)alpha;
+    t.t.beta = 1.0;
+    t.flops = 2LL * C.m * C.n * A.n;
     return;
   }
   const int g = gemm_tile_;

@@ -129,6 +129,10 @@ constexpr int kSolveGemmRows = 256;
 constexpr int kAccumMaxK2 = 32;
 // smallest m, n and k of a GEMM instruction the TF32 form runs on the tensor cores
 constexpr int kTcMinDim = 64;
+// products of whole dense leaves of at least kBigLeaf rows and columns are one instruction
+// each (a Schur update of large leaves); their triangular solves take triangles of kBigTri rows
+constexpr int kBigLeaf = 512;
+constexpr int kBigTri = 256;
 
 class Generator {
  public:
@@ -145,6 +149,10 @@ class Generator {
   // edge of the output tiles products are split into (64 or 128; larger tiles: fewer, longer
   // tasks)
   void set_gemm_tile(int t) { gemm_tile_ = t >= 128 ? 128 : 64; }
+  // contraction precision of the whole-leaf Schur updates: PP_PREC_BF16 runs them on the tensor
+  // cores from BF16 shadows of their operands (SHADOW instructions, one per operand block,
+  // emitted at its first use); the other instructions stay FP64
+  void set_precision(int prec) { prec_ = prec; }
   void solve_program(int nrhs);    // B := U^-1 L^-1 B on the RHS object (n x nrhs)
   int rhs_obj() const { return rhs_obj_; }
 
@@ -170,6 +178,19 @@ class Generator {
   bool inverses_ = false;
   int gemm_tile_ = 64;
   bool solve_ = false;  // building a solve program
+  int prec_ = PP_PREC_FP64;
+  // shadow object of an operand view (obj, r0, c0, m, n, t), dropped when the object is written
+  struct ShadowKey {
+    int obj, r0, c0, m, n;
+    bool t;
+    bool operator==(const ShadowKey& o) const {
+      return obj == o.obj && r0 == o.r0 && c0 == o.c0 && m == o.m && n == o.n && t == o.t;
+    }
+  };
+  std::vector<std::vector<std::pair<ShadowKey, int>>> shadows_;  // per program object
+  View shadow_of(const View& X);
+  bool whole_leaf(const View& v) const;
+  int tri_limit(int target_extent) const;
   void trmv(int inv, int upper, int m, const View& B);
   std::vector<std::pair<int, int>> inv_obj_;  // program obj of a diagonal leaf -> (L^-1, U^-1) objs
   bool inverse_of(const Mat& T, int& invL, int& invU) const;

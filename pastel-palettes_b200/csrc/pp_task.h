@@ -43,7 +43,11 @@ enum pp_op {
                         CholeskyQR3; rank-deficient columns become zero): the range finder of
                         a sketched low-rank update; no reference counterpart                   */
   PP_OP_COPY = 14,   /* C[m x n] := A[m x n] (p[1]); no reference counterpart                   */
-  PP_OP_COUNT = 15
+  PP_OP_SHADOW = 15, /* BF16 shadow of an FP64 operand for the tensor-core GEMM: the m x k matrix
+                        X(r, c) = p[1][r * ld[1] + c] (or p[1][c * ld[1] + r] with PP_T(1)),
+                        rounded to BF16 and written at p[0] in the tiled layout below (m a
+                        multiple of 128, k of 64); no reference counterpart                   */
+  PP_OP_COUNT = 16
 };
 
 /* flags: bit (4+i) = operand i is stored transposed (operand 0 is the target). */
@@ -58,6 +62,20 @@ enum pp_op {
 /* precision of the contraction inside GEMM-class tasks */
 #define PP_PREC_FP64 0
 #define PP_PREC_TF32 1
+/* PP_PREC_BF16: a GEMM whose operands are BF16 shadows (PP_OP_SHADOW) in the tiled layout:
+ * p[1] the m x k shadow of op(A), p[2] the n x k shadow of op(B)^T; products summed in FP32 on
+ * the tensor cores, C (FP64) := beta C + alpha sum.  m a multiple of 128, n of 256, k of 64. */
+#define PP_PREC_BF16 2
+
+/* Tiled BF16 layout of an R x K operand (R a multiple of 128, K of 64): 16 KB chunks of 128 rows
+ * x 64 columns, chunk (R / 128 block rb, K / 64 block kc) at byte ((rb * (K / 64)) + kc) * 16384;
+ * inside a chunk, element (r, c) at byte ((c / 8) * 16 + r / 8) * 128 + (r % 8) * 16 + (c % 8) * 2
+ * (8 x 8 core matrices of 128 contiguous bytes, adjacent along r 128 bytes apart, along c 2048
+ * bytes apart): the operand layout the tensor core reads from shared memory without swizzling,
+ * so one chunk moves with one bulk copy. */
+#define PP_SHADOW_CHUNK_ROWS 128
+#define PP_SHADOW_CHUNK_COLS 64
+#define PP_SHADOW_CHUNK_BYTES 16384
 
 typedef struct pp_task {
   int32_t op;

@@ -303,7 +303,7 @@ __device__ __forceinline__ void dev_gemm(double* __restrict__ C, int ldc, const 
 #define TC_B_BYTES (TC_N * TC_K * 4)
 #define TC_LBO_A (TC_M / 8 * 128)  /* bytes between k16 columns of A's core matrices */
 #define TC_LBO_B (TC_N / 8 * 128)
-#define TC_TMEM_COLS 64
+#define TC_TMEM_COLS 512  /* all of an SM's tensor memory: the VM runs one CTA per SM */
 
 struct TcCtx {
   uint32_t tmem;      // accumulator base address in tensor memory
@@ -312,6 +312,13 @@ struct TcCtx {
   long long limit;    // nanoseconds before a wait for the tensor core gives up
   int pending;        // a commit whose completion was not observed (after a timeout)
   int active;         // tensor memory and the mbarrier were set up for this CTA
+  // BF16 pipeline (dev_gemm_bf16): shared address of its 10 mbarriers, the number of stage
+  // fills and accumulator tiles used so far (every thread counts the same), an abort flag in
+  // shared memory, and the last stage fill / tile commit whose completion nobody waited for
+  uint32_t bars;
+  uint32_t q;
+  uint32_t u;
+  int* abort;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -451,6 +458,245 @@ __device__ __noinline__ bool dev_gemm_tc(double* __restrict__ C, int ldc, const 
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       __syncthreads();
     }
+  return ok;
+}
+
+// ------------------------------------------------------------------------- BF16 Schur GEMM
+// Operands are BF16 shadows in the tiled layout of pp_task.h (PP_OP_SHADOW writes them), so
+// every 128-row x 64-column chunk of an operand moves into shared memory with ONE bulk copy of
+// 16 KB (the TMA engine's untiled mode: no tensor map, no per-element work) and lands in the
+// canonical no-swizzle K-major layout tcgen05.mma reads.
+//
+// C[m x n] (FP64) = beta C + alpha A B, tile loop over 128 x 256 sub-tiles of C, k in chunks of
+// 64 through a 3-stage ring of shared-memory stages (A chunk + two B chunks = 48 KB each).
+// Roles inside the CTA (warp specialised):
+//   warp 0, one lane   producer: waits for a free stage, posts the expected bytes on the
+//                      stage's "full" mbarrier and issues the three bulk copies;
+//   warp 1, one lane   MMA issuer: per stage four K=16 steps x two 128 x 128 MMAs
+//                      (kind::f16, BF16 inputs, FP32 accumulators in tensor memory), then
+//                      tcgen05.commit to the stage's "empty" mbarrier; after a sub-tile's last
+//                      stage, a commit to the accumulator buffer's "full" mbarrier;
+//   warps 4..7         epilogue: tcgen05.ld of the accumulator buffer (warp w reads TMEM lanes
+//                      32 (w % 4) ..), C += alpha acc in FP64, then an arrive on the buffer's
+//                      "empty" mbarrier.
+// Two accumulator buffers of 256 TMEM columns: the epilogue of one sub-tile overlaps the MMAs
+// of the next, and the producer runs up to three stages ahead of the MMAs.
+#define BG_STAGES 3
+#define BG_CHUNK PP_SHADOW_CHUNK_BYTES
+#define BG_STAGE_BYTES (3 * BG_CHUNK)
+#define BG_TILE_N 256
+// instruction descriptor: D F32 (bits 4-5 = 1), A and B BF16 (bits 7-9, 10-12 = 1), both
+// K-major, N = 128 (bits 17-22 = N >> 3), M = 128 (bits 24-28 = M >> 4)
+constexpr uint32_t kIdescBf16 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(128 >> 3) << 17) |
+                                ((uint32_t)(128 >> 4) << 24);
+
+__device__ __forceinline__ uint32_t bf16_bits(double x) {
+  // round to nearest even through FP32 (finite values; NaN stays a quiet NaN)
+  uint32_t u = __float_as_uint(__double2float_rn(x));
+  if ((u & 0x7F800000u) == 0x7F800000u) return (u >> 16) | ((u & 0xFFFFu) ? 0x40u : 0u);
+  u += 0x7FFFu + ((u >> 16) & 1u);
+  return u >> 16;
+}
+
+__device__ __forceinline__ size_t tiled_at(int r, int c, int K) {
+  const size_t chunk = (size_t)(r >> 7) * (K >> 6) + (c >> 6);
+  const int rr = r & 127, cc = c & 63;
+  return chunk * BG_CHUNK + (size_t)((((cc >> 3) << 4) + (rr >> 3)) << 7) + ((rr & 7) << 4) + ((cc & 7) << 1);
+}
+
+// S := the tiled BF16 shadow of X (m x k), X(r, c) = A[r lda + c] or A[c lda + r] (tA); each
+// thread converts 8 consecutive columns of a row and stores them as one 16-byte word
+__device__ __noinline__ void dev_shadow(uint8_t* S, const double* A, int lda, bool tA, int m, int k) {
+  const int cg = k >> 3, units = m * cg;
+  for (int u = threadIdx.x; u < units; u += NT) {
+    int r, c;
+    if (tA) { r = u % m; c = (u / m) << 3; }   // lanes along r: A[c lda + r] coalesced
+    else { r = u / cg; c = (u % cg) << 3; }    // lanes along c: 64 contiguous bytes each
+    uint32_t h[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      h[q] = bf16_bits(tA ? ldcg(&A[(size_t)(c + q) * lda + r]) : ldcg(&A[(size_t)r * lda + c + q]));
+    uint4 v;
+    v.x = h[0] | (h[1] << 16);
+    v.y = h[2] | (h[3] << 16);
+    v.z = h[4] | (h[5] << 16);
+    v.w = h[6] | (h[7] << 16);
+    *reinterpret_cast<uint4*>(S + tiled_at(r, c, k)) = v;
+  }
+  // the shadow is read by bulk copies (the async proxy) of other CTAs
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+  __syncthreads();
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t addr, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(addr), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t addr) {
+  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.shared::cta.b64 st, [%0];\n}\n" ::"r"(addr) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t addr, uint32_t bytes) {
+  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n" ::"r"(addr),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+// bounded wait that also gives up when another role of the CTA has given up
+__device__ __forceinline__ bool mbar_wait_or_abort(uint32_t addr, uint32_t phase, long long limit_ns,
+                                                   volatile int* abort) {
+  const unsigned long long t0 = gtimer_ns();
+  for (;;) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(addr), "r"(phase)
+        : "memory");
+    if (done) return true;
+    if (*abort) return false;
+    if ((long long)(gtimer_ns() - t0) > limit_ns) {
+      *abort = 1;
+      return false;
+    }
+  }
+}
+__device__ __forceinline__ void tc_mma_bf16(uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+      "l"(ad), "l"(bd), "r"(kIdescBf16), "r"(acc)
+      : "memory");
+}
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __noinline__ bool dev_gemm_bf16(double* __restrict__ C, int ldc, const uint8_t* __restrict__ As,
+                                           const uint8_t* __restrict__ Bs, int m, int n, int k, double alpha,
+                                           double beta, double* smem, TcCtx& tc) {
+  uint8_t* sbase = reinterpret_cast<uint8_t*>(smem);
+  const uint32_t s0 = smem_u32(sbase);
+  const uint32_t stage0 = (s0 + 1023u) & ~1023u;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nch = k >> 6, kchunks = k >> 6;
+  const int tiles_n = n / BG_TILE_N, tiles = (m >> 7) * tiles_n;
+  volatile int* abort = tc.abort;
+  if (tid == 0) *abort = 0;
+  // shared memory written by earlier tasks (generic proxy) is overwritten by bulk copies
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  __syncthreads();
+  auto full = [&](uint32_t s) { return tc.bars + 8u * s; };
+  auto empty = [&](uint32_t s) { return tc.bars + 8u * (BG_STAGES + s); };
+  auto tfull = [&](uint32_t b) { return tc.bars + 8u * (2 * BG_STAGES + b); };
+  auto tempty = [&](uint32_t b) { return tc.bars + 8u * (2 * BG_STAGES + 2 + b); };
+  if (warp == 0) {
+    if (lane == 0) {  // producer
+      // the shadows were written with ordinary stores by other CTAs (acquired through the
+      // dependency counters); order them before this thread's bulk copies read them
+      asm volatile("fence.proxy.async.global;" ::: "memory");
+      uint32_t q = tc.q;
+      for (int t = 0; t < tiles && !*abort; ++t) {
+        const int rb = (t / tiles_n), cb = (t % tiles_n) * 2;
+        for (int kc = 0; kc < nch; ++kc, ++q) {
+          const uint32_t s = q % BG_STAGES, ph = (q / BG_STAGES) & 1u;
+          if (!mbar_wait_or_abort(empty(s), ph ^ 1u, tc.limit, abort)) break;
+          const uint32_t dst = stage0 + s * BG_STAGE_BYTES;
+          mbar_expect_tx(full(s), BG_STAGE_BYTES);
+          bulk_g2s(dst, As + ((size_t)rb * kchunks + kc) * BG_CHUNK, BG_CHUNK, full(s));
+          bulk_g2s(dst + BG_CHUNK, Bs + ((size_t)cb * kchunks + kc) * BG_CHUNK, BG_CHUNK, full(s));
+          bulk_g2s(dst + 2 * BG_CHUNK, Bs + ((size_t)(cb + 1) * kchunks + kc) * BG_CHUNK, BG_CHUNK, full(s));
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {  // MMA issuer
+      uint32_t q = tc.q, u = tc.u;
+      for (int t = 0; t < tiles && !*abort; ++t, ++u) {
+        const uint32_t b = u & 1u;
+        if (!mbar_wait_or_abort(tempty(b), ((u >> 1) & 1u) ^ 1u, tc.limit, abort)) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t acc0 = tc.tmem + b * BG_TILE_N;
+        bool ok = true;
+        for (int kc = 0; kc < nch; ++kc, ++q) {
+          const uint32_t s = q % BG_STAGES, ph = (q / BG_STAGES) & 1u;
+          if (!mbar_wait_or_abort(full(s), ph, tc.limit, abort)) { ok = false; break; }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t a = stage0 + s * BG_STAGE_BYTES;
+#pragma unroll
+          for (int ks = 0; ks < 4; ++ks) {
+            const uint32_t acc = (kc > 0 || ks > 0) ? 1u : 0u;
+            const uint64_t ad = umma_desc(a + ks * 4096u, 2048u, 128u);
+            tc_mma_bf16(acc0, ad, umma_desc(a + BG_CHUNK + ks * 4096u, 2048u, 128u), acc);
+            tc_mma_bf16(acc0 + 128u, ad, umma_desc(a + 2 * BG_CHUNK + ks * 4096u, 2048u, 128u), acc);
+          }
+          tc_commit(empty(s));  // the stage is free once these MMAs have read it
+        }
+        if (!ok) break;
+        tc_commit(tfull(b));  // the accumulator tile is complete
+      }
+    }
+  } else if (warp >= 4) {  // epilogue
+    const int qd = warp & 3;
+    uint32_t u = tc.u;
+    for (int t = 0; t < tiles; ++t, ++u) {
+      const uint32_t b = u & 1u;
+      const bool ok = mbar_wait_or_abort(tfull(b), (u >> 1) & 1u, tc.limit, abort);
+      if (__any_sync(0xffffffffu, !ok)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int i0 = (t / tiles_n) << 7, j0 = (t % tiles_n) * BG_TILE_N;
+      const int row = i0 + 32 * qd + lane;
+      double* crow = C + (size_t)row * ldc + j0;
+#pragma unroll 1
+      for (int p = 0; p < BG_TILE_N / 32; ++p) {
+        uint32_t v[32];
+        const uint32_t taddr = tc.tmem + ((uint32_t)(32 * qd) << 16) + b * BG_TILE_N + 32u * p;
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+            "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+              "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]),
+              "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+              "=r"(v[30]), "=r"(v[31])
+            : "r"(taddr)
+            : "memory");
+        double cv[32];
+        if (beta != 0.0) {
+#pragma unroll
+          for (int c = 0; c < 32; c += 2) {
+            const double2 x = __ldcg(reinterpret_cast<const double2*>(crow + 32 * p + c));
+            cv[c] = x.x;
+            cv[c + 1] = x.y;
+          }
+        } else {
+#pragma unroll
+          for (int c = 0; c < 32; ++c) cv[c] = 0.0;
+        }
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int c = 0; c < 32; c += 2) {
+          double2 y;
+          y.x = fma(alpha, (double)__uint_as_float(v[c]), cv[c]);
+          y.y = fma(alpha, (double)__uint_as_float(v[c + 1]), cv[c + 1]);
+          *reinterpret_cast<double2*>(crow + 32 * p + c) = y;
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(tempty(b));
+    }
+  }
+  __syncthreads();
+  const bool ok = !*abort;
+  // every thread advances the pipeline counters alike (the next BF16 task continues the phases)
+  tc.q += (uint32_t)(tiles * nch);
+  tc.u += (uint32_t)tiles;
+  if (!ok) tc.pending = 1;
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  __syncthreads();
   return ok;
 }
 
@@ -1509,6 +1755,14 @@ __device__ bool run_task(const pp_task& T, double* smem, TcCtx& tc, int& err) {
       else dev_trsmu(T.p[0], T.ld[0], T.p[1], T.ld[1], T.m, T.n, smem);
       return true;
     case PP_OP_GEMM:
+      if (T.prec == PP_PREC_BF16) {
+        if (!tc.active || T.m < 128 || T.m % 128 || T.n < BG_TILE_N || T.n % BG_TILE_N || T.k < 64 || T.k % 64)
+          return false;
+        if (!dev_gemm_bf16(T.p[0], T.ld[0], reinterpret_cast<const uint8_t*>(T.p[1]),
+                           reinterpret_cast<const uint8_t*>(T.p[2]), T.m, T.n, T.k, T.alpha, T.beta, smem, tc))
+          err = PP_VM_MMA_TIMEOUT;
+        return true;
+      }
       if (T.prec == PP_PREC_TF32) {
         if (!tc.active) return false;  // launched without tensor memory
         if (!dev_gemm_tc(T.p[0], T.ld[0], T.p[1], T.ld[1], T.flags & PP_T(1), T.p[2], T.ld[2], T.flags & PP_T(2),
@@ -1539,6 +1793,10 @@ __device__ bool run_task(const pp_task& T, double* smem, TcCtx& tc, int& err) {
       return true;
     case PP_OP_COPY:
       dev_copy(T.p[0], T.ld[0], T.p[1], T.ld[1], T.m, T.n);
+      return true;
+    case PP_OP_SHADOW:
+      if (T.m < 128 || T.m % 128 || T.k < 64 || T.k % 64) return false;
+      dev_shadow(reinterpret_cast<uint8_t*>(T.p[0]), T.p[1], T.ld[1], T.flags & PP_T(1), T.m, T.k);
       return true;
     default: return false;
   }
@@ -1577,7 +1835,9 @@ __global__ void __launch_bounds__(NT, 1)
   __shared__ unsigned long long s_t0;
   __shared__ uint32_t s_tmem;
   __shared__ __align__(8) unsigned long long s_mbar;
-  TcCtx tc{0u, 0u, 0u, wait_ns, 0, 0};
+  __shared__ __align__(8) unsigned long long s_bg[2 * BG_STAGES + 4];  // BF16 pipeline mbarriers
+  __shared__ int s_abort;
+  TcCtx tc{0u, 0u, 0u, wait_ns, 0, 0, 0u, 0u, 0u, &s_abort};
   if (use_tc) {
     // TF32 tasks: 64 TMEM columns (128 lanes x 64 FP32 accumulators) and one mbarrier per CTA
     if ((threadIdx.x >> 5) == 0) {
@@ -1588,6 +1848,11 @@ __global__ void __launch_bounds__(NT, 1)
     }
     if (threadIdx.x == 0) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_mbar)) : "memory");
+      // BF16 pipeline: stage full / empty (one arrival each: the producer's expect_tx, the MMA
+      // issuer's commit), accumulator full (a commit) / empty (one arrival per epilogue warp)
+      for (int i = 0; i < 2 * BG_STAGES + 2; ++i) mbar_init(smem_u32(&s_bg[i]), 1);
+      for (int i = 2 * BG_STAGES + 2; i < 2 * BG_STAGES + 4; ++i) mbar_init(smem_u32(&s_bg[i]), 4);
+      s_abort = 0;
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -1595,6 +1860,7 @@ __global__ void __launch_bounds__(NT, 1)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     tc.tmem = s_tmem;
     tc.mbar = smem_u32(&s_mbar);
+    tc.bars = smem_u32(&s_bg[0]);
     tc.active = 1;
   }
   // Continuation: of the successors this CTA's task makes ready, the first in the
@@ -1675,7 +1941,13 @@ __global__ void __launch_bounds__(NT, 1)
   if (use_tc) {
     // an MMA group whose completion was never observed still owns the accumulators:
     // give it one more bounded wait before the columns are returned
-    if (tc.pending) mbar_wait(tc.mbar, tc.phase ^ 1u, tc.limit);
+    if (tc.pending) {
+      mbar_wait(tc.mbar, tc.phase ^ 1u, tc.limit);
+      // a BF16 task that gave up may still have bulk copies and MMAs in flight: they finish
+      // within microseconds; give them a bounded 2 ms before the columns are returned
+      const unsigned long long t0 = gtimer_ns();
+      while (gtimer_ns() - t0 < 2000000ull) __nanosleep(1000);
+    }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if ((threadIdx.x >> 5) == 0) {
