@@ -27,6 +27,29 @@ def _free_port():
         return s.getsockname()[1]
 
 
+def _cpu_job(pp, oracle, h, prob, tol=1e-10):
+    """One factor + solve + FP64 refinement of a replica's problem with the oracle (the program
+    the GPU runs, executed on the host); returns (seconds, refinement solves)."""
+    import time
+    n = prob.n
+    b = pp.rhs(n, 1, seed=7)
+    A = prob.dense()
+    t0 = time.perf_counter()
+    fac = oracle.HostArenas(h, 0)
+    fac.run(threads=2)
+    sol = oracle.HostArenas(h, 1, 1)
+    sol.matrix[:] = fac.matrix
+    x, r = np.zeros((n, 1)), b.copy()
+    for it in range(1, 31):
+        sol.rhs[:n] = r.ravel()
+        sol.run(threads=1)
+        x += sol.rhs[:n].reshape(n, 1)
+        r = b - A @ x
+        if np.abs(r).max() / (prob.norm_inf * np.abs(x).max() + np.abs(b).max()) <= tol:
+            break
+    return time.perf_counter() - t0, it
+
+
 def _replica(rank, world, port, q):
     import torch.distributed as dist
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
@@ -39,9 +62,9 @@ def _replica(rank, world, port, q):
         ctx = pp.Context(device=-1)
         # this rank's replica: the workload's construction at a small size, seed offset by rank
         h, prob = pp.make_kernel_problem(ctx, 1024, 2, "inv", 1e-3, 256, 16, seed=1234 + rank)
-        times, iters = bench.cpu_steps(pp, oracle, h, prob, 1, 2)
-        rate, tmax = bench.whole_job_rate(dist, world, times[0], 1, "cpu")
-        q.put((rank, times[0], iters[0], rate, tmax, float(prob.points[0, 0])))
+        t, iters = _cpu_job(pp, oracle, h, prob)
+        rate, tmax = bench.whole_job_rate(dist, world, t, 1, "cpu")
+        q.put((rank, t, iters, rate, tmax, float(prob.points[0, 0])))
     finally:
         dist.destroy_process_group()
 
