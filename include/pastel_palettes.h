@@ -59,7 +59,7 @@ typedef struct pp_program_info {
   int n_tasks;
   long long n_edges;
   long long flops;                  /* algorithmic FLOPs of all instructions */
-  long long op_count[16];           /* instructions per pp_op (pp_task.h)   */
+  long long op_count[24];           /* instructions per pp_op (pp_task.h)   */
   long long arena_elems[5];         /* matrix, work, scratch, rhs, rand     */
   double host_build_ms;             /* op generation + DAG + encoding        */
 } pp_program_info;
@@ -272,6 +272,17 @@ pp_status pp_kernel_residual_dev(pp_context* ctx, int kernel, double p0, double 
  * reference's matrices come from a separate Java compressor). */
 pp_status pp_hmatrix_assemble_dense_dev(pp_hmatrix* h, int kernel, double p0, double shift, const double* pts_dev,
                                         int dim, void* stream);
+/* Builds the whole H-matrix on the device from its points (device, n x dim, in the H-matrix's
+ * cluster order), without a host image: the device arena is allocated (zero-filled) if needed,
+ * the dense blocks are assembled as pp_hmatrix_assemble_dense_dev does, and every low-rank block
+ * is compressed by a randomized range finder with one power step on the VM (instructions KMUL:
+ * kernel matrix times a block of vectors, evaluated from the points; ORTH; LRTRUNC: truncation
+ * to the singular values above the rank tolerance times the largest, at most the block's rank).
+ * The kernel must be smooth on the admissible blocks (the four kernels of
+ * pp_kernel_residual_dev are).  Stream ordered; pp_hmatrix_sync reports a failed launch.
+ * No reference counterpart (the reference's matrices come from a separate Java compressor). */
+pp_status pp_hmatrix_construct_dev(pp_hmatrix* h, int kernel, double p0, double shift, const double* pts_dev,
+                                   int dim, void* stream);
 /* One job of pp_kernel_residual_batch_dev (device pointers). */
 typedef struct pp_residual_job {
   int kernel;           /* as pp_kernel_residual_dev */

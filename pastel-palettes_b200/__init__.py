@@ -30,7 +30,7 @@ LIB_PATH = os.path.join(_HERE, "libpastel_palettes.so")
 PP_OK, PP_INVALID_ARG, PP_OOM, PP_TIMEOUT, PP_NUMERICAL, PP_CUDA_ERROR, PP_UNSUPPORTED, PP_INTERNAL = range(8)
 STATUS_NAMES = ["OK", "INVALID_ARG", "OOM", "TIMEOUT", "NUMERICAL", "CUDA_ERROR", "UNSUPPORTED", "INTERNAL"]
 OP_NAMES = ["nop", "getrf", "trsml", "trsmr", "trsmrt", "trsmu", "gemm", "gemm3", "gemm4", "accum", "sum", "trinv",
-            "trmv", "orth", "copy", "shadow"]
+            "trmv", "orth", "copy", "shadow", "kmul", "lrtrunc"]
 DENSE, LOWRANK, HIER = 0, 1, 2
 FP64, TF32, BF16 = 0, 1, 2  # contraction precision of the factor's GEMM instructions
 ARENAS = ["matrix", "work", "scratch", "rhs", "rand"]
@@ -102,7 +102,7 @@ class _TuneResult(C.Structure):
 
 class _ProgramInfo(C.Structure):
     _fields_ = [("n_tasks", C.c_int), ("n_edges", C.c_longlong), ("flops", C.c_longlong),
-                ("op_count", C.c_longlong * 16), ("arena_elems", C.c_longlong * 5), ("host_build_ms", C.c_double)]
+                ("op_count", C.c_longlong * 24), ("arena_elems", C.c_longlong * 5), ("host_build_ms", C.c_double)]
 
 
 _lib = None
@@ -149,6 +149,7 @@ def lib():
             "pp_kernel_residual_dev": (i, [vp, i, d, d, vp, i, i, vp, vp, vp, i, vp]),
             "pp_kernel_residual_batch_dev": (i, [vp, i, C.POINTER(_ResidualJob), vp]),
             "pp_hmatrix_assemble_dense_dev": (i, [vp, i, d, d, vp, i, vp]),
+            "pp_hmatrix_construct_dev": (i, [vp, i, d, d, vp, i, vp]),
             "pp_datamap2d_check_overlap": (i, [C.c_uint64, C.c_size_t, C.c_size_t, C.c_size_t,
                                                C.c_uint64, C.c_size_t, C.c_size_t, C.c_size_t]),
             "pp_operation_dependency": (i, [i, vp, vp, i, vp, vp]),
@@ -411,6 +412,19 @@ class Hierarchical:
         self.ctx.check(lib().pp_hmatrix_assemble_dense_dev(self._h, int(prob.kernel), float(prob.p0),
                                                            float(prob.shift), pts.data_ptr(), int(pts.shape[1]),
                                                            _stream_handle(stream)), "assemble_dense")
+        return pts
+
+    def construct(self, prob, pts=None, stream=None):
+        """The whole H-matrix built on the device from the problem's points (no host image):
+        dense blocks evaluated, low-rank blocks compressed by a randomized range finder on the
+        VM and truncated at the rank tolerance.  pts: the points as a device tensor (n x dim),
+        made from prob when not given; returned (keep it alive until the stream has run)."""
+        import torch
+        if pts is None:
+            pts = torch.from_numpy(np.ascontiguousarray(prob.points, dtype=np.float64)).cuda()
+        self.ctx.check(lib().pp_hmatrix_construct_dev(self._h, int(prob.kernel), float(prob.p0), float(prob.shift),
+                                                      pts.data_ptr(), int(pts.shape[1]), _stream_handle(stream)),
+                       "construct")
         return pts
 
     def set_gemm_tile(self, edge):
@@ -835,22 +849,51 @@ def make_dense_problem(ctx, n=1024, leaf=256, seed=1234):
     return h, A
 
 
+def offdiag_rowsum_max_dev(ctx, pts_dev, kernel, p0, stream=None):
+    """max_i sum_{j != i} |K(p_i, p_j)| on the device (the kernels here are positive): the
+    matrix-free residual of the unshifted matrix applied to ones, minus the diagonal K(0)."""
+    import torch
+    n = pts_dev.shape[0]
+    x = torch.ones((n, 1), dtype=torch.float64, device=pts_dev.device)
+    b = torch.zeros_like(x)
+    r = torch.empty_like(x)
+    ctx.kernel_residual(kernel, p0, 0.0, pts_dev, x, b, r, stream)
+    if stream is not None:
+        stream.synchronize()
+    else:
+        torch.cuda.synchronize()
+    return float((-r).max().item()) - float(kernel_eval(kernel, 0.0, p0))
+
+
 def make_kernel_problem(ctx, n, dim, kernel, p0, leaf, rank, admissibility=0, eta=1.0, shift=None,
-                        shift_factor=2.0, seed=1234, rank_tol=None):
+                        shift_factor=2.0, seed=1234, rank_tol=None, construct="host", stream=None):
     """Kernel-matrix configuration: points U[0,1]^dim (Morton order), A_ij = K(|x_i - x_j|),
-    diagonal shifted by `shift` or by shift_factor * max off-diagonal row sum."""
+    diagonal shifted by `shift` or by shift_factor * max off-diagonal row sum.
+    construct="host": blocks filled on the host (exact dense blocks, truncated SVD of the
+    low-rank ones) for a later upload; "device": the row sums and every block computed on the
+    device (Hierarchical.construct), no host image; prob.points_dev holds the device points."""
     rng = np.random.default_rng(seed)
     pts = rng.uniform(0.0, 1.0, (n, dim))
     pts = pts[morton_order(pts)]
     kid = KERNELS[kernel] if isinstance(kernel, str) else kernel
-    off = offdiag_rowsum_max(pts, kid, p0)
+    pts_dev = None
+    if construct == "device":
+        import torch
+        pts_dev = torch.from_numpy(np.ascontiguousarray(pts)).cuda()
+        off = offdiag_rowsum_max_dev(ctx, pts_dev, kid, p0, stream)
+    else:
+        off = offdiag_rowsum_max(pts, kid, p0)
     if shift is None:
         shift = shift_factor * off
     prob = KernelProblem(n, dim, kid, p0, shift, pts, off)
+    prob.points_dev = pts_dev
     h = Hierarchical.geometric(ctx, pts, leaf, admissibility, eta, rank)
     if rank_tol:
         h.set_rank_tolerance(rank_tol)
-    fill_kernel_hmatrix(h, prob, seed + 1, rank_tol=rank_tol)
+    if construct == "device":
+        h.construct(prob, pts_dev, stream)
+    else:
+        fill_kernel_hmatrix(h, prob, seed + 1, rank_tol=rank_tol)
     return h, prob
 
 

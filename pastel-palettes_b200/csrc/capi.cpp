@@ -95,6 +95,9 @@ struct pp_hmatrix {
   std::vector<double> rand_host;
   VmPlan factor;
   std::map<int, std::unique_ptr<VmPlan>> solves;
+  VmPlan construct;              // device construction of the low-rank blocks
+  int c_kernel = -1, c_dim = 0;  // what the construction program was built for
+  double c_p0 = 0.0;
   VmPlan* last = nullptr;
   // stream-ordered memory mode (set by the server for the requests it owns)
   cudaStream_t astream = nullptr;
@@ -125,12 +128,13 @@ struct pp_hmatrix {
     }
   }
   std::vector<VmPlan*> all_plans() {
-    std::vector<VmPlan*> v{&factor};
+    std::vector<VmPlan*> v{&factor, &construct};
     for (auto& kv : solves) v.push_back(kv.second.get());
     return v;
   }
   ~pp_hmatrix() {
     factor.release();
+    construct.release();
     for (auto& kv : solves) kv.second->release();
     if (pinned) cudaHostUnregister(H->host.data());
     dfree(d_arena);
@@ -185,6 +189,8 @@ pp_status build_program(pp_hmatrix* h, int which, int nrhs, VmPlan& plan) {
       if (h->precision == PP_PREC_BF16) g.set_precision(PP_PREC_BF16);
       g.getrf_program();
       if (h->precision == PP_PREC_TF32) plan.prog.set_gemm_precision(h->precision);
+    } else if (which == 2) {
+      g.construct_program(h->c_kernel, h->c_dim, h->c_p0, h->H->rank_tol);
     } else {
       g.solve_program(nrhs);
     }
@@ -457,15 +463,9 @@ pp_status pp_hmatrix_set_lowrank(pp_hmatrix* h, int b, const double* U, int ldu,
   return PP_OK;
 }
 
-pp_status pp_hmatrix_upload(pp_hmatrix* h, void* stream) {
-  if (!h) return PP_INVALID_ARG;
+// the random sketch of the accumulations (its size depends on the factor program's arenas)
+static pp_status upload_rand(pp_hmatrix* h) {
   pp_context* ctx = h->ctx;
-  if (!has_device(ctx)) return fail(ctx, PP_CUDA_ERROR, "no CUDA device in this context");
-  const size_t bytes = sizeof(double) * (size_t)std::max<int64_t>(h->H->arena_elems, 1);
-  if (!h->d_arena) PP_CUDA(h->dalloc((void**)&h->d_arena, bytes));
-  PP_CUDA(cudaMemcpyAsync(h->d_arena, h->H->host.data(), sizeof(double) * h->H->block_elems, cudaMemcpyHostToDevice,
-                          (cudaStream_t)stream));
-  // the random sketch depends on the factor program's arena sizes
   pp_status st = build_program(h, 0, 0, h->factor);
   if (st != PP_OK) return st;
   if (!h->d_rand) {
@@ -476,10 +476,23 @@ pp_status pp_hmatrix_upload(pp_hmatrix* h, void* stream) {
   return PP_OK;
 }
 
+pp_status pp_hmatrix_upload(pp_hmatrix* h, void* stream) {
+  if (!h) return PP_INVALID_ARG;
+  pp_context* ctx = h->ctx;
+  if (!has_device(ctx)) return fail(ctx, PP_CUDA_ERROR, "no CUDA device in this context");
+  const size_t bytes = sizeof(double) * (size_t)std::max<int64_t>(h->H->arena_elems, 1);
+  if (!h->d_arena) PP_CUDA(h->dalloc((void**)&h->d_arena, bytes));
+  h->H->ensure_host();
+  PP_CUDA(cudaMemcpyAsync(h->d_arena, h->H->host.data(), sizeof(double) * h->H->block_elems, cudaMemcpyHostToDevice,
+                          (cudaStream_t)stream));
+  return upload_rand(h);
+}
+
 pp_status pp_hmatrix_download(pp_hmatrix* h, void* stream) {
   if (!h) return PP_INVALID_ARG;
   pp_context* ctx = h->ctx;
   if (!h->d_arena) return fail(ctx, PP_INVALID_ARG, "H-matrix not uploaded");
+  h->H->ensure_host();
   PP_CUDA(cudaMemcpyAsync(h->H->host.data(), h->d_arena, sizeof(double) * h->H->block_elems, cudaMemcpyDeviceToHost,
                           (cudaStream_t)stream));
   PP_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
@@ -490,7 +503,9 @@ pp_status pp_hmatrix_pin_host(pp_hmatrix* h) {
   if (!h) return PP_INVALID_ARG;
   pp_context* ctx = h->ctx;
   if (!has_device(ctx)) return fail(ctx, PP_CUDA_ERROR, "no CUDA device in this context");
-  if (h->pinned || h->H->host.empty()) return PP_OK;
+  if (h->pinned) return PP_OK;
+  h->H->ensure_host();
+  if (h->H->host.empty()) return PP_OK;
   PP_CUDA(cudaHostRegister(h->H->host.data(), sizeof(double) * h->H->host.size(), cudaHostRegisterDefault));
   h->pinned = true;
   return PP_OK;
@@ -573,6 +588,7 @@ long long pp_hmatrix_storage_elems(const pp_hmatrix* h) { return h ? h->H->stora
 double* pp_hmatrix_host_arena(pp_hmatrix* h, long long* elems) {
   if (!h) return nullptr;
   if (elems) *elems = h->H->arena_elems;
+  h->H->ensure_host();
   return h->H->host.data();
 }
 const double* pp_hmatrix_device_arena(const pp_hmatrix* h) { return h ? h->d_arena : nullptr; }
@@ -706,6 +722,43 @@ pp_status pp_hmatrix_assemble_dense_dev(pp_hmatrix* h, int kernel, double p0, do
   return PP_OK;
 }
 
+pp_status pp_hmatrix_construct_dev(pp_hmatrix* h, int kernel, double p0, double shift, const double* pts, int dim,
+                                   void* stream) {
+  if (!h) return PP_INVALID_ARG;
+  pp_context* ctx = h->ctx;
+  if (!has_device(ctx)) return fail(ctx, PP_CUDA_ERROR, "no CUDA device in this context");
+  if (!pts || dim < 1 || dim > 3 || kernel < 0 || kernel > 3)
+    return fail(ctx, PP_INVALID_ARG, "pp_hmatrix_construct_dev: bad argument");
+  if (kernel <= 1 ? !(p0 >= 0.0 && std::isfinite(p0)) : !(p0 > 0.0 && std::isfinite(p0)))
+    return fail(ctx, PP_INVALID_ARG, "pp_hmatrix_construct_dev: p0 out of range for the kernel");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (!h->d_arena) {
+    const size_t bytes = sizeof(double) * (size_t)std::max<int64_t>(h->H->arena_elems, 1);
+    PP_CUDA(h->dalloc((void**)&h->d_arena, bytes));
+    PP_CUDA(cudaMemsetAsync(h->d_arena, 0, bytes, s));
+  }
+  pp_status st = upload_rand(h);
+  if (st != PP_OK) return st;
+  st = pp_hmatrix_assemble_dense_dev(h, kernel, p0, shift, pts, dim, stream);
+  if (st != PP_OK) return st;
+  if (h->construct.built && (h->c_kernel != kernel || h->c_dim != dim || h->c_p0 != p0)) {
+    h->construct.release();
+    h->construct = VmPlan();
+  }
+  h->c_kernel = kernel;
+  h->c_dim = dim;
+  h->c_p0 = p0;
+  st = build_program(h, 2, 0, h->construct);
+  if (st != PP_OK) return st;
+  if (h->construct.n_tasks == 0) return PP_OK;  // no low-rank blocks
+  st = plan_to_device(h, h->construct);
+  if (st != PP_OK) return st;
+  // the program's right-hand-side arena holds the n x dim points
+  PP_CUDA(cudaMemcpyAsync(h->construct.d_rhs, pts, sizeof(double) * (size_t)h->H->n * dim, cudaMemcpyDeviceToDevice,
+                          s));
+  return launch_plan(h, h->construct, s, 0);
+}
+
 pp_status pp_kernel_residual_batch_dev(pp_context* ctx, int njobs, const pp_residual_job* jobs, void* stream) {
   if (!has_device(ctx)) return fail(ctx, PP_CUDA_ERROR, "no CUDA device in this context");
   if (njobs < 0 || (njobs > 0 && !jobs)) return fail(ctx, PP_INVALID_ARG, "kernel residual batch: bad argument");
@@ -815,12 +868,13 @@ pp_status pp_hmatrix_program_edges(pp_hmatrix* h, int which, int nrhs, int64_t* 
   if (st != PP_OK) return st;
   int64_t e = 0;
   std::vector<int64_t> lis;
+  const pp::dependency_table& deps = plan->prog.dep_table();
   for (int t = 0; t < plan->n_tasks; ++t) {
-    plan->prog.deps.getDepFrom(t, lis);
+    deps.getDepFrom(t, lis);
     for (int64_t s : lis) {
       from[e] = t;
       to[e] = s;
-      type[e] = (int32_t)plan->prog.deps.lookup(t, s);
+      type[e] = (int32_t)deps.lookup(t, s);
       ++e;
     }
   }

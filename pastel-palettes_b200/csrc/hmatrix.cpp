@@ -103,7 +103,6 @@ Hierarchical* Hierarchical::dense_tiled(int n, int leaf) {
   };
   h->root = build(0, n, 0, 0);
   h->add_inverses();
-  h->host.assign((size_t)h->arena_elems, 0.0);
   return h;
 }
 
@@ -194,15 +193,20 @@ Hierarchical* Hierarchical::geometric(int n, int dim, const double* pts, int lea
   };
   h->root = block(0, 0, 0);
   h->add_inverses();
-  h->host.assign((size_t)h->arena_elems, 0.0);
-  for (auto& nd : h->nodes)
-    if (nd.kind == HNode::LR) h->host[h->objs[nd.rank_obj].off] = nd.rank;
   return h;
+}
+
+void Hierarchical::ensure_host() const {
+  if (!host.empty() || arena_elems == 0) return;
+  host.assign((size_t)arena_elems, 0.0);
+  for (auto& nd : nodes)
+    if (nd.kind == HNode::LR && nd.rank_obj >= 0) host[objs[nd.rank_obj].off] = nd.rank;
 }
 
 int Hierarchical::stored_rank(int node) const {
   const HNode& nd = nodes.at(node);
   if (nd.kind != HNode::LR || nd.rank_obj < 0) return -1;
+  if (host.empty()) return nd.rank;
   return (int)host[objs[nd.rank_obj].off];
 }
 
@@ -211,7 +215,7 @@ void Hierarchical::set_rank_tolerance(double tol) {
   for (auto& nd : nodes)
     if (nd.kind == HNode::LR) {
       if (rank_tol > 0.0) nd.rank = nd.kmax;
-      else nd.rank = std::min(nd.kmax, std::max(0, (int)host[objs[nd.rank_obj].off]));
+      else if (!host.empty()) nd.rank = std::min(nd.kmax, std::max(0, (int)host[objs[nd.rank_obj].off]));
     }
 }
 
@@ -230,6 +234,7 @@ int Hierarchical::depth() const {
 void Hierarchical::set_dense(int id, const double* a, int lda) {
   const HNode& nd = nodes.at(id);
   if (nd.kind != HNode::D) throw std::invalid_argument("set_dense: block is not dense");
+  ensure_host();
   const StorageObj& o = objs[nd.obj];
   for (int i = 0; i < nd.m; ++i) std::memcpy(&host[o.off + (int64_t)i * o.ld], a + (int64_t)i * lda, sizeof(double) * nd.n);
 }
@@ -238,6 +243,7 @@ void Hierarchical::set_lowrank(int id, const double* U, int ldu, const double* V
   HNode& nd = nodes.at(id);
   if (nd.kind != HNode::LR) throw std::invalid_argument("set_lowrank: block is not low-rank");
   if (rank < 0 || rank > nd.kmax) throw std::invalid_argument("set_lowrank: rank exceeds kmax");
+  ensure_host();
   nd.rank = rank_tol > 0.0 ? nd.kmax : rank;
   if (nd.rank_obj >= 0 && !host.empty()) host[objs[nd.rank_obj].off] = rank;
   const StorageObj& ou = objs[nd.obj];
@@ -249,6 +255,7 @@ void Hierarchical::set_lowrank(int id, const double* U, int ldu, const double* V
 }
 
 void Hierarchical::to_dense(double* out) const {
+  ensure_host();
   for (const HNode& nd : nodes) {
     if (nd.kind == HNode::D) {
       const StorageObj& o = objs[nd.obj];

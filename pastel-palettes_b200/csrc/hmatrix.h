@@ -62,7 +62,10 @@ class Hierarchical {
   // inverses of the diagonal leaves' triangular factors, which the factorization writes and
   // the solves read (never uploaded, downloaded or restored)
   int64_t block_elems = 0;
-  std::vector<double> host;  // host image of the arena (filled by set_dense / set_lowrank)
+  // host image of the arena (filled by set_dense / set_lowrank), allocated at its first use
+  // (ensure_host): a matrix built on the device never needs one
+  mutable std::vector<double> host;
+  void ensure_host() const;
 
   // All-dense 2x2 partition of an n x n matrix down to blocks of <= leaf rows.
   static Hierarchical* dense_tiled(int n, int leaf);

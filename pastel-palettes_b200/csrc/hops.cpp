@@ -115,7 +115,9 @@ void Program::build_dag() {
   const int n = (int)tasks.size();
   succ.assign(n, {});
   pred.assign(n, {});
-  deps.clear();
+  pred_bits.assign(n, {});
+  deps_.clear();
+  deps_built_ = false;
   struct Acc { int task; Region r; };
   std::vector<std::vector<Acc>> acc(objs.size());
   std::vector<int> mark(n, -1), depbits(n, 0);
@@ -148,8 +150,8 @@ void Program::build_dag() {
     std::sort(touched.begin(), touched.end());
     for (int p : touched) {
       pred[t].push_back(p);
+      pred_bits[t].push_back((uint8_t)depbits[p]);
       succ[p].push_back(t);
-      deps.update(p, t, (dependency_t)depbits[p]);
       ++edges;
     }
   }
@@ -159,6 +161,16 @@ void Program::build_dag() {
     for (int s : succ[t]) b = std::max(b, blevel[s]);
     blevel[t] = b + std::max<int64_t>(tasks[t].flops, 1 << 14);
   }
+}
+
+const dependency_table& Program::dep_table() {
+  if (!deps_built_) {
+    deps_.clear();
+    for (size_t t = 0; t < pred.size(); ++t)
+      for (size_t q = 0; q < pred[t].size(); ++q) deps_.update(pred[t][q], (int64_t)t, (dependency_t)pred_bits[t][q]);
+    deps_built_ = true;
+  }
+  return deps_;
 }
 
 h_ops_dag Program::to_dag() const {
@@ -228,11 +240,14 @@ void Program::merge(const Program& o) {
   succ.resize(tasks.size());
   pred.resize(tasks.size());
   blevel.resize(tasks.size());
+  pred_bits.resize(tasks.size());
   for (size_t t = 0; t < o.tasks.size(); ++t) {
     for (int x : o.succ[t]) succ[task0 + t].push_back(x + task0);
     for (int x : o.pred[t]) pred[task0 + t].push_back(x + task0);
+    if (t < o.pred_bits.size()) pred_bits[task0 + t] = o.pred_bits[t];
     blevel[task0 + t] = o.blevel[t];
   }
+  deps_built_ = false;
   edges += o.edges;
 }
 
@@ -592,6 +607,83 @@ void Generator::solve_program(int nrhs) {
   trsmu(node(H_.root), asD(b));
 }
 
+// C := K(P_I, P_J) B in row blocks of at most 256 rows (one CTA each)
+void Generator::kmul(const View& C, const View& PI, const View& PJ, const View& B, int kernel, double p0) {
+  constexpr int kRows = 256;
+  for (int r = 0; r < C.m; r += kRows) {
+    const int h = std::min(kRows, C.m - r);
+    HTask& t = emit(PP_OP_KMUL);
+    bind(t, 0, C.sub(r, 0, h, C.n), true);
+    bind(t, 1, PI.sub(r, 0, h, PI.n), false);
+    bind(t, 2, PJ, false);
+    bind(t, 3, B, false);
+    t.t.m = h;
+    t.t.n = PJ.m;
+    t.t.k = C.n;
+    t.t.l = PI.n;
+    t.t.ctrl = kernel;
+    t.t.alpha = p0;
+    t.flops = (int64_t)h * PJ.m * (2 * C.n + 20);
+  }
+}
+
+void Generator::orth(const View& Y) {
+  HTask& o = emit(PP_OP_ORTH);
+  bind(o, 0, Y, true);
+  o.t.m = Y.m;
+  o.t.n = Y.n;
+  o.t.k = Y.n;
+  o.flops = 3 * (2LL * Y.m * Y.n * Y.n + (int64_t)Y.m * Y.n * Y.n);
+}
+
+void Generator::construct_program(int kernel, int dim, double p0, double tol) {
+  if (dim < 1 || dim > 3) throw std::invalid_argument("construct: dim must be 1..3");
+  rhs_obj_ = P_.add_obj(P_.arena_id(inst_, AR_RHS), H_.n, dim, false);
+  View pts;
+  pts.obj = rhs_obj_;
+  pts.m = H_.n;
+  pts.n = dim;
+  for (const HNode& nd : H_.nodes) {
+    if (nd.kind != HNode::LR) continue;
+    const int k = nd.kmax;
+    if (k > kAccumMaxK2 || k > nd.m || k > nd.n) throw std::runtime_error("construct: block rank above 32 or its size");
+    View U, V, R;
+    U.obj = node_obj_[nd.obj];
+    U.m = nd.m;
+    U.n = k;
+    V.obj = node_obj_[nd.objV];
+    V.m = nd.n;
+    V.n = k;
+    R.obj = rand_obj(k);
+    R.m = nd.n;
+    R.n = k;
+    const View PI = pts.sub(nd.r0, 0, nd.m, dim), PJ = pts.sub(nd.c0, 0, nd.n, dim);
+    kmul(U, PI, PJ, R, kernel, p0);  // U = K Omega
+    orth(U);
+    kmul(V, PJ, PI, U, kernel, p0);  // V = K^T U
+    orth(V);
+    kmul(U, PI, PJ, V, kernel, p0);  // U = K V   (one power step)
+    orth(U);
+    kmul(V, PJ, PI, U, kernel, p0);  // V = K^T U: U V^T = U U^T K
+    HTask& t = emit(PP_OP_LRTRUNC);
+    bind(t, 0, U, true);
+    bind(t, 1, V, true);
+    t.t.m = nd.m;
+    t.t.n = nd.n;
+    t.t.k = k;
+    t.t.o = H_.rank_tol > 0.0 ? k : nd.rank;
+    t.t.beta = tol;
+    if (nd.rank_obj >= 0) {
+      View rv;
+      rv.obj = node_obj_[nd.rank_obj];
+      rv.m = 1;
+      rv.n = 1;
+      bind(t, 5, rv, true);
+    }
+    t.flops = 2LL * (nd.m + nd.n) * k * k * 3;
+  }
+}
+
 void Generator::getrf(const Mat& A) {
   if (A.kind == Mat::LR) throw std::logic_error("getrf on a low-rank block");
   const int s = tri_split(A, T_);
@@ -783,6 +875,20 @@ void Generator::gemm_tiles(const View& C, const View& A, const View& B, int alph
       bind(t, 1, A, false);
       bind(t, 2, B, false);
     }
+    t.t.m = C.m;
+    t.t.n = C.n;
+    t.t.k = A.n;
+    t.t.alpha = (double)alpha;
+    t.t.beta = 1.0;
+    t.flops = 2LL * C.m * C.n * A.n;
+    return;
+  }
+  if (!solve_ && !work_target && C.m >= kBigLeaf && C.n >= kBigLeaf && A.n <= 64 && whole_leaf(C)) {
+    // a low-rank update of a whole large leaf: one pass over the leaf in one instruction
+    HTask& t = emit(PP_OP_GEMM);
+    bind(t, 0, C, true);
+    bind(t, 1, A, false);
+    bind(t, 2, B, false);
     t.t.m = C.m;
     t.t.n = C.n;
     t.t.k = A.n;

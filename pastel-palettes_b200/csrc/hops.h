@@ -82,9 +82,15 @@ class Program {
   std::vector<int64_t> arena_elems;  // per arena id
   // DAG over tasks (program order is topological)
   std::vector<std::vector<int>> succ, pred;
-  dependency_table deps;
+  std::vector<std::vector<uint8_t>> pred_bits;  // dependency_t bits of each pred edge
+  // the typed edges as the reference's dependency_table (rts/dependency.h), built on request
+  const dependency_table& dep_table();
   std::vector<int64_t> blevel;  // FLOP-weighted longest path to an exit
   int64_t edges = 0;
+ private:
+  dependency_table deps_;
+  bool deps_built_ = false;
+ public:
 
   int add_instance();  // returns instance id
   int add_obj(int arena, int rows, int cols, bool tracked = true);
@@ -154,6 +160,11 @@ class Generator {
   // emitted at its first use); the other instructions stay FP64
   void set_precision(int prec) { prec_ = prec; }
   void solve_program(int nrhs);    // B := U^-1 L^-1 B on the RHS object (n x nrhs)
+  // Device construction of the low-rank blocks from points (the RHS arena holds the n x dim
+  // points): per block a randomized range finder with one power step, U = orth(K Omega),
+  // V = K^T orth(K orth(K^T U)) ..., then truncation of U V^T to the singular values above
+  // `tol` times the largest (at most the block's rank); kernel as PP_OP_KMUL
+  void construct_program(int kernel, int dim, double p0, double tol);
   int rhs_obj() const { return rhs_obj_; }
 
   // building blocks (exposed for tests)
@@ -192,6 +203,8 @@ class Generator {
   bool whole_leaf(const View& v) const;
   int tri_limit(int target_extent) const;
   void trmv(int inv, int upper, int m, const View& B);
+  void kmul(const View& C, const View& PI, const View& PJ, const View& B, int kernel, double p0);
+  void orth(const View& Y);
   std::vector<std::pair<int, int>> inv_obj_;  // program obj of a diagonal leaf -> (L^-1, U^-1) objs
   bool inverse_of(const Mat& T, int& invL, int& invU) const;
   void emit_inverses();

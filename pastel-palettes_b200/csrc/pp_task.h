@@ -47,7 +47,17 @@ enum pp_op {
                         X(r, c) = p[1][r * ld[1] + c] (or p[1][c * ld[1] + r] with PP_T(1)),
                         rounded to BF16 and written at p[0] in the tiled layout below (m a
                         multiple of 128, k of 64); no reference counterpart                   */
-  PP_OP_COUNT = 16
+  PP_OP_KMUL = 16,   /* C[m x k] (p[0]) := K(P_I, P_J) B: a kernel matrix evaluated from points
+                        times B (p[3], n x k, k <= 32); P_I = p[1] (m points), P_J = p[2] (n
+                        points), rows of dim = l coordinates (ld[1], ld[2]); kernel ctrl (0
+                        1/(r + p0), 1 Laplace, 2 exp(-r/p0), 3 Matern-3/2), p0 = alpha; no
+                        diagonal shift (the blocks it serves are admissible: disjoint rows and
+                        columns).  Randomized compression on the device; no reference
+                        counterpart (the reference's matrices come from a Java compressor)   */
+  PP_OP_LRTRUNC = 17,/* U V^T (U = p[0] m x k with orthonormal columns, V = p[1] n x k) := its
+                        best rank-r form, r the singular values above beta times the largest
+                        (at most o), columns beyond r zero; r written to p[5] when set          */
+  PP_OP_COUNT = 18
 };
 
 /* flags: bit (4+i) = operand i is stored transposed (operand 0 is the target). */

@@ -1599,7 +1599,7 @@ __device__ __noinline__ void jacobi_eig(double* G, double* Z, int k, double* cs,
 // times S^T is its coordinates in the kept singular directions.  Returns r.
 template <int KB>
 __device__ __noinline__ int accum_truncate(const double* G, const double* Z, int k, double tol, double* S, int lds,
-                                           int* perm) {
+                                           int* perm, int rmax = PP_VM_MAX_RANK) {
   if (threadIdx.x == 0) {
     for (int i = 0; i < k; ++i) perm[i] = i;
     for (int i = 0; i < k; ++i) {
@@ -1613,7 +1613,7 @@ __device__ __noinline__ int accum_truncate(const double* G, const double* Z, int
     const double l0 = G[perm[0] * ACC_LG + perm[0]];
     int r = 0;
     if (l0 > 0.0)
-      while (r < k && G[perm[r] * ACC_LG + perm[r]] > tol * tol * l0) ++r;
+      while (r < k && r < rmax && G[perm[r] * ACC_LG + perm[r]] > tol * tol * l0) ++r;
     perm[KB] = r;
   }
   __syncthreads();
@@ -1688,6 +1688,39 @@ __device__ __forceinline__ void orth_impl(double* Y, int m, int k, double* smem)
   accum_cholqr<KB, true>(Y, m, k, false, G, red);
   accum_cholqr<KB, true>(Y, m, k, false, G, red);
 }
+
+// U V^T (U: m x k orthonormal columns, V: n x k, both global) := its best rank-r form: the
+// singular values are those of V; rotate both factors into the eigenbasis of V^T V (Jacobi)
+// and keep the directions above tol times the largest (at most rmax), as ACCUM's adaptive form
+template <int KB>
+__device__ __forceinline__ void lrtrunc_impl(const pp_task& T, double* smem) {
+  using SM = AccumSmem<KB>;
+  constexpr int LS = 2 * KB;
+  double *U = T.p[0], *V = T.p[1];
+  const int lu = T.ld[0], lv = T.ld[1], m = T.m, n = T.n, k = T.k;
+  double* red = smem;
+  double* S = red + SM::RED;
+  double* G = S + SM::S;
+  accum_tn_any<KB, true, true>(V, lv, k, V, lv, false, k, nullptr, 0, false, 0, n, G, nullptr, ACC_LG, red);
+  double* Z = red;
+  double* cs = red + KB * ACC_LG;
+  double* flag = cs + 2 * KB;
+  int* pq = reinterpret_cast<int*>(flag + 2);
+  jacobi_eig(G, Z, k, cs, pq, flag);
+  const int r = accum_truncate<KB>(G, Z, k, T.beta, S, LS, pq, T.o > 0 ? T.o : k);
+  accum_rows_any<KB, true>(V, lv, V, lv, k, nullptr, 0, false, 0, 1.0, S, S, LS, k, n);
+  accum_rows_any<KB, true>(U, lu, U, lu, k, nullptr, 0, false, 0, 1.0, S, S, LS, k, m);
+  __syncthreads();
+  if (threadIdx.x == 0 && T.p[5]) T.p[5][0] = (double)r;
+  __syncthreads();
+}
+
+__device__ __noinline__ void dev_lrtrunc(const pp_task& T, double* smem) {
+  if (T.k <= 16) lrtrunc_impl<16>(T, smem);
+  else lrtrunc_impl<32>(T, smem);
+}
+
+__device__ __noinline__ void dev_kmul(const pp_task& T, double* smem);
 
 __device__ __noinline__ void dev_orth(double* Y, int m, int k, double* smem) {
   if (k <= 16) orth_impl<16>(Y, m, k, smem);
@@ -1793,6 +1826,15 @@ __device__ bool run_task(const pp_task& T, double* smem, TcCtx& tc, int& err) {
       return true;
     case PP_OP_COPY:
       dev_copy(T.p[0], T.ld[0], T.p[1], T.ld[1], T.m, T.n);
+      return true;
+    case PP_OP_KMUL:
+      if (T.k < 1 || T.k > PP_VM_MAX_RANK || T.l < 1 || T.l > 3 || T.ctrl < 0 || T.ctrl > 3 || T.m < 0 || T.n < 0)
+        return false;
+      dev_kmul(T, smem);
+      return true;
+    case PP_OP_LRTRUNC:
+      if (T.k < 1 || T.k > PP_VM_MAX_RANK || T.m < T.k || T.n < T.k) return false;
+      dev_lrtrunc(T, smem);
       return true;
     case PP_OP_SHADOW:
       if (T.m < 128 || T.m % 128 || T.k < 64 || T.k % 64) return false;
@@ -2014,6 +2056,62 @@ __device__ __forceinline__ double kernel_eval_nr(double d2, double p0, double in
   if (KIND == 2) return exp(-d * inv_p0);
   const double s = 1.7320508075688772 * d * inv_p0;
   return (1.0 + s) * exp(-s);
+}
+
+// C[m x k] = K(P_I, P_J) B (PP_OP_KMUL): a thread per row of C, the columns j of the kernel
+// matrix in chunks of KM_JC whose points and B rows are staged in shared memory (read by all
+// threads as broadcasts); points padded to three coordinates with zeros
+#define KM_JC 128
+template <int KIND>
+__device__ __noinline__ void kmul_impl(const pp_task& T, double* smem) {
+  const int m = T.m, n = T.n, k = T.k, dim = T.l;
+  const double p0 = T.alpha, inv_p0 = KIND >= 2 ? 1.0 / p0 : 0.0;
+  double* C = T.p[0];
+  const double *PI = T.p[1], *PJ = T.p[2], *B = T.p[3];
+  const int ldc = T.ld[0], ldi = T.ld[1], ldj = T.ld[2], ldb = T.ld[3];
+  double* sp = smem;               // KM_JC x 3
+  double* sb = smem + KM_JC * 3;   // KM_JC x PP_VM_MAX_RANK
+  for (int r0 = 0; r0 < m; r0 += NT) {
+    const int r = r0 + threadIdx.x;
+    double pr[3] = {0.0, 0.0, 0.0};
+    if (r < m)
+      for (int d = 0; d < dim; ++d) pr[d] = ldcg(&PI[(size_t)r * ldi + d]);
+    double acc[PP_VM_MAX_RANK];
+#pragma unroll
+    for (int c = 0; c < PP_VM_MAX_RANK; ++c) acc[c] = 0.0;
+    for (int j0 = 0; j0 < n; j0 += KM_JC) {
+      const int jc = min(KM_JC, n - j0);
+      __syncthreads();
+      for (int e = threadIdx.x; e < KM_JC * 3; e += NT) {
+        const int j = e / 3, d = e % 3;
+        sp[e] = (j < jc && d < dim) ? ldcg(&PJ[(size_t)(j0 + j) * ldj + d]) : 0.0;
+      }
+      for (int e = threadIdx.x; e < jc * PP_VM_MAX_RANK; e += NT) {
+        const int j = e / PP_VM_MAX_RANK, c = e % PP_VM_MAX_RANK;
+        sb[e] = c < k ? ldcg(&B[(size_t)(j0 + j) * ldb + c]) : 0.0;
+      }
+      __syncthreads();
+      for (int j = 0; j < jc; ++j) {
+        const double u0 = pr[0] - sp[3 * j], u1 = pr[1] - sp[3 * j + 1], u2 = pr[2] - sp[3 * j + 2];
+        const double d2 = fma(u2, u2, fma(u1, u1, u0 * u0));
+        const double a = kernel_eval_nr<KIND>(d2, p0, inv_p0);
+#pragma unroll
+        for (int c = 0; c < PP_VM_MAX_RANK; ++c) acc[c] = fma(a, sb[j * PP_VM_MAX_RANK + c], acc[c]);
+      }
+    }
+    if (r < m)
+      for (int c = 0; c < k; ++c) C[(size_t)r * ldc + c] = acc[c];
+  }
+  __syncthreads();
+}
+
+__device__ __noinline__ void dev_kmul(const pp_task& T, double* smem) {
+  switch (T.ctrl) {
+    case 0: kmul_impl<0>(T, smem); break;
+    case 1: kmul_impl<1>(T, smem); break;
+    case 2: kmul_impl<2>(T, smem); break;
+    default: kmul_impl<3>(T, smem); break;
+  }
 }
 
 #define KR_THREADS 128
