@@ -35,7 +35,8 @@
 #define NT PP_VM_THREADS
 #define TL PP_VM_TILE
 #define LDS (PP_VM_TILE + 1)   /* padded smem row stride (doubles) */
-#define VM_SMEM_BYTES 163840   /* one CTA per SM: ACCUM keeps its ny x k1 sketch on chip */
+#define VM_SMEM_BYTES 180224   /* 176 KB, one CTA per SM: ACCUM keeps its ny x k1 sketch on chip;
+                                  the BF16 GEMM holds 3 stages of 48 KB + its epilogue's buffers */
 
 namespace {
 
@@ -282,6 +283,10 @@ __device__ __forceinline__ void dev_gemm(double* __restrict__ C, int ldc, const 
   else if (n == 1) gemm_cfg<256, 1, 1, 1, 16>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
   else if (n <= 16) gemm_cfg<128, 16, 8, 1, 32>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
   else if (m <= 16) gemm_cfg<16, 128, 1, 8, 32>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
+  // tall or wide skinny products over a long k (a dense block times a low-rank factor): 10 loads
+  // in flight per thread, 16 FMAs per thread and k step
+  else if (n <= 32 && m >= 128) gemm_cfg<128, 32, 4, 4, 16>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
+  else if (m <= 32 && n >= 128) gemm_cfg<32, 128, 4, 4, 16>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
   else if (m > 64 && n > 64) gemm_cfg<128, 128, 8, 8, 8>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
   else gemm_cfg<64, 64, 4, 4, 32>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
 }
@@ -639,7 +644,11 @@ __device__ __noinline__ bool dev_gemm_bf16(double* __restrict__ C, int ldc, cons
       }
     }
   } else if (warp >= 4) {  // epilogue
+    // per warp a 32 x 32 FP32 transpose buffer (row stride 33: conflict-free both ways): the
+    // warp reads its 32 accumulator rows from TMEM (a thread per row), then updates C a row at
+    // a time with the lanes along the columns, so every load and store of C is coalesced
     const int qd = warp & 3;
+    float* tb = reinterpret_cast<float*>(sbase + (stage0 - s0) + BG_STAGES * BG_STAGE_BYTES) + qd * (32 * 33);
     uint32_t u = tc.u;
     for (int t = 0; t < tiles; ++t, ++u) {
       const uint32_t b = u & 1u;
@@ -647,8 +656,7 @@ __device__ __noinline__ bool dev_gemm_bf16(double* __restrict__ C, int ldc, cons
       if (__any_sync(0xffffffffu, !ok)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const int i0 = (t / tiles_n) << 7, j0 = (t % tiles_n) * BG_TILE_N;
-      const int row = i0 + 32 * qd + lane;
-      double* crow = C + (size_t)row * ldc + j0;
+      double* cblk = C + (size_t)(i0 + 32 * qd) * ldc + j0 + lane;
 #pragma unroll 1
       for (int p = 0; p < BG_TILE_N / 32; ++p) {
         uint32_t v[32];
@@ -663,26 +671,22 @@ __device__ __noinline__ bool dev_gemm_bf16(double* __restrict__ C, int ldc, cons
               "=r"(v[30]), "=r"(v[31])
             : "r"(taddr)
             : "memory");
-        double cv[32];
-        if (beta != 0.0) {
-#pragma unroll
-          for (int c = 0; c < 32; c += 2) {
-            const double2 x = __ldcg(reinterpret_cast<const double2*>(crow + 32 * p + c));
-            cv[c] = x.x;
-            cv[c + 1] = x.y;
-          }
-        } else {
-#pragma unroll
-          for (int c = 0; c < 32; ++c) cv[c] = 0.0;
-        }
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-        for (int c = 0; c < 32; c += 2) {
-          double2 y;
-          y.x = fma(alpha, (double)__uint_as_float(v[c]), cv[c]);
-          y.y = fma(alpha, (double)__uint_as_float(v[c + 1]), cv[c + 1]);
-          *reinterpret_cast<double2*>(crow + 32 * p + c) = y;
+        for (int c = 0; c < 32; ++c) tb[lane * 33 + c] = __uint_as_float(v[c]);
+        __syncwarp();
+        // this piece's C columns, row by row: 16 coalesced loads in flight, then their stores
+#pragma unroll 1
+        for (int r0 = 0; r0 < 32; r0 += 16) {
+          double cv[16];
+          double* cp = cblk + 32 * p + (size_t)r0 * ldc;
+#pragma unroll
+          for (int rr = 0; rr < 16; ++rr) cv[rr] = beta != 0.0 ? __ldcg(cp + (size_t)rr * ldc) : 0.0;
+#pragma unroll
+          for (int rr = 0; rr < 16; ++rr)
+            cp[(size_t)rr * ldc] = fma(alpha, (double)tb[(r0 + rr) * 33 + lane], cv[rr]);
         }
+        __syncwarp();
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       __syncwarp();
