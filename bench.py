@@ -1,15 +1,18 @@
 #!/usr/bin/env python
-"""bench.py — H-LU factor+solve/s at <= 1e-10 backward error (FP64 HODLR, N = 8192).
+"""bench.py — H-LU factor+solve/s at <= 1e-10 residual, mixed precision vs FP64.
 
-Workload: the H-matrix of kernel 1/(r+1e-3) on 8192 Morton-sorted points of U[0,1]^2,
-diagonal shifted by 2 * max off-diagonal row sum, weak admissibility, leaf 256, rank 16.
-One "step" processes a batch of such factor+solve jobs in merged persistent launches:
-restore every instance, batched H-LU factorization, then batched solves + FP64 iterative
-refinement until ||b - Ax||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= 1e-10 for every job;
-the step is captured once as a CUDA graph and replayed.  Inputs are synthetic and seeded.
-Multi-GPU: independent replicas, one per rank (no collective on the data path).
+Headline workload (the mixed-precision + iterative-refinement configuration): N = 65536 points
+of U[0,1]^3 in Morton order, Laplace kernel 1/(4 pi (r + 1e-3)), diagonal shifted by 2 x the
+largest off-diagonal row sum, standard admissibility eta = 1, leaf 512, adaptive rank <= 32 at
+1e-8, 8 right-hand sides, refined in FP64 to a normwise backward error <= 1e-10.  The H-matrix is
+built on the device from the points.  A "step" is one job: restore the matrix, factor, solve
+and refine.  Two forms of the same job: the mixed form (Schur updates of the 512 leaves on the
+tensor cores from BF16 shadows, FP32 accumulation; GETRF, TRSM, low-rank work and the refinement
+residual in FP64) is the headline `value`; the plain FP64 form is timed beside it (`forms`).
+Further legs: the FP64 HODLR batch (N = 8192, 64 jobs per merged launch), the serving loop.
+Inputs are synthetic and seeded.  Multi-GPU: independent replicas, one per rank.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl ours|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
 import argparse
 import importlib.util
@@ -23,11 +26,15 @@ import time
 import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
+METRIC = "H-LU factor+solve/s at 1e-10 residual, mixed vs FP64"
+C3 = dict(n=65536, dim=3, kernel="laplace", p0=1e-3, leaf=512, admissibility=1, eta=1.0, kmax=32, rank_tol=1e-8,
+          nrhs=8, tol=1e-10, seed=1234, gemm_tile=128)
+C3_NAME = "laplace3d-n65536-leaf512-eta1-rank32tol1e-8-8rhs-bf16schur-fp64ir1e-10"
+# the FP64 HODLR batch leg
 WORKLOAD = dict(n=8192, dim=2, kernel="inv", p0=1e-3, leaf=256, rank=16, admissibility=0, seed=1234, tol=1e-10)
 WORKLOAD_NAME = "hodlr-inv2d-n8192-leaf256-rank16-fp64-ir1e-10"
-METRIC = "H-LU factor+solve/s at 1e-10 residual (FP64 HODLR N=8192)"
-# DRAM bytes (read + write) of one job's factor work inside the batched factor launch, from one
-# ncu capture of the batch-4 launch (dram__bytes.sum.per_second x gpu__time_duration.sum / 4);
+# DRAM bytes (read + write) of one job's factor work inside the batched HODLR factor launch, from
+# one ncu capture of the batch-4 launch (dram__bytes.sum.per_second x gpu__time_duration.sum / 4);
 # the jobs touch disjoint arenas, so the launch's traffic scales with the batch
 FACTOR_DRAM_BYTES_PER_JOB = 117.5e6
 
@@ -113,6 +120,8 @@ def program_bytes(pp, h, which=0, nrhs=1):
             e = 2 * m * n + m * m // 2
         elif op == 3:
             e = 2 * m * n + n * n // 2
+        elif op == 6 and int(t["prec"]) == 2:  # BF16 shadows (2 bytes per element) into FP64 C
+            e = (2 if t["beta"] != 0 else 1) * m * n + (m * k + k * n) // 4
         elif op == 6:
             e = (2 if t["beta"] != 0 else 1) * m * n + m * k + k * n
         elif op == 9:
@@ -129,9 +138,13 @@ def program_bytes(pp, h, which=0, nrhs=1):
             e = m * m // 2 + 2 * m * n
         elif op in (13, 14):  # ORTH (in place) / COPY: m x n read and written
             e = 2 * m * n
+        elif op == 15:  # SHADOW: m x k FP64 read, m x k BF16 written
+            e = m * k + m * k // 4
         else:
             e = 0
         total += 8 * e
+    sel = (tasks["op"] == 6) & (tasks["prec"] == 2)
+    info = dict(info, bf16_flops=float((2 * tasks["m"][sel].astype(np.int64) * tasks["n"][sel] * tasks["k"][sel]).sum()))
     return total, info
 
 
@@ -199,22 +212,24 @@ def config_keys(batch, precision, world):
 
 
 def run_reference_arm(args, rank, world):
+    """The reference's CPU path on the headline job, on rank 0: each step one estimate of the job
+    from the census sample (reference_c3_seconds); value = 1 / median."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    times, iters, job = reference_cpu_jobs(args.warmup + args.steps, threads)
+    C3["n"] = args.n
+    times, desc = [], ""
+    for _ in range(args.warmup + args.steps):
+        t, desc = reference_c3_seconds(threads)
+        times.append(t)
     t = times[args.warmup:]
     value = 1.0 / float(np.median(t))
-    sample = (f"one job of the batch per step ({len(t)} steps after {args.warmup} warm-up; value = 1 / median): "
-              f"the workload's reference-ISA factor program ({len(job.tasks)} instructions, fixture "
-              f"tests/golden/hodlr8192_refisa_program.npz) on the oracle's restated reference routines over its "
-              f"DAG with {threads} threads, the oracle's substitution solve, FP64 refinement ({iters} solves)")
     line = {"metric": METRIC, "value": value, "unit": "factor+solve/s", "impl": "reference", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.median(t)),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config_keys(args.batch, "fp64", world),
+            "config": c3_config_keys(world),
             "cpu_baseline": {"value": value, "unit": "factor+solve/s", "cores": threads, "kind": "port",
-                             "sample": sample},
+                             "sample": f"one estimate per step, value = 1 / median over {len(t)} steps: " + desc},
             "e2e": {"value": value, "unit": "factor+solve/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -425,41 +440,200 @@ def uneven_batch_leg(pp, ctx, n_inst, steps, warmup, seed=4096, smin=1024, smax=
                         "adaptive rank <= 24 @ 1e-7, TF32 GEMMs + FP64 refinement, one merged launch, graph replay"}
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--batch", type=int, default=64, help="jobs per merged launch")
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "tf32"],
-                    help="factor GEMM precision of the headline form (tf32: tensor cores + FP64 refinement)")
-    ap.add_argument("--compare", type=int, default=1, help="also time the other precision form")
-    ap.add_argument("--serve-requests", type=int, default=16, help="requests of the serving leg (0: skip)")
-    ap.add_argument("--autotune", type=int, default=1, help="pick tile and grid of the batch by timing")
-    ap.add_argument("--gemm-tile", type=int, default=0, help="product tile edge (64 or 128) when not autotuning")
-    ap.add_argument("--uneven", type=int, default=0, help="instances of the configuration-4 style uneven batch "
-                                                           "leg (0: skip; host construction takes minutes)")
-    ap.add_argument("--serve-rate", type=float, default=40.0, help="Poisson arrival rate of the serving leg (1/s)")
-    args = ap.parse_args()
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference":  # the oracle alone: this library is not loaded
-        run_reference_arm(args, rank, world)
-        return
-    pp = load_pp()
+# ----------------------------------------------------------------------------- headline job
+def c3_config_keys(world):
+    return {"workload": C3_NAME, **C3, "batch": 1,
+            "precision": "mixed: bf16 schur updates of the 512 leaves (fp32 accumulation); fp64 getrf, trsm, "
+                         "low-rank work and refinement residual",
+            "comparison": "plain fp64 form of the same job (forms.fp64)",
+            "construction": "on the device from the points (dense blocks assembled, low-rank blocks by a "
+                            "randomized range finder), before the clock for value, inside it for e2e",
+            "l2": "not flushed: the 29 GB matrix and its 29 GB original are far larger than L2",
+            "parallelism": f"replicas{world}"}
 
-    import torch
-    import torch.distributed as dist
-    from datetime import timedelta
-    torch.cuda.set_device(local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+class C3Job:
+    """One job of the headline workload on this rank's GPU (seed offset by rank): the H-matrix built
+    on the device from its points, its original kept for restores, 8 right-hand sides."""
+
+    def __init__(self, pp, ctx, torch, s, rank):
+        self.pp, self.ctx, self.torch, self.s = pp, ctx, torch, s
+        c = C3
+        t0 = time.perf_counter()
+        with torch.cuda.stream(s):
+            self.h, self.prob = pp.make_kernel_problem(ctx, c["n"], c["dim"], c["kernel"], c["p0"], c["leaf"],
+                                                       c["kmax"], c["admissibility"], c["eta"], seed=c["seed"] + rank,
+                                                       rank_tol=c["rank_tol"], construct="device", stream=s)
+            self.h.sync(s)
+            self.h.keep_original(s)
+        s.synchronize()
+        self.setup_s = time.perf_counter() - t0
+        self.h.set_gemm_tile(c["gemm_tile"])
+        self.b = torch.from_numpy(pp.rhs(c["n"], c["nrhs"], seed=7 + rank)).cuda()
+        self.rank = rank
+
+    def run_form(self, prec, steps, warmup, barrier):
+        """restore + factor + refinement to the tolerance, device-timed per step (CUDA events on
+        the job's stream); the factor launch is timed inside the same steps."""
+        pp, torch, h, s = self.pp, self.torch, self.h, self.s
+        h.set_precision(prec)
+        t0 = time.perf_counter()
+        info = h.program_info(0)
+        build_s = time.perf_counter() - t0
+        fbytes, finfo = program_bytes(pp, h, 0)
+        ref = pp.Refiner(h, self.ctx, self.prob, stream=s)
+        tol = C3["tol"]
+        with torch.cuda.stream(s):
+            for _ in range(warmup):
+                h.restore(s)
+                h.factor(s)
+                ref.solve(self.b, tol=tol)
+        h.sync(s)
+        barrier()
+        l0 = ref.launches
+        tot, fac, rfn, worst, iters = 0.0, [], [], 0.0, 0
+        for _ in range(steps):
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            with torch.cuda.stream(s):
+                ev[0].record(s)
+                h.restore(s)
+                ev[1].record(s)
+                h.factor(s)
+                ev[2].record(s)
+                _, hist = ref.solve(self.b, tol=tol)
+                ev[3].record(s)
+            ev[3].synchronize()
+            tot += ev[0].elapsed_time(ev[3]) / 1e3
+            fac.append(ev[1].elapsed_time(ev[2]))
+            rfn.append(ev[2].elapsed_time(ev[3]))
+            worst = max(worst, hist[-1])
+            iters = len(hist)
+        h.sync(s)
+        barrier()
+        if worst > tol:
+            raise SystemExit(f"a timed step ended above {tol}: {worst}")
+        return {"total_s": tot, "ms_per_step": 1e3 * tot / steps, "steps": steps, "warmup": warmup,
+                "factor_ms": float(np.median(fac)), "refine_ms": float(np.median(rfn)), "refinement_solves": iters,
+                "worst_backward_error": worst, "factor_tasks": info["n_tasks"], "factor_flops": info["flops"],
+                "factor_bytes": fbytes, "bf16_flops": finfo["bf16_flops"], "program_build_s": build_s,
+                "gpu_launches_per_step": 2 + (ref.launches - l0) / max(1, steps)}
+
+    def e2e(self, prec, steps, barrier):
+        """End to end from host buffers: points and right-hand sides up from pinned host memory,
+        the off-diagonal row sums (diagonal shift), the H-matrix built on the device, factor,
+        refinement, solutions down; one warm-up step, then `steps` timed."""
+        pp, torch, h, s, prob = self.pp, self.torch, self.h, self.s, self.prob
+        h.set_precision(prec)
+        pts_host = torch.from_numpy(np.ascontiguousarray(prob.points)).pin_memory()
+        b_host = self.b.cpu().pin_memory()
+        x_host = torch.empty_like(b_host).pin_memory()
+        pts_dev = torch.empty(pts_host.shape, dtype=torch.float64, device="cuda")
+        b_dev = torch.empty(b_host.shape, dtype=torch.float64, device="cuda")
+        ref = pp.Refiner(h, self.ctx, prob, stream=s)
+        tot = 0.0
+        barrier()
+        for i in range(steps + 1):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(s):
+                e0.record(s)
+                pts_dev.copy_(pts_host, non_blocking=True)
+                b_dev.copy_(b_host, non_blocking=True)
+                off = pp.offdiag_rowsum_max_dev(self.ctx, pts_dev, prob.kernel, prob.p0, s)
+                if abs(2.0 * off - prob.shift) > 1e-9 * prob.shift:
+                    raise SystemExit("e2e: the diagonal shift differs from the job's")
+                h.construct(prob, pts_dev, s)
+                h.factor(s)
+                x, hist = ref.solve(b_dev, tol=C3["tol"])
+                x_host.copy_(x, non_blocking=True)
+                e1.record(s)
+            e1.synchronize()
+            if hist[-1] > C3["tol"]:
+                raise SystemExit("e2e step ended above the tolerance")
+            if i > 0:
+                tot += e0.elapsed_time(e1) / 1e3
+        h.sync(s)
+        barrier()
+        # leave the matrix as the other forms expect it: the original is still kept on the device
+        n, d, r = prob.n, prob.dim, self.b.shape[1]
+        return {"total_s": tot, "steps": steps, "h2d": 8 * n * (d + r), "d2h": 8 * n * r,
+                "mode": "one job at a time through the C ABI: points and right-hand sides up from pinned host "
+                        "memory, row sums for the diagonal shift, H-matrix built on the device (dense blocks "
+                        "assembled, low-rank blocks compressed), mixed factor, FP64 refinement, solutions down"}
+
+    def roofline(self, mixed, fp64):
+        hbm_peak, peak_kind = peaks()
+        fac_s = mixed["factor_ms"] / 1e3
+        achieved = mixed["factor_bytes"] / fac_s / 1e9
+        out = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+               "traffic": None, "kernel": "vm_kernel (mixed factor launch, one job)", "launch_ms": 1e3 * fac_s,
+               "algorithmic_bytes": mixed["factor_bytes"],
+               "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"}
+        bf16_peak = bf16_peak_tflops()
+        tc = mixed["bf16_flops"] / fac_s / 1e12
+        out["tensor"] = {"achieved_tflops": tc, "peak_tflops": bf16_peak, "frac": tc / bf16_peak,
+                         "flops": mixed["bf16_flops"], "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained "
+                                                                      "(the launch runs for seconds)"}
+        if fp64:
+            fp64_peak = fp64_peak_tflops(self.torch)
+            f = fp64["factor_flops"] / (fp64["factor_ms"] / 1e3) / 1e12
+            out["fp64_form"] = {"achieved_tflops": f, "peak_tflops": fp64_peak, "frac": f / fp64_peak,
+                                "launch_ms": fp64["factor_ms"],
+                                "peak_source": "measured in this run: torch float64 matmul 8192^3"}
+        return out
+
+    def release(self):
+        """Frees the job's device memory (the matrix, its original and the plans)."""
+        self.h = self.prob = self.b = None
+        import gc
+        gc.collect()
+        self.torch.cuda.empty_cache()
+
+
+def bf16_peak_tflops():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d.get("bf16_tflops_sustained", d.get("bf16_tflops", 1400.0))
+    return 1400.0
+
+
+def reference_c3_seconds(threads):
+    """The reference's CPU path on the headline job, estimated from a bounded sample: every
+    instruction class of the job's plain FP64 factorization and solve programs (the census
+    fixture) timed on the oracle's restated reference routines and weighted by its count, plus one
+    FP64 matrix-free residual (timed on a 1024-row slab of the kernel matrix times the 8 right-hand
+    sides, scaled to N rows); one refinement solve, as the FP64 form needs.  Host threads assumed
+    to scale ideally.  Returns (seconds per job, description)."""
+    import oracle.census as oc
+    from oracle.hodlr import distances, kernel_eval
+    tf, d0 = oc.program_seconds(0, threads)
+    ts, d1 = oc.program_seconds(1, threads)
+    n, nrhs = C3["n"], C3["nrhs"]
+    rng = np.random.default_rng(C3["seed"])
+    pts = rng.uniform(0.0, 1.0, (n, C3["dim"]))
+    x = rng.standard_normal((n, nrhs))
+    slab = 1024
+    t0 = time.perf_counter()
+    K = kernel_eval(1, distances(pts[:slab], pts), C3["p0"])
+    _ = K @ x
+    tr = (time.perf_counter() - t0) * (n / slab) / threads
+    total = tf + ts + tr
+    desc = (f"estimate from a bounded sample ({threads} threads assumed to scale ideally): the job's FP64 "
+            f"factor program ({d0['instructions']} instructions in {d0['classes']} classes, "
+            f"{d0['flops'] / 1e12:.1f} TFLOP) and 8-RHS solve program ({d1['instructions']} instructions) from "
+            f"tests/golden/c3_census.npz, every class timed once on the oracle's restated reference routines "
+            f"and weighted by its count ({tf:.0f} s + {ts:.1f} s), plus one residual from a timed 1024-row slab "
+            f"of the kernel matrix ({tr:.1f} s)")
+    return total, desc
+
+
+def c2_batch_leg(args, pp, ctx, torch, dist, rank, world, barrier, s):
+    """The FP64 HODLR batch: 64 jobs of the N = 8192 configuration (copies of one seeded matrix,
+    distinct right-hand sides) per merged persistent launch; restore + factor + refinement solves
+    captured as one CUDA graph and replayed; L2 flushed between steps.  Returns its JSON object."""
     tol = WORKLOAD["tol"]
     B = args.batch
-    ctx = pp.Context(device=local)
     hs, probs = make_batch(pp, ctx, B, rank)
     s = torch.cuda.Stream()
     with torch.cuda.stream(s):
@@ -472,11 +646,6 @@ def main():
     b_host = [torch.from_numpy(pp.rhs(n, 1, seed=7 + i)).pin_memory() for i in range(B)]
     bs = [x.cuda() for x in b_host]
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MiB > L2
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
 
     def run_form(prec, clk=None):
         """Device-timed steps of one precision form: batched restore + factor + refinement
@@ -534,8 +703,7 @@ def main():
     if args.compare:
         bt, _, gc, _, cmp_stats = run_form(forms[other])
         del gc, bt
-    with Clocks(local) as clk:
-        batch, ref, g, out, main_stats = run_form(forms[args.precision])
+    batch, ref, g, out, main_stats = run_form(forms[args.precision])
     iters = main_stats["refinement_solves"]
     total_max = main_stats["total_s"]
     value = main_stats["value"]
@@ -619,11 +787,6 @@ def main():
                          "frac": B * finfo["flops"] / fac_s / 1e12 / fp64_peak,
                          "peak_source": "measured in this run: torch float64 matmul 8192^3"}}
 
-    uneven = uneven_batch_leg(pp, ctx, args.uneven, max(3, args.steps // 2), args.warmup) if args.uneven > 0 else None
-    serving = None
-    if args.serve_requests > 0:
-        serving = serving_leg(pp, ctx, args.serve_requests, args.serve_rate, seed=2024 + rank)
-
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -632,32 +795,110 @@ def main():
                "sample": f"5 jobs of the workload after 1 warm-up, value = 1 / median: the reference-ISA factor "
                          f"program on the oracle's restated reference routines over its DAG ({threads} threads), "
                          f"the oracle's substitution solve, FP64 refinement ({its} solves)"}
+    del g, g2
+    return {"metric": "H-LU factor+solve/s at 1e-10 residual (FP64 HODLR N=8192, batch of 64)", "value": value,
+            "unit": "factor+solve/s", "ms_per_step": 1e3 * total_max / args.steps, "steps": args.steps,
+            "forms": {args.precision: {k: v for k, v in main_stats.items() if k != "total_s"},
+                      **({other: {k: v for k, v in cmp_stats.items() if k != "total_s"}} if cmp_stats else {})},
+            "config": config_keys(B, args.precision, world),
+            "details": {"graph": "restore+factor+solves captured", "factor_tasks_per_job": finfo["n_tasks"],
+                        "factor_flops_per_job": finfo["flops"], "refinement_solves": iters,
+                        "single_job_step_ms": float(np.median(lat))},
+            "e2e": {"value": e2e_value, "unit": "factor+solve/s", "h2d_bytes_per_step": B * (hs[0].arena_bytes() + 8 * n),
+                    "d2h_bytes_per_step": B * 8 * n, "mode": e2e_mode, "serial_value": e2e_serial,
+                    "serial_mode": "one step at a time: upload, factor + refinement, download, then the next"},
+            "roofline": roofline, "cpu_baseline": cpu,
+            "plain_fp64_single_instance": {
+                "value": 1e3 / float(np.median(lat)), "unit": "factor+solve/s",
+                "note": "one job per persistent launch, FP64, refinement to the same tolerance (the reference's "
+                        "execution model: one DAG per launch)"},
+            "gpu_launches_per_step": launches_per_step}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fp64-steps", type=int, default=2, help="timed steps of the plain FP64 comparison form "
+                                                              "(after one warm-up step; 0: skip)")
+    ap.add_argument("--n", type=int, default=C3["n"], help="points of the headline workload (smaller: quick runs)")
+    ap.add_argument("--batch", type=int, default=64, help="jobs per merged launch of the HODLR batch leg (0: skip)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "tf32"], help="HODLR batch leg: headline form")
+    ap.add_argument("--compare", type=int, default=1, help="HODLR batch leg: also time the other precision form")
+    ap.add_argument("--autotune", type=int, default=1, help="HODLR batch leg: pick tile and grid by timing")
+    ap.add_argument("--gemm-tile", type=int, default=0, help="HODLR batch leg: product tile edge when not tuning")
+    ap.add_argument("--serve-requests", type=int, default=16, help="requests of the serving leg (0: skip)")
+    ap.add_argument("--serve-rate", type=float, default=40.0, help="Poisson arrival rate of the serving leg (1/s)")
+    ap.add_argument("--uneven", type=int, default=0, help="instances of the uneven batch leg (0: skip)")
+    args = ap.parse_args()
+    C3["n"] = args.n
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":  # the oracle alone: this library is not loaded
+        run_reference_arm(args, rank, world)
+        return
+    pp = load_pp()
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    ctx = pp.Context(device=local)
+    s = torch.cuda.Stream()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    job = C3Job(pp, ctx, torch, s, rank)
+    with Clocks(local) as clk:
+        mixed = job.run_form(pp.BF16, args.steps, args.warmup, barrier)
+    value, total_max = whole_job_rate(dist, world, mixed["total_s"], args.steps, "cuda")
+    fp64 = None
+    if args.fp64_steps > 0:
+        fp64 = job.run_form(pp.FP64, args.fp64_steps, 1, barrier)
+        fp64["value"], fp64["total_s"] = whole_job_rate(dist, world, fp64["total_s"], args.fp64_steps, "cuda")
+    e2e = job.e2e(pp.BF16, max(2, args.steps // 2), barrier)
+    e2e_value, _ = whole_job_rate(dist, world, e2e["total_s"], e2e["steps"], "cuda")
+    roofline = job.roofline(mixed, fp64)
+    c3_config = c3_config_keys(world)
+    job.release()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        t_est, sample = reference_c3_seconds(os.cpu_count() or 1)
+        cpu = {"value": 1.0 / t_est, "unit": "factor+solve/s", "cores": os.cpu_count() or 1, "kind": "port",
+               "sample": sample}
+    legs = {}
+    if args.batch > 0:
+        legs["hodlr_batch"] = c2_batch_leg(args, pp, ctx, torch, dist, rank, world, barrier, s)
+    if args.uneven > 0:
+        legs["uneven_batch"] = uneven_batch_leg(pp, ctx, args.uneven, max(3, args.steps // 2), args.warmup)
+    if args.serve_requests > 0:
+        legs["serving"] = serving_leg(pp, ctx, args.serve_requests, args.serve_rate, seed=2024 + rank)
 
     if rank == 0:
+        forms = {"bf16": {k: v for k, v in mixed.items() if k != "total_s"}}
+        forms["bf16"]["value"] = value
+        if fp64:
+            forms["fp64"] = {k: v for k, v in fp64.items() if k != "total_s"}
         line = {"metric": METRIC, "value": value, "unit": "factor+solve/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1e3 * total_max / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64" if args.precision == "fp64" else "tf32 gemm + f64", "data": "synthetic",
-                "forms": {args.precision: {k: v for k, v in main_stats.items() if k != "total_s"},
-                          **({other: {k: v for k, v in cmp_stats.items() if k != "total_s"}} if cmp_stats else {})},
-                "config": config_keys(B, args.precision, world),
-                "details": {"graph": "restore+factor+solves captured", "factor_tasks_per_job": finfo["n_tasks"],
-                            "factor_flops_per_job": finfo["flops"], "refinement_solves": iters,
-                            "single_job_step_ms": float(np.median(lat))},
-                "e2e": {"value": e2e_value, "unit": "factor+solve/s",
-                        "h2d_bytes_per_step": B * (hs[0].arena_bytes() + 8 * n),
-                        "d2h_bytes_per_step": B * 8 * n, "mode": e2e_mode,
-                        "serial_value": e2e_serial,
-                        "serial_mode": "one step at a time: upload, factor + refinement, download, then the next"},
-                "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "serving": serving,
-                "uneven_batch": uneven,
-                "plain_fp64_single_instance": {
-                    "value": 1e3 / float(np.median(lat)), "unit": "factor+solve/s",
-                    "note": "one job per persistent launch, FP64, refinement to the same tolerance (the "
-                            "reference's execution model: one DAG per launch)"},
-                "gpu_launches": launches_per_step * args.steps}
+                "scaling": "weak", "vs_baseline": None, "dtype": "bf16 schur + f64", "data": "synthetic",
+                "config": c3_config, "forms": forms,
+                "mixed_vs_fp64": (value / fp64["value"]) if fp64 else None,
+                "e2e": {"value": e2e_value, "unit": "factor+solve/s", "h2d_bytes_per_step": e2e["h2d"],
+                        "d2h_bytes_per_step": e2e["d2h"], "mode": e2e["mode"]},
+                "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "legs": legs,
+                "gpu_launches": mixed["gpu_launches_per_step"] * args.steps}
         print(json.dumps(line), flush=True)
-    del g, g2
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
