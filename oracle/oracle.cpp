@@ -328,11 +328,12 @@ double from_bf16(uint16_t h) {
   std::memcpy(&f, &u, 4);
   return (double)f;
 }
-// byte offset of element (r, c) of an R x K operand in the tiled layout (pp_task.h)
-inline int64_t tiled_at(int r, int c, int K) {
-  const int64_t chunk = (int64_t)(r / 128) * (K / 64) + c / 64;
-  const int rr = r % 128, cc = c % 64;
-  return chunk * 16384 + ((cc / 8) * 16 + rr / 8) * 128 + (rr % 8) * 16 + (cc % 8) * 2;
+// byte offset of element (r, c) of an R x K operand in the tiled layout (pp_task.h) with chunks of
+// cr rows x 64 columns
+inline int64_t tiled_at(int r, int c, int K, int cr) {
+  const int64_t chunk = (int64_t)(r / cr) * (K / 64) + c / 64;
+  const int rr = r % cr, cc = c % 64;
+  return chunk * (int64_t)cr * 128 + ((cc / 8) * (cr / 8) + rr / 8) * 128 + (rr % 8) * 16 + (cc % 8) * 2;
 }
 
 int run_one(const pp_task& T, std::vector<double>& tmp) {
@@ -346,7 +347,8 @@ int run_one(const pp_task& T, std::vector<double>& tmp) {
     case PP_OP_TRSMU: o_trsmu(T.p[0], T.p[1], T.m, T.n, T.ld[0], T.ld[1]); return 0;
     case PP_OP_GEMM:
       if (T.prec == PP_PREC_BF16) {  // engine instruction: products of the BF16 shadows, FP64 sums
-        if (T.m % 128 || T.n % 128 || T.k % 64) return -1;
+        if (T.m % 128 || T.n % 32 || T.k % 64) return -1;
+        const int bcr = T.n % 256 == 0 ? 128 : (T.n < 128 ? T.n : 128);  // the B shadow's chunk rows
         const uint8_t* As = reinterpret_cast<const uint8_t*>(T.p[1]);
         const uint8_t* Bs = reinterpret_cast<const uint8_t*>(T.p[2]);
         for (int r = 0; r < T.m; ++r)
@@ -354,8 +356,8 @@ int run_one(const pp_task& T, std::vector<double>& tmp) {
             double s = 0.0;
             for (int q = 0; q < T.k; ++q) {
               uint16_t a, b;
-              std::memcpy(&a, As + tiled_at(r, q, T.k), 2);
-              std::memcpy(&b, Bs + tiled_at(c, q, T.k), 2);
+              std::memcpy(&a, As + tiled_at(r, q, T.k, 128), 2);
+              std::memcpy(&b, Bs + tiled_at(c, q, T.k, bcr), 2);
               s += from_bf16(a) * from_bf16(b);
             }
             double& x = T.p[0][(int64_t)r * T.ld[0] + c];
@@ -366,13 +368,16 @@ int run_one(const pp_task& T, std::vector<double>& tmp) {
       o_gemm(T.alpha, T.beta, T.p[0], T.p[1], T.p[2], T.m, T.n, T.k, T.ld[0], T.ld[1], T.ld[2], t1, t2);
       return 0;
     case PP_OP_SHADOW: {  // engine instruction: BF16 copy of an operand in the tiled layout
-      if (T.m % 128 || T.k % 64) return -1;
+      const int cr = T.ctrl ? T.ctrl : 128;  // chunk rows of the layout
+      if (T.m % cr || T.k % 64) return -1;
       uint8_t* S = reinterpret_cast<uint8_t*>(T.p[0]);
+      const int mr = T.l > 0 ? T.l : T.m, nc = T.n > 0 ? T.n : T.k;  // source rows / columns; zeros beyond
       for (int r = 0; r < T.m; ++r)
         for (int c = 0; c < T.k; ++c) {
-          const double x = t1 ? T.p[1][(int64_t)c * T.ld[1] + r] : T.p[1][(int64_t)r * T.ld[1] + c];
+          const double x = (r >= mr || c >= nc) ? 0.0
+                           : t1 ? T.p[1][(int64_t)c * T.ld[1] + r] : T.p[1][(int64_t)r * T.ld[1] + c];
           const uint16_t h = to_bf16(x);
-          std::memcpy(S + tiled_at(r, c, T.k), &h, 2);
+          std::memcpy(S + tiled_at(r, c, T.k, cr), &h, 2);
         }
       return 0;
     }

@@ -515,11 +515,12 @@ int Generator::tri_limit(int target_extent) const {
   return (!solve_ && target_extent >= kBigLeaf) ? std::max(Ttri_, kBigTri) : Ttri_;
 }
 
-// The BF16 shadow of an operand view (m x n logical, m a multiple of 128, n of 64), written by a
-// SHADOW instruction at its first use and reused until the view's object is written again.
-View Generator::shadow_of(const View& X) {
+// The BF16 shadow of an operand view (m x n logical, m a multiple of cr), columns padded to a
+// multiple of 64, written by a SHADOW instruction at its first use and reused until the view's
+// object is written again.
+View Generator::shadow_of(const View& X, int cr) {
   if ((int)shadows_.size() < (int)P_.objs.size()) shadows_.resize(P_.objs.size());
-  const ShadowKey key{X.obj, X.r0, X.c0, X.m, X.n, X.t};
+  const ShadowKey key{X.obj, X.r0, X.c0, X.m, X.n, X.t, cr};
   for (auto& e : shadows_[X.obj])
     if (e.first == key) {
       View s;
@@ -528,24 +529,55 @@ View Generator::shadow_of(const View& X) {
       s.n = P_.objs[e.second].cols;
       return s;
     }
-  // X.m rows of X.n BF16 values: X.n / 4 doubles per row (the tiled layout is opaque to the DAG)
+  const int K = (X.n + 63) & ~63;
+  // X.m rows of K BF16 values: K / 4 doubles per row (the tiled layout is opaque to the DAG)
   View s;
-  s.obj = P_.add_obj(P_.arena_id(inst_, AR_SCRATCH), X.m, X.n / 4, true);
+  s.obj = P_.add_obj(P_.arena_id(inst_, AR_SCRATCH), X.m, K / 4, true);
   s.m = X.m;
-  s.n = X.n / 4;
+  s.n = K / 4;
   HTask& t = emit(PP_OP_SHADOW);
   bind(t, 0, s, true);
   bind(t, 1, X, false);
   t.t.m = X.m;
-  t.t.k = X.n;
+  t.t.k = K;
+  t.t.n = X.n < K ? X.n : 0;
+  t.t.ctrl = cr == 128 ? 0 : cr;
   t.flops = 0;
   if ((int)shadows_.size() < (int)P_.objs.size()) shadows_.resize(P_.objs.size());
   shadows_[X.obj].push_back({key, s.obj});
   return s;
 }
 
+// C := C + alpha A B on the tensor cores from BF16 shadows (the mixed form), for the products of
+// a factorization that the BF16 GEMM instruction takes: C's rows a multiple of 128 and its columns
+// 32, 64, 128 or a multiple of 256; one of A, B a whole dense leaf of at least kBigLeaf rows and
+// columns, or C a whole leaf (a Schur update, dense or low-rank); inner dimension padded to 64.
+// Returns false (nothing emitted) when the product does not qualify.
+bool Generator::bf16_product(const View& C, const View& A, const View& B, int alpha) {
+  if (prec_ != PP_PREC_BF16 || solve_ || C.t) return false;
+  const bool wide = C.n % 256 == 0;
+  if (C.m % 128 != 0 || !(wide || C.n == 32 || C.n == 64 || C.n == 128)) return false;
+  auto big = [&](const View& v) { return whole_leaf(v) && v.m >= kBigLeaf && v.n >= kBigLeaf; };
+  const bool c_leaf = big(C);
+  if (!(c_leaf || big(A) || big(B))) return false;
+  if (!c_leaf && A.n % 64 != 0) return false;  // skinny products: k is a leaf's edge
+  const int K = (A.n + 63) & ~63;
+  const View As = shadow_of(A, 128);
+  const View Bs = shadow_of(B.T(), wide ? 128 : C.n);
+  HTask& t = emit(PP_OP_GEMM);
+  bind(t, 0, C, true);
+  bind(t, 1, As, false);
+  bind(t, 2, Bs, false);
+  t.t.prec = PP_PREC_BF16;
+  t.t.m = C.m;
+  t.t.n = C.n;
+  t.t.k = K;
+  t.t.alpha = (double)alpha;
+  t.t.beta = 1.0;
+  t.flops = 2LL * C.m * C.n * A.n;
+  return true;
+}
 
-// --------------------------------------------------------------------------- H-LU
 void Generator::getrf_program() {
   getrf(node(H_.root));
   if (inverses_) emit_inverses();
@@ -856,25 +888,16 @@ void Generator::gemm_tiles(const View& C, const View& A, const View& B, int alph
     s.flops = (int64_t)C.m * C.n * parts;
     return;
   }
+  // the mixed form: Schur updates of large leaves and products with a large dense leaf on the
+  // tensor cores
+  if (bf16_product(C, A, B, alpha)) return;
   if (!solve_ && !work_target && C.m >= kBigLeaf && C.n >= kBigLeaf && whole_leaf(C) && whole_leaf(A) &&
       whole_leaf(B)) {
     // a Schur update of whole large leaves: one instruction (its CTA loops over the tile)
-    const bool bf16 = prec_ == PP_PREC_BF16 && C.m % 128 == 0 && C.n % 256 == 0 && A.n % 64 == 0;
-    View As, Bs;
-    if (bf16) {
-      As = shadow_of(A);
-      Bs = shadow_of(B.T());
-    }
     HTask& t = emit(PP_OP_GEMM);
     bind(t, 0, C, true);
-    if (bf16) {
-      bind(t, 1, As, false);
-      bind(t, 2, Bs, false);
-      t.t.prec = PP_PREC_BF16;
-    } else {
-      bind(t, 1, A, false);
-      bind(t, 2, B, false);
-    }
+    bind(t, 1, A, false);
+    bind(t, 2, B, false);
     t.t.m = C.m;
     t.t.n = C.n;
     t.t.k = A.n;

@@ -194,12 +194,16 @@ class Generator {
   struct ShadowKey {
     int obj, r0, c0, m, n;
     bool t;
+    int cr;
     bool operator==(const ShadowKey& o) const {
-      return obj == o.obj && r0 == o.r0 && c0 == o.c0 && m == o.m && n == o.n && t == o.t;
+      return obj == o.obj && r0 == o.r0 && c0 == o.c0 && m == o.m && n == o.n && t == o.t && cr == o.cr;
     }
   };
   std::vector<std::vector<std::pair<ShadowKey, int>>> shadows_;  // per program object
-  View shadow_of(const View& X);
+  // the shadow of X in the tiled layout with chunks of cr rows (128 for an A operand; for a B
+  // operand 128 or its row count), columns padded with zeros to a multiple of 64
+  View shadow_of(const View& X, int cr = 128);
+  bool bf16_product(const View& C, const View& A, const View& B, int alpha);
   bool whole_leaf(const View& v) const;
   int tri_limit(int target_extent) const;
   void trmv(int inv, int upper, int m, const View& B);

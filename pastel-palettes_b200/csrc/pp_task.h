@@ -46,7 +46,8 @@ enum pp_op {
   PP_OP_SHADOW = 15, /* BF16 shadow of an FP64 operand for the tensor-core GEMM: the m x k matrix
                         X(r, c) = p[1][r * ld[1] + c] (or p[1][c * ld[1] + r] with PP_T(1)),
                         rounded to BF16 and written at p[0] in the tiled layout below (m a
-                        multiple of 128, k of 64); no reference counterpart                   */
+                        multiple of 128, k of 64); rows from l and columns from n on (when set)
+                        are written as zeros (padding); no reference counterpart               */
   PP_OP_KMUL = 16,   /* C[m x k] (p[0]) := K(P_I, P_J) B: a kernel matrix evaluated from points
                         times B (p[3], n x k, k <= 32); P_I = p[1] (m points), P_J = p[2] (n
                         points), rows of dim = l coordinates (ld[1], ld[2]); kernel ctrl (0
@@ -74,15 +75,18 @@ enum pp_op {
 #define PP_PREC_TF32 1
 /* PP_PREC_BF16: a GEMM whose operands are BF16 shadows (PP_OP_SHADOW) in the tiled layout:
  * p[1] the m x k shadow of op(A), p[2] the n x k shadow of op(B)^T; products summed in FP32 on
- * the tensor cores, C (FP64) := beta C + alpha sum.  m a multiple of 128, n of 256, k of 64. */
+ * the tensor cores, C (FP64) := beta C + alpha sum.  m a multiple of 128, k of 64, n 32, 64, 128
+ * or a multiple of 256. */
 #define PP_PREC_BF16 2
 
-/* Tiled BF16 layout of an R x K operand (R a multiple of 128, K of 64): 16 KB chunks of 128 rows
- * x 64 columns, chunk (R / 128 block rb, K / 64 block kc) at byte ((rb * (K / 64)) + kc) * 16384;
- * inside a chunk, element (r, c) at byte ((c / 8) * 16 + r / 8) * 128 + (r % 8) * 16 + (c % 8) * 2
- * (8 x 8 core matrices of 128 contiguous bytes, adjacent along r 128 bytes apart, along c 2048
- * bytes apart): the operand layout the tensor core reads from shared memory without swizzling,
- * so one chunk moves with one bulk copy. */
+/* Tiled BF16 layout of an R x K operand (R a multiple of the chunk height h = 128, 64 or 32 — the
+ * SHADOW task's ctrl, 0 meaning 128 — and K of 64): chunks of h rows x 64 columns (h * 128 bytes),
+ * chunk (R / h block rb, K / 64 block kc) at byte ((rb * (K / 64)) + kc) * h * 128; inside a chunk,
+ * element (r, c) at byte ((c / 8) * (h / 8) + r / 8) * 128 + (r % 8) * 16 + (c % 8) * 2 (8 x 8
+ * core matrices of 128 contiguous bytes, adjacent along r 128 bytes apart, along c h * 16 bytes
+ * apart): the operand layout the tensor core reads from shared memory without swizzling, so one
+ * chunk moves with one bulk copy.  A GEMM's A shadow has h = 128; its B shadow has h = 128 when n
+ * is a multiple of 256, else h = n (32, 64 or 128). */
 #define PP_SHADOW_CHUNK_ROWS 128
 #define PP_SHADOW_CHUNK_COLS 64
 #define PP_SHADOW_CHUNK_BYTES 16384

@@ -491,9 +491,8 @@ __device__ __noinline__ bool dev_gemm_tc(double* __restrict__ C, int ldc, const 
 #define BG_STAGE_BYTES (3 * BG_CHUNK)
 #define BG_TILE_N 256
 // instruction descriptor: D F32 (bits 4-5 = 1), A and B BF16 (bits 7-9, 10-12 = 1), both
-// K-major, N = 128 (bits 17-22 = N >> 3), M = 128 (bits 24-28 = M >> 4)
-constexpr uint32_t kIdescBf16 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(128 >> 3) << 17) |
-                                ((uint32_t)(128 >> 4) << 24);
+// K-major, M = 128 (bits 24-28 = M >> 4); N (bits 17-22 = N >> 3) is added per task
+constexpr uint32_t kIdescBf16Base = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(128 >> 4) << 24);
 
 __device__ __forceinline__ uint32_t bf16_bits(double x) {
   // round to nearest even through FP32 (finite values; NaN stays a quiet NaN)
@@ -503,15 +502,20 @@ __device__ __forceinline__ uint32_t bf16_bits(double x) {
   return u >> 16;
 }
 
-__device__ __forceinline__ size_t tiled_at(int r, int c, int K) {
-  const size_t chunk = (size_t)(r >> 7) * (K >> 6) + (c >> 6);
-  const int rr = r & 127, cc = c & 63;
-  return chunk * BG_CHUNK + (size_t)((((cc >> 3) << 4) + (rr >> 3)) << 7) + ((rr & 7) << 4) + ((cc & 7) << 1);
+// byte offset of element (r, c) of an R x K operand in the tiled layout with chunks of cr rows
+// (32, 64 or 128) and 64 columns
+__device__ __forceinline__ size_t tiled_at(int r, int c, int K, int cr) {
+  const size_t chunk = (size_t)(r / cr) * (K >> 6) + (c >> 6);
+  const int rr = r % cr, cc = c & 63;
+  return chunk * ((size_t)cr * 128) + (size_t)((((cc >> 3) * (cr >> 3)) + (rr >> 3)) << 7) + ((rr & 7) << 4) +
+         ((cc & 7) << 1);
 }
 
-// S := the tiled BF16 shadow of X (m x k), X(r, c) = A[r lda + c] or A[c lda + r] (tA); each
-// thread converts 8 consecutive columns of a row and stores them as one 16-byte word
-__device__ __noinline__ void dev_shadow(uint8_t* S, const double* A, int lda, bool tA, int m, int k) {
+// S := the tiled BF16 shadow of X (m x k, padded with zeros beyond the source's mr rows and nc
+// columns), X(r, c) = A[r lda + c] or A[c lda + r] (tA); each thread converts 8 consecutive
+// columns of a row and stores them as one 16-byte word
+__device__ __noinline__ void dev_shadow(uint8_t* S, const double* A, int lda, bool tA, int m, int k, int mr, int nc,
+                                       int cr) {
   const int cg = k >> 3, units = m * cg;
   for (int u = threadIdx.x; u < units; u += NT) {
     int r, c;
@@ -520,13 +524,15 @@ __device__ __noinline__ void dev_shadow(uint8_t* S, const double* A, int lda, bo
     uint32_t h[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q)
-      h[q] = bf16_bits(tA ? ldcg(&A[(size_t)(c + q) * lda + r]) : ldcg(&A[(size_t)r * lda + c + q]));
+      h[q] = (r < mr && c + q < nc)
+                 ? bf16_bits(tA ? ldcg(&A[(size_t)(c + q) * lda + r]) : ldcg(&A[(size_t)r * lda + c + q]))
+                 : 0u;
     uint4 v;
     v.x = h[0] | (h[1] << 16);
     v.y = h[2] | (h[3] << 16);
     v.z = h[4] | (h[5] << 16);
     v.w = h[6] | (h[7] << 16);
-    *reinterpret_cast<uint4*>(S + tiled_at(r, c, k)) = v;
+    *reinterpret_cast<uint4*>(S + tiled_at(r, c, k, cr)) = v;
   }
   // the shadow is read by bulk copies (the async proxy) of other CTAs
   asm volatile("fence.proxy.async.global;" ::: "memory");
@@ -568,15 +574,26 @@ __device__ __forceinline__ bool mbar_wait_or_abort(uint32_t addr, uint32_t phase
     }
   }
 }
-__device__ __forceinline__ void tc_mma_bf16(uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t acc) {
+__device__ __forceinline__ void tc_mma_bf16(uint32_t tmem, uint64_t ad, uint64_t bd, uint32_t idesc, uint32_t acc) {
   asm volatile(
       "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
       " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
-      "l"(ad), "l"(bd), "r"(kIdescBf16), "r"(acc)
+      "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
       : "memory");
 }
 __device__ __forceinline__ void tc_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+// C[r][lane] = beta C + alpha T[r][lane] for the warp's 32 rows (row stride ldc), T the 32 x 32
+// FP32 transpose buffer (row stride 33): 32 coalesced loads in flight per lane, then the stores
+__device__ __noinline__ void bg_rows_update(double* __restrict__ cp, int ldc, const float* tb, int lane, double alpha,
+                                            double beta) {
+  double cv[32];
+#pragma unroll
+  for (int rr = 0; rr < 32; ++rr) cv[rr] = beta != 0.0 ? __ldcg(cp + (size_t)rr * ldc) : 0.0;
+#pragma unroll
+  for (int rr = 0; rr < 32; ++rr) cp[(size_t)rr * ldc] = fma(alpha, (double)tb[rr * 33 + lane], cv[rr]);
 }
 
 __device__ __noinline__ bool dev_gemm_bf16(double* __restrict__ C, int ldc, const uint8_t* __restrict__ As,
@@ -587,7 +604,15 @@ __device__ __noinline__ bool dev_gemm_bf16(double* __restrict__ C, int ldc, cons
   const uint32_t stage0 = (s0 + 1023u) & ~1023u;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nch = k >> 6, kchunks = k >> 6;
-  const int tiles_n = n / BG_TILE_N, tiles = (m >> 7) * tiles_n;
+  // tile width: 256 (two 128-column MMAs) when n is a multiple of 256, else n itself (32, 64, 128:
+  // one MMA of that width reading the first n rows of one B chunk)
+  const int tw = (n % BG_TILE_N == 0) ? BG_TILE_N : n, nbc = tw > 128 ? 2 : 1;
+  const int tiles_n = n / tw, tiles = (m >> 7) * tiles_n;
+  // B chunks of cb_rows rows (the B shadow's chunk height: 128, or n itself below 128)
+  const int cb_rows = tw > 128 ? 128 : tw;
+  const uint32_t b_chunk = (uint32_t)cb_rows * 128u, b_lbo = (uint32_t)cb_rows * 16u;
+  const uint32_t stage_bytes = BG_CHUNK + (uint32_t)nbc * b_chunk;
+  const uint32_t idesc = kIdescBf16Base | ((uint32_t)((tw > 128 ? 128 : tw) >> 3) << 17);
   volatile int* abort = tc.abort;
   if (tid == 0) *abort = 0;
   // shared memory written by earlier tasks (generic proxy) is overwritten by bulk copies
@@ -604,15 +629,16 @@ __device__ __noinline__ bool dev_gemm_bf16(double* __restrict__ C, int ldc, cons
       asm volatile("fence.proxy.async.global;" ::: "memory");
       uint32_t q = tc.q;
       for (int t = 0; t < tiles && !*abort; ++t) {
-        const int rb = (t / tiles_n), cb = (t % tiles_n) * 2;
+        const int rb = (t / tiles_n), cb = (t % tiles_n) * nbc;
         for (int kc = 0; kc < nch; ++kc, ++q) {
           const uint32_t s = q % BG_STAGES, ph = (q / BG_STAGES) & 1u;
           if (!mbar_wait_or_abort(empty(s), ph ^ 1u, tc.limit, abort)) break;
           const uint32_t dst = stage0 + s * BG_STAGE_BYTES;
-          mbar_expect_tx(full(s), BG_STAGE_BYTES);
+          mbar_expect_tx(full(s), stage_bytes);
           bulk_g2s(dst, As + ((size_t)rb * kchunks + kc) * BG_CHUNK, BG_CHUNK, full(s));
-          bulk_g2s(dst + BG_CHUNK, Bs + ((size_t)cb * kchunks + kc) * BG_CHUNK, BG_CHUNK, full(s));
-          bulk_g2s(dst + 2 * BG_CHUNK, Bs + ((size_t)(cb + 1) * kchunks + kc) * BG_CHUNK, BG_CHUNK, full(s));
+          bulk_g2s(dst + BG_CHUNK, Bs + ((size_t)cb * kchunks + kc) * b_chunk, b_chunk, full(s));
+          if (nbc == 2)
+            bulk_g2s(dst + BG_CHUNK + b_chunk, Bs + ((size_t)(cb + 1) * kchunks + kc) * b_chunk, b_chunk, full(s));
         }
       }
     }
@@ -634,8 +660,10 @@ __device__ __noinline__ bool dev_gemm_bf16(double* __restrict__ C, int ldc, cons
           for (int ks = 0; ks < 4; ++ks) {
             const uint32_t acc = (kc > 0 || ks > 0) ? 1u : 0u;
             const uint64_t ad = umma_desc(a + ks * 4096u, 2048u, 128u);
-            tc_mma_bf16(acc0, ad, umma_desc(a + BG_CHUNK + ks * 4096u, 2048u, 128u), acc);
-            tc_mma_bf16(acc0 + 128u, ad, umma_desc(a + 2 * BG_CHUNK + ks * 4096u, 2048u, 128u), acc);
+            tc_mma_bf16(acc0, ad, umma_desc(a + BG_CHUNK + ks * 2u * b_lbo, b_lbo, 128u), idesc, acc);
+            if (nbc == 2)
+              tc_mma_bf16(acc0 + 128u, ad, umma_desc(a + BG_CHUNK + b_chunk + ks * 2u * b_lbo, b_lbo, 128u), idesc,
+                          acc);
           }
           tc_commit(empty(s));  // the stage is free once these MMAs have read it
         }
@@ -655,10 +683,10 @@ __device__ __noinline__ bool dev_gemm_bf16(double* __restrict__ C, int ldc, cons
       const bool ok = mbar_wait_or_abort(tfull(b), (u >> 1) & 1u, tc.limit, abort);
       if (__any_sync(0xffffffffu, !ok)) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const int i0 = (t / tiles_n) << 7, j0 = (t % tiles_n) * BG_TILE_N;
+      const int i0 = (t / tiles_n) << 7, j0 = (t % tiles_n) * tw;
       double* cblk = C + (size_t)(i0 + 32 * qd) * ldc + j0 + lane;
 #pragma unroll 1
-      for (int p = 0; p < BG_TILE_N / 32; ++p) {
+      for (int p = 0; p < tw / 32; ++p) {
         uint32_t v[32];
         const uint32_t taddr = tc.tmem + ((uint32_t)(32 * qd) << 16) + b * BG_TILE_N + 32u * p;
         asm volatile(
@@ -675,17 +703,7 @@ __device__ __noinline__ bool dev_gemm_bf16(double* __restrict__ C, int ldc, cons
 #pragma unroll
         for (int c = 0; c < 32; ++c) tb[lane * 33 + c] = __uint_as_float(v[c]);
         __syncwarp();
-        // this piece's C columns, row by row: 16 coalesced loads in flight, then their stores
-#pragma unroll 1
-        for (int r0 = 0; r0 < 32; r0 += 16) {
-          double cv[16];
-          double* cp = cblk + 32 * p + (size_t)r0 * ldc;
-#pragma unroll
-          for (int rr = 0; rr < 16; ++rr) cv[rr] = beta != 0.0 ? __ldcg(cp + (size_t)rr * ldc) : 0.0;
-#pragma unroll
-          for (int rr = 0; rr < 16; ++rr)
-            cp[(size_t)rr * ldc] = fma(alpha, (double)tb[(r0 + rr) * 33 + lane], cv[rr]);
-        }
+        bg_rows_update(cblk + 32 * p, ldc, tb, lane, alpha, beta);
         __syncwarp();
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -1793,7 +1811,8 @@ __device__ bool run_task(const pp_task& T, double* smem, TcCtx& tc, int& err) {
       return true;
     case PP_OP_GEMM:
       if (T.prec == PP_PREC_BF16) {
-        if (!tc.active || T.m < 128 || T.m % 128 || T.n < BG_TILE_N || T.n % BG_TILE_N || T.k < 64 || T.k % 64)
+        if (!tc.active || T.m < 128 || T.m % 128 || T.k < 64 || T.k % 64 ||
+            !(T.n == 32 || T.n == 64 || T.n == 128 || (T.n >= BG_TILE_N && T.n % BG_TILE_N == 0)))
           return false;
         if (!dev_gemm_bf16(T.p[0], T.ld[0], reinterpret_cast<const uint8_t*>(T.p[1]),
                            reinterpret_cast<const uint8_t*>(T.p[2]), T.m, T.n, T.k, T.alpha, T.beta, smem, tc))
@@ -1841,8 +1860,11 @@ __device__ bool run_task(const pp_task& T, double* smem, TcCtx& tc, int& err) {
       dev_lrtrunc(T, smem);
       return true;
     case PP_OP_SHADOW:
-      if (T.m < 128 || T.m % 128 || T.k < 64 || T.k % 64) return false;
-      dev_shadow(reinterpret_cast<uint8_t*>(T.p[0]), T.p[1], T.ld[1], T.flags & PP_T(1), T.m, T.k);
+      if (T.m < 32 || T.k < 64 || T.k % 64) return false;
+      if (T.l < 0 || T.l > T.m || T.n < 0 || T.n > T.k) return false;
+      if (!(T.ctrl == 0 || T.ctrl == 32 || T.ctrl == 64 || T.ctrl == 128) || T.m % (T.ctrl ? T.ctrl : 128)) return false;
+      dev_shadow(reinterpret_cast<uint8_t*>(T.p[0]), T.p[1], T.ld[1], T.flags & PP_T(1), T.m, T.k,
+                 T.l > 0 ? T.l : T.m, T.n > 0 ? T.n : T.k, T.ctrl ? T.ctrl : 128);
       return true;
     default: return false;
   }

@@ -166,3 +166,48 @@ def test_bf16_program_matches_oracle_and_refines(pp, oracle, bctx):
     b = pp.rhs(n, 8)
     x, hist = pp.Refiner(h2, bctx, prob2).solve(dev(b), tol=1e-10)
     assert hist[-1] <= 1e-10, hist
+
+
+def _shadow_task_ex(pp, sh, src, rows, k_src, ld, cr):
+    """SHADOW with the inner dimension padded to a multiple of 64 and chunks of cr rows."""
+    K = (k_src + 63) // 64 * 64
+    t = shadow_task(pp, sh, src, rows, K, False, ld)
+    t[0]["n"] = k_src if k_src < K else 0
+    t[0]["ctrl"] = 0 if cr == 128 else cr
+    return t, K
+
+
+@pytest.mark.parametrize("m,n,k", [(512, 32, 512), (256, 64, 128), (512, 512, 32), (128, 128, 64)])
+def test_bf16_skinny_and_padded_products_vs_oracle(pp, oracle, bctx, m, n, k):
+    """Products the mixed form runs beside the Schur updates: a dense leaf times a low-rank factor
+    (n = 32: B shadow of 32-row chunks) and rank-k updates of a leaf (k = 32 padded to 64)."""
+    rng = np.random.default_rng(m + n + k)
+    C, A, Bt = rng.standard_normal((m, n)), rng.standard_normal((m, k)), rng.standard_normal((n, k))
+    K = (k + 63) // 64 * 64
+    cr = 128 if n % 256 == 0 else n
+    out = {}
+    for side in ("dev", "host"):
+        mk = (lambda x: dev(x)) if side == "dev" else (lambda x: x.copy())
+        Cx, Ax, Bx = mk(C), mk(A), mk(Bt)
+        As = torch.zeros(m * K // 4, dtype=torch.float64, device="cuda") if side == "dev" else np.zeros(m * K // 4)
+        Bs = torch.zeros(n * K // 4, dtype=torch.float64, device="cuda") if side == "dev" else np.zeros(n * K // 4)
+        ta, _ = _shadow_task_ex(pp, ptr(As), ptr(Ax), m, k, k, 128)
+        tb, _ = _shadow_task_ex(pp, ptr(Bs), ptr(Bx), n, k, k, cr)
+        g = np.zeros(1, dtype=pp.TASK_DTYPE)
+        g[0]["op"], g[0]["prec"] = GEMM, BF16
+        g[0]["m"], g[0]["n"], g[0]["k"] = m, n, K
+        g[0]["alpha"], g[0]["beta"] = -1.0, 1.0
+        g[0]["p"][0], g[0]["p"][1], g[0]["p"][2] = ptr(Cx), ptr(As), ptr(Bs)
+        g[0]["ld"][0] = n
+        tasks = np.concatenate([ta, tb, g])
+        tasks[0]["succ_begin"], tasks[0]["n_succ"] = 0, 1
+        tasks[1]["succ_begin"], tasks[1]["n_succ"] = 1, 1
+        if side == "dev":
+            bctx.vm_execute(tasks, np.array([2, 2], np.int32), np.array([0, 0, 2], np.int32))
+            out[side] = (Cx.cpu().numpy(), As.cpu().numpy(), Bs.cpu().numpy())
+        else:
+            assert oracle.lib().oracle_run_program(tasks.ctypes.data, 3) == 0
+            out[side] = (Cx, As, Bs)
+    (Cd, Asd, Bsd), (Ch, Ash, Bsh) = out["dev"], out["host"]
+    assert np.array_equal(Asd, Ash) and np.array_equal(Bsd, Bsh)
+    assert rel(Cd - C, Ch - C) < 1e-5
