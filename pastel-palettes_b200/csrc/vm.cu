@@ -35,7 +35,7 @@
 #define NT PP_VM_THREADS
 #define TL PP_VM_TILE
 #define LDS (PP_VM_TILE + 1)   /* padded smem row stride (doubles) */
-#define VM_SMEM_BYTES 180224   /* 176 KB, one CTA per SM: ACCUM keeps its ny x k1 sketch on chip;
+#define VM_SMEM_BYTES 184320   /* 180 KB, one CTA per SM: ACCUM keeps its ny x k1 sketch on chip;
                                   the BF16 GEMM holds 3 stages of 48 KB + its epilogue's buffers */
 
 namespace {
@@ -519,8 +519,10 @@ __device__ __noinline__ void dev_shadow(uint8_t* S, const double* A, int lda, bo
   const int cg = k >> 3, units = m * cg;
   for (int u = threadIdx.x; u < units; u += NT) {
     int r, c;
-    if (tA) { r = u % m; c = (u / m) << 3; }   // lanes along r: A[c lda + r] coalesced
-    else { r = u / cg; c = (u % cg) << 3; }    // lanes along c: 64 contiguous bytes each
+    // lanes along r: the 16-byte stores of 32 consecutive rows fill 512 contiguous bytes (four
+    // core matrices); loads are coalesced across lanes (tA) or 64 contiguous bytes per lane
+    r = u % m;
+    c = (u / m) << 3;
     uint32_t h[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q)
@@ -594,6 +596,22 @@ __device__ __noinline__ void bg_rows_update(double* __restrict__ cp, int ldc, co
   for (int rr = 0; rr < 32; ++rr) cv[rr] = beta != 0.0 ? __ldcg(cp + (size_t)rr * ldc) : 0.0;
 #pragma unroll
   for (int rr = 0; rr < 32; ++rr) cp[(size_t)rr * ldc] = fma(alpha, (double)tb[rr * 33 + lane], cv[rr]);
+}
+
+// the same for two adjacent 32-column pieces (buffers T and T + 32 x 33): 64 loads in flight
+__device__ __noinline__ void bg_rows_update2(double* __restrict__ cp, int ldc, const float* tb, int lane, double alpha,
+                                             double beta) {
+  double cv[64];
+#pragma unroll
+  for (int rr = 0; rr < 32; ++rr) {
+    cv[rr] = beta != 0.0 ? __ldcg(cp + (size_t)rr * ldc) : 0.0;
+    cv[32 + rr] = beta != 0.0 ? __ldcg(cp + (size_t)rr * ldc + 32) : 0.0;
+  }
+#pragma unroll
+  for (int rr = 0; rr < 32; ++rr) {
+    cp[(size_t)rr * ldc] = fma(alpha, (double)tb[rr * 33 + lane], cv[rr]);
+    cp[(size_t)rr * ldc + 32] = fma(alpha, (double)tb[32 * 33 + rr * 33 + lane], cv[32 + rr]);
+  }
 }
 
 __device__ __noinline__ bool dev_gemm_bf16(double* __restrict__ C, int ldc, const uint8_t* __restrict__ As,
@@ -672,11 +690,12 @@ __device__ __noinline__ bool dev_gemm_bf16(double* __restrict__ C, int ldc, cons
       }
     }
   } else if (warp >= 4) {  // epilogue
-    // per warp a 32 x 32 FP32 transpose buffer (row stride 33: conflict-free both ways): the
-    // warp reads its 32 accumulator rows from TMEM (a thread per row), then updates C a row at
-    // a time with the lanes along the columns, so every load and store of C is coalesced
+    // per warp two 32 x 32 FP32 transpose buffers (row stride 33: conflict-free both ways): the
+    // warp reads its 32 accumulator rows from TMEM (a thread per row), then updates C a row at a
+    // time with the lanes along the columns, so every load and store of C is coalesced; two
+    // 32-column pieces at a time, so each lane has 64 loads of C in flight
     const int qd = warp & 3;
-    float* tb = reinterpret_cast<float*>(sbase + (stage0 - s0) + BG_STAGES * BG_STAGE_BYTES) + qd * (32 * 33);
+    float* tb = reinterpret_cast<float*>(sbase + (stage0 - s0) + BG_STAGES * BG_STAGE_BYTES) + qd * (2 * 32 * 33);
     uint32_t u = tc.u;
     for (int t = 0; t < tiles; ++t, ++u) {
       const uint32_t b = u & 1u;
@@ -685,25 +704,31 @@ __device__ __noinline__ bool dev_gemm_bf16(double* __restrict__ C, int ldc, cons
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const int i0 = (t / tiles_n) << 7, j0 = (t % tiles_n) * tw;
       double* cblk = C + (size_t)(i0 + 32 * qd) * ldc + j0 + lane;
+      const int pieces = tw / 32;
 #pragma unroll 1
-      for (int p = 0; p < tw / 32; ++p) {
-        uint32_t v[32];
-        const uint32_t taddr = tc.tmem + ((uint32_t)(32 * qd) << 16) + b * BG_TILE_N + 32u * p;
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
-            "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
-              "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]),
-              "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
-              "=r"(v[30]), "=r"(v[31])
-            : "r"(taddr)
-            : "memory");
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      for (int p = 0; p < pieces; p += 2) {
+        const int np = pieces - p >= 2 ? 2 : 1;
+        for (int h = 0; h < np; ++h) {
+          uint32_t v[32];
+          const uint32_t taddr = tc.tmem + ((uint32_t)(32 * qd) << 16) + b * BG_TILE_N + 32u * (p + h);
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+              "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+                "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+                "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+              : "r"(taddr)
+              : "memory");
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          float* th = tb + h * (32 * 33);
 #pragma unroll
-        for (int c = 0; c < 32; ++c) tb[lane * 33 + c] = __uint_as_float(v[c]);
+          for (int c = 0; c < 32; ++c) th[lane * 33 + c] = __uint_as_float(v[c]);
+        }
         __syncwarp();
-        bg_rows_update(cblk + 32 * p, ldc, tb, lane, alpha, beta);
+        if (np == 2) bg_rows_update2(cblk + 32 * p, ldc, tb, lane, alpha, beta);
+        else bg_rows_update(cblk + 32 * p, ldc, tb, lane, alpha, beta);
         __syncwarp();
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");

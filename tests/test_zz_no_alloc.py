@@ -17,9 +17,9 @@ pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
 
 TOL = 1e-12  # relative Frobenius tolerance the accumulation tests use
-# sketch sizes ny * k1 that shared memory holds (dev_accum): 19424 doubles when k1, k2 <= 16,
-# 11200 otherwise
-YCAP = {16: 19424, 32: 11200}
+# sketch sizes ny * k1 that shared memory holds (dev_accum): 19936 doubles when k1, k2 <= 16,
+# 11712 otherwise
+YCAP = {16: 19936, 32: 11712}
 
 
 def _inputs(rng, ny, nx, k1, k2):
