@@ -101,6 +101,6 @@ class Hierarchical {
 };
 
 // largest diagonal leaf whose triangular factors get explicit inverses
-constexpr int kInvMax = 256;
+constexpr int kInvMax = 512;
 
 }  // namespace pp

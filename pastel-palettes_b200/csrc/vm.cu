@@ -512,29 +512,50 @@ __device__ __forceinline__ size_t tiled_at(int r, int c, int K, int cr) {
 }
 
 // S := the tiled BF16 shadow of X (m x k, padded with zeros beyond the source's mr rows and nc
-// columns), X(r, c) = A[r lda + c] or A[c lda + r] (tA); each thread converts 8 consecutive
-// columns of a row and stores them as one 16-byte word
+// columns), X(r, c) = A[r lda + c] or A[c lda + r] (tA).  Each thread converts 8 consecutive
+// columns of a row and stores them as one 16-byte word, lanes along the rows (the stores of 32
+// consecutive rows fill 512 contiguous bytes).  With tA the loads are coalesced as they stand;
+// otherwise 128 x 64 blocks of X are first staged in shared memory with coalesced loads.
 __device__ __noinline__ void dev_shadow(uint8_t* S, const double* A, int lda, bool tA, int m, int k, int mr, int nc,
-                                       int cr) {
-  const int cg = k >> 3, units = m * cg;
-  for (int u = threadIdx.x; u < units; u += NT) {
-    int r, c;
-    // lanes along r: the 16-byte stores of 32 consecutive rows fill 512 contiguous bytes (four
-    // core matrices); loads are coalesced across lanes (tA) or 64 contiguous bytes per lane
-    r = u % m;
-    c = (u / m) << 3;
-    uint32_t h[8];
+                                       int cr, double* smem) {
+  if (tA) {
+    const int units = m * (k >> 3);
+    for (int u = threadIdx.x; u < units; u += NT) {
+      const int r = u % m, c = (u / m) << 3;
+      uint32_t h[8];
 #pragma unroll
-    for (int q = 0; q < 8; ++q)
-      h[q] = (r < mr && c + q < nc)
-                 ? bf16_bits(tA ? ldcg(&A[(size_t)(c + q) * lda + r]) : ldcg(&A[(size_t)r * lda + c + q]))
-                 : 0u;
-    uint4 v;
-    v.x = h[0] | (h[1] << 16);
-    v.y = h[2] | (h[3] << 16);
-    v.z = h[4] | (h[5] << 16);
-    v.w = h[6] | (h[7] << 16);
-    *reinterpret_cast<uint4*>(S + tiled_at(r, c, k, cr)) = v;
+      for (int q = 0; q < 8; ++q) h[q] = (r < mr && c + q < nc) ? bf16_bits(ldcg(&A[(size_t)(c + q) * lda + r])) : 0u;
+      uint4 v;
+      v.x = h[0] | (h[1] << 16);
+      v.y = h[2] | (h[3] << 16);
+      v.z = h[4] | (h[5] << 16);
+      v.w = h[6] | (h[7] << 16);
+      *reinterpret_cast<uint4*>(S + tiled_at(r, c, k, cr)) = v;
+    }
+  } else {
+    constexpr int BR = 128, BC = 64, LD = BC + 1;
+    for (int r0 = 0; r0 < m; r0 += BR)
+      for (int c0 = 0; c0 < k; c0 += BC) {
+        const int rows = min(BR, m - r0);
+        for (int e = threadIdx.x; e < rows * BC; e += NT) {
+          const int rr = e / BC, cc = e % BC, r = r0 + rr, c = c0 + cc;
+          smem[rr * LD + cc] = (r < mr && c < nc) ? ldcg(&A[(size_t)r * lda + c]) : 0.0;
+        }
+        __syncthreads();
+        for (int u = threadIdx.x; u < rows * (BC >> 3); u += NT) {
+          const int rr = u % rows, cg = (u / rows) << 3;
+          uint32_t h[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) h[q] = bf16_bits(smem[rr * LD + cg + q]);
+          uint4 v;
+          v.x = h[0] | (h[1] << 16);
+          v.y = h[2] | (h[3] << 16);
+          v.z = h[4] | (h[5] << 16);
+          v.w = h[6] | (h[7] << 16);
+          *reinterpret_cast<uint4*>(S + tiled_at(r0 + rr, c0 + cg, k, cr)) = v;
+        }
+        __syncthreads();
+      }
   }
   // the shadow is read by bulk copies (the async proxy) of other CTAs
   asm volatile("fence.proxy.async.global;" ::: "memory");
@@ -1076,12 +1097,12 @@ __device__ __noinline__ void dev_trinv(double* I, int ldi, const double* A, int 
   else dev_trsmu_big(I, ldi, A, lda, c0 + w, w, smem);
 }
 
-// Rows [r0, r0 + rows) of M S into O (row r at O row r - r0), M (m x m, m <= PP_VM_TRI) lower
+// Rows [r0, r0 + rows) of M S into O (row r at O row r - r0), M (m x m, m <= 32 TC) lower
 // or upper triangular, S (m x n).  S is staged in shared memory first (so O may be S itself);
 // warp w takes RU rows at a time, lanes stride the columns, and every load of the RU rows is
 // issued before the first product; a warp reduction per row and right-hand side finishes the
 // dot products, so a row's result does not depend on which rows the call covers.
-template <int NB, int RU>
+template <int NB, int RU, int TC>
 __device__ __noinline__ void trmv_impl(double* O, int ldo, const double* S, int lds, const double* M, int ldm, int m,
                                        int n, int upper, int rbeg, int rows, double* smem) {
   double* Bs = smem;  // m x NB
@@ -1090,7 +1111,6 @@ __device__ __noinline__ void trmv_impl(double* O, int ldo, const double* S, int 
     Bs[e] = q < n ? ldcg(&S[(size_t)r * lds + q]) : 0.0;
   }
   __syncthreads();
-  constexpr int TC = PP_VM_TRI / 32;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int rend = rbeg + rows;
   for (int r0 = rbeg + w * RU; r0 < rend; r0 += (NT / 32) * RU) {
@@ -1135,14 +1155,20 @@ __device__ __noinline__ void trmv_impl(double* O, int ldo, const double* S, int 
 // TRMV: the whole product in place (l == 0) or rows [o, o + l) of it out of place (l > 0)
 __device__ __forceinline__ bool dev_trmv(const pp_task& T, double* smem) {
   const int m = T.m, n = T.n;
-  if (m > PP_VM_TRI || n < 1 || n > 16) return false;
+  if (m > PP_VM_INV || n < 1 || n > 16) return false;
   const bool part = T.l > 0;
   if (part && (T.o < 0 || T.o + T.l > m || !T.p[2])) return false;
   const double* S = part ? T.p[2] : T.p[0];
   const int lds = part ? T.ld[2] : T.ld[0], r0 = part ? T.o : 0, rows = part ? T.l : m;
-  if (n == 1) trmv_impl<1, 8>(T.p[0], T.ld[0], S, lds, T.p[1], T.ld[1], m, n, T.ctrl, r0, rows, smem);
-  else if (n <= 4) trmv_impl<4, 4>(T.p[0], T.ld[0], S, lds, T.p[1], T.ld[1], m, n, T.ctrl, r0, rows, smem);
-  else trmv_impl<16, 2>(T.p[0], T.ld[0], S, lds, T.p[1], T.ld[1], m, n, T.ctrl, r0, rows, smem);
+  if (m <= 256) {
+    if (n == 1) trmv_impl<1, 8, 8>(T.p[0], T.ld[0], S, lds, T.p[1], T.ld[1], m, n, T.ctrl, r0, rows, smem);
+    else if (n <= 4) trmv_impl<4, 4, 8>(T.p[0], T.ld[0], S, lds, T.p[1], T.ld[1], m, n, T.ctrl, r0, rows, smem);
+    else trmv_impl<16, 2, 8>(T.p[0], T.ld[0], S, lds, T.p[1], T.ld[1], m, n, T.ctrl, r0, rows, smem);
+  } else {  // leaves of up to 512 rows: 16 columns per lane, half the rows per pass of loads
+    if (n == 1) trmv_impl<1, 4, 16>(T.p[0], T.ld[0], S, lds, T.p[1], T.ld[1], m, n, T.ctrl, r0, rows, smem);
+    else if (n <= 4) trmv_impl<4, 2, 16>(T.p[0], T.ld[0], S, lds, T.p[1], T.ld[1], m, n, T.ctrl, r0, rows, smem);
+    else trmv_impl<16, 1, 16>(T.p[0], T.ld[0], S, lds, T.p[1], T.ld[1], m, n, T.ctrl, r0, rows, smem);
+  }
   return true;
 }
 
@@ -1864,7 +1890,7 @@ __device__ bool run_task(const pp_task& T, double* smem, TcCtx& tc, int& err) {
       dev_sum(T.p[0], T.ld[0], T.p[1], T.ld[1], T.m, T.n, T.k, T.beta);
       return true;
     case PP_OP_TRINV:
-      if (T.m > PP_VM_TRI || T.n < 1 || T.o < 0 || T.o + T.n > T.m) return false;
+      if (T.m > PP_VM_INV || T.n < 1 || T.o < 0 || T.o + T.n > T.m) return false;
       dev_trinv(T.p[0], T.ld[0], T.p[1], T.ld[1], T.m, T.n, T.o, T.ctrl, smem);
       return true;
     case PP_OP_TRMV: return dev_trmv(T, smem);
@@ -1889,7 +1915,7 @@ __device__ bool run_task(const pp_task& T, double* smem, TcCtx& tc, int& err) {
       if (T.l < 0 || T.l > T.m || T.n < 0 || T.n > T.k) return false;
       if (!(T.ctrl == 0 || T.ctrl == 32 || T.ctrl == 64 || T.ctrl == 128) || T.m % (T.ctrl ? T.ctrl : 128)) return false;
       dev_shadow(reinterpret_cast<uint8_t*>(T.p[0]), T.p[1], T.ld[1], T.flags & PP_T(1), T.m, T.k,
-                 T.l > 0 ? T.l : T.m, T.n > 0 ? T.n : T.k, T.ctrl ? T.ctrl : 128);
+                 T.l > 0 ? T.l : T.m, T.n > 0 ? T.n : T.k, T.ctrl ? T.ctrl : 128, smem);
       return true;
     default: return false;
   }

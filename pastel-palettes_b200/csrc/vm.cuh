@@ -8,6 +8,7 @@
 #define PP_VM_THREADS 256
 #define PP_VM_TILE 64          /* largest dense block GETRF / TRSM* keep in shared memory */
 #define PP_VM_TRI 256          /* largest triangle of a TRSM* task (blocked by PP_VM_TILE)   */
+#define PP_VM_INV 512          /* largest leaf of a TRINV / TRMV task (explicit inverses)       */
 #define PP_VM_MAX_RANK 32      /* largest k1 of ACCUM (register-resident reductions)    */
 
 enum pp_vm_error { PP_VM_OK = 0, PP_VM_TIMEOUT = 1, PP_VM_BAD_TASK = 2, PP_VM_MMA_TIMEOUT = 3 };
