@@ -936,8 +936,10 @@ void Generator::gemm_tiles(const View& C, const View& A, const View& B, int alph
       t.t.k = A.n;
       t.t.alpha = (double)alpha;
       t.t.beta = 1.0;
-      // intermediates of low-rank products (work buffers) may sum in any fixed order
-      if (P_.objs[C.obj].arena == P_.arena_id(inst_, AR_WORK)) t.t.flags |= PP_FREE_ORDER;
+      // intermediates of low-rank products (work buffers) and the solves' products may sum in
+      // any fixed order (compared within a tolerance; the factorization's dense products keep
+      // the reference's ascending order)
+      if (solve_ || P_.objs[C.obj].arena == P_.arena_id(inst_, AR_WORK)) t.t.flags |= PP_FREE_ORDER;
       t.flops = 2LL * mi * nj * A.n;
     }
 }

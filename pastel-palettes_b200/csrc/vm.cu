@@ -271,11 +271,28 @@ __device__ __noinline__ void gemv_row(double* __restrict__ C, const double* __re
   __syncthreads();
 }
 
+template <int NB, int RU, int TC>
+__device__ __noinline__ void trmv_impl(double* O, int ldo, const double* S, int lds, const double* M, int ldm, int m,
+                                       int n, int mode, int rbeg, int rows, double* smem, double alpha = 1.0,
+                                       double beta = 0.0);
+
 __device__ __forceinline__ void dev_gemm(double* __restrict__ C, int ldc, const double* __restrict__ A, int lda, bool tA,
                          const double* __restrict__ B, int ldb, bool tB, int m, int n, int k, double alpha,
                          double beta, double* smem, bool free_order = false) {
   if (free_order && m == 1 && n <= 32 && k >= 64)
     gemv_row(C, A, lda, tA, B, ldb, tB, n, k, alpha, beta, smem);
+  else if (free_order && !tA && !tB && m > 16 && n <= 16 && k >= 64 && k <= 512) {
+    // rows of A times a skinny B (the solves' products): B staged in shared memory, warps take
+    // rows of A with lanes along k and every load of a row batch issued first, a warp reduction
+    // per row and column; no per-element ascending-k order (work and right-hand-side targets)
+    if (k <= 256) {
+      if (n <= 4) trmv_impl<4, 4, 8>(C, ldc, B, ldb, A, lda, k, n, 2, 0, m, smem, alpha, beta);
+      else trmv_impl<16, 2, 8>(C, ldc, B, ldb, A, lda, k, n, 2, 0, m, smem, alpha, beta);
+    } else {
+      if (n <= 4) trmv_impl<4, 2, 16>(C, ldc, B, ldb, A, lda, k, n, 2, 0, m, smem, alpha, beta);
+      else trmv_impl<16, 1, 16>(C, ldc, B, ldb, A, lda, k, n, 2, 0, m, smem, alpha, beta);
+    }
+  }
   else if (free_order && m <= 16 && n <= 16 && k >= 256)
     gemm_splitk(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
   else if (m <= 16 && n <= 16) gemm_cfg<16, 16, 1, 1, 128>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
@@ -1098,13 +1115,15 @@ __device__ __noinline__ void dev_trinv(double* I, int ldi, const double* A, int 
 }
 
 // Rows [r0, r0 + rows) of M S into O (row r at O row r - r0), M (m x m, m <= 32 TC) lower
-// or upper triangular, S (m x n).  S is staged in shared memory first (so O may be S itself);
+// (mode 0) or upper (mode 1) triangular or full (mode 2, then any number of rows), S (m x n);
+// O := beta O + alpha (M S) (alpha 1, beta 0 for the solves' inverses).  S is staged in shared memory first (so O may be S itself);
 // warp w takes RU rows at a time, lanes stride the columns, and every load of the RU rows is
 // issued before the first product; a warp reduction per row and right-hand side finishes the
 // dot products, so a row's result does not depend on which rows the call covers.
 template <int NB, int RU, int TC>
 __device__ __noinline__ void trmv_impl(double* O, int ldo, const double* S, int lds, const double* M, int ldm, int m,
-                                       int n, int upper, int rbeg, int rows, double* smem) {
+                                       int n, int mode, int rbeg, int rows, double* smem, double alpha,
+                                       double beta) {
   double* Bs = smem;  // m x NB
   for (int e = threadIdx.x; e < m * NB; e += NT) {
     const int r = e / NB, q = e % NB;
@@ -1120,7 +1139,7 @@ __device__ __noinline__ void trmv_impl(double* O, int ldo, const double* S, int 
 #pragma unroll
       for (int t = 0; t < TC; ++t) {
         const int r = r0 + u, c = lane + 32 * t;
-        const bool in = r < rend && c < m && (upper ? c >= r : c <= r);
+        const bool in = r < rend && c < m && (mode == 2 || (mode == 1 ? c >= r : c <= r));
         v[u][t] = in ? ldcg(&M[(size_t)r * ldm + c]) : 0.0;
       }
 #pragma unroll
@@ -1145,7 +1164,10 @@ __device__ __noinline__ void trmv_impl(double* O, int ldo, const double* S, int 
       if (lane == 0 && r < rend) {
 #pragma unroll
         for (int q = 0; q < NB; ++q)
-          if (q < n) O[(size_t)(r - rbeg) * ldo + q] = acc[q];
+          if (q < n) {
+            double* o = &O[(size_t)(r - rbeg) * ldo + q];
+            *o = beta != 0.0 ? fma(alpha, acc[q], ldcg(o)) : alpha * acc[q];
+          }
       }
     }
   }
