@@ -287,9 +287,11 @@ __device__ __forceinline__ void dev_gemm(double* __restrict__ C, int ldc, const 
     // per row and column; no per-element ascending-k order (work and right-hand-side targets)
     if (k <= 256) {
       if (n <= 4) trmv_impl<4, 4, 8>(C, ldc, B, ldb, A, lda, k, n, 2, 0, m, smem, alpha, beta);
+      else if (n <= 8) trmv_impl<8, 2, 8>(C, ldc, B, ldb, A, lda, k, n, 2, 0, m, smem, alpha, beta);
       else trmv_impl<16, 2, 8>(C, ldc, B, ldb, A, lda, k, n, 2, 0, m, smem, alpha, beta);
     } else {
       if (n <= 4) trmv_impl<4, 2, 16>(C, ldc, B, ldb, A, lda, k, n, 2, 0, m, smem, alpha, beta);
+      else if (n <= 8) trmv_impl<8, 2, 16>(C, ldc, B, ldb, A, lda, k, n, 2, 0, m, smem, alpha, beta);
       else trmv_impl<16, 1, 16>(C, ldc, B, ldb, A, lda, k, n, 2, 0, m, smem, alpha, beta);
     }
   }
@@ -304,7 +306,7 @@ __device__ __forceinline__ void dev_gemm(double* __restrict__ C, int ldc, const 
   // in flight per thread, 16 FMAs per thread and k step
   else if (n <= 32 && m >= 128) gemm_cfg<128, 32, 4, 4, 16>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
   else if (m <= 32 && n >= 128) gemm_cfg<32, 128, 4, 4, 16>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
-  else if (m > 64 && n > 64) gemm_cfg<128, 128, 8, 8, 8>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
+  else if (m > 64 && n > 64) gemm_cfg<128, 128, 8, 8, 16>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
   else gemm_cfg<64, 64, 4, 4, 32>(C, ldc, A, lda, tA, B, ldb, tB, m, n, k, alpha, beta, smem);
 }
 
@@ -1124,10 +1126,13 @@ template <int NB, int RU, int TC>
 __device__ __noinline__ void trmv_impl(double* O, int ldo, const double* S, int lds, const double* M, int ldm, int m,
                                        int n, int mode, int rbeg, int rows, double* smem, double alpha,
                                        double beta) {
-  double* Bs = smem;  // m x NB
+  // S staged as m rows of NB values, row stride NB + 1 for NB > 1: the lanes of a warp read
+  // consecutive rows, which then fall in distinct shared-memory banks
+  constexpr int SB = NB > 1 ? NB + 1 : 1;
+  double* Bs = smem;
   for (int e = threadIdx.x; e < m * NB; e += NT) {
     const int r = e / NB, q = e % NB;
-    Bs[e] = q < n ? ldcg(&S[(size_t)r * lds + q]) : 0.0;
+    Bs[r * SB + q] = q < n ? ldcg(&S[(size_t)r * lds + q]) : 0.0;
   }
   __syncthreads();
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1152,7 +1157,7 @@ __device__ __noinline__ void trmv_impl(double* O, int ldo, const double* S, int 
         const int c = lane + 32 * t;
         if (c < m) {
 #pragma unroll
-          for (int q = 0; q < NB; ++q) acc[q] = fma(v[u][t], Bs[c * NB + q], acc[q]);
+          for (int q = 0; q < NB; ++q) acc[q] = fma(v[u][t], Bs[c * SB + q], acc[q]);
         }
       }
 #pragma unroll
@@ -1185,10 +1190,12 @@ __device__ __forceinline__ bool dev_trmv(const pp_task& T, double* smem) {
   if (m <= 256) {
     if (n == 1) trmv_impl<1, 8, 8>(T.p[0], T.ld[0], S, lds, T.p[1], T.ld[1], m, n, T.ctrl, r0, rows, smem);
     else if (n <= 4) trmv_impl<4, 4, 8>(T.p[0], T.ld[0], S, lds, T.p[1], T.ld[1], m, n, T.ctrl, r0, rows, smem);
+    else if (n <= 8) trmv_impl<8, 2, 8>(T.p[0], T.ld[0], S, lds, T.p[1], T.ld[1], m, n, T.ctrl, r0, rows, smem);
     else trmv_impl<16, 2, 8>(T.p[0], T.ld[0], S, lds, T.p[1], T.ld[1], m, n, T.ctrl, r0, rows, smem);
   } else {  // leaves of up to 512 rows: 16 columns per lane, half the rows per pass of loads
     if (n == 1) trmv_impl<1, 4, 16>(T.p[0], T.ld[0], S, lds, T.p[1], T.ld[1], m, n, T.ctrl, r0, rows, smem);
     else if (n <= 4) trmv_impl<4, 2, 16>(T.p[0], T.ld[0], S, lds, T.p[1], T.ld[1], m, n, T.ctrl, r0, rows, smem);
+    else if (n <= 8) trmv_impl<8, 2, 16>(T.p[0], T.ld[0], S, lds, T.p[1], T.ld[1], m, n, T.ctrl, r0, rows, smem);
     else trmv_impl<16, 1, 16>(T.p[0], T.ld[0], S, lds, T.p[1], T.ld[1], m, n, T.ctrl, r0, rows, smem);
   }
   return true;
