@@ -322,62 +322,66 @@ def pipelined_e2e(pp, ctx, torch, hs, probs, b_host, bs, x_host, g_a, out_a, ref
     return len(hs) * n_steps, total, mode
 
 
-def serving_leg(pp, ctx, n_requests, rate, seed=2024, smin=1024, smax=3072):
-    """Poisson arrivals of factor+solve requests into the server (continuous admission).
-    Sizes log-uniform in [smin, smax], kernel uniform among Laplace 1/r, exp (length 0.1) and
-    Matern-3/2 (length 0.2) on U[0,1]^3, 1-16 right-hand sides, 0-4 follow-up sets reusing
-    the resident factors, FP64 refinement to 1e-10.  Matrices are built on the host before the
-    clock starts (construction is its own stage); latency = arrival -> solutions on the host."""
-    rng = np.random.default_rng(seed)
-    kinds = [("laplace", 1e-3), ("exp", 0.1), ("matern32", 0.2)]
-    reqs = []
-    for i in range(n_requests):
-        n = int(round(np.exp(rng.uniform(np.log(smin), np.log(smax))) / 64)) * 64
-        kern, p0 = kinds[int(rng.integers(0, 3))]
-        nrhs = int(rng.integers(1, 17))
-        sets = 1 + int(rng.integers(0, 5))
-        h, prob = pp.make_kernel_problem(ctx, n, 3, kern, p0, 128, 16, seed=seed + 17 * i)
-        rhs = rng.uniform(-1, 1, (sets, n, nrhs))
-        reqs.append((h, prob, rhs))
-    gaps = rng.exponential(1.0 / rate, n_requests)
-    srv = pp.Server(ctx, hbm_budget_bytes=64 << 30, max_inflight=4)
-    # one untimed warm-up request (a server's first admission pays one-time host and driver setup)
-    hw, pw = pp.make_kernel_problem(ctx, smin, 3, "laplace", 1e-3, 128, 16, seed=seed - 1)
-    srv.submit(hw, pw, rng.uniform(-1, 1, (1, smin, 4)), tol=WORKLOAD["tol"])
-    srv.wait_all()
-    ids = []
-    t0 = time.perf_counter()
-    t_next = 0.0
-    for (h, prob, rhs), g in zip(reqs, gaps):
-        t_next += g
-        delay = t_next - (time.perf_counter() - t0)
-        if delay > 0:
-            time.sleep(delay)
-        ids.append(srv.submit(h, prob, rhs, tol=WORKLOAD["tol"]))
-    srv.wait_all()
-    st = [srv.poll(i) for i in ids]
-    srv.close()
-    if any(x["status"] != "done" for x in st):
-        raise SystemExit(f"serving: a request failed: {[x['message'] for x in st if x['status'] != 'done']}")
-    lat = np.array([x["t_done_ms"] - x["t_submit_ms"] for x in st])
-    span_s = (max(x["t_done_ms"] for x in st) - min(x["t_submit_ms"] for x in st)) / 1e3
-    for (h, prob, rhs), x in zip(reqs, st):  # per-request record on stderr (the JSON keeps the summary)
-        print(f"serve n={prob.n} kernel={prob.kernel} nrhs={rhs.shape[2]} sets={rhs.shape[0]} "
-              f"iterations={x['iterations']} queued_ms={x['t_admit_ms'] - x['t_submit_ms']:.1f} "
-              f"run_ms={x['t_done_ms'] - x['t_admit_ms']:.1f} enqueue_ms={x['t_enqueued_ms'] - x['t_admit_ms']:.1f} "
-              f"submit_ms={x['t_submit_ms']:.1f}", file=sys.stderr)
-    vectors = sum(rhs.shape[0] * rhs.shape[2] for _, _, rhs in reqs)
-    return {"requests": n_requests, "arrival_rate_per_s": rate, "p50_ms": float(np.percentile(lat, 50)),
-            "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
-            "solves_per_s": vectors / span_s, "solves_unit": "right-hand-side vectors solved to 1e-10 per second",
-            "max_queued_ms": max(x["t_admit_ms"] - x["t_submit_ms"] for x in st),
-            "max_run_ms": max(x["t_done_ms"] - x["t_admit_ms"] for x in st),
-            "max_enqueue_ms": max(x["t_enqueued_ms"] - x["t_admit_ms"] for x in st),
-            "worst_backward_error": max(x["backward_error"] for x in st),
-            "refinement_solves": int(sum(x["iterations"] for x in st)),
+def serving_leg(pp, ctx, n_requests, rates, seed=2024, smin=2048, smax=65536):
+    """Poisson arrivals of factor+solve requests into the server (continuous admission), at each
+    of the swept rates.  N log-uniform in [smin, smax] (multiple of 64), kernel uniform among
+    Laplace 1/r, exp (length 0.1) and Matern-3/2 (length 0.2) on U[0,1]^3, weak admissibility,
+    leaf 128, adaptive rank <= 32 at 1e-7, 1-16 right-hand sides, 0-4 follow-up sets reusing the
+    resident factors, FP64 refinement to 1e-10.  Each request's H-matrix is built on the device at
+    admission (inside its latency); the client computes the diagonal shift (device row sums)
+    before submitting.  Latency = submission -> solutions on the host."""
+    out = []
+    for ri, rate in enumerate(rates):
+        rng = np.random.default_rng(seed + 1000 * ri)
+        kinds = [("laplace", 1e-3), ("exp", 0.1), ("matern32", 0.2)]
+        reqs = []
+        t_prep = time.perf_counter()
+        for i in range(n_requests):
+            n = int(round(np.exp(rng.uniform(np.log(smin), np.log(smax))) / 64)) * 64
+            kern, p0 = kinds[int(rng.integers(0, 3))]
+            nrhs = int(rng.integers(1, 17))
+            sets = 1 + int(rng.integers(0, 5))
+            h, prob = pp.make_kernel_problem(ctx, n, 3, kern, p0, 128, 32, seed=seed + 17 * i + ri, rank_tol=1e-7,
+                                             construct="none")
+            prob.points_dev = None
+            reqs.append((h, prob, rng.uniform(-1, 1, (sets, n, nrhs))))
+        t_prep = time.perf_counter() - t_prep
+        gaps = rng.exponential(1.0 / rate, n_requests)
+        srv = pp.Server(ctx, hbm_budget_bytes=96 << 30, max_inflight=4)
+        # one untimed warm-up request (a server's first admission pays one-time host and driver setup)
+        hw, pw = pp.make_kernel_problem(ctx, smin, 3, "laplace", 1e-3, 128, 32, seed=seed - 1, rank_tol=1e-7,
+                                        construct="none")
+        srv.submit(hw, pw, rng.uniform(-1, 1, (1, smin, 4)), tol=C3["tol"])
+        srv.wait_all()
+        ids, t0, t_next = [], time.perf_counter(), 0.0
+        for (h, prob, rhs), g in zip(reqs, gaps):
+            t_next += g
+            delay = t_next - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            ids.append(srv.submit(h, prob, rhs, tol=C3["tol"]))
+        srv.wait_all(timeout_ms=1800e3)
+        st = [srv.poll(i) for i in ids]
+        srv.close()
+        if any(x["status"] != "done" for x in st):
+            raise SystemExit(f"serving: a request failed: {[x['message'] for x in st if x['status'] != 'done'][:3]}")
+        lat = np.array([x["t_done_ms"] - x["t_submit_ms"] for x in st])
+        span_s = (max(x["t_done_ms"] for x in st) - min(x["t_submit_ms"] for x in st)) / 1e3
+        vectors = sum(rhs.shape[0] * rhs.shape[2] for _, _, rhs in reqs)
+        sizes = [p.n for _, p, _ in reqs]
+        out.append({"arrival_rate_per_s": rate, "requests": n_requests, "p50_ms": float(np.percentile(lat, 50)),
+                    "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
+                    "solves_per_s": vectors / span_s, "requests_per_s": n_requests / span_s,
+                    "max_queued_ms": max(x["t_admit_ms"] - x["t_submit_ms"] for x in st),
+                    "max_enqueue_ms": max(x["t_enqueued_ms"] - x["t_admit_ms"] for x in st),
+                    "worst_backward_error": max(x["backward_error"] for x in st),
+                    "refinement_solves": int(sum(x["iterations"] for x in st)), "n_median": float(np.median(sizes)),
+                    "n_max": int(max(sizes)), "client_prep_s": t_prep})
+    return {"rates": out, "solves_unit": "right-hand-side vectors solved to 1e-10 per second", "slots": 4,
             "workload": f"N log-uniform [{smin},{smax}] (multiple of 64), 3-D points, kernels laplace/exp/matern32, "
-                        f"leaf 128, rank 16, 1-16 RHS, 0-4 follow-up sets, Poisson arrivals; matrices built "
-                        f"before the clock", "slots": 4}
+                        f"weak admissibility, leaf 128, adaptive rank <= 32 @ 1e-7, 1-16 RHS, 0-4 follow-up sets, "
+                        f"Poisson arrivals; H-matrices built on the device at admission (inside the latency), the "
+                        f"diagonal shift computed by the client before submission"}
 
 
 def uneven_batch_leg(pp, ctx, n_inst, steps, warmup, seed=4096, smin=1024, smax=16384):
@@ -385,22 +389,23 @@ def uneven_batch_leg(pp, ctx, n_inst, steps, warmup, seed=4096, smin=1024, smax=
     launch.  N log-uniform in [smin, smax] (multiple of 64), points U[0,1]^2, kernel
     exp(-r / 0.1) + 1e-2 I, leaf 128, adaptive rank <= 24 at 1e-7, TF32 GEMM instructions with
     FP64 refinement to 1e-10, tile / grid autotuned, restore + factor + refinement captured as a
-    CUDA graph and replayed.  Matrices are built on the host before the clock."""
+    CUDA graph and replayed.  The matrices are built on the device before the clock."""
     import torch
     rng = np.random.default_rng(seed)
     hs, probs = [], []
-    for i in range(n_inst):
-        n = int(round(np.exp(rng.uniform(np.log(smin), np.log(smax))) / 64)) * 64
-        h, prob = pp.make_kernel_problem(ctx, n, 2, "exp", 0.1, 128, 24, shift=1e-2, seed=seed + 31 * i, rank_tol=1e-7)
-        h.set_precision(pp.TF32)
-        hs.append(h)
-        probs.append(prob)
     s = torch.cuda.Stream()
+    t_build = time.perf_counter()
     with torch.cuda.stream(s):
-        for h in hs:
-            h.upload(s)
+        for i in range(n_inst):
+            n = int(round(np.exp(rng.uniform(np.log(smin), np.log(smax))) / 64)) * 64
+            h, prob = pp.make_kernel_problem(ctx, n, 2, "exp", 0.1, 128, 24, shift=1e-2, seed=seed + 31 * i,
+                                             rank_tol=1e-7, construct="device", stream=s)
             h.keep_original(s)
+            h.set_precision(pp.TF32)
+            hs.append(h)
+            probs.append(prob)
     s.synchronize()
+    t_build = time.perf_counter() - t_build
     batch = pp.Batch(ctx, hs)
     tune = batch.autotune(s)
     ref = pp.BatchRefiner(batch, probs, stream=s)
@@ -435,9 +440,11 @@ def uneven_batch_leg(pp, ctx, n_inst, steps, warmup, seed=4096, smin=1024, smax=
     return {"instances": n_inst, "n_min": min(sizes), "n_max": max(sizes), "n_total": int(sum(sizes)),
             "factor_solve_per_s": n_inst * steps / total, "ms_per_step": 1e3 * total / steps,
             "refinement_solves": iters, "worst_backward_error": worst, "factor_gflop_per_step": flops / 1e9,
-            "factor_gflops": flops / (total / steps) / 1e9, "autotune": tune,
-            "workload": "config-4 style: N log-uniform [1024,16384], exp(-r/0.1)+1e-2 I on U[0,1]^2, leaf 128, "
-                        "adaptive rank <= 24 @ 1e-7, TF32 GEMMs + FP64 refinement, one merged launch, graph replay"}
+            "factor_gflops": flops / (total / steps) / 1e9, "autotune": tune, "construction_s": t_build,
+            "workload": "N log-uniform [1024,16384], exp(-r/0.1)+1e-2 I on U[0,1]^2, weak admissibility, leaf 128, "
+                        "adaptive rank <= 24 @ 1e-7 (built on the device before the clock), TF32 form of the GEMM "
+                        "instructions + FP64 refinement, all instances in one merged launch, restore + factor + "
+                        "refinement captured as a CUDA graph"}
 
 
 # ----------------------------------------------------------------------------- headline job
@@ -830,9 +837,9 @@ def main():
     ap.add_argument("--compare", type=int, default=1, help="HODLR batch leg: also time the other precision form")
     ap.add_argument("--autotune", type=int, default=1, help="HODLR batch leg: pick tile and grid by timing")
     ap.add_argument("--gemm-tile", type=int, default=0, help="HODLR batch leg: product tile edge when not tuning")
-    ap.add_argument("--serve-requests", type=int, default=16, help="requests of the serving leg (0: skip)")
-    ap.add_argument("--serve-rate", type=float, default=40.0, help="Poisson arrival rate of the serving leg (1/s)")
-    ap.add_argument("--uneven", type=int, default=0, help="instances of the uneven batch leg (0: skip)")
+    ap.add_argument("--serve-requests", type=int, default=200, help="requests per rate of the serving leg (0: skip)")
+    ap.add_argument("--serve-rates", default="5,10,20", help="Poisson arrival rates of the serving leg (1/s)")
+    ap.add_argument("--uneven", type=int, default=512, help="instances of the uneven batch leg (0: skip)")
     args = ap.parse_args()
     C3["n"] = args.n
     rank = int(os.environ.get("RANK", "0"))
@@ -882,7 +889,8 @@ def main():
     if args.uneven > 0:
         legs["uneven_batch"] = uneven_batch_leg(pp, ctx, args.uneven, max(3, args.steps // 2), args.warmup)
     if args.serve_requests > 0:
-        legs["serving"] = serving_leg(pp, ctx, args.serve_requests, args.serve_rate, seed=2024 + rank)
+        legs["serving"] = serving_leg(pp, ctx, args.serve_requests, [float(x) for x in args.serve_rates.split(",")],
+                                      seed=2024 + rank)
 
     if rank == 0:
         forms = {"bf16": {k: v for k, v in mixed.items() if k != "total_s"}}

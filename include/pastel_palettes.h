@@ -242,9 +242,11 @@ typedef struct pp_request_stats {
   char message[128];       /* why a request failed                                            */
 } pp_request_stats;
 pp_status pp_server_create(pp_context* ctx, const pp_serve_config* cfg, pp_server** out);
-/* queues a request; the server takes ownership of h (built and filled, not uploaded) and
- * destroys it when the request retires.  Returns PP_OOM when the request alone exceeds the
- * budget. */
+/* queues a request; the server takes ownership of h (built, not uploaded) and destroys it when
+ * the request retires.  An H-matrix filled on the host (set_dense / set_lowrank) is uploaded at
+ * admission; one that never had a host image is built on the device from the request's points
+ * at admission (pp_hmatrix_construct_dev), inside the request's latency.  Returns PP_OOM when
+ * the request alone exceeds the budget. */
 pp_status pp_server_submit(pp_server* s, pp_hmatrix* h, const pp_request_desc* d, long long* id);
 pp_status pp_server_poll(pp_server* s, long long id, pp_request_stats* st);
 /* waits until no request is queued or running (PP_TIMEOUT after timeout_ms) */

@@ -871,13 +871,15 @@ def make_kernel_problem(ctx, n, dim, kernel, p0, leaf, rank, admissibility=0, et
     diagonal shifted by `shift` or by shift_factor * max off-diagonal row sum.
     construct="host": blocks filled on the host (exact dense blocks, truncated SVD of the
     low-rank ones) for a later upload; "device": the row sums and every block computed on the
-    device (Hierarchical.construct), no host image; prob.points_dev holds the device points."""
+    device (Hierarchical.construct), no host image; prob.points_dev holds the device points;
+    "none": the row sums on the device, the blocks left unbuilt (a served request: the server
+    builds them on the device at admission)."""
     rng = np.random.default_rng(seed)
     pts = rng.uniform(0.0, 1.0, (n, dim))
     pts = pts[morton_order(pts)]
     kid = KERNELS[kernel] if isinstance(kernel, str) else kernel
     pts_dev = None
-    if construct == "device":
+    if construct in ("device", "none"):
         import torch
         pts_dev = torch.from_numpy(np.ascontiguousarray(pts)).cuda()
         off = offdiag_rowsum_max_dev(ctx, pts_dev, kid, p0, stream)
@@ -892,7 +894,7 @@ def make_kernel_problem(ctx, n, dim, kernel, p0, leaf, rank, admissibility=0, et
         h.set_rank_tolerance(rank_tol)
     if construct == "device":
         h.construct(prob, pts_dev, stream)
-    else:
+    elif construct == "host":
         fill_kernel_hmatrix(h, prob, seed + 1, rank_tol=rank_tol)
     return h, prob
 

@@ -1271,6 +1271,7 @@ struct ServeRequest {
   int n = 0, dim = 0, kernel = 0, nrhs = 0, n_sets = 0, max_iter = 0;
   double p0 = 0, shift = 0, norm_inf = 0, tol = 0;
   std::vector<double> pts, rhs;
+  bool construct = false;  // the H-matrix has no host image: build it on the device at admission
   double* x_out = nullptr;  // caller's host buffer
   cudaStream_t stream = nullptr;
   cudaEvent_t ev = nullptr;
@@ -1345,7 +1346,13 @@ bool pp_server::start(ServeRequest* q) {
   if (!srv_check(q, cudaMemcpyAsync(q->d_pts, q->pts.data(), sizeof(double) * q->pts.size(), cudaMemcpyHostToDevice,
                                     q->stream), "points"))
     return false;
-  if (!srv_status(q, pp_hmatrix_upload(h, q->stream), ctx, "upload")) return false;
+  if (q->construct) {  // no host image: the blocks are built on the device from the points
+    if (!srv_status(q, pp_hmatrix_construct_dev(h, q->kernel, q->p0, q->shift, q->d_pts, q->dim, q->stream), ctx,
+                    "construct"))
+      return false;
+  } else if (!srv_status(q, pp_hmatrix_upload(h, q->stream), ctx, "upload")) {
+    return false;
+  }
   if (!srv_status(q, plan_to_device(h, h->factor), ctx, "factor plan")) return false;
   if (!srv_status(q, launch_plan(h, h->factor, q->stream, grid), ctx, "factor")) return false;
   return start_set(q);
@@ -1539,11 +1546,18 @@ pp_status pp_server_submit(pp_server* s, pp_hmatrix* h, const pp_request_desc* d
   q->x_out = d->x_out;
   q->pts.assign(d->points, d->points + (size_t)n * d->dim);
   q->rhs.assign(d->rhs, d->rhs + (size_t)n * d->nrhs * d->n_sets);
+  q->construct = h->H->host.empty();
   std::lock_guard<std::mutex> lk(s->mu);
   // programs are built here (host work) so that the device bytes are known before admission
   VmPlan* sp = solve_plan(h, d->nrhs);
   pp_status st = build_program(h, 0, 0, h->factor);
   if (st == PP_OK) st = build_program(h, 1, d->nrhs, *sp);
+  if (st == PP_OK && q->construct) {
+    h->c_kernel = d->kernel;
+    h->c_dim = d->dim;
+    h->c_p0 = d->p0;
+    st = build_program(h, 2, 0, h->construct);
+  }
   if (st != PP_OK) return st;
   if (h->d_arena) return fail(ctx, PP_INVALID_ARG, "pp_server_submit: the H-matrix must not be uploaded yet");
   auto plan_bytes = [](const VmPlan& p) {
@@ -1554,7 +1568,7 @@ pp_status pp_server_submit(pp_server* s, pp_hmatrix* h, const pp_request_desc* d
   };
   const long long vec = (long long)sizeof(double) * n * d->nrhs;
   q->bytes = (long long)sizeof(double) * (h->H->arena_elems + h->factor.prog.arena_elems[pp::AR_RAND]) +
-             plan_bytes(h->factor) + plan_bytes(*sp) + 4 * vec +
+             plan_bytes(h->factor) + plan_bytes(*sp) + (q->construct ? plan_bytes(h->construct) : 0) + 4 * vec +
              (long long)sizeof(double) * ((long long)n * d->dim + (long long)pp_kernel_residual_part_elems(n, d->nrhs)) +
              (1 << 20);
   if (q->bytes > s->budget) return fail(ctx, PP_OOM, "pp_server_submit: request exceeds the whole HBM budget");

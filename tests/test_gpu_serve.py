@@ -95,3 +95,33 @@ def test_serve_rejects_request_over_budget(pp, gctx):
     with pytest.raises(pp.PPError, match="OOM"):
         srv.submit(h, prob, rhs)
     srv.close()
+
+
+def test_serve_builds_unfilled_matrices_on_the_device(pp, gctx):
+    """Requests whose H-matrices were never filled on the host: the server builds them on the
+    device from the request's points at admission, and the results meet the tolerance against
+    the dense FP64 matrix; the same request alone and in a mix gives the same solution."""
+    def unbuilt(n, kernel, p0, seed):
+        h, prob = pp.make_kernel_problem(gctx, n, 3, kernel, p0, 128, 24, seed=seed, rank_tol=1e-7,
+                                         construct="none")
+        rhs = np.random.default_rng(seed + 1).uniform(-1, 1, (2, n, 3))
+        return h, prob, rhs
+
+    srv = pp.Server(gctx, hbm_budget_bytes=8 << 30, max_inflight=3)
+    jobs = [unbuilt(n, k, p0, 70 + i) for i, (n, k, p0) in
+            enumerate([(2048, "laplace", 1e-3), (3072, "exp", 0.1), (2560, "matern32", 0.2)])]
+    ids = [srv.submit(h, prob, rhs, tol=1e-10) for h, prob, rhs in jobs]
+    srv.wait_all()
+    xs = []
+    for rid, (_, prob, rhs) in zip(ids, jobs):
+        st = srv.poll(rid)
+        assert st["status"] == "done", st["message"]
+        x = srv.result(rid)
+        xs.append(x)
+        for s in range(rhs.shape[0]):
+            assert dense_backward_error(prob, x[s], rhs[s]) <= 1e-10
+    h, prob, rhs = unbuilt(2048, "laplace", 1e-3, 70)
+    rid = srv.submit(h, prob, rhs, tol=1e-10)
+    srv.wait_all()
+    assert rel(srv.result(rid), xs[0]) <= 1e-12
+    srv.close()
