@@ -387,7 +387,9 @@ def serving_leg(pp, ctx, n_requests, rates, seed=2024, smin=2048, smax=65536):
 def uneven_batch_leg(pp, ctx, n_inst, steps, warmup, seed=4096, smin=1024, smax=16384):
     """Configuration-4 style batch: n_inst H-matrices of uneven size in one merged persistent
     launch.  N log-uniform in [smin, smax] (multiple of 64), points U[0,1]^2, kernel
-    exp(-r / 0.1) + 1e-2 I, leaf 128, adaptive rank <= 24 at 1e-7, TF32 GEMM instructions with
+    exp(-r / 0.1) + 1e-2 I, standard admissibility (eta 1: the short-range kernel's far blocks have
+    ranks 8-12 at 1e-7, while weak admissibility would need more than 24 near the diagonal and the
+    refinement would stall), leaf 128, adaptive rank <= 24 at 1e-7, TF32 GEMM instructions with
     FP64 refinement to 1e-10, tile / grid autotuned, restore + factor + refinement captured as a
     CUDA graph and replayed.  The matrices are built on the device before the clock."""
     import torch
@@ -398,8 +400,8 @@ def uneven_batch_leg(pp, ctx, n_inst, steps, warmup, seed=4096, smin=1024, smax=
     with torch.cuda.stream(s):
         for i in range(n_inst):
             n = int(round(np.exp(rng.uniform(np.log(smin), np.log(smax))) / 64)) * 64
-            h, prob = pp.make_kernel_problem(ctx, n, 2, "exp", 0.1, 128, 24, shift=1e-2, seed=seed + 31 * i,
-                                             rank_tol=1e-7, construct="device", stream=s)
+            h, prob = pp.make_kernel_problem(ctx, n, 2, "exp", 0.1, 128, 24, admissibility=1, eta=1.0, shift=1e-2,
+                                             seed=seed + 31 * i, rank_tol=1e-7, construct="device", stream=s)
             h.keep_original(s)
             h.set_precision(pp.TF32)
             hs.append(h)
@@ -434,6 +436,8 @@ def uneven_batch_leg(pp, ctx, n_inst, steps, warmup, seed=4096, smin=1024, smax=
         total += e0.elapsed_time(e1) / 1e3
         worst = max(worst, max(ref.errors(bs, *out)))
     batch.sync(s)
+    if worst > WORKLOAD["tol"]:
+        raise SystemExit(f"uneven batch: a timed step ended above {WORKLOAD['tol']}: {worst}")
     sizes = [p.n for p in probs]
     flops = batch.program_info(0)["flops"]
     del g
@@ -441,7 +445,7 @@ def uneven_batch_leg(pp, ctx, n_inst, steps, warmup, seed=4096, smin=1024, smax=
             "factor_solve_per_s": n_inst * steps / total, "ms_per_step": 1e3 * total / steps,
             "refinement_solves": iters, "worst_backward_error": worst, "factor_gflop_per_step": flops / 1e9,
             "factor_gflops": flops / (total / steps) / 1e9, "autotune": tune, "construction_s": t_build,
-            "workload": "N log-uniform [1024,16384], exp(-r/0.1)+1e-2 I on U[0,1]^2, weak admissibility, leaf 128, "
+            "workload": "N log-uniform [1024,16384], exp(-r/0.1)+1e-2 I on U[0,1]^2, standard admissibility eta 1, leaf 128, "
                         "adaptive rank <= 24 @ 1e-7 (built on the device before the clock), TF32 form of the GEMM "
                         "instructions + FP64 refinement, all instances in one merged launch, restore + factor + "
                         "refinement captured as a CUDA graph"}
@@ -834,11 +838,11 @@ def main():
     ap.add_argument("--n", type=int, default=C3["n"], help="points of the headline workload (smaller: quick runs)")
     ap.add_argument("--batch", type=int, default=64, help="jobs per merged launch of the HODLR batch leg (0: skip)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "tf32"], help="HODLR batch leg: headline form")
-    ap.add_argument("--compare", type=int, default=1, help="HODLR batch leg: also time the other precision form")
+    ap.add_argument("--compare", type=int, default=0, help="HODLR batch leg: also time the other precision form")
     ap.add_argument("--autotune", type=int, default=1, help="HODLR batch leg: pick tile and grid by timing")
     ap.add_argument("--gemm-tile", type=int, default=0, help="HODLR batch leg: product tile edge when not tuning")
     ap.add_argument("--serve-requests", type=int, default=200, help="requests per rate of the serving leg (0: skip)")
-    ap.add_argument("--serve-rates", default="5,10,20", help="Poisson arrival rates of the serving leg (1/s)")
+    ap.add_argument("--serve-rates", default="2,4,8", help="Poisson arrival rates of the serving leg (1/s)")
     ap.add_argument("--uneven", type=int, default=512, help="instances of the uneven batch leg (0: skip)")
     args = ap.parse_args()
     C3["n"] = args.n
@@ -864,6 +868,7 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
+    t_start = time.perf_counter()
     job = C3Job(pp, ctx, torch, s, rank)
     with Clocks(local) as clk:
         mixed = job.run_form(pp.BF16, args.steps, args.warmup, barrier)
@@ -877,6 +882,7 @@ def main():
     roofline = job.roofline(mixed, fp64)
     c3_config = c3_config_keys(world)
     job.release()
+    print(f"bench: headline job {time.perf_counter() - t_start:.0f} s", file=sys.stderr, flush=True)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -884,13 +890,19 @@ def main():
         cpu = {"value": 1.0 / t_est, "unit": "factor+solve/s", "cores": os.cpu_count() or 1, "kind": "port",
                "sample": sample}
     legs = {}
+    t_leg = time.perf_counter()
     if args.batch > 0:
         legs["hodlr_batch"] = c2_batch_leg(args, pp, ctx, torch, dist, rank, world, barrier, s)
+        print(f"bench: hodlr batch leg {time.perf_counter() - t_leg:.0f} s", file=sys.stderr, flush=True)
+    t_leg = time.perf_counter()
     if args.uneven > 0:
         legs["uneven_batch"] = uneven_batch_leg(pp, ctx, args.uneven, max(3, args.steps // 2), args.warmup)
+        print(f"bench: uneven batch leg {time.perf_counter() - t_leg:.0f} s", file=sys.stderr, flush=True)
+    t_leg = time.perf_counter()
     if args.serve_requests > 0:
         legs["serving"] = serving_leg(pp, ctx, args.serve_requests, [float(x) for x in args.serve_rates.split(",")],
                                       seed=2024 + rank)
+        print(f"bench: serving leg {time.perf_counter() - t_leg:.0f} s", file=sys.stderr, flush=True)
 
     if rank == 0:
         forms = {"bf16": {k: v for k, v in mixed.items() if k != "total_s"}}
