@@ -893,6 +893,8 @@ def main():
         cpu = {"value": 1.0 / t_est, "unit": "factor+solve/s", "cores": os.cpu_count() or 1, "kind": "port",
                "sample": sample}
     legs = {}
+    if world > 1:  # the legs are single-GPU measurements; replicas run the headline job only
+        args.batch = args.uneven = args.serve_requests = 0
     t_leg = time.perf_counter()
     if args.batch > 0:
         legs["hodlr_batch"] = c2_batch_leg(args, pp, ctx, torch, dist, rank, world, barrier, s)
