@@ -15,6 +15,9 @@ reports, per program (factor, solve):
 
   python pastel-palettes_b200/trace_tool.py [--n 8192] [--leaf 256] [--rank 16] [--batch 16]
                                             [--gemm-tile 64|128] [--out trace.npz]
+  python pastel-palettes_b200/trace_tool.py --workload laplace3d [--n 65536] [--form bf16|fp64]
+      the mixed-precision configuration instead (3-D Laplace, leaf 512, eta 1, adaptive rank
+      <= 32 at 1e-8, built on the device): its factor and its 8-RHS solve
 """
 import argparse
 import collections
@@ -91,6 +94,33 @@ def analyse(name, tasks, trace, ef, et, out=print):
         out(f"   ready->start latency: median {np.median(lat) / 1e3:.2f} us, p90 {np.percentile(lat, 90) / 1e3:.2f} us")
 
 
+def trace_laplace3d(pp, ctx, torch, args):
+    """Factor and 8-RHS solve of the mixed-precision configuration, traced."""
+    n = args.n if args.n != 8192 else 65536
+    h, prob = pp.make_kernel_problem(ctx, n, 3, "laplace", 1e-3, 512, 32, admissibility=1, eta=1.0, rank_tol=1e-8,
+                                     seed=1234, construct="device")
+    h.sync()
+    h.keep_original()
+    h.set_gemm_tile(128)
+    h.set_precision(pp.BF16 if args.form == "bf16" else pp.FP64)
+    b = torch.from_numpy(pp.rhs(n, 8)).cuda()
+    x = torch.empty_like(b)
+    for which, nrhs in ((0, 1), (1, 8)):
+        tasks, _, _, _ = h.encode_program(which, nrhs, [0] * 5)
+        ef, et, _ = h.edges(which, nrhs)
+        h.enable_trace(which, nrhs)
+        for _ in range(2):
+            if which == 0:
+                h.restore()
+                h.factor()
+            else:
+                h.solve(b, x)
+            h.sync()
+        tr = h.read_trace(which, nrhs)
+        analyse(f"{'factor' if which == 0 else 'solve, 8 RHS'} of the 3-D Laplace job, N = {n}, {args.form} form",
+                tasks, tr, ef, et)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=8192)
@@ -99,11 +129,16 @@ def main():
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--gemm-tile", type=int, default=128, help="output tile edge of the factor's products")
     ap.add_argument("--out", default=None, help="also save the raw trace (npz)")
+    ap.add_argument("--workload", default="hodlr", choices=["hodlr", "laplace3d"])
+    ap.add_argument("--form", default="bf16", choices=["bf16", "fp64"])
     args = ap.parse_args()
     import torch
 
     pp = _load()
     ctx = pp.Context(device=0)
+    if args.workload == "laplace3d":
+        trace_laplace3d(pp, ctx, torch, args)
+        return
     h, prob = pp.make_kernel_problem(ctx, args.n, 2, "inv", 1e-3, args.leaf, args.rank, seed=1234)
     h.set_gemm_tile(args.gemm_tile)
     h.upload()
