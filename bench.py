@@ -37,6 +37,10 @@ WORKLOAD_NAME = "hodlr-inv2d-n8192-leaf256-rank16-fp64-ir1e-10"
 # one ncu capture of the batch-4 launch (dram__bytes.sum.per_second x gpu__time_duration.sum / 4);
 # the jobs touch disjoint arenas, so the launch's traffic scales with the batch
 FACTOR_DRAM_BYTES_PER_JOB = 117.5e6
+# DRAM bytes (read + write) per algorithmic byte of the mixed factor launch of the headline job,
+# from one ncu capture of the same launch at N = 16384 (28.2 GB read + 25.9 GB written against
+# 72.9 GB of algorithmic bytes); the full-size launch's traffic is estimated by this ratio
+C3_DRAM_PER_ALGORITHMIC_BYTE = (28.221709056e9 + 25.890199552e9) / 72.9413632e9
 
 
 def load_pp():
@@ -579,7 +583,10 @@ class C3Job:
         fac_s = mixed["factor_ms"] / 1e3
         achieved = mixed["factor_bytes"] / fac_s / 1e9
         out = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-               "traffic": None, "kernel": "vm_kernel (mixed factor launch, one job)", "launch_ms": 1e3 * fac_s,
+               "traffic": C3_DRAM_PER_ALGORITHMIC_BYTE * mixed["factor_bytes"],
+               "traffic_source": "ncu DRAM bytes of the same launch at N = 16384 (0.74 per algorithmic byte), scaled "
+                                 "by the algorithmic bytes of this launch",
+               "kernel": "vm_kernel (mixed factor launch, one job)", "launch_ms": 1e3 * fac_s,
                "algorithmic_bytes": mixed["factor_bytes"],
                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"}
         bf16_peak = bf16_peak_tflops()
