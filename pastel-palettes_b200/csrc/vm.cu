@@ -533,48 +533,73 @@ __device__ __forceinline__ size_t tiled_at(int r, int c, int K, int cr) {
 // S := the tiled BF16 shadow of X (m x k, padded with zeros beyond the source's mr rows and nc
 // columns), X(r, c) = A[r lda + c] or A[c lda + r] (tA).  Each thread converts 8 consecutive
 // columns of a row and stores them as one 16-byte word, lanes along the rows (the stores of 32
-// consecutive rows fill 512 contiguous bytes).  With tA the loads are coalesced as they stand;
-// otherwise 128 x 64 blocks of X are first staged in shared memory with coalesced loads.
+// consecutive rows fill 512 contiguous bytes).  With tA the loads are coalesced as they stand
+// (four words per thread at a time: 32 loads in flight); otherwise 128 x 64 blocks of X are
+// staged in shared memory with coalesced loads, 32 per thread in flight, the loads of the next
+// block issued before the current one is converted.
 __device__ __noinline__ void dev_shadow(uint8_t* S, const double* A, int lda, bool tA, int m, int k, int mr, int nc,
                                        int cr, double* smem) {
+  auto pack = [](const uint32_t* h) {
+    uint4 v;
+    v.x = h[0] | (h[1] << 16);
+    v.y = h[2] | (h[3] << 16);
+    v.z = h[4] | (h[5] << 16);
+    v.w = h[6] | (h[7] << 16);
+    return v;
+  };
   if (tA) {
+    constexpr int W = 4;
     const int units = m * (k >> 3);
-    for (int u = threadIdx.x; u < units; u += NT) {
-      const int r = u % m, c = (u / m) << 3;
-      uint32_t h[8];
+    for (int u0 = threadIdx.x; u0 < units; u0 += W * NT) {
+      double x[W][8];
 #pragma unroll
-      for (int q = 0; q < 8; ++q) h[q] = (r < mr && c + q < nc) ? bf16_bits(ldcg(&A[(size_t)(c + q) * lda + r])) : 0u;
-      uint4 v;
-      v.x = h[0] | (h[1] << 16);
-      v.y = h[2] | (h[3] << 16);
-      v.z = h[4] | (h[5] << 16);
-      v.w = h[6] | (h[7] << 16);
-      *reinterpret_cast<uint4*>(S + tiled_at(r, c, k, cr)) = v;
+      for (int j = 0; j < W; ++j) {
+        const int u = u0 + j * NT, r = u % m, c = (u / m) << 3;
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          x[j][q] = (u < units && r < mr && c + q < nc) ? ldcg(&A[(size_t)(c + q) * lda + r]) : 0.0;
+      }
+#pragma unroll
+      for (int j = 0; j < W; ++j) {
+        const int u = u0 + j * NT, r = u % m, c = (u / m) << 3;
+        if (u >= units) break;
+        uint32_t h[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) h[q] = bf16_bits(x[j][q]);
+        *reinterpret_cast<uint4*>(S + tiled_at(r, c, k, cr)) = pack(h);
+      }
     }
   } else {
-    constexpr int BR = 128, BC = 64, LD = BC + 1;
-    for (int r0 = 0; r0 < m; r0 += BR)
-      for (int c0 = 0; c0 < k; c0 += BC) {
-        const int rows = min(BR, m - r0);
-        for (int e = threadIdx.x; e < rows * BC; e += NT) {
-          const int rr = e / BC, cc = e % BC, r = r0 + rr, c = c0 + cc;
-          smem[rr * LD + cc] = (r < mr && c < nc) ? ldcg(&A[(size_t)r * lda + c]) : 0.0;
-        }
-        __syncthreads();
-        for (int u = threadIdx.x; u < rows * (BC >> 3); u += NT) {
-          const int rr = u % rows, cg = (u / rows) << 3;
-          uint32_t h[8];
+    constexpr int BR = 128, BC = 64, LD = BC + 1, PER = BR * BC / NT;
+    const int nbc = k / BC, nb = ((m + BR - 1) / BR) * nbc;
+    double v[PER];
+    auto fetch = [&](int b) {
+      const int r0 = (b / nbc) * BR, c0 = (b % nbc) * BC;
 #pragma unroll
-          for (int q = 0; q < 8; ++q) h[q] = bf16_bits(smem[rr * LD + cg + q]);
-          uint4 v;
-          v.x = h[0] | (h[1] << 16);
-          v.y = h[2] | (h[3] << 16);
-          v.z = h[4] | (h[5] << 16);
-          v.w = h[6] | (h[7] << 16);
-          *reinterpret_cast<uint4*>(S + tiled_at(r0 + rr, c0 + cg, k, cr)) = v;
-        }
-        __syncthreads();
+      for (int p = 0; p < PER; ++p) {
+        const int e = threadIdx.x + p * NT, r = r0 + e / BC, c = c0 + e % BC;
+        v[p] = (r < m && r < mr && c < nc) ? ldcg(&A[(size_t)r * lda + c]) : 0.0;
       }
+    };
+    fetch(0);
+    for (int b = 0; b < nb; ++b) {
+      const int r0 = (b / nbc) * BR, c0 = (b % nbc) * BC, rows = min(BR, m - r0);
+#pragma unroll
+      for (int p = 0; p < PER; ++p) {
+        const int e = threadIdx.x + p * NT;
+        smem[(e / BC) * LD + e % BC] = v[p];
+      }
+      __syncthreads();
+      if (b + 1 < nb) fetch(b + 1);
+      for (int u = threadIdx.x; u < rows * (BC >> 3); u += NT) {
+        const int rr = u % rows, cg = (u / rows) << 3;
+        uint32_t h[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) h[q] = bf16_bits(smem[rr * LD + cg + q]);
+        *reinterpret_cast<uint4*>(S + tiled_at(r0 + rr, c0 + cg, k, cr)) = pack(h);
+      }
+      __syncthreads();
+    }
   }
   // the shadow is read by bulk copies (the async proxy) of other CTAs
   asm volatile("fence.proxy.async.global;" ::: "memory");
@@ -627,20 +652,40 @@ __device__ __forceinline__ void tc_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
 
+__device__ __forceinline__ void red_add_f64(double* p, double v) {
+  asm volatile("red.relaxed.gpu.global.add.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
+
 // C[r][lane] = beta C + alpha T[r][lane] for the warp's 32 rows (row stride ldc), T the 32 x 32
-// FP32 transpose buffer (row stride 33): 32 coalesced loads in flight per lane, then the stores
+// FP32 transpose buffer (row stride 33).  With beta = 1 and alpha = +-1 (every Schur update) the
+// sum goes to the L2 as a fire-and-forget FP64 reduction: one rounding of C + alpha T, the value
+// fma(alpha, T, C) gives, with no load latency on the epilogue's path.  Otherwise 32 coalesced
+// loads in flight per lane, then the stores.
 __device__ __noinline__ void bg_rows_update(double* __restrict__ cp, int ldc, const float* tb, int lane, double alpha,
                                             double beta) {
+  if (beta == 1.0 && (alpha == 1.0 || alpha == -1.0)) {
+#pragma unroll
+    for (int rr = 0; rr < 32; ++rr) red_add_f64(cp + (size_t)rr * ldc, alpha * (double)tb[rr * 33 + lane]);
+    return;
+  }
   double cv[32];
 #pragma unroll
   for (int rr = 0; rr < 32; ++rr) cv[rr] = beta != 0.0 ? __ldcg(cp + (size_t)rr * ldc) : 0.0;
 #pragma unroll
-  for (int rr = 0; rr < 32; ++rr) cp[(size_t)rr * ldc] = fma(alpha, (double)tb[rr * 33 + lane], cv[rr]);
+  for (int rr = 0; rr < 32; ++rr) cp[(size_t)rr * ldc] = fma(alpha, (double)tb[rr * 33 + lane], beta * cv[rr]);
 }
 
 // the same for two adjacent 32-column pieces (buffers T and T + 32 x 33): 64 loads in flight
 __device__ __noinline__ void bg_rows_update2(double* __restrict__ cp, int ldc, const float* tb, int lane, double alpha,
                                              double beta) {
+  if (beta == 1.0 && (alpha == 1.0 || alpha == -1.0)) {
+#pragma unroll
+    for (int rr = 0; rr < 32; ++rr) {
+      red_add_f64(cp + (size_t)rr * ldc, alpha * (double)tb[rr * 33 + lane]);
+      red_add_f64(cp + (size_t)rr * ldc + 32, alpha * (double)tb[32 * 33 + rr * 33 + lane]);
+    }
+    return;
+  }
   double cv[64];
 #pragma unroll
   for (int rr = 0; rr < 32; ++rr) {
@@ -649,8 +694,8 @@ __device__ __noinline__ void bg_rows_update2(double* __restrict__ cp, int ldc, c
   }
 #pragma unroll
   for (int rr = 0; rr < 32; ++rr) {
-    cp[(size_t)rr * ldc] = fma(alpha, (double)tb[rr * 33 + lane], cv[rr]);
-    cp[(size_t)rr * ldc + 32] = fma(alpha, (double)tb[32 * 33 + rr * 33 + lane], cv[32 + rr]);
+    cp[(size_t)rr * ldc] = fma(alpha, (double)tb[rr * 33 + lane], beta * cv[rr]);
+    cp[(size_t)rr * ldc + 32] = fma(alpha, (double)tb[32 * 33 + rr * 33 + lane], beta * cv[32 + rr]);
   }
 }
 
