@@ -370,14 +370,23 @@ int run_one(const pp_task& T, std::vector<double>& tmp) {
     case PP_OP_SHADOW: {  // engine instruction: BF16 copy of an operand in the tiled layout
       const int cr = T.ctrl ? T.ctrl : 128;  // chunk rows of the layout
       if (T.m % cr || T.k % 64) return -1;
+      // split shadow (pp_task.h PP_SPLIT_*): nseg copies of the source columns, bf16(x) or the
+      // residual bf16(x - bf16(x)) where the segment's bit of the low mask is set
+      const int nseg = T.o ? T.o >> 8 : 1, lo_mask = T.o & 0xFF;
+      if (T.o && (nseg != 3 || T.k % (64 * nseg))) return -1;
+      const int ks = T.k / nseg;
       uint8_t* S = reinterpret_cast<uint8_t*>(T.p[0]);
-      const int mr = T.l > 0 ? T.l : T.m, nc = T.n > 0 ? T.n : T.k;  // source rows / columns; zeros beyond
+      const int mr = T.l > 0 ? T.l : T.m, nc = T.n > 0 ? T.n : ks;  // source rows / columns; zeros beyond
       for (int r = 0; r < T.m; ++r)
-        for (int c = 0; c < T.k; ++c) {
+        for (int c = 0; c < ks; ++c) {
           const double x = (r >= mr || c >= nc) ? 0.0
                            : t1 ? T.p[1][(int64_t)c * T.ld[1] + r] : T.p[1][(int64_t)r * T.ld[1] + c];
           const uint16_t h = to_bf16(x);
-          std::memcpy(S + tiled_at(r, c, T.k, cr), &h, 2);
+          const uint16_t lo = to_bf16(x - from_bf16(h));
+          for (int sg = 0; sg < nseg; ++sg) {
+            const uint16_t v = ((lo_mask >> sg) & 1) ? lo : h;
+            std::memcpy(S + tiled_at(r, c + sg * ks, T.k, cr), &v, 2);
+          }
         }
       return 0;
     }

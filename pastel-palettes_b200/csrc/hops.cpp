@@ -518,9 +518,9 @@ int Generator::tri_limit(int target_extent) const {
 // The BF16 shadow of an operand view (m x n logical, m a multiple of cr), columns padded to a
 // multiple of 64, written by a SHADOW instruction at its first use and reused until the view's
 // object is written again.
-View Generator::shadow_of(const View& X, int cr) {
+View Generator::shadow_of(const View& X, int cr, int split) {
   if ((int)shadows_.size() < (int)P_.objs.size()) shadows_.resize(P_.objs.size());
-  const ShadowKey key{X.obj, X.r0, X.c0, X.m, X.n, X.t, cr};
+  const ShadowKey key{X.obj, X.r0, X.c0, X.m, X.n, X.t, cr, split};
   for (auto& e : shadows_[X.obj])
     if (e.first == key) {
       View s;
@@ -529,19 +529,20 @@ View Generator::shadow_of(const View& X, int cr) {
       s.n = P_.objs[e.second].cols;
       return s;
     }
-  const int K = (X.n + 63) & ~63;
-  // X.m rows of K BF16 values: K / 4 doubles per row (the tiled layout is opaque to the DAG)
+  const int K = (X.n + 63) & ~63, KT = split ? (split >> 8) * K : K;
+  // X.m rows of KT BF16 values: KT / 4 doubles per row (the tiled layout is opaque to the DAG)
   View s;
-  s.obj = P_.add_obj(P_.arena_id(inst_, AR_SCRATCH), X.m, K / 4, true);
+  s.obj = P_.add_obj(P_.arena_id(inst_, AR_SCRATCH), X.m, KT / 4, true);
   s.m = X.m;
-  s.n = K / 4;
+  s.n = KT / 4;
   HTask& t = emit(PP_OP_SHADOW);
   bind(t, 0, s, true);
   bind(t, 1, X, false);
   t.t.m = X.m;
-  t.t.k = K;
+  t.t.k = KT;
   t.t.n = X.n < K ? X.n : 0;
   t.t.ctrl = cr == 128 ? 0 : cr;
+  t.t.o = split;
   t.flops = 0;
   if ((int)shadows_.size() < (int)P_.objs.size()) shadows_.resize(P_.objs.size());
   shadows_[X.obj].push_back({key, s.obj});
@@ -578,6 +579,30 @@ bool Generator::bf16_product(const View& C, const View& A, const View& B, int al
   return true;
 }
 
+bool Generator::split_product(const View& C, const View& A, const View& B, int64_t flops) {
+  const bool wide = C.n % 256 == 0;
+  if (C.t || C.m % 128 != 0 || !(wide || C.n == 32 || C.n == 64 || C.n == 128) || A.n % 64 != 0) return false;
+  const View As = shadow_of(A, 128, PP_SPLIT_A);
+  const View Bs = shadow_of(B.T(), wide ? 128 : C.n, PP_SPLIT_B);
+  HTask& t = emit(PP_OP_GEMM);
+  bind(t, 0, C, true);
+  bind(t, 1, As, false);
+  bind(t, 2, Bs, false);
+  t.t.prec = PP_PREC_BF16;
+  t.t.m = C.m;
+  t.t.n = C.n;
+  t.t.k = 3 * A.n;
+  t.t.alpha = 1.0;
+  t.t.beta = 0.0;
+  t.flops = flops;
+  return true;
+}
+
+bool Generator::mixed_inverse(const Mat& T, int& invL, int& invU) const {
+  if (prec_ != PP_PREC_BF16 || solve_ || T.m < kBigLeaf || !inverse_of(T, invL, invU)) return false;
+  return T.d.obj < (int)inv_done_.size() && inv_done_[T.d.obj];
+}
+
 void Generator::getrf_program() {
   getrf(node(H_.root));
   if (inverses_) emit_inverses();
@@ -596,32 +621,42 @@ bool Generator::inverse_of(const Mat& T, int& invL, int& invU) const {
 
 // TRINV tasks: after its GETRF a diagonal leaf is final; its L^-1 and U^-1 are built in
 // column blocks of T_ on idle CTAs while the factorization goes on elsewhere.
+// The mixed form emits a large leaf's TRINV tasks right after its GETRF instead (its panel
+// solves use the inverses); the rest follow the factorization here.
 void Generator::emit_inverses() {
   for (const HNode& nd : H_.nodes) {
     if (nd.kind != HNode::D || nd.invL < 0) continue;
-    View A;
-    A.obj = node_obj_[nd.obj];
-    A.m = nd.m;
-    A.n = nd.n;
-    for (int which = 0; which < 2; ++which) {
-      View I;
-      I.obj = node_obj_[which == 0 ? nd.invL : nd.invU];
-      I.m = nd.m;
-      I.n = nd.m;
-      for (int c0 = 0; c0 < nd.m; c0 += T_) {
-        const int w = std::min(T_, nd.m - c0);
-        HTask& t = emit(PP_OP_TRINV);
-        bind(t, 0, I.sub(0, c0, nd.m, w), true);
-        bind(t, 1, A, false);
-        t.t.m = nd.m;
-        t.t.n = w;
-        t.t.o = c0;
-        t.t.ctrl = which;
-        const int64_t rows = which == 0 ? nd.m - c0 : c0 + w;  // rows the sweep touches
-        t.flops = (int64_t)w * rows * rows;
-      }
+    const int obj = node_obj_[nd.obj];
+    if (obj < (int)inv_done_.size() && inv_done_[obj]) continue;
+    emit_inverse(obj, nd.m);
+  }
+}
+
+void Generator::emit_inverse(int leaf_obj, int m) {
+  View A;
+  A.obj = leaf_obj;
+  A.m = m;
+  A.n = m;
+  for (int which = 0; which < 2; ++which) {
+    View I;
+    I.obj = which == 0 ? inv_obj_[leaf_obj].first : inv_obj_[leaf_obj].second;
+    I.m = m;
+    I.n = m;
+    for (int c0 = 0; c0 < m; c0 += T_) {
+      const int w = std::min(T_, m - c0);
+      HTask& t = emit(PP_OP_TRINV);
+      bind(t, 0, I.sub(0, c0, m, w), true);
+      bind(t, 1, A, false);
+      t.t.m = m;
+      t.t.n = w;
+      t.t.o = c0;
+      t.t.ctrl = which;
+      const int64_t rows = which == 0 ? m - c0 : c0 + w;  // rows the sweep touches
+      t.flops = (int64_t)w * rows * rows;
     }
   }
+  if ((int)inv_done_.size() <= leaf_obj) inv_done_.resize(leaf_obj + 1, 0);
+  inv_done_[leaf_obj] = 1;
 }
 
 void Generator::solve_program(int nrhs) {
@@ -725,16 +760,27 @@ void Generator::getrf(const Mat& A) {
     t.t.m = A.m;
     t.t.n = A.n;
     t.flops = flops_getrf(A.m, A.n);
-    return;
+  } else {
+    Mat p[2][2];
+    int nr, nc;
+    partition(A, s, A.kind == Mat::H ? hsplit_c(A) : s, p, nr, nc);
+    getrf(p[0][0]);
+    trsml(p[0][0], p[0][1]);
+    trsmr(p[0][0], p[1][0]);
+    gemm(p[1][1], p[1][0], p[0][1], -1);
+    getrf(p[1][1]);
   }
-  Mat p[2][2];
-  int nr, nc;
-  partition(A, s, A.kind == Mat::H ? hsplit_c(A) : s, p, nr, nc);
-  getrf(p[0][0]);
-  trsml(p[0][0], p[0][1]);
-  trsmr(p[0][0], p[1][0]);
-  gemm(p[1][1], p[1][0], p[0][1], -1);
-  getrf(p[1][1]);
+  int invL, invU;
+  if (prec_ == PP_PREC_BF16 && !solve_ && A.m >= kBigLeaf && inverse_of(A, invL, invU)) emit_inverse(A.d.obj, A.m);
+}
+
+// An inverse of m x m as a view (the whole object).
+static View whole(int obj, int m) {
+  View v;
+  v.obj = obj;
+  v.m = m;
+  v.n = m;
+  return v;
 }
 
 void Generator::trsml(const Mat& L, const Mat& B) {
@@ -744,6 +790,10 @@ void Generator::trsml(const Mat& L, const Mat& B) {
     trmv(invL, 0, L.m, B.d);
     return;
   }
+  // mixed form: B := L^-1 B as one product with the explicit inverse
+  if (B.kind == Mat::D && !B.d.t && mixed_inverse(L, invL, invU) &&
+      split_product(B.d, whole(invL, L.m), B.d, (int64_t)B.n * L.m * (L.m - 1)))
+    return;
   const int s = tri_split(L, tri_limit(B.n));
   if (s < 0) {
     if (B.kind != Mat::D || B.d.t) throw std::logic_error("trsml: target must be a dense untransposed block");
@@ -771,6 +821,11 @@ void Generator::trsml(const Mat& L, const Mat& B) {
 
 void Generator::trsmr(const Mat& U, const Mat& B) {
   if (B.kind == Mat::LR) { trsmrt(U, B.v); return; }
+  int invL, invU;
+  // mixed form: B := B U^-1 as one product with the explicit inverse
+  if (B.kind == Mat::D && !B.d.t && mixed_inverse(U, invL, invU) &&
+      split_product(B.d, B.d, whole(invU, U.m), (int64_t)B.m * U.m * U.m))
+    return;
   const int s = tri_split(U, tri_limit(B.m));
   if (s < 0) {
     if (B.kind != Mat::D || B.d.t) throw std::logic_error("trsmr: target must be a dense untransposed block");
@@ -799,6 +854,9 @@ void Generator::trsmr(const Mat& U, const Mat& B) {
 
 void Generator::trsmrt(const Mat& U, const View& V) {
   if (V.t) throw std::logic_error("trsmrt: V must be untransposed");
+  int invL, invU;
+  // mixed form: V := U^-T V as one product with the explicit inverse
+  if (mixed_inverse(U, invL, invU) && split_product(V, whole(invU, U.m).T(), V, (int64_t)V.n * U.m * U.m)) return;
   const int s = tri_split(U, Ttri_);
   if (s < 0) {
     for (int c = 0; c < V.n; c += T_) {

@@ -194,16 +194,27 @@ class Generator {
   struct ShadowKey {
     int obj, r0, c0, m, n;
     bool t;
-    int cr;
+    int cr, split;
     bool operator==(const ShadowKey& o) const {
-      return obj == o.obj && r0 == o.r0 && c0 == o.c0 && m == o.m && n == o.n && t == o.t && cr == o.cr;
+      return obj == o.obj && r0 == o.r0 && c0 == o.c0 && m == o.m && n == o.n && t == o.t && cr == o.cr &&
+             split == o.split;
     }
   };
   std::vector<std::vector<std::pair<ShadowKey, int>>> shadows_;  // per program object
   // the shadow of X in the tiled layout with chunks of cr rows (128 for an A operand; for a B
-  // operand 128 or its row count), columns padded with zeros to a multiple of 64
-  View shadow_of(const View& X, int cr = 128);
+  // operand 128 or its row count), columns padded with zeros to a multiple of 64; split: 0, or
+  // PP_SPLIT_A / PP_SPLIT_B (three segments of the padded columns, pp_task.h)
+  View shadow_of(const View& X, int cr = 128, int split = 0);
   bool bf16_product(const View& C, const View& A, const View& B, int alpha);
+  // C := A B from split shadows (about 2^-16 accurate), C possibly aliasing A or B; false when
+  // the shapes do not fit the BF16 GEMM
+  bool split_product(const View& C, const View& A, const View& B, int64_t flops);
+  // the mixed form's triangular solves of a factorization against a whole diagonal leaf of
+  // kBigLeaf or more: the product with the leaf's explicit inverse (its TRINV tasks emitted
+  // right after the leaf's GETRF) as one split-shadow product; returns the inverse objects
+  bool mixed_inverse(const Mat& T, int& invL, int& invU) const;
+  void emit_inverse(int leaf_obj, int m);
+  std::vector<char> inv_done_;  // program obj of a diagonal leaf -> its TRINV tasks are emitted
   bool whole_leaf(const View& v) const;
   int tri_limit(int target_extent) const;
   void trmv(int inv, int upper, int m, const View& B);

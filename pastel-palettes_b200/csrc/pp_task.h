@@ -47,7 +47,10 @@ enum pp_op {
                         X(r, c) = p[1][r * ld[1] + c] (or p[1][c * ld[1] + r] with PP_T(1)),
                         rounded to BF16 and written at p[0] in the tiled layout below (m a
                         multiple of 128, k of 64); rows from l and columns from n on (when set)
-                        are written as zeros (padding); no reference counterpart               */
+                        are written as zeros (padding).  o != 0: a split shadow (PP_SPLIT_*):
+                        the k columns are o >> 8 segments of k / (o >> 8), each a copy of X's
+                        columns holding bf16(x), or the residual bf16(x - bf16(x)) where bit s
+                        of o & 0xFF is set; no reference counterpart                            */
   PP_OP_KMUL = 16,   /* C[m x k] (p[0]) := K(P_I, P_J) B: a kernel matrix evaluated from points
                         times B (p[3], n x k, k <= 32); P_I = p[1] (m points), P_J = p[2] (n
                         points), rows of dim = l coordinates (ld[1], ld[2]); kernel ctrl (0
@@ -78,6 +81,13 @@ enum pp_op {
  * the tensor cores, C (FP64) := beta C + alpha sum.  m a multiple of 128, k of 64, n 32, 64, 128
  * or a multiple of 256. */
 #define PP_PREC_BF16 2
+
+/* Split shadows (SHADOW o): a product A B summed over K' = 3 K from the shadows
+ * [hi(A) lo(A) hi(A)] and [hi(B) hi(B) lo(B)] is hi hi + lo hi + hi lo, the product of the
+ * operands to about 2^-16 of their magnitude instead of BF16's 2^-8 (the mixed form's solves
+ * against explicit inverses of the diagonal leaves). */
+#define PP_SPLIT_A ((3 << 8) | 0x2)
+#define PP_SPLIT_B ((3 << 8) | 0x4)
 
 /* Tiled BF16 layout of an R x K operand (R a multiple of the chunk height h = 128, 64 or 32 — the
  * SHADOW task's ctrl, 0 meaning 128 — and K of 64): chunks of h rows x 64 columns (h * 128 bytes),

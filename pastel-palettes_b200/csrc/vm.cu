@@ -536,20 +536,41 @@ __device__ __forceinline__ size_t tiled_at(int r, int c, int K, int cr) {
 // consecutive rows fill 512 contiguous bytes).  With tA the loads are coalesced as they stand
 // (four words per thread at a time: 32 loads in flight); otherwise 128 x 64 blocks of X are
 // staged in shared memory with coalesced loads, 32 per thread in flight, the loads of the next
-// block issued before the current one is converted.
+// block issued before the current one is converted.  A split shadow (split = PP_SPLIT_*, k = nseg
+// segments of ks columns) writes each word once per segment: bf16(x), or the residual
+// bf16(x - bf16(x)) in the segments of the low mask.
+__device__ __forceinline__ void shadow_word(uint8_t* S, int r, int c, int k, int ks, int cr, int split,
+                                            const double* x) {
+  uint32_t h[8], l[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    h[q] = bf16_bits(x[q]);
+    l[q] = split ? bf16_bits(x[q] - (double)__uint_as_float(h[q] << 16)) : 0u;
+  }
+  uint4 vh, vl;
+  vh.x = h[0] | (h[1] << 16);
+  vh.y = h[2] | (h[3] << 16);
+  vh.z = h[4] | (h[5] << 16);
+  vh.w = h[6] | (h[7] << 16);
+  if (!split) {
+    *reinterpret_cast<uint4*>(S + tiled_at(r, c, k, cr)) = vh;
+    return;
+  }
+  vl.x = l[0] | (l[1] << 16);
+  vl.y = l[2] | (l[3] << 16);
+  vl.z = l[4] | (l[5] << 16);
+  vl.w = l[6] | (l[7] << 16);
+  const int nseg = split >> 8;
+  for (int sg = 0; sg < nseg; ++sg)
+    *reinterpret_cast<uint4*>(S + tiled_at(r, c + sg * ks, k, cr)) = ((split >> sg) & 1) ? vl : vh;
+}
+
 __device__ __noinline__ void dev_shadow(uint8_t* S, const double* A, int lda, bool tA, int m, int k, int mr, int nc,
-                                       int cr, double* smem) {
-  auto pack = [](const uint32_t* h) {
-    uint4 v;
-    v.x = h[0] | (h[1] << 16);
-    v.y = h[2] | (h[3] << 16);
-    v.z = h[4] | (h[5] << 16);
-    v.w = h[6] | (h[7] << 16);
-    return v;
-  };
+                                       int cr, int split, double* smem) {
+  const int ks = split ? k / (split >> 8) : k;  // source columns (one segment)
   if (tA) {
     constexpr int W = 4;
-    const int units = m * (k >> 3);
+    const int units = m * (ks >> 3);
     for (int u0 = threadIdx.x; u0 < units; u0 += W * NT) {
       double x[W][8];
 #pragma unroll
@@ -563,15 +584,12 @@ __device__ __noinline__ void dev_shadow(uint8_t* S, const double* A, int lda, bo
       for (int j = 0; j < W; ++j) {
         const int u = u0 + j * NT, r = u % m, c = (u / m) << 3;
         if (u >= units) break;
-        uint32_t h[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) h[q] = bf16_bits(x[j][q]);
-        *reinterpret_cast<uint4*>(S + tiled_at(r, c, k, cr)) = pack(h);
+        shadow_word(S, r, c, k, ks, cr, split, x[j]);
       }
     }
   } else {
     constexpr int BR = 128, BC = 64, LD = BC + 1, PER = BR * BC / NT;
-    const int nbc = k / BC, nb = ((m + BR - 1) / BR) * nbc;
+    const int nbc = ks / BC, nb = ((m + BR - 1) / BR) * nbc;
     double v[PER];
     auto fetch = [&](int b) {
       const int r0 = (b / nbc) * BR, c0 = (b % nbc) * BC;
@@ -593,10 +611,10 @@ __device__ __noinline__ void dev_shadow(uint8_t* S, const double* A, int lda, bo
       if (b + 1 < nb) fetch(b + 1);
       for (int u = threadIdx.x; u < rows * (BC >> 3); u += NT) {
         const int rr = u % rows, cg = (u / rows) << 3;
-        uint32_t h[8];
+        double x[8];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) h[q] = bf16_bits(smem[rr * LD + cg + q]);
-        *reinterpret_cast<uint4*>(S + tiled_at(r0 + rr, c0 + cg, k, cr)) = pack(h);
+        for (int q = 0; q < 8; ++q) x[q] = smem[rr * LD + cg + q];
+        shadow_word(S, r0 + rr, c0 + cg, k, ks, cr, split, x);
       }
       __syncthreads();
     }
@@ -1988,8 +2006,9 @@ __device__ bool run_task(const pp_task& T, double* smem, TcCtx& tc, int& err) {
       if (T.m < 32 || T.k < 64 || T.k % 64) return false;
       if (T.l < 0 || T.l > T.m || T.n < 0 || T.n > T.k) return false;
       if (!(T.ctrl == 0 || T.ctrl == 32 || T.ctrl == 64 || T.ctrl == 128) || T.m % (T.ctrl ? T.ctrl : 128)) return false;
+      if (T.o != 0 && (T.o >> 8 != 3 || (T.o & ~0x7FF) || T.k % (64 * 3) || T.n > T.k / 3)) return false;
       dev_shadow(reinterpret_cast<uint8_t*>(T.p[0]), T.p[1], T.ld[1], T.flags & PP_T(1), T.m, T.k,
-                 T.l > 0 ? T.l : T.m, T.n > 0 ? T.n : T.k, T.ctrl ? T.ctrl : 128, smem);
+                 T.l > 0 ? T.l : T.m, T.n > 0 ? T.n : (T.o ? T.k / 3 : T.k), T.ctrl ? T.ctrl : 128, T.o, smem);
       return true;
     default: return false;
   }

@@ -211,3 +211,72 @@ def test_bf16_skinny_and_padded_products_vs_oracle(pp, oracle, bctx, m, n, k):
     (Cd, Asd, Bsd), (Ch, Ash, Bsh) = out["dev"], out["host"]
     assert np.array_equal(Asd, Ash) and np.array_equal(Bsd, Bsh)
     assert rel(Cd - C, Ch - C) < 1e-5
+
+
+SPLIT_A, SPLIT_B = (3 << 8) | 2, (3 << 8) | 4
+
+
+@pytest.mark.parametrize("transposed,split,cr", [(False, SPLIT_A, 128), (True, SPLIT_A, 128),
+                                                 (False, SPLIT_B, 128), (True, SPLIT_B, 32)])
+def test_split_shadow_bitwise_vs_oracle(pp, oracle, bctx, transposed, split, cr):
+    """Split shadows (three segments: bf16(x) or the residual bf16(x - bf16(x))), the operands of
+    the mixed form's products with explicit inverses; 480 source columns padded to 512."""
+    rng = np.random.default_rng(12 + split)
+    rows, k_src = 256, 480
+    K = 512
+    src = rng.standard_normal((k_src, rows) if transposed else (rows, k_src)) * 10.0 ** rng.integers(-3, 3)
+    ld = src.shape[1]
+    out = []
+    for side in ("dev", "host"):
+        sh = torch.zeros(rows * 3 * K // 4, dtype=torch.float64, device="cuda") if side == "dev" else \
+            np.zeros(rows * 3 * K // 4)
+        s = dev(src) if side == "dev" else src
+        t = shadow_task(pp, ptr(sh), ptr(s), rows, 3 * K, transposed, ld)
+        t[0]["n"], t[0]["o"], t[0]["ctrl"] = k_src, split, 0 if cr == 128 else cr
+        if side == "dev":
+            bctx.vm_execute(t, np.zeros(0, np.int32), np.zeros(1, np.int32))
+            out.append(sh.cpu().numpy())
+        else:
+            assert oracle.lib().oracle_run_program(t.ctypes.data, 1) == 0
+            out.append(sh)
+    assert np.array_equal(out[0].view(np.uint16), out[1].view(np.uint16))
+
+
+@pytest.mark.parametrize("m,n,k", [(512, 512, 512), (512, 32, 512), (256, 256, 256)])
+def test_split_product_accuracy(pp, oracle, bctx, m, n, k):
+    """C := A B (beta 0) from split shadows [hi lo hi] x [hi hi lo] (K = 3 k): within 2e-5 of the
+    FP64 product relative to |A| |B| (BF16 alone: about 4e-3), and within 1e-5 of the oracle's
+    FP64 sum of the same products (the tensor cores sum the 3 k terms in FP32)."""
+    rng = np.random.default_rng(m + n + k)
+    A, Bt = rng.standard_normal((m, k)), rng.standard_normal((n, k))
+    cr = 128 if n % 256 == 0 else n
+    out = {}
+    for side in ("dev", "host"):
+        mk = (lambda x: dev(x)) if side == "dev" else (lambda x: x.copy())
+        Cx, Ax, Bx = mk(np.full((m, n), 7.0)), mk(A), mk(Bt)
+        z = lambda e: torch.zeros(e, dtype=torch.float64, device="cuda") if side == "dev" else np.zeros(e)
+        As, Bs = z(m * 3 * k // 4), z(n * 3 * k // 4)
+        ta = shadow_task(pp, ptr(As), ptr(Ax), m, 3 * k, False, k)
+        ta[0]["o"] = SPLIT_A
+        tb = shadow_task(pp, ptr(Bs), ptr(Bx), n, 3 * k, False, k)
+        tb[0]["o"], tb[0]["ctrl"] = SPLIT_B, 0 if cr == 128 else cr
+        g = np.zeros(1, dtype=pp.TASK_DTYPE)
+        g[0]["op"], g[0]["prec"] = GEMM, BF16
+        g[0]["m"], g[0]["n"], g[0]["k"] = m, n, 3 * k
+        g[0]["alpha"], g[0]["beta"] = 1.0, 0.0
+        g[0]["p"][0], g[0]["p"][1], g[0]["p"][2] = ptr(Cx), ptr(As), ptr(Bs)
+        g[0]["ld"][0] = n
+        tasks = np.concatenate([ta, tb, g])
+        tasks[0]["succ_begin"], tasks[0]["n_succ"] = 0, 1
+        tasks[1]["succ_begin"], tasks[1]["n_succ"] = 1, 1
+        if side == "dev":
+            bctx.vm_execute(tasks, np.array([2, 2], np.int32), np.array([0, 0, 2], np.int32))
+            out[side] = Cx.cpu().numpy()
+        else:
+            assert oracle.lib().oracle_run_program(tasks.ctypes.data, 3) == 0
+            out[side] = Cx
+    want = A @ Bt.T
+    scale = np.abs(A) @ np.abs(Bt).T
+    assert (np.abs(out["dev"] - want) / scale).max() < 2e-5
+    assert (np.abs(out["host"] - want) / scale).max() < 2e-5
+    assert rel(out["dev"], out["host"]) < 1e-5
