@@ -350,7 +350,7 @@ pp_status pp_vm_execute(pp_context* ctx, const void* tasks, int n_tasks, const i
  * is fully reserved by an admission budget, and host frameworks that own the device memory
  * pool.  Its scratch is one static device array of PP_ACCUM_NOALLOC_MAX_SCRATCH doubles
  * (8 MiB), held by every GPU that loads the library until the process exits.  The accumulation
- * keeps its ny x k1 sketch in shared memory while that fits (ny * k1 up to about 12 000 - 20 000
+ * keeps its ny x k1 sketch in shared memory while that fits (ny * k1 up to about 17 000 - 20 000
  * doubles, by rank); a larger sketch goes to the array, so ny * k1 <= 2^20 is the limit.
  * 1 <= k1, k2 <= 32 and k1 <= min(ny, nx); other requests return PP_INVALID_ARG without
  * touching the device.  The call runs on the context's device.

@@ -1327,19 +1327,60 @@ __device__ __noinline__ void dev_gemm4(const pp_task& T, double* smem) {
 //   3x: G = Y^T Y (+ shift), G = C^T C, Y := Y C^-1
 //   P  = Y^T [U1 U2]                      (one pass over the ny rows)
 //   V1 := V1 P1^T + alpha V2 P2^T,  U1 := Y
-// Y stays in shared memory when it fits (ny k1 <= the Y capacity), else in the task's
-// global scratch.  The long reductions are warp-sliced (lanes own output columns, warps
-// own row slices) and the warp partials are combined in a fixed order, so results are
-// deterministic.
+// Y stays in shared memory when it fits (ny k1 <= the Y capacity: a 512 x 32 sketch does),
+// else in the task's global scratch.  The long reductions are warp-sliced (lanes own output
+// columns, warps own row slices) and the warp partials are summed in a fixed order through
+// two slots, so results are deterministic.
 #define ACC_LG (PP_VM_MAX_RANK + 1)
 
 template <int KB>
 struct AccumSmem {
-  static constexpr int RED = 4 * KB * 2 * KB;    // 4 partial slots of a KB x 2KB output
-  static constexpr int S = KB * 2 * KB;          // S (then P): k1 x (k1 + k2), ld 2 KB
-  static constexpr int G = KB * ACC_LG + KB;     // Gram / Cholesky factor + reciprocals
-  static constexpr int YCAP = VM_SMEM_BYTES / 8 - RED - S - G;
+  // a partial slot holds a KB x 2KB output (ld 2KB); the first one also holds the Jacobi
+  // workspace (Z, rotations, pairs) of the adaptive truncation
+  static constexpr int SLOT0 = KB * 2 * KB, JAC = KB * ACC_LG + 3 * KB + 4;
+  static constexpr int SLOT = SLOT0 > JAC ? SLOT0 : (JAC + 7) & ~7;
+  static constexpr int RED = 2 * SLOT;
+  static constexpr int SOFF = SLOT;            // S (then P): k1 x (k1 + k2), ld 2 KB, in the second
+                                               // slot (written only after the slots are summed)
+  static constexpr int G = KB * ACC_LG + KB;   // Gram / Cholesky factor + reciprocals
+  static constexpr int YCAP = VM_SMEM_BYTES / 8 - RED - G;
 };
+
+// whether ACCUM keeps its ny x k1 sketch in shared memory (rows padded to k1 + 1 doubles, so
+// that a thread per row reads distinct banks); otherwise it lives in the task's scratch (ld k1)
+__host__ __device__ constexpr bool accum_y_on_chip(long long ny, int k1, int k2) {
+  return ny * (k1 + 1) <= ((k1 <= 16 && k2 <= 16) ? AccumSmem<16>::YCAP : AccumSmem<32>::YCAP);
+}
+
+// out1 = the first b1, out2 = the next b2 columns of the a x (b1 + b2) sum of the two slots
+// (each read before any is written, so out may alias the slots)
+template <int KB>
+__device__ __forceinline__ void accum_combine(const double* red, int a, int b1, int b2, double* out1, double* out2,
+                                              int ldo) {
+  constexpr int SW = 2 * KB, SL = AccumSmem<KB>::SLOT, PER = (KB * 2 * KB + NT - 1) / NT;
+  const int bt = b1 + b2;
+  double v[PER];
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const int e = threadIdx.x + q * NT;
+    v[q] = 0.0;
+    if (e < a * bt) {
+      const int i = e / bt, j = e % bt, col = j < b1 ? j : KB + (j - b1);
+      v[q] = red[i * SW + col] + red[SL + i * SW + col];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < PER; ++q) {
+    const int e = threadIdx.x + q * NT;
+    if (e < a * bt) {
+      const int i = e / bt, j = e % bt;
+      if (j < b1) out1[i * ldo + j] = v[q];
+      else out2[i * ldo + (j - b1)] = v[q];
+    }
+  }
+  __syncthreads();
+}
 
 template <bool GLOBAL>
 __device__ __forceinline__ double ld_any(const double* p) {
@@ -1390,36 +1431,22 @@ __device__ __noinline__ void accum_tn(const double* X, int lx, int a, const doub
       }
     }
   }
-  // warps 4..7 deposit, warps 0..3 add theirs, one thread per output adds the four slots
-  constexpr int SW = 2 * KB;  // slot row width
-  if (w >= 4) {
+  // warp partials through two slots: warps 6, 7 store theirs, then 4, 5, then 2, 3, then 0, 1
+  // add theirs; the two slots are summed last
+  constexpr int SW = 2 * KB, SL = AccumSmem<KB>::SLOT;
+  for (int rd = 3; rd >= 0; --rd) {
+    if ((w >> 1) == rd) {
+      double* slot = red + (w & 1) * SL;
 #pragma unroll
-    for (int i = 0; i < KB; ++i)
-      if (i < a) {
-        if (lane < b1) red[((w - 4) * KB + i) * SW + lane] = acc1[i];
-        if (lane < b2) red[((w - 4) * KB + i) * SW + KB + lane] = acc2[i];
-      }
+      for (int i = 0; i < KB; ++i)
+        if (i < a) {
+          if (lane < b1) slot[i * SW + lane] = rd == 3 ? acc1[i] : acc1[i] + slot[i * SW + lane];
+          if (lane < b2) slot[i * SW + KB + lane] = rd == 3 ? acc2[i] : acc2[i] + slot[i * SW + KB + lane];
+        }
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  if (w < 4) {
-#pragma unroll
-    for (int i = 0; i < KB; ++i)
-      if (i < a) {
-        if (lane < b1) red[(w * KB + i) * SW + lane] = acc1[i] + red[(w * KB + i) * SW + lane];
-        if (lane < b2) red[(w * KB + i) * SW + KB + lane] = acc2[i] + red[(w * KB + i) * SW + KB + lane];
-      }
-  }
-  __syncthreads();
-  const int bt = b1 + b2;
-  for (int e = threadIdx.x; e < a * bt; e += NT) {
-    const int i = e / bt, j = e % bt;
-    const int col = j < b1 ? j : KB + (j - b1);
-    const double v = red[(0 * KB + i) * SW + col] + red[(1 * KB + i) * SW + col] + red[(2 * KB + i) * SW + col] +
-                     red[(3 * KB + i) * SW + col];
-    if (j < b1) out1[i * ldo + j] = v;
-    else out2[i * ldo + (j - b1)] = v;
-  }
-  __syncthreads();
+  accum_combine<KB>(red, a, b1, b2, out1, out2, ldo);
 }
 
 // FP64 tensor-core form of accum_tn for untransposed W (the usual case): per warp, its row
@@ -1476,7 +1503,7 @@ __device__ __noinline__ void accum_tn_mma(const double* X, int lx, int a, const 
           if (8 * j < b2) dmma(c2[i][j][0], c2[i][j][1], fa[s][i], f2[s][j]);
         }
   }
-  constexpr int SW = 2 * KB;
+  constexpr int SW = 2 * KB, SL = AccumSmem<KB>::SLOT;
   auto deposit = [&](int slot, bool add) {
 #pragma unroll
     for (int i = 0; i < MT; ++i)
@@ -1486,29 +1513,21 @@ __device__ __noinline__ void accum_tn_mma(const double* X, int lx, int a, const 
         for (int e = 0; e < 2; ++e) {
           const int r = 8 * i + qr, c = 8 * j + 2 * qc + e;
           if (r < a && c < b1) {
-            double* p = &red[(slot * KB + r) * SW + c];
+            double* p = &red[slot * SL + r * SW + c];
             *p = add ? c1[i][j][e] + *p : c1[i][j][e];
           }
           if (r < a && c < b2) {
-            double* p = &red[(slot * KB + r) * SW + KB + c];
+            double* p = &red[slot * SL + r * SW + KB + c];
             *p = add ? c2[i][j][e] + *p : c2[i][j][e];
           }
         }
   };
-  if (w >= 4) deposit(w - 4, false);
-  __syncthreads();
-  if (w < 4) deposit(w, true);
-  __syncthreads();
-  const int bt = b1 + b2;
-  for (int e = threadIdx.x; e < a * bt; e += NT) {
-    const int i = e / bt, j = e % bt;
-    const int col = j < b1 ? j : KB + (j - b1);
-    const double v = red[(0 * KB + i) * SW + col] + red[(1 * KB + i) * SW + col] + red[(2 * KB + i) * SW + col] +
-                     red[(3 * KB + i) * SW + col];
-    if (j < b1) out1[i * ldo + j] = v;
-    else out2[i * ldo + (j - b1)] = v;
+  // warps 6, 7 store, then 4, 5, then 2, 3, then 0, 1 add (two slots), then the slots are summed
+  for (int rd = 3; rd >= 0; --rd) {
+    if ((w >> 1) == rd) deposit(w & 1, rd != 3);
+    __syncthreads();
   }
-  __syncthreads();
+  accum_combine<KB>(red, a, b1, b2, out1, out2, ldo);
 }
 
 // out = X^T [W1 W2]: the tensor-core form when both W are untransposed, else the SIMT form
@@ -1614,66 +1633,58 @@ __device__ __forceinline__ void accum_rows_any(double* Y, int ly, const double* 
   else accum_rows<KB, A1G>(Y, ly, A1, la1, c1, A2, la2, tA2, c2, alpha, S1, S2, lds, k, L);
 }
 
-// One CholeskyQR pass on Y (m x k, ld k): G = Y^T Y (+ shift I), G = C^T C, Y := Y C^-1.
-// A non-positive pivot marks a rank-deficient column, which is zeroed.
+// One CholeskyQR pass on Y (m x k, ld ly): G = Y^T Y (+ shift I), G = C^T C, Y := Y C^-1.
+// A non-positive pivot marks a rank-deficient column, which is zeroed.  The Cholesky and the
+// substitution are rolled loops (a few hundred instructions): this code runs once per task in
+// a kernel whose other instructions evict it from the instruction cache, and fully unrolled
+// forms of it (thousands of instructions, each line fetched once) ran ten times longer.
 template <int KB, bool YG>
-__device__ __noinline__ void accum_cholqr(double* Y, int m, int k, bool shifted, double* G, double* red) {
+__device__ __noinline__ void accum_cholqr(double* Y, int ly, int m, int k, bool shifted, double* G, double* red) {
   double* rinv = G + KB * ACC_LG;
-  accum_tn_any<KB, YG, YG>(Y, k, k, Y, k, false, k, nullptr, 0, false, 0, m, G, nullptr, ACC_LG, red);
-  if (threadIdx.x < 32) {  // right-looking Cholesky: lane c holds column c of G in registers
+  accum_tn_any<KB, YG, YG>(Y, ly, k, Y, ly, false, k, nullptr, 0, false, 0, m, G, nullptr, ACC_LG, red);
+  if (threadIdx.x < 32) {  // right-looking Cholesky in shared memory: row j of C over row j of G
     const int lane = threadIdx.x;
-    double g[KB];
-#pragma unroll
-    for (int j = 0; j < KB; ++j) g[j] = (j < k && lane < k) ? G[j * ACC_LG + lane] : 0.0;
     double tr = 0.0;
     for (int j = 0; j < k; ++j) tr += G[j * ACC_LG + j];
     const double tiny = 1e-28 * tr;
-    if (shifted) {
+    if (shifted && lane < k) {
       // shift of shifted CholeskyQR3: 11 (m k + k (k + 1)) u ||Y||_F^2, u = 2^-53
-      const double sh = 11.0 * ((double)m * k + (double)k * (k + 1)) * 1.1102230246251565e-16 * tr;
-#pragma unroll
-      for (int j = 0; j < KB; ++j)
-        if (j == lane) g[j] += sh;
+      G[lane * ACC_LG + lane] += 11.0 * ((double)m * k + (double)k * (k + 1)) * 1.1102230246251565e-16 * tr;
     }
-#pragma unroll
-    for (int j = 0; j < KB; ++j) {
-      if (j < k) {
-        const double d = __shfl_sync(0xffffffffu, g[j], j);  // G[j][j]
-        const bool live = d > tiny;
-        const double ri = live ? rsqrt(d) : 0.0;  // 1 / c_jj
-        if (lane == j) g[j] = d * ri;
-        if (lane > j) g[j] = g[j] * ri;  // C[j][lane]
-        // G[c1][lane] -= C[j][c1] C[j][lane] for j < c1 <= lane
-#pragma unroll
-        for (int c1 = j + 1; c1 < KB; ++c1) {
-          const double cjc1 = __shfl_sync(0xffffffffu, g[j], c1);
-          if (c1 < k && lane >= c1) g[c1] = fma(-cjc1, g[j], g[c1]);
-        }
-        if (lane == j) G[KB * ACC_LG + j] = ri;
+    __syncwarp();
+    for (int j = 0; j < k; ++j) {
+      const double d = G[j * ACC_LG + j];
+      const bool live = d > tiny;
+      const double ri = live ? rsqrt(d) : 0.0;  // 1 / c_jj
+      __syncwarp();
+      if (lane >= j && lane < k) G[j * ACC_LG + lane] = lane == j ? d * ri : G[j * ACC_LG + lane] * ri;  // C[j][lane]
+      if (lane == j) rinv[j] = ri;
+      __syncwarp();
+      // G[c1][lane] -= C[j][c1] C[j][lane] for j < c1 <= lane
+      if (lane > j && lane < k) {
+        const double cjl = G[j * ACC_LG + lane];
+        for (int c1 = j + 1; c1 <= lane; ++c1)
+          G[c1 * ACC_LG + lane] = fma(-G[j * ACC_LG + c1], cjl, G[c1 * ACC_LG + lane]);
       }
+      __syncwarp();
     }
-#pragma unroll
-    for (int j = 0; j < KB; ++j)
-      if (j < k && lane < k) G[j * ACC_LG + lane] = g[j];
   }
   __syncthreads();
-  // Y := Y C^-1, a thread per row: x_j = (y_j - sum_{p<j} x_p c_pj) / c_jj
+  // Y := Y C^-1, a thread per row, right-looking: x_j = s_j / c_jj, then s_c -= x_j c_jc for
+  // c > j (each s_c receives its updates in ascending j, the order of the substitution
+  // x_j = (y_j - sum_{p<j} x_p c_pj) / c_jj); x[0] is always the current column
   for (int r = threadIdx.x; r < m; r += NT) {
     double x[KB];
 #pragma unroll
-    for (int j = 0; j < KB; ++j) x[j] = j < k ? ld_any<YG>(&Y[(size_t)r * k + j]) : 0.0;
+    for (int j = 0; j < KB; ++j) x[j] = j < k ? ld_any<YG>(&Y[(size_t)r * ly + j]) : 0.0;
+    for (int j = 0; j < k; ++j) {
+      const double xj = x[0] * rinv[j];
+      Y[(size_t)r * ly + j] = xj;
+      const double* crow = G + j * ACC_LG + j;
 #pragma unroll
-    for (int j = 0; j < KB; ++j) {
-      if (j < k) {
-        double s = x[j];
-#pragma unroll
-        for (int p = 0; p < j; ++p) s = fma(-x[p], G[p * ACC_LG + j], s);
-        x[j] = s * rinv[j];
-      }
+      for (int c = 1; c < KB; ++c) x[c - 1] = (j + c < k) ? fma(-xj, crow[c], x[c]) : x[c];
+      x[KB - 1] = 0.0;
     }
-#pragma unroll
-    for (int j = 0; j < KB; ++j)
-      if (j < k) Y[(size_t)r * k + j] = x[j];
   }
   __syncthreads();
 }
@@ -1681,80 +1692,96 @@ __device__ __noinline__ void accum_cholqr(double* Y, int m, int k, bool shifted,
 // Symmetric eigen-decomposition G = Z diag(lambda) Z^T of a k x k matrix (k <= 32, shared
 // memory, ld ACC_LG) by cyclic Jacobi in round-robin order: every step rotates k/2 disjoint
 // index pairs at once (every pair once per sweep), all threads applying the column rotations
-// (G J, Z J) and then the row rotations (J^T G); sweeps stop when the off-diagonal mass is
-// below 1e-30 of the diagonal's (1e-15 in norm) or after 12.  The rotation of a pair is the
-// symmetric Schur decomposition of its 2 x 2 block (Golub & Van Loan, sym.schur2).
-__device__ __noinline__ void jacobi_eig(double* G, double* Z, int k, double* cs, int* pq, double* flag) {
+// (G J, Z J) and then the row rotations (J^T G).  Each thread handles two (row, pair) elements
+// of a step and derives its pair's rotation itself, in registers, before any element of G
+// changes.  A pair is rotated only while |g_pq| > 1e-17 max_i g_ii: the eigenvalues then carry
+// absolute errors far below the truncation's threshold (tol^2 times the largest, tol >= 1e-8),
+// and the off-diagonal mass left couples kept and dropped directions by less than that; sweeps
+// stop after one without a rotation, or after 12.  The rotation of a pair is the symmetric
+// Schur decomposition of its 2 x 2 block (Golub & Van Loan, sym.schur2), t = tan(theta) written
+// as 2 g_pq sgn(d) / (|d| + h), d = g_qq - g_pp, h = sqrt(d^2 + 4 g_pq^2): cos = r / s,
+// sin = 2 g_pq sgn(d) / s with r = |d| + h, s = sqrt(r^2 + 4 g_pq^2) (one square root and one
+// reciprocal square root).
+__device__ __noinline__ void jacobi_eig(double* G, double* Z, int k, double* flag) {
   const int kk = (k + 1) & ~1, np = kk / 2;  // an odd k gets a dummy index k that never rotates
+  const int ne = k * np;                     // (row, pair) elements of a step, at most 2 NT
   for (int e = threadIdx.x; e < k * k; e += NT) Z[(e / k) * ACC_LG + e % k] = (e / k == e % k) ? 1.0 : 0.0;
-  __syncthreads();
   for (int sweep = 0; sweep < 12; ++sweep) {
     if (threadIdx.x < 32) {
-      double off = 0.0, dia = 0.0;
-      for (int e = threadIdx.x; e < k * k; e += 32) {
-        const int i = e / k, j = e % k;
-        const double v = G[i * ACC_LG + j];
-        if (i == j) dia += v * v;
-        else off += v * v;
-      }
+      double dm = 0.0;
+      for (int i = threadIdx.x; i < k; i += 32) dm = fmax(dm, fabs(G[i * ACC_LG + i]));
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        off += __shfl_xor_sync(0xffffffffu, off, o);
-        dia += __shfl_xor_sync(0xffffffffu, dia, o);
+      for (int o = 16; o > 0; o >>= 1) dm = fmax(dm, __shfl_xor_sync(0xffffffffu, dm, o));
+      if (threadIdx.x == 0) {
+        flag[0] = 0.0;  // rotations in this sweep
+        flag[1] = 1e-17 * dm;
       }
-      if (threadIdx.x == 0) flag[0] = off <= 1e-30 * dia ? 1.0 : 0.0;
     }
     __syncthreads();
-    const bool done = flag[0] != 0.0;
-    __syncthreads();
-    if (done) break;
+    const double thr = flag[1];
     for (int r = 0; r < kk - 1; ++r) {
-      if (threadIdx.x < np) {
-        const int i = threadIdx.x;
-        const int pos_a = i, pos_b = kk - 1 - i;
-        int p = pos_a == 0 ? 0 : 1 + (pos_a - 1 + r) % (kk - 1);
-        int q = pos_b == 0 ? 0 : 1 + (pos_b - 1 + r) % (kk - 1);
-        if (p > q) { const int t = p; p = q; q = t; }
-        double c = 1.0, sn = 0.0;
-        if (q < k) {
-          const double app = G[p * ACC_LG + p], aqq = G[q * ACC_LG + q], apq = G[p * ACC_LG + q];
-          if (apq != 0.0) {
-            const double tau = (aqq - app) / (2.0 * apq);
-            const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-            c = 1.0 / sqrt(1.0 + t * t);
-            sn = t * c;
+      int rowi[2], pp[2], qq[2];
+      double cc[2], ss[2];
+      bool rot[2];
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        const int e = threadIdx.x + t * NT;
+        rot[t] = false;
+        rowi[t] = 0;
+        pp[t] = qq[t] = 0;
+        cc[t] = 1.0;
+        ss[t] = 0.0;
+        if (e < ne) {
+          const int i = e / np, jp = e % np;
+          const int pos_b = kk - 1 - jp;
+          int p = jp == 0 ? 0 : 1 + (jp - 1 + r) % (kk - 1);
+          int q = pos_b == 0 ? 0 : 1 + (pos_b - 1 + r) % (kk - 1);
+          if (p > q) { const int tq = p; p = q; q = tq; }
+          rowi[t] = i;
+          pp[t] = p;
+          qq[t] = q;
+          if (q < k) {
+            const double app = G[p * ACC_LG + p], aqq = G[q * ACC_LG + q], apq = G[p * ACC_LG + q];
+            if (fabs(apq) > thr) {
+              const double d = aqq - app, g2 = 2.0 * apq * (d >= 0.0 ? 1.0 : -1.0);
+              const double h = sqrt(fma(d, d, g2 * g2)), rr = fabs(d) + h;
+              const double w = rsqrt(fma(rr, rr, g2 * g2));
+              cc[t] = rr * w;
+              ss[t] = g2 * w;
+              rot[t] = true;
+              if (i == 0) flag[0] = 1.0;
+            }
           }
         }
-        pq[2 * i] = p;
-        pq[2 * i + 1] = q;
-        cs[2 * i] = c;
-        cs[2 * i + 1] = sn;
+      }
+      __syncthreads();  // every rotation is known before G changes
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {  // columns: G J, Z J
+        if (!rot[t]) continue;
+        const int i = rowi[t], p = pp[t], q = qq[t];
+        const double c = cc[t], sn = ss[t];
+        const double gp = G[i * ACC_LG + p], gq = G[i * ACC_LG + q];
+        G[i * ACC_LG + p] = c * gp - sn * gq;
+        G[i * ACC_LG + q] = sn * gp + c * gq;
+        const double zp = Z[i * ACC_LG + p], zq = Z[i * ACC_LG + q];
+        Z[i * ACC_LG + p] = c * zp - sn * zq;
+        Z[i * ACC_LG + q] = sn * zp + c * zq;
       }
       __syncthreads();
-      for (int e = threadIdx.x; e < k * np; e += NT) {  // columns: G J, Z J
-        const int i = e / np, j = e % np, p = pq[2 * j], q = pq[2 * j + 1];
-        if (q < k) {
-          const double c = cs[2 * j], sn = cs[2 * j + 1];
-          const double gp = G[i * ACC_LG + p], gq = G[i * ACC_LG + q];
-          G[i * ACC_LG + p] = c * gp - sn * gq;
-          G[i * ACC_LG + q] = sn * gp + c * gq;
-          const double zp = Z[i * ACC_LG + p], zq = Z[i * ACC_LG + q];
-          Z[i * ACC_LG + p] = c * zp - sn * zq;
-          Z[i * ACC_LG + q] = sn * zp + c * zq;
-        }
-      }
-      __syncthreads();
-      for (int e = threadIdx.x; e < k * np; e += NT) {  // rows: J^T G
-        const int i = e / np, j = e % np, p = pq[2 * j], q = pq[2 * j + 1];
-        if (q < k) {
-          const double c = cs[2 * j], sn = cs[2 * j + 1];
-          const double gp = G[p * ACC_LG + i], gq = G[q * ACC_LG + i];
-          G[p * ACC_LG + i] = c * gp - sn * gq;
-          G[q * ACC_LG + i] = sn * gp + c * gq;
-        }
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {  // rows: J^T G
+        if (!rot[t]) continue;
+        const int i = rowi[t], p = pp[t], q = qq[t];
+        const double c = cc[t], sn = ss[t];
+        const double gp = G[p * ACC_LG + i], gq = G[q * ACC_LG + i];
+        G[p * ACC_LG + i] = c * gp - sn * gq;
+        G[q * ACC_LG + i] = sn * gp + c * gq;
       }
       __syncthreads();
     }
+    const bool done = flag[0] == 0.0;
+    __syncthreads();
+    if (done) break;
   }
 }
 
@@ -1800,21 +1827,22 @@ __device__ __forceinline__ void accum_impl(const pp_task& T, double* smem) {
   const double *U2 = T.p[2], *V2 = T.p[3], *R = T.p[4];
   const int lu1 = T.ld[0], lv1 = T.ld[1], lu2 = T.ld[2], lv2 = T.ld[3], lr = T.ld[4];
   double* red = smem;
-  double* S = red + SM::RED;   // k1 x 2KB: S1 | S2, later P1 | P2
-  double* G = S + SM::S;
+  double* S = red + SM::SOFF;  // k1 x 2KB: S1 | S2, later P1 | P2
+  double* G = red + SM::RED;
   double* Y = YG ? T.tmp : G + SM::G;
+  const int ly = YG ? k1 : k1 + 1;  // on chip: rows padded (a thread per row reads distinct banks)
   const double al = T.alpha;
   constexpr int LS = 2 * KB;
   // S1 = R^T V1, S2 = R^T V2
   accum_tn_any<KB, true, true>(R, lr, k1, V1, lv1, false, k1, V2, lv2, tV2, k2, nx, S, S + KB, LS, red);
   // Y = U1 S1^T + alpha U2 S2^T
-  accum_rows_any<KB, true>(Y, k1, U1, lu1, k1, U2, lu2, tU2, k2, al, S, S + KB, LS, k1, ny);
+  accum_rows_any<KB, true>(Y, ly, U1, lu1, k1, U2, lu2, tU2, k2, al, S, S + KB, LS, k1, ny);
   __syncthreads();
-  accum_cholqr<KB, YG>(Y, ny, k1, true, G, red);
-  accum_cholqr<KB, YG>(Y, ny, k1, false, G, red);
-  accum_cholqr<KB, YG>(Y, ny, k1, false, G, red);
+  accum_cholqr<KB, YG>(Y, ly, ny, k1, true, G, red);
+  accum_cholqr<KB, YG>(Y, ly, ny, k1, false, G, red);
+  accum_cholqr<KB, YG>(Y, ly, ny, k1, false, G, red);
   // P1 = Y^T U1, P2 = Y^T U2
-  accum_tn_any<KB, YG, true>(Y, k1, k1, U1, lu1, false, k1, U2, lu2, tU2, k2, ny, S, S + KB, LS, red);
+  accum_tn_any<KB, YG, true>(Y, ly, k1, U1, lu1, false, k1, U2, lu2, tU2, k2, ny, S, S + KB, LS, red);
   // V1 := V1 P1^T + alpha V2 P2^T (rows read before written)
   accum_rows_any<KB, true>(V1, lv1, V1, lv1, k1, V2, lv2, tV2, k2, al, S, S + KB, LS, k1, nx);
   __syncthreads();
@@ -1827,31 +1855,53 @@ __device__ __forceinline__ void accum_impl(const pp_task& T, double* smem) {
     double* cs = red + KB * ACC_LG;
     double* flag = cs + 2 * KB;
     int* pq = reinterpret_cast<int*>(flag + 2);
-    jacobi_eig(G, Z, k1, cs, pq, flag);
+    jacobi_eig(G, Z, k1, flag);
     const int r = accum_truncate<KB>(G, Z, k1, T.beta, S, LS, pq);
     accum_rows_any<KB, true>(V1, lv1, V1, lv1, k1, nullptr, 0, false, 0, 1.0, S, S, LS, k1, nx);
-    accum_rows_any<KB, YG>(Y, k1, Y, k1, k1, nullptr, 0, false, 0, 1.0, S, S, LS, k1, ny);
+    accum_rows_any<KB, YG>(Y, ly, Y, ly, k1, nullptr, 0, false, 0, 1.0, S, S, LS, k1, ny);
     __syncthreads();
     if (threadIdx.x == 0 && T.p[5]) T.p[5][0] = (double)r;
   }
   // U1 := Y
   for (int e = threadIdx.x; e < ny * k1; e += NT) {
     const int r = e / k1, c = e % k1;
-    U1[(size_t)r * lu1 + c] = ld_any<YG>(&Y[e]);
+    U1[(size_t)r * lu1 + c] = ld_any<YG>(&Y[(size_t)r * ly + c]);
   }
   __syncthreads();
 }
 
 // Y (m x k, ld k, global) := an orthonormal basis of its range by shifted CholeskyQR3, the
-// range finder of the sketched low-rank update (same passes as inside ACCUM)
+// range finder of the sketched low-rank update (same passes as inside ACCUM); a Y of up to the
+// sketch capacity is copied to shared memory for the three passes and back
 template <int KB>
 __device__ __forceinline__ void orth_impl(double* Y, int m, int k, double* smem) {
   using SM = AccumSmem<KB>;
   double* red = smem;
-  double* G = red + SM::RED + SM::S;
-  accum_cholqr<KB, true>(Y, m, k, true, G, red);
-  accum_cholqr<KB, true>(Y, m, k, false, G, red);
-  accum_cholqr<KB, true>(Y, m, k, false, G, red);
+  double* G = red + SM::RED;
+  const int total = m * k, ls = k + 1;
+  if ((long long)m * ls <= SM::YCAP) {
+    double* Ys = G + SM::G;  // rows padded to k + 1
+    for (int e0 = threadIdx.x; e0 < total; e0 += 8 * NT) {
+      double v[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) v[q] = e0 + q * NT < total ? ldcg(&Y[e0 + q * NT]) : 0.0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int e = e0 + q * NT;
+        if (e < total) Ys[(e / k) * ls + e % k] = v[q];
+      }
+    }
+    __syncthreads();
+    accum_cholqr<KB, false>(Ys, ls, m, k, true, G, red);
+    accum_cholqr<KB, false>(Ys, ls, m, k, false, G, red);
+    accum_cholqr<KB, false>(Ys, ls, m, k, false, G, red);
+    for (int e = threadIdx.x; e < total; e += NT) Y[e] = Ys[(e / k) * ls + e % k];
+    __syncthreads();
+    return;
+  }
+  accum_cholqr<KB, true>(Y, k, m, k, true, G, red);
+  accum_cholqr<KB, true>(Y, k, m, k, false, G, red);
+  accum_cholqr<KB, true>(Y, k, m, k, false, G, red);
 }
 
 // U V^T (U: m x k orthonormal columns, V: n x k, both global) := its best rank-r form: the
@@ -1864,14 +1914,14 @@ __device__ __forceinline__ void lrtrunc_impl(const pp_task& T, double* smem) {
   double *U = T.p[0], *V = T.p[1];
   const int lu = T.ld[0], lv = T.ld[1], m = T.m, n = T.n, k = T.k;
   double* red = smem;
-  double* S = red + SM::RED;
-  double* G = S + SM::S;
+  double* S = red + SM::SOFF;
+  double* G = red + SM::RED;
   accum_tn_any<KB, true, true>(V, lv, k, V, lv, false, k, nullptr, 0, false, 0, n, G, nullptr, ACC_LG, red);
   double* Z = red;
   double* cs = red + KB * ACC_LG;
   double* flag = cs + 2 * KB;
   int* pq = reinterpret_cast<int*>(flag + 2);
-  jacobi_eig(G, Z, k, cs, pq, flag);
+  jacobi_eig(G, Z, k, flag);
   const int r = accum_truncate<KB>(G, Z, k, T.beta, S, LS, pq, T.o > 0 ? T.o : k);
   accum_rows_any<KB, true>(V, lv, V, lv, k, nullptr, 0, false, 0, 1.0, S, S, LS, k, n);
   accum_rows_any<KB, true>(U, lu, U, lu, k, nullptr, 0, false, 0, 1.0, S, S, LS, k, m);
@@ -1903,11 +1953,12 @@ __device__ __noinline__ void dev_copy(double* C, int ldc, const double* A, int l
 
 __device__ __noinline__ void dev_accum(const pp_task& T, double* smem) {
   const int ny = T.m, k1 = T.k, k2 = T.l;
+  const bool on_chip = accum_y_on_chip(ny, k1, k2);
   if (k1 <= 16 && k2 <= 16) {
-    if ((long long)ny * k1 <= AccumSmem<16>::YCAP) accum_impl<16, false>(T, smem);
+    if (on_chip) accum_impl<16, false>(T, smem);
     else accum_impl<16, true>(T, smem);
   } else {
-    if ((long long)ny * k1 <= AccumSmem<32>::YCAP) accum_impl<32, false>(T, smem);
+    if (on_chip) accum_impl<32, false>(T, smem);
     else accum_impl<32, true>(T, smem);
   }
 }
@@ -2679,11 +2730,9 @@ static __device__ __align__(256) double g_accum_noalloc_scratch[PP_NOALLOC_SCRAT
 long long pp_accum_noalloc_capacity() { return PP_NOALLOC_SCRATCH_DOUBLES; }
 
 long long pp_accum_scratch_doubles(long long ny, int k1, int k2) {
-  // dev_accum keeps the ny x k1 sketch Y in shared memory while it fits the rest of the
-  // 160 KB; only a larger Y goes to the task's scratch, and nothing else does
-  const long long y = ny * k1;
-  const long long cap = (k1 <= 16 && k2 <= 16) ? AccumSmem<16>::YCAP : AccumSmem<32>::YCAP;
-  return y <= cap ? 0 : y;
+  // dev_accum keeps the ny x k1 sketch Y in shared memory while it fits beside the rest of the
+  // 180 KB; only a larger Y goes to the task's scratch, and nothing else does
+  return accum_y_on_chip(ny, k1, k2) ? 0 : ny * k1;
 }
 
 namespace {
