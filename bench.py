@@ -124,8 +124,9 @@ def program_bytes(pp, h, which=0, nrhs=1):
             e = 2 * m * n + m * m // 2
         elif op == 3:
             e = 2 * m * n + n * n // 2
-        elif op == 6 and int(t["prec"]) == 2:  # BF16 shadows (2 bytes per element) into FP64 C
-            e = (2 if t["beta"] != 0 else 1) * m * n + (m * k + k * n) // 4
+        elif op == 6 and int(t["prec"]) == 2:  # BF16 shadows (2 bytes per element) into FP64 C; l: a
+            # second operand pair summed in the same pass over C
+            e = (2 if t["beta"] != 0 else 1) * m * n + (m * (k + l) + (k + l) * n) // 4
         elif op == 6:
             e = (2 if t["beta"] != 0 else 1) * m * n + m * k + k * n
         elif op == 9:
@@ -142,13 +143,14 @@ def program_bytes(pp, h, which=0, nrhs=1):
             e = m * m // 2 + 2 * m * n
         elif op in (13, 14):  # ORTH (in place) / COPY: m x n read and written
             e = 2 * m * n
-        elif op == 15:  # SHADOW: m x k FP64 read, m x k BF16 written
-            e = m * k + m * k // 4
+        elif op == 15:  # SHADOW: m x k FP64 read, m x k BF16 written (split: m x k / 3 read)
+            e = (m * k // 3 if int(t["o"]) else m * k) + m * k // 4
         else:
             e = 0
         total += 8 * e
     sel = (tasks["op"] == 6) & (tasks["prec"] == 2)
-    info = dict(info, bf16_flops=float((2 * tasks["m"][sel].astype(np.int64) * tasks["n"][sel] * tasks["k"][sel]).sum()))
+    kk = tasks["k"][sel].astype(np.int64) + tasks["l"][sel]
+    info = dict(info, bf16_flops=float((2 * tasks["m"][sel].astype(np.int64) * tasks["n"][sel] * kk).sum()))
     return total, info
 
 

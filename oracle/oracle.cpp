@@ -347,10 +347,13 @@ int run_one(const pp_task& T, std::vector<double>& tmp) {
     case PP_OP_TRSMU: o_trsmu(T.p[0], T.p[1], T.m, T.n, T.ld[0], T.ld[1]); return 0;
     case PP_OP_GEMM:
       if (T.prec == PP_PREC_BF16) {  // engine instruction: products of the BF16 shadows, FP64 sums
-        if (T.m % 128 || T.n % 32 || T.k % 64) return -1;
+        // a second pair (p[3], p[4], inner dimension l) adds its products to the same sums
+        if (T.m % 128 || T.n % 32 || T.k % 64 || T.l < 0 || T.l % 64 || (T.l > 0 && (!T.p[3] || !T.p[4]))) return -1;
         const int bcr = T.n % 256 == 0 ? 128 : (T.n < 128 ? T.n : 128);  // the B shadow's chunk rows
         const uint8_t* As = reinterpret_cast<const uint8_t*>(T.p[1]);
         const uint8_t* Bs = reinterpret_cast<const uint8_t*>(T.p[2]);
+        const uint8_t* As2 = reinterpret_cast<const uint8_t*>(T.p[3]);
+        const uint8_t* Bs2 = reinterpret_cast<const uint8_t*>(T.p[4]);
         for (int r = 0; r < T.m; ++r)
           for (int c = 0; c < T.n; ++c) {
             double s = 0.0;
@@ -358,6 +361,12 @@ int run_one(const pp_task& T, std::vector<double>& tmp) {
               uint16_t a, b;
               std::memcpy(&a, As + tiled_at(r, q, T.k, 128), 2);
               std::memcpy(&b, Bs + tiled_at(c, q, T.k, bcr), 2);
+              s += from_bf16(a) * from_bf16(b);
+            }
+            for (int q = 0; q < T.l; ++q) {
+              uint16_t a, b;
+              std::memcpy(&a, As2 + tiled_at(r, q, T.l, 128), 2);
+              std::memcpy(&b, Bs2 + tiled_at(c, q, T.l, bcr), 2);
               s += from_bf16(a) * from_bf16(b);
             }
             double& x = T.p[0][(int64_t)r * T.ld[0] + c];

@@ -188,6 +188,7 @@ pp_status build_program(pp_hmatrix* h, int which, int nrhs, VmPlan& plan) {
     if (which == 0) {
       if (h->precision == PP_PREC_BF16) g.set_precision(PP_PREC_BF16);
       g.getrf_program();
+      if (h->precision == PP_PREC_BF16) plan.prog.merge_bf16_updates();
       if (h->precision == PP_PREC_TF32) plan.prog.set_gemm_precision(h->precision);
     } else if (which == 2) {
       g.construct_program(h->c_kernel, h->c_dim, h->c_p0, h->H->rank_tol);

@@ -99,6 +99,68 @@ int64_t Program::set_gemm_precision(int prec) {
   return c;
 }
 
+// Consecutive BF16 updates of the same target C (C += alpha A1 B1, then C += alpha A2 B2, the
+// second the next task after the first to touch C's object, both with one pair, the same
+// alpha and beta 1, the first one's inputs not rewritten in between) become one task at the
+// second one's place: C += alpha (A1 B1 + A2 B2).  Program order stays a valid sequential
+// execution: nothing between the two reads or writes C, and the first one's inputs hold the
+// same values at the later place.  Pairs are taken in order: (1st, 2nd), (3rd, 4th), ...
+int64_t Program::merge_bf16_updates() {
+  const int n = (int)tasks.size();
+  std::vector<int> last(objs.size(), -1), last_w(objs.size(), -1);
+  std::vector<char> dead(n, 0);
+  int64_t merged = 0;
+  auto single = [](const HTask& h) {
+    return h.t.op == PP_OP_GEMM && h.t.prec == PP_PREC_BF16 && h.t.beta == 1.0 && h.t.l == 0 && h.has[0] &&
+           h.has[1] && h.has[2] && !h.has[3] && !h.has[4];
+  };
+  for (int t = 0; t < n; ++t) {
+    HTask& h = tasks[t];
+    if (single(h)) {
+      const View& C = h.opnd[0];
+      const int p = last[C.obj];
+      if (p >= 0 && !dead[p] && single(tasks[p])) {
+        HTask& g = tasks[p];
+        const View& D = g.opnd[0];
+        bool ok = D.obj == C.obj && D.r0 == C.r0 && D.c0 == C.c0 && D.m == C.m && D.n == C.n && D.t == C.t &&
+                  g.t.alpha == h.t.alpha && g.t.m == h.t.m && g.t.n == h.t.n && !g.opnd[1].t && !g.opnd[2].t &&
+                  !h.opnd[1].t && !h.opnd[2].t;
+        for (int sl = 1; sl <= 2 && ok; ++sl) ok = last_w[g.opnd[sl].obj] < p;
+        if (ok) {
+          h.opnd[3] = h.opnd[1];
+          h.opnd[4] = h.opnd[2];
+          h.has[3] = h.has[4] = true;
+          h.t.ld[3] = h.t.ld[1];
+          h.t.ld[4] = h.t.ld[2];
+          h.opnd[1] = g.opnd[1];
+          h.opnd[2] = g.opnd[2];
+          h.t.ld[1] = g.t.ld[1];
+          h.t.ld[2] = g.t.ld[2];
+          h.t.l = h.t.k;
+          h.t.k = g.t.k;
+          for (const Region& r : g.regions)
+            if (r.ro) h.regions.push_back(r);
+          h.flops += g.flops;
+          dead[p] = 1;
+          ++merged;
+        }
+      }
+    }
+    for (const Region& r : h.regions) {
+      last[r.obj] = t;
+      if (!r.ro) last_w[r.obj] = t;
+    }
+  }
+  if (merged) {
+    std::vector<HTask> kept;
+    kept.reserve(n - merged);
+    for (int t = 0; t < n; ++t)
+      if (!dead[t]) kept.push_back(std::move(tasks[t]));
+    tasks.swap(kept);
+  }
+  return merged;
+}
+
 static inline bool rect_overlap(const Region& a, const Region& b) {
   return a.r0 < b.r0 + b.nr && b.r0 < a.r0 + a.nr && a.c0 < b.c0 + b.nc && b.c0 < a.c0 + a.nc;
 }

@@ -102,6 +102,10 @@ class Program {
   // Contraction precision of every GEMM instruction (PP_PREC_TF32: tensor cores with FP32
   // accumulation; GETRF, TRSM*, ACCUM and SUM stay FP64).  Returns the tasks changed.
   int64_t set_gemm_precision(int prec);
+  // the mixed form's BF16 updates of one target that follow each other with nothing else
+  // touching the target in between become one task with two operand pairs (one pass over the
+  // target instead of two); returns the number of merges.  Call before build_dag.
+  int64_t merge_bf16_updates();
 
   void build_dag();
   h_ops_dag to_dag() const;
@@ -128,9 +132,12 @@ constexpr int kTrmvCols = 16;
 constexpr int kTrmvSplitMin = 128;
 constexpr int kTrmvParts = 4;
 constexpr int kTrmvPartRows = 64;
-// rows of one product instruction of the solve with at most 16 columns (more CTAs on the
-// matrix-vector products of the critical path)
-constexpr int kSolveGemmRows = 256;
+// rows of one product instruction of the solve with at most 16 columns: every row slice of a
+// right-hand-side block is a dependency chain of its own (the updates of one slice are ordered,
+// of different slices not), and a 64-row instruction streams its slice of a 512-column leaf in
+// four rounds of loads per warp, so the chains of the critical path advance four times faster
+// than with 256 rows
+constexpr int kSolveGemmRows = 64;
 // largest rank of the added term of one ACCUM (the VM keeps it in registers)
 constexpr int kAccumMaxK2 = 32;
 // smallest m, n and k of a GEMM instruction the TF32 form runs on the tensor cores

@@ -79,7 +79,8 @@ enum pp_op {
 /* PP_PREC_BF16: a GEMM whose operands are BF16 shadows (PP_OP_SHADOW) in the tiled layout:
  * p[1] the m x k shadow of op(A), p[2] the n x k shadow of op(B)^T; products summed in FP32 on
  * the tensor cores, C (FP64) := beta C + alpha sum.  m a multiple of 128, k of 64, n 32, 64, 128
- * or a multiple of 256. */
+ * or a multiple of 256.  l > 0 (a multiple of 64): a second pair p[3] (m x l), p[4] (n x l) whose
+ * products join the same sums (two consecutive updates of C in one pass over it). */
 #define PP_PREC_BF16 2
 
 /* Split shadows (SHADOW o): a product A B summed over K' = 3 K from the shadows

@@ -717,14 +717,17 @@ __device__ __noinline__ void bg_rows_update2(double* __restrict__ cp, int ldc, c
   }
 }
 
+// With a second pair (As2, Bs2, inner dimension k2 > 0) the k loop runs over the chunks of both
+// pairs into the same accumulator: C := beta C + alpha (A B + A2 B2), one pass over C.
 __device__ __noinline__ bool dev_gemm_bf16(double* __restrict__ C, int ldc, const uint8_t* __restrict__ As,
                                            const uint8_t* __restrict__ Bs, int m, int n, int k, double alpha,
-                                           double beta, double* smem, TcCtx& tc) {
+                                           double beta, double* smem, TcCtx& tc, const uint8_t* __restrict__ As2,
+                                           const uint8_t* __restrict__ Bs2, int k2) {
   uint8_t* sbase = reinterpret_cast<uint8_t*>(smem);
   const uint32_t s0 = smem_u32(sbase);
   const uint32_t stage0 = (s0 + 1023u) & ~1023u;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int nch = k >> 6, kchunks = k >> 6;
+  const int kchunks = k >> 6, kchunks2 = k2 >> 6, nch = kchunks + kchunks2;
   // tile width: 256 (two 128-column MMAs) when n is a multiple of 256, else n itself (32, 64, 128:
   // one MMA of that width reading the first n rows of one B chunk)
   const int tw = (n % BG_TILE_N == 0) ? BG_TILE_N : n, nbc = tw > 128 ? 2 : 1;
@@ -756,10 +759,14 @@ __device__ __noinline__ bool dev_gemm_bf16(double* __restrict__ C, int ldc, cons
           if (!mbar_wait_or_abort(empty(s), ph ^ 1u, tc.limit, abort)) break;
           const uint32_t dst = stage0 + s * BG_STAGE_BYTES;
           mbar_expect_tx(full(s), stage_bytes);
-          bulk_g2s(dst, As + ((size_t)rb * kchunks + kc) * BG_CHUNK, BG_CHUNK, full(s));
-          bulk_g2s(dst + BG_CHUNK, Bs + ((size_t)cb * kchunks + kc) * b_chunk, b_chunk, full(s));
+          const bool first = kc < kchunks;  // chunk of the first pair, else of the second
+          const uint8_t* a = first ? As : As2;
+          const uint8_t* b = first ? Bs : Bs2;
+          const int kcp = first ? kc : kc - kchunks, kch = first ? kchunks : kchunks2;
+          bulk_g2s(dst, a + ((size_t)rb * kch + kcp) * BG_CHUNK, BG_CHUNK, full(s));
+          bulk_g2s(dst + BG_CHUNK, b + ((size_t)cb * kch + kcp) * b_chunk, b_chunk, full(s));
           if (nbc == 2)
-            bulk_g2s(dst + BG_CHUNK + b_chunk, Bs + ((size_t)(cb + 1) * kchunks + kc) * b_chunk, b_chunk, full(s));
+            bulk_g2s(dst + BG_CHUNK + b_chunk, b + ((size_t)(cb + 1) * kch + kcp) * b_chunk, b_chunk, full(s));
         }
       }
     }
@@ -1694,10 +1701,11 @@ __device__ __noinline__ void accum_cholqr(double* Y, int ly, int m, int k, bool 
 // index pairs at once (every pair once per sweep), all threads applying the column rotations
 // (G J, Z J) and then the row rotations (J^T G).  Each thread handles two (row, pair) elements
 // of a step and derives its pair's rotation itself, in registers, before any element of G
-// changes.  A pair is rotated only while |g_pq| > 1e-17 max_i g_ii: the eigenvalues then carry
-// absolute errors far below the truncation's threshold (tol^2 times the largest, tol >= 1e-8),
-// and the off-diagonal mass left couples kept and dropped directions by less than that; sweeps
-// stop after one without a rotation, or after 12.  The rotation of a pair is the symmetric
+// changes.  A pair is rotated only while |g_pq| > 1e-15 max_i g_ii: above the rounding noise a
+// rotation of the largest entries leaves behind (a few units in the last place of max g_ii, so
+// the sweeps end), and about the precision the Gram matrix has in the first place (its entries
+// are rounded to about 1e-16 of the largest); sweeps stop after one without a rotation, or after
+// 12.  The rotation of a pair is the symmetric
 // Schur decomposition of its 2 x 2 block (Golub & Van Loan, sym.schur2), t = tan(theta) written
 // as 2 g_pq sgn(d) / (|d| + h), d = g_qq - g_pp, h = sqrt(d^2 + 4 g_pq^2): cos = r / s,
 // sin = 2 g_pq sgn(d) / s with r = |d| + h, s = sqrt(r^2 + 4 g_pq^2) (one square root and one
@@ -1714,7 +1722,7 @@ __device__ __noinline__ void jacobi_eig(double* G, double* Z, int k, double* fla
       for (int o = 16; o > 0; o >>= 1) dm = fmax(dm, __shfl_xor_sync(0xffffffffu, dm, o));
       if (threadIdx.x == 0) {
         flag[0] = 0.0;  // rotations in this sweep
-        flag[1] = 1e-17 * dm;
+        flag[1] = 1e-15 * dm;
       }
     }
     __syncthreads();
@@ -1734,8 +1742,12 @@ __device__ __noinline__ void jacobi_eig(double* G, double* Z, int k, double* fla
         if (e < ne) {
           const int i = e / np, jp = e % np;
           const int pos_b = kk - 1 - jp;
-          int p = jp == 0 ? 0 : 1 + (jp - 1 + r) % (kk - 1);
-          int q = pos_b == 0 ? 0 : 1 + (pos_b - 1 + r) % (kk - 1);
+          // round-robin positions: 1 + (pos - 1 + r) mod (kk - 1), the sum below 2 (kk - 1)
+          int ua = jp - 1 + r, ub = pos_b - 1 + r;
+          if (ua >= kk - 1) ua -= kk - 1;
+          if (ub >= kk - 1) ub -= kk - 1;
+          int p = jp == 0 ? 0 : 1 + ua;
+          int q = pos_b == 0 ? 0 : 1 + ub;
           if (p > q) { const int tq = p; p = q; q = tq; }
           rowi[t] = i;
           pp[t] = p;
@@ -2005,11 +2017,13 @@ __device__ bool run_task(const pp_task& T, double* smem, TcCtx& tc, int& err) {
       return true;
     case PP_OP_GEMM:
       if (T.prec == PP_PREC_BF16) {
-        if (!tc.active || T.m < 128 || T.m % 128 || T.k < 64 || T.k % 64 ||
+        if (!tc.active || T.m < 128 || T.m % 128 || T.k < 64 || T.k % 64 || T.l < 0 || T.l % 64 ||
+            (T.l > 0 && (!T.p[3] || !T.p[4])) ||
             !(T.n == 32 || T.n == 64 || T.n == 128 || (T.n >= BG_TILE_N && T.n % BG_TILE_N == 0)))
           return false;
         if (!dev_gemm_bf16(T.p[0], T.ld[0], reinterpret_cast<const uint8_t*>(T.p[1]),
-                           reinterpret_cast<const uint8_t*>(T.p[2]), T.m, T.n, T.k, T.alpha, T.beta, smem, tc))
+                           reinterpret_cast<const uint8_t*>(T.p[2]), T.m, T.n, T.k, T.alpha, T.beta, smem, tc,
+                           reinterpret_cast<const uint8_t*>(T.p[3]), reinterpret_cast<const uint8_t*>(T.p[4]), T.l))
           err = PP_VM_MMA_TIMEOUT;
         return true;
       }

@@ -28,8 +28,11 @@ def test_bf16_program_shadows_each_operand_once(pp, oracle, hctx):
     g = tasks[(tasks["op"] == 6) & (tasks["prec"] == 2)]
     n_blocks = 4
     panels = sum(n_blocks - 1 - k for k in range(n_blocks))  # per side
-    # Schur updates of whole leaves: sum over k of (n_blocks - 1 - k)^2
-    assert (g["k"] == 512).sum() == sum((n_blocks - 1 - k) ** 2 for k in range(n_blocks))
+    # Schur updates of whole leaves: sum over k of (n_blocks - 1 - k)^2, consecutive updates of the
+    # same leaf two to a task (a second operand pair, inner dimension l)
+    schur = g[g["k"] == 512]
+    assert len(schur) + (schur["l"] > 0).sum() == sum((n_blocks - 1 - k) ** 2 for k in range(n_blocks))
+    assert (schur["l"] == 512).sum() > 0 and set(np.unique(schur["l"])) <= {0, 512}
     # panel solves: one split product (K = 3 x 512) per L-panel and per U-panel block, and no
     # triangular solve task on a whole leaf
     assert (g["k"] == 3 * 512).sum() == 2 * panels

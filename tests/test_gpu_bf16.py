@@ -280,3 +280,46 @@ def test_split_product_accuracy(pp, oracle, bctx, m, n, k):
     assert (np.abs(out["dev"] - want) / scale).max() < 2e-5
     assert (np.abs(out["host"] - want) / scale).max() < 2e-5
     assert rel(out["dev"], out["host"]) < 1e-5
+
+
+@pytest.mark.parametrize("m,n,k1,k2", [(512, 512, 512, 512), (256, 512, 512, 64), (512, 32, 64, 512)])
+def test_bf16_gemm_two_pairs_vs_oracle(pp, oracle, bctx, m, n, k1, k2):
+    """C -= A1 B1 + A2 B2 in one pass over C (the merged form of two consecutive updates of one
+    leaf): against the oracle's FP64 sums of the same BF16 products, within 1e-5 of the update."""
+    rng = np.random.default_rng(m + n + k1 + 7 * k2)
+    C = rng.standard_normal((m, n))
+    ops = [(rng.standard_normal((m, k)), rng.standard_normal((n, k)), k) for k in (k1, k2)]
+    cr = 128 if n % 256 == 0 else n
+    out = {}
+    for side in ("dev", "host"):
+        mk = (lambda x: dev(x)) if side == "dev" else (lambda x: x.copy())
+        z = (lambda e: torch.zeros(e, dtype=torch.float64, device="cuda")) if side == "dev" else np.zeros
+        Cx = mk(C)
+        recs, sh = [], []
+        for A, Bt, k in ops:
+            Ax, Bx = mk(A), mk(Bt)
+            As, Bs = z(m * k // 4), z(n * k // 4)
+            ta = shadow_task(pp, ptr(As), ptr(Ax), m, k, False, k)
+            tb = shadow_task(pp, ptr(Bs), ptr(Bx), n, k, False, k)
+            tb[0]["ctrl"] = 0 if cr == 128 else cr
+            recs += [ta, tb]
+            sh += [As, Bs, Ax, Bx]
+        g = np.zeros(1, dtype=pp.TASK_DTYPE)
+        g[0]["op"], g[0]["prec"] = GEMM, BF16
+        g[0]["m"], g[0]["n"], g[0]["k"], g[0]["l"] = m, n, k1, k2
+        g[0]["alpha"], g[0]["beta"] = -1.0, 1.0
+        g[0]["p"][0], g[0]["p"][1], g[0]["p"][2] = ptr(Cx), ptr(sh[0]), ptr(sh[1])
+        g[0]["p"][3], g[0]["p"][4] = ptr(sh[4]), ptr(sh[5])
+        g[0]["ld"][0] = n
+        tasks = np.concatenate(recs + [g])
+        for i in range(4):
+            tasks[i]["succ_begin"], tasks[i]["n_succ"] = i, 1
+        if side == "dev":
+            bctx.vm_execute(tasks, np.full(4, 4, np.int32), np.array([0, 0, 0, 0, 4], np.int32))
+            out[side] = Cx.cpu().numpy()
+        else:
+            assert oracle.lib().oracle_run_program(tasks.ctypes.data, 5) == 0
+            out[side] = Cx
+    assert rel(out["dev"] - C, out["host"] - C) < 1e-5
+    want = C - sum(A @ Bt.T for A, Bt, _ in ops)
+    assert rel(out["host"], want) < 1e-2  # BF16 rounding of the operands
