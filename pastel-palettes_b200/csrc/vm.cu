@@ -1677,20 +1677,35 @@ __device__ __noinline__ void accum_cholqr(double* Y, int ly, int m, int k, bool 
     }
   }
   __syncthreads();
-  // Y := Y C^-1, a thread per row, right-looking: x_j = s_j / c_jj, then s_c -= x_j c_jc for
-  // c > j (each s_c receives its updates in ascending j, the order of the substitution
-  // x_j = (y_j - sum_{p<j} x_p c_pj) / c_jj); x[0] is always the current column
-  for (int r = threadIdx.x; r < m; r += NT) {
-    double x[KB];
+  // Y := Y C^-1, a thread per row (two rows at a time, two independent chains), right-looking:
+  // x_j = s_j / c_jj, then s_c -= x_j c_jc for c > j (each s_c receives its updates in
+  // ascending j, the order of the substitution x_j = (y_j - sum_{p<j} x_p c_pj) / c_jj); x[0]
+  // is always the current column.  Positions past column k - 1 take updates from entries
+  // beyond C's rows (in bounds of G and its reciprocals) but are never stored and never feed
+  // a column below k.
+  for (int r = threadIdx.x; r < m; r += 2 * NT) {
+    const int r2 = r + NT;
+    const bool two = r2 < m;
+    double x[KB], z[KB];
 #pragma unroll
-    for (int j = 0; j < KB; ++j) x[j] = j < k ? ld_any<YG>(&Y[(size_t)r * ly + j]) : 0.0;
+    for (int j = 0; j < KB; ++j) {
+      x[j] = j < k ? ld_any<YG>(&Y[(size_t)r * ly + j]) : 0.0;
+      z[j] = (two && j < k) ? ld_any<YG>(&Y[(size_t)r2 * ly + j]) : 0.0;
+    }
     for (int j = 0; j < k; ++j) {
-      const double xj = x[0] * rinv[j];
+      const double rj = rinv[j];
+      const double xj = x[0] * rj, zj = z[0] * rj;
       Y[(size_t)r * ly + j] = xj;
+      if (two) Y[(size_t)r2 * ly + j] = zj;
       const double* crow = G + j * ACC_LG + j;
 #pragma unroll
-      for (int c = 1; c < KB; ++c) x[c - 1] = (j + c < k) ? fma(-xj, crow[c], x[c]) : x[c];
+      for (int c = 1; c < KB; ++c) {
+        const double g = crow[c];
+        x[c - 1] = fma(-xj, g, x[c]);
+        z[c - 1] = fma(-zj, g, z[c]);
+      }
       x[KB - 1] = 0.0;
+      z[KB - 1] = 0.0;
     }
   }
   __syncthreads();
@@ -1698,22 +1713,53 @@ __device__ __noinline__ void accum_cholqr(double* Y, int ly, int m, int k, bool 
 
 // Symmetric eigen-decomposition G = Z diag(lambda) Z^T of a k x k matrix (k <= 32, shared
 // memory, ld ACC_LG) by cyclic Jacobi in round-robin order: every step rotates k/2 disjoint
-// index pairs at once (every pair once per sweep), all threads applying the column rotations
-// (G J, Z J) and then the row rotations (J^T G).  Each thread handles two (row, pair) elements
-// of a step and derives its pair's rotation itself, in registers, before any element of G
-// changes.  A pair is rotated only while |g_pq| > 1e-15 max_i g_ii: above the rounding noise a
+// index pairs at once (every pair once per sweep).  A step is one pass of independent 2 x 2
+// block updates: the thread of block (pair a, pair b) reads G's entries at rows {p_a, q_a} and
+// columns {p_b, q_b}, derives both pairs' rotations itself from the diagonal blocks (read before
+// any entry changes), and writes J_a^T G_ab J_b; Z's columns of pair b turn with J_b in the same
+// pass.  A pair is rotated only while |g_pq| > 1e-15 max_i g_ii: above the rounding noise a
 // rotation of the largest entries leaves behind (a few units in the last place of max g_ii, so
 // the sweeps end), and about the precision the Gram matrix has in the first place (its entries
 // are rounded to about 1e-16 of the largest); sweeps stop after one without a rotation, or after
-// 12.  The rotation of a pair is the symmetric
-// Schur decomposition of its 2 x 2 block (Golub & Van Loan, sym.schur2), t = tan(theta) written
-// as 2 g_pq sgn(d) / (|d| + h), d = g_qq - g_pp, h = sqrt(d^2 + 4 g_pq^2): cos = r / s,
-// sin = 2 g_pq sgn(d) / s with r = |d| + h, s = sqrt(r^2 + 4 g_pq^2) (one square root and one
-// reciprocal square root).
+// 12.  The rotation of a pair is the symmetric Schur decomposition of its 2 x 2 block (Golub &
+// Van Loan, sym.schur2), t = tan(theta) written as 2 g_pq sgn(d) / (|d| + h), d = g_qq - g_pp,
+// h = sqrt(d^2 + 4 g_pq^2): cos = r / s, sin = 2 g_pq sgn(d) / s with r = |d| + h,
+// s = sqrt(r^2 + 4 g_pq^2) (one square root and one reciprocal square root).
+__device__ __forceinline__ void jacobi_pair(const double* G, int k, int kk, int r, int jp, double thr, int& p, int& q,
+                                            double& c, double& sn) {
+  // round-robin positions of pair jp in step r: 1 + (pos - 1 + r) mod (kk - 1), the sum below
+  // 2 (kk - 1); position 0 stays
+  const int pos_b = kk - 1 - jp;
+  int ua = jp - 1 + r, ub = pos_b - 1 + r;
+  if (ua >= kk - 1) ua -= kk - 1;
+  if (ub >= kk - 1) ub -= kk - 1;
+  p = jp == 0 ? 0 : 1 + ua;
+  q = pos_b == 0 ? 0 : 1 + ub;
+  if (p > q) {
+    const int t = p;
+    p = q;
+    q = t;
+  }
+  c = 1.0;
+  sn = 0.0;
+  if (q < k) {
+    const double app = G[p * ACC_LG + p], aqq = G[q * ACC_LG + q], apq = G[p * ACC_LG + q];
+    if (fabs(apq) > thr) {
+      const double d = aqq - app, g2 = 2.0 * apq * (d >= 0.0 ? 1.0 : -1.0);
+      const double h = sqrt(fma(d, d, g2 * g2)), rr = fabs(d) + h;
+      const double w = rsqrt(fma(rr, rr, g2 * g2));
+      c = rr * w;
+      sn = g2 * w;
+    }
+  }
+}
+
 __device__ __noinline__ void jacobi_eig(double* G, double* Z, int k, double* flag) {
   const int kk = (k + 1) & ~1, np = kk / 2;  // an odd k gets a dummy index k that never rotates
-  const int ne = k * np;                     // (row, pair) elements of a step, at most 2 NT
   for (int e = threadIdx.x; e < k * k; e += NT) Z[(e / k) * ACC_LG + e % k] = (e / k == e % k) ? 1.0 : 0.0;
+  // this thread's block (pair a, pair b) and, for Z, rows zi and zi + 16 of pair b
+  const int ta = threadIdx.x / 16, tb = threadIdx.x % 16;
+  const bool blk = ta < np && tb < np;
   for (int sweep = 0; sweep < 12; ++sweep) {
     if (threadIdx.x < 32) {
       double dm = 0.0;
@@ -1728,66 +1774,38 @@ __device__ __noinline__ void jacobi_eig(double* G, double* Z, int k, double* fla
     __syncthreads();
     const double thr = flag[1];
     for (int r = 0; r < kk - 1; ++r) {
-      int rowi[2], pp[2], qq[2];
-      double cc[2], ss[2];
-      bool rot[2];
-#pragma unroll
-      for (int t = 0; t < 2; ++t) {
-        const int e = threadIdx.x + t * NT;
-        rot[t] = false;
-        rowi[t] = 0;
-        pp[t] = qq[t] = 0;
-        cc[t] = 1.0;
-        ss[t] = 0.0;
-        if (e < ne) {
-          const int i = e / np, jp = e % np;
-          const int pos_b = kk - 1 - jp;
-          // round-robin positions: 1 + (pos - 1 + r) mod (kk - 1), the sum below 2 (kk - 1)
-          int ua = jp - 1 + r, ub = pos_b - 1 + r;
-          if (ua >= kk - 1) ua -= kk - 1;
-          if (ub >= kk - 1) ub -= kk - 1;
-          int p = jp == 0 ? 0 : 1 + ua;
-          int q = pos_b == 0 ? 0 : 1 + ub;
-          if (p > q) { const int tq = p; p = q; q = tq; }
-          rowi[t] = i;
-          pp[t] = p;
-          qq[t] = q;
-          if (q < k) {
-            const double app = G[p * ACC_LG + p], aqq = G[q * ACC_LG + q], apq = G[p * ACC_LG + q];
-            if (fabs(apq) > thr) {
-              const double d = aqq - app, g2 = 2.0 * apq * (d >= 0.0 ? 1.0 : -1.0);
-              const double h = sqrt(fma(d, d, g2 * g2)), rr = fabs(d) + h;
-              const double w = rsqrt(fma(rr, rr, g2 * g2));
-              cc[t] = rr * w;
-              ss[t] = g2 * w;
-              rot[t] = true;
-              if (i == 0) flag[0] = 1.0;
-            }
-          }
+      int pa = 0, qa = 0, pb = 0, qb = 0;
+      double ca = 1.0, sa = 0.0, cb = 1.0, sb = 0.0;
+      // pair b's rotation also turns Z's rows ta, ta + 16 (every ta, also beyond np)
+      if (tb < np) jacobi_pair(G, k, kk, r, tb, thr, pb, qb, cb, sb);
+      if (blk) jacobi_pair(G, k, kk, r, ta, thr, pa, qa, ca, sa);
+      const bool ra = sa != 0.0, rb = sb != 0.0;
+      double g11 = 0.0, g12 = 0.0, g21 = 0.0, g22 = 0.0;
+      const bool qa_in = qa < k, qb_in = qb < k;
+      if (blk && (ra || rb)) {
+        g11 = G[pa * ACC_LG + pb];
+        if (qb_in) g12 = G[pa * ACC_LG + qb];
+        if (qa_in) g21 = G[qa * ACC_LG + pb];
+        if (qa_in && qb_in) g22 = G[qa * ACC_LG + qb];
+      }
+      if (ta == tb && ra) flag[0] = 1.0;
+      __syncthreads();  // every entry is read before any changes
+      if (blk && (ra || rb)) {
+        // columns: [g11 g12; g21 g22] J_b
+        const double h11 = cb * g11 - sb * g12, h12 = sb * g11 + cb * g12;
+        const double h21 = cb * g21 - sb * g22, h22 = sb * g21 + cb * g22;
+        // rows: J_a^T [h]
+        G[pa * ACC_LG + pb] = ca * h11 - sa * h21;
+        if (qb_in) G[pa * ACC_LG + qb] = ca * h12 - sa * h22;
+        if (qa_in) G[qa * ACC_LG + pb] = sa * h11 + ca * h21;
+        if (qa_in && qb_in) G[qa * ACC_LG + qb] = sa * h12 + ca * h22;
+      }
+      if (tb < np && rb && qb_in) {  // Z J_b: rows ta and ta + 16 of pair b's columns
+        for (int i = ta; i < k; i += 16) {
+          const double zp = Z[i * ACC_LG + pb], zq = Z[i * ACC_LG + qb];
+          Z[i * ACC_LG + pb] = cb * zp - sb * zq;
+          Z[i * ACC_LG + qb] = sb * zp + cb * zq;
         }
-      }
-      __syncthreads();  // every rotation is known before G changes
-#pragma unroll
-      for (int t = 0; t < 2; ++t) {  // columns: G J, Z J
-        if (!rot[t]) continue;
-        const int i = rowi[t], p = pp[t], q = qq[t];
-        const double c = cc[t], sn = ss[t];
-        const double gp = G[i * ACC_LG + p], gq = G[i * ACC_LG + q];
-        G[i * ACC_LG + p] = c * gp - sn * gq;
-        G[i * ACC_LG + q] = sn * gp + c * gq;
-        const double zp = Z[i * ACC_LG + p], zq = Z[i * ACC_LG + q];
-        Z[i * ACC_LG + p] = c * zp - sn * zq;
-        Z[i * ACC_LG + q] = sn * zp + c * zq;
-      }
-      __syncthreads();
-#pragma unroll
-      for (int t = 0; t < 2; ++t) {  // rows: J^T G
-        if (!rot[t]) continue;
-        const int i = rowi[t], p = pp[t], q = qq[t];
-        const double c = cc[t], sn = ss[t];
-        const double gp = G[p * ACC_LG + i], gq = G[q * ACC_LG + i];
-        G[p * ACC_LG + i] = c * gp - sn * gq;
-        G[q * ACC_LG + i] = sn * gp + c * gq;
       }
       __syncthreads();
     }
