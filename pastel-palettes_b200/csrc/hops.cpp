@@ -1043,7 +1043,7 @@ void Generator::gemm_tiles(const View& C, const View& A, const View& B, int alph
   const int g = gemm_tile_;
   const int TN = std::min(C.n, g);
   int TM = std::min(C.m, std::max(g, g * g / std::max(TN, 1)));
-  if (solve_ && C.n <= 16) TM = std::min(TM, kSolveGemmRows);
+  if (solve_ && C.n <= 16) TM = std::min(TM, A.n >= kBigLeaf ? kSolveGemmRowsBig : kSolveGemmRows);
   for (int i = 0; i < C.m; i += TM)
     for (int j = 0; j < C.n; j += TN) {
       const int mi = std::min(TM, C.m - i), nj = std::min(TN, C.n - j);

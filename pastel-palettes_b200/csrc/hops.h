@@ -134,10 +134,13 @@ constexpr int kTrmvParts = 4;
 constexpr int kTrmvPartRows = 64;
 // rows of one product instruction of the solve with at most 16 columns: every row slice of a
 // right-hand-side block is a dependency chain of its own (the updates of one slice are ordered,
-// of different slices not), and a 64-row instruction streams its slice of a 512-column leaf in
-// four rounds of loads per warp, so the chains of the critical path advance four times faster
-// than with 256 rows
-constexpr int kSolveGemmRows = 64;
+// of different slices not).  Products with a leaf of kBigLeaf columns or more take 64-row
+// instructions, which stream their slice of a 512-column leaf in four rounds of loads per warp,
+// so the chains of a single job's critical path advance four times faster than with 256 rows;
+// the others keep 256 rows (low-rank factors are short, and batched jobs of smaller leaves have
+// parallelism enough, where fewer instructions cost less)
+constexpr int kSolveGemmRowsBig = 64;
+constexpr int kSolveGemmRows = 256;
 // largest rank of the added term of one ACCUM (the VM keeps it in registers)
 constexpr int kAccumMaxK2 = 32;
 // smallest m, n and k of a GEMM instruction the TF32 form runs on the tensor cores
