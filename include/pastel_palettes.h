@@ -307,6 +307,48 @@ typedef struct pp_residual_job {
  * CUDA graph); calls on different streams must not overlap. */
 pp_status pp_kernel_residual_batch_dev(pp_context* ctx, int njobs, const pp_residual_job* jobs, void* stream);
 
+/* --- batched restarted GMRES around the H-LU solve -------------------------
+ * No counterpart in the reference (it has no solve or refinement path).  For a batch of
+ * kernel problems whose plain refinement stalls (H-LU factors too coarse for the spectral
+ * radius of I - (LU)^-1 A to stay below 1), GMRES on A (LU)^-1 with the FP64 matrix-free
+ * residual converges to the same tolerance.  The caller owns every vector (device memory):
+ * V[i]: (m + 1) x n[i] basis, Z[i]: m x n[i] preconditioned basis, x[i]: solution, r[i]: the
+ * residual b - A x that starts a cycle.  A cycle is
+ *   pp_gmres_start;  for j < m: Z_j = solve(V_j) (pp_batch_solve), V_{j+1} = 0 - A Z_j
+ *   (pp_kernel_residual_batch_dev with b = 0), pp_gmres_arnoldi(j);  pp_gmres_finish;
+ *   r = b - A x.
+ * Each call is one launch on `stream`, one CTA per instance (largest first), no host
+ * synchronization and no allocation (capturable).  1 <= m <= PP_GMRES_MAX_RESTART. */
+#define PP_GMRES_MAX_RESTART 64
+typedef struct pp_gmres pp_gmres;
+pp_status pp_gmres_create(pp_context* ctx, int count, const int* n, int m, double* const* V, double* const* Z,
+                          double* const* x, double* const* r, pp_gmres** out);
+void pp_gmres_destroy(pp_gmres* g);
+/* beta = ||r||_2, v_0 = r / beta (an instance with r = 0 stays frozen for the cycle) */
+pp_status pp_gmres_start(pp_gmres* g, void* stream);
+/* Arnoldi step j (0 <= j < m) of every instance: V_{j+1} holds -A z_j on entry; CGS2 against
+ * V_0..V_j, normalised; the Hessenberg column rotated; |g_{j+1}| is the residual estimate */
+pp_status pp_gmres_arnoldi(pp_gmres* g, int j, void* stream);
+/* x += Z y, y the least-squares solution of the cycle's active dimension */
+pp_status pp_gmres_finish(pp_gmres* g, void* stream);
+/* (synchronous) per instance, in creation order: active dimension and residual estimate of
+ * the current cycle, out[2 i] and out[2 i + 1] */
+pp_status pp_gmres_status(pp_gmres* g, double* out);
+
+/* --- DAG build on the device ---------------------------------------------
+ * Replaces the host-side dependency discovery of the reference (rts/ops.cpp:42-61
+ * Operation::checkDependencyFrom over earlier instructions, the edge table of
+ * rts/dependency.cpp:7-76) for programs built after this call: every (instruction, region)
+ * access walks its object's earlier accesses on the GPU (dag.cu).  The edges, their
+ * flow / anti / out types and every instruction's predecessor and successor order are those of
+ * the host build; when the device build cannot run (a CUDA error, or a walk with more partial
+ * writes than it keeps) the host build runs instead and pp_last_error says why.  on = 1 needs
+ * a device context; 0 (the default) builds on the host. */
+pp_status pp_context_set_device_dag(pp_context* ctx, int on);
+/* the factor (which 0) or solve (1, nrhs) program's DAG build: wall milliseconds, and 1 when it
+ * ran on the device (builds the program first if needed) */
+pp_status pp_hmatrix_dag_info(pp_hmatrix* h, int which, int nrhs, double* dag_ms, int* on_device);
+
 /* --- rts (DAG primitives, rts/ops.h, rts/dependency.h) ------------------- */
 /* DataMap2D::checkOverlap (rts/ops.cpp:7-40); regions: ptr, pitch, width (bytes), height */
 int pp_datamap2d_check_overlap(uintptr_t ptr_a, size_t pitch_a, size_t width_a, size_t height_a, uintptr_t ptr_b,

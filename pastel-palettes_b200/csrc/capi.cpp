@@ -31,6 +31,7 @@ struct pp_context {
   std::string err;
   double* d_resid = nullptr;  // partial sums of the matrix-free residual (grown on demand)
   size_t resid_elems = 0;
+  int dag_device = 0;         // 1: dependency discovery of new programs on the device (dag.cu)
   ~pp_context() { cudaFree(d_resid); }
 };
 
@@ -47,6 +48,8 @@ struct VmPlan {
   double *d_work = nullptr, *d_scratch = nullptr, *d_rhs = nullptr;
   int64_t work_elems = 0, scratch_elems = 0, rhs_elems = 0;
   double build_ms = 0;
+  double dag_ms = 0;       // wall time of the DAG build alone
+  int dag_on_device = 0;   // 1: built by build_dag_device
   int grid = 0;
   int use_tc = 0;  // holds TF32 contractions (tensor memory per CTA)
   unsigned long long* d_trace = nullptr;  // per-task (start, end, sm | cta << 32) when tracing
@@ -195,7 +198,20 @@ pp_status build_program(pp_hmatrix* h, int which, int nrhs, VmPlan& plan) {
     } else {
       g.solve_program(nrhs);
     }
-    plan.prog.build_dag();
+    auto td = std::chrono::steady_clock::now();
+    bool dev = false;
+    if (ctx->dag_device && has_device(ctx)) {
+      std::string derr;
+      int prev = -1;
+      cudaGetDevice(&prev);
+      if (prev != ctx->device) cudaSetDevice(ctx->device);
+      dev = pp::build_dag_device(plan.prog, derr, nullptr);
+      if (prev != ctx->device && prev >= 0) cudaSetDevice(prev);
+      if (!dev) ctx->err = "device DAG build fell back to the host: " + derr;  // not an error
+    }
+    if (!dev) plan.prog.build_dag();
+    plan.dag_on_device = dev ? 1 : 0;
+    plan.dag_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - td).count();
   } catch (const std::exception& e) {
     plan.prog = pp::Program();
     return fail(ctx, PP_UNSUPPORTED, std::string("program generation: ") + e.what());
@@ -712,6 +728,8 @@ pp_status pp_hmatrix_assemble_dense_dev(pp_hmatrix* h, int kernel, double p0, do
     return fail(ctx, PP_INVALID_ARG, "pp_hmatrix_assemble_dense_dev: bad argument");
   if (kernel <= 1 && !(p0 >= 0.0 && std::isfinite(p0)))
     return fail(ctx, PP_INVALID_ARG, "pp_hmatrix_assemble_dense_dev: p0 negative or not finite");
+  if (h->H->point_dim != 0 && dim != h->H->point_dim)
+    return fail(ctx, PP_INVALID_ARG, "pp_hmatrix_assemble_dense_dev: dim differs from the tree's point dimension");
   if (!h->d_arena) return fail(ctx, PP_INVALID_ARG, "pp_hmatrix_assemble_dense_dev: upload the H-matrix first");
   std::vector<pp_assemble_block> blocks;
   for (const pp::HNode& nd : h->H->nodes) {
@@ -732,6 +750,8 @@ pp_status pp_hmatrix_construct_dev(pp_hmatrix* h, int kernel, double p0, double 
     return fail(ctx, PP_INVALID_ARG, "pp_hmatrix_construct_dev: bad argument");
   if (kernel <= 1 ? !(p0 >= 0.0 && std::isfinite(p0)) : !(p0 > 0.0 && std::isfinite(p0)))
     return fail(ctx, PP_INVALID_ARG, "pp_hmatrix_construct_dev: p0 out of range for the kernel");
+  if (h->H->point_dim != 0 && dim != h->H->point_dim)
+    return fail(ctx, PP_INVALID_ARG, "pp_hmatrix_construct_dev: dim differs from the tree's point dimension");
   cudaStream_t s = (cudaStream_t)stream;
   if (!h->d_arena) {
     const size_t bytes = sizeof(double) * (size_t)std::max<int64_t>(h->H->arena_elems, 1);
@@ -1628,6 +1648,115 @@ void pp_server_destroy(pp_server* s) {
     if (kv.second->h) pp_hmatrix_destroy(kv.second->h);  // queued, never admitted
   if (s->pool) cudaMemPoolDestroy(s->pool);  // released once the queued frees have run
   delete s;
+}
+
+// ---------------------------------------------------------------- batched GMRES
+struct pp_gmres {
+  pp_context* ctx = nullptr;
+  int count = 0, m = 0;
+  pp_gmres_slot* d_slots = nullptr;  // device copy, ordered by n descending
+  double* d_state = nullptr;
+  std::vector<int> order;            // order[k]: creation index of device slot k
+  size_t state_elems = 0;
+  ~pp_gmres() {
+    cudaFree(d_slots);
+    cudaFree(d_state);
+  }
+};
+
+pp_status pp_gmres_create(pp_context* ctx, int count, const int* n, int m, double* const* V, double* const* Z,
+                          double* const* x, double* const* r, pp_gmres** out) {
+  if (!out) return PP_INVALID_ARG;
+  *out = nullptr;
+  if (!has_device(ctx)) return fail(ctx, PP_CUDA_ERROR, "no CUDA device in this context");
+  if (count <= 0 || !n || !V || !Z || !x || !r || m < 1 || m > PP_GMRES_MAX_RESTART)
+    return fail(ctx, PP_INVALID_ARG, "pp_gmres_create: bad argument (1 <= m <= " +
+                                         std::to_string(PP_GMRES_MAX_RESTART) + ")");
+  for (int i = 0; i < count; ++i)
+    if (n[i] <= 0 || !V[i] || !Z[i] || !x[i] || !r[i])
+      return fail(ctx, PP_INVALID_ARG, "pp_gmres_create: bad instance " + std::to_string(i));
+  auto* g = new pp_gmres;
+  g->ctx = ctx;
+  g->count = count;
+  g->m = m;
+  g->state_elems = pp_gmres_state_elems(m);
+  g->order.resize(count);
+  for (int i = 0; i < count; ++i) g->order[i] = i;
+  // largest instances first: their CTAs start in the first wave
+  std::stable_sort(g->order.begin(), g->order.end(), [&](int a, int b) { return n[a] > n[b]; });
+  cudaError_t e = cudaMalloc((void**)&g->d_state, sizeof(double) * g->state_elems * count);
+  if (e == cudaSuccess) e = cudaMemset(g->d_state, 0, sizeof(double) * g->state_elems * count);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&g->d_slots, sizeof(pp_gmres_slot) * count);
+  if (e == cudaSuccess) {
+    std::vector<pp_gmres_slot> hs(count);
+    for (int k = 0; k < count; ++k) {
+      const int i = g->order[k];
+      hs[k] = pp_gmres_slot{n[i], m, V[i], Z[i], x[i], r[i], g->d_state + g->state_elems * i};
+    }
+    e = cudaMemcpy(g->d_slots, hs.data(), sizeof(pp_gmres_slot) * count, cudaMemcpyHostToDevice);
+  }
+  if (e != cudaSuccess) {
+    delete g;
+    return cuda_fail(ctx, e, "pp_gmres_create");
+  }
+  *out = g;
+  return PP_OK;
+}
+
+void pp_gmres_destroy(pp_gmres* g) { delete g; }
+
+pp_status pp_gmres_start(pp_gmres* g, void* stream) {
+  if (!g) return PP_INVALID_ARG;
+  pp_context* ctx = g->ctx;
+  PP_CUDA(pp_gmres_start(g->d_slots, g->count, (cudaStream_t)stream));
+  return PP_OK;
+}
+
+pp_status pp_gmres_arnoldi(pp_gmres* g, int j, void* stream) {
+  if (!g) return PP_INVALID_ARG;
+  pp_context* ctx = g->ctx;
+  if (j < 0 || j >= g->m) return fail(ctx, PP_INVALID_ARG, "pp_gmres_arnoldi: step outside [0, m)");
+  PP_CUDA(pp_gmres_arnoldi(g->d_slots, g->count, j, (cudaStream_t)stream));
+  return PP_OK;
+}
+
+pp_status pp_gmres_finish(pp_gmres* g, void* stream) {
+  if (!g) return PP_INVALID_ARG;
+  pp_context* ctx = g->ctx;
+  PP_CUDA(pp_gmres_finish(g->d_slots, g->count, (cudaStream_t)stream));
+  return PP_OK;
+}
+
+pp_status pp_gmres_status(pp_gmres* g, double* out) {
+  if (!g || !out) return PP_INVALID_ARG;
+  pp_context* ctx = g->ctx;
+  std::vector<double> st(g->state_elems * g->count);
+  PP_CUDA(cudaDeviceSynchronize());
+  PP_CUDA(cudaMemcpy(st.data(), g->d_state, sizeof(double) * st.size(), cudaMemcpyDeviceToHost));
+  const size_t meta = g->state_elems - 4;
+  for (int i = 0; i < g->count; ++i) {
+    out[2 * i] = st[g->state_elems * i + meta];
+    out[2 * i + 1] = st[g->state_elems * i + meta + 3];
+  }
+  return PP_OK;
+}
+
+// ---------------------------------------------------------------- DAG build placement
+pp_status pp_context_set_device_dag(pp_context* ctx, int on) {
+  if (!ctx || (on != 0 && on != 1)) return PP_INVALID_ARG;
+  if (on && !has_device(ctx)) return fail(ctx, PP_INVALID_ARG, "device DAG build needs a device context");
+  ctx->dag_device = on;
+  return PP_OK;
+}
+
+pp_status pp_hmatrix_dag_info(pp_hmatrix* h, int which, int nrhs, double* dag_ms, int* on_device) {
+  if (!h || (which != 0 && which != 1) || (which == 1 && nrhs <= 0)) return PP_INVALID_ARG;
+  VmPlan* plan = which == 0 ? &h->factor : solve_plan(h, nrhs);
+  pp_status st = build_program(h, which, nrhs, *plan);
+  if (st != PP_OK) return st;
+  if (dag_ms) *dag_ms = plan->dag_ms;
+  if (on_device) *on_device = plan->dag_on_device;
+  return PP_OK;
 }
 
 }  // extern "C"

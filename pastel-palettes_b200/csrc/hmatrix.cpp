@@ -120,6 +120,7 @@ Hierarchical* Hierarchical::geometric(int n, int dim, const double* pts, int lea
     throw std::invalid_argument("geometric: n, dim, leaf and kmax must be positive");
   auto* h = new Hierarchical();
   h->n = n;
+  h->point_dim = dim;
   std::vector<Cluster> cl;
   std::function<int(int, int)> make = [&](int b, int sz) -> int {
     Cluster c;

@@ -62,6 +62,8 @@ class Hierarchical {
   // inverses of the diagonal leaves' triangular factors, which the factorization writes and
   // the solves read (never uploaded, downloaded or restored)
   int64_t block_elems = 0;
+  // dimension of the points a geometric tree was built on (0: the all-dense tree)
+  int point_dim = 0;
   // host image of the arena (filled by set_dense / set_lowrank), allocated at its first use
   // (ensure_host): a matrix built on the device never needs one
   mutable std::vector<double> host;

@@ -217,6 +217,13 @@ void Program::build_dag() {
       ++edges;
     }
   }
+  finish_dag();
+}
+
+void Program::finish_dag() {
+  const int n = (int)tasks.size();
+  deps_.clear();
+  deps_built_ = false;
   blevel.assign(n, 0);
   for (int t = n - 1; t >= 0; --t) {
     int64_t b = 0;

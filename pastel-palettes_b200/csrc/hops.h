@@ -108,6 +108,8 @@ class Program {
   int64_t merge_bf16_updates();
 
   void build_dag();
+  // bottom levels (and a fresh dependency table) once succ / pred / pred_bits are set
+  void finish_dag();
   h_ops_dag to_dag() const;
   // Pointer binding and device-table encoding.  bases[arena id] = base address.
   void encode(const std::vector<double*>& bases, std::vector<pp_task>& out, std::vector<int32_t>& succ_out,
@@ -120,6 +122,12 @@ class Program {
   bool encode_reference(int workers, std::vector<std::vector<int32_t>>& streams, std::string& err,
                         int64_t* tmp_elems_per_worker) const;
 };
+
+// The same DAG as Program::build_dag, with the dependency discovery on the current CUDA device
+// (dag.cu).  Returns false with `err` set when it cannot (a CUDA error, or a dependency walk
+// with more partial writes than it keeps); the caller then builds on the host.  device_ms: wall
+// time of the device part (upload, walks, sort, download).
+bool build_dag_device(Program& prog, std::string& err, double* device_ms);
 
 // largest triangle of one solve-phase TRSML / TRSMU instruction (the VM's blocked
 // triangular routines take up to 256 rows)

@@ -88,3 +88,20 @@ cudaError_t pp_assemble_dense(const pp_assemble_block* blocks, int nblocks, int 
 cudaError_t pp_axpy(double* x, const double* dx, size_t count, cudaStream_t s);
 /* out[0] = max |x|, out[1] = max |r| (as double bit patterns; out is zeroed first) */
 cudaError_t pp_absmax2(const double* x, const double* r, size_t count, unsigned long long* out, cudaStream_t s);
+
+/* ---- batched restarted GMRES around the H-LU solve (krylov.cu) ---- */
+#define PP_GMRES_MAX_RESTART 64  /* largest restart length (Arnoldi steps per cycle) */
+/* one instance of a batched GMRES: device pointers, n rows, restart length m */
+struct pp_gmres_slot {
+  int n, m;
+  double* V;   /* (m + 1) x n basis, vector k at V + k n              */
+  double* Z;   /* m x n preconditioned basis, z_k = (LU)^-1 v_k         */
+  double* x;   /* n: solution, x += Z y at the end of a cycle          */
+  double* r;   /* n: residual b - A x at the start of a cycle         */
+  double* st;  /* pp_gmres_state_elems(m) doubles of small state       */
+};
+size_t pp_gmres_state_elems(int m);
+/* each launches one CTA per slot of the device array `slots` */
+cudaError_t pp_gmres_start(const pp_gmres_slot* slots, int count, cudaStream_t s);
+cudaError_t pp_gmres_arnoldi(const pp_gmres_slot* slots, int count, int j, cudaStream_t s);
+cudaError_t pp_gmres_finish(const pp_gmres_slot* slots, int count, cudaStream_t s);

@@ -87,3 +87,15 @@ def test_device_construction_adaptive_rank_factor_and_refine(pp, gctx):
     b = pp.rhs(n, 4)
     x, hist = pp.Refiner(h, gctx, prob).solve(torch.from_numpy(b).cuda(), tol=1e-10)
     assert hist[-1] <= 1e-10, hist
+
+
+def test_device_assembly_refuses_wrong_point_dimension(pp, gctx):
+    """Points of another dimension than the tree's would be read past their end: refused."""
+    h, prob = pp.make_kernel_problem(gctx, 512, 2, "inv", 1e-3, 128, 16)
+    h.upload()
+    pts = torch.zeros(512, 3, dtype=torch.float64, device="cuda")
+    L = pp.lib()
+    assert L.pp_hmatrix_assemble_dense_dev(h.handle, int(prob.kernel), float(prob.p0), float(prob.shift),
+                                           pts.data_ptr(), 3, None) == pp.PP_INVALID_ARG
+    assert L.pp_hmatrix_construct_dev(h.handle, int(prob.kernel), float(prob.p0), float(prob.shift),
+                                      pts.data_ptr(), 3, None) == pp.PP_INVALID_ARG
