@@ -148,6 +148,7 @@ def lib():
             "pp_dense_residual_dev": (i, [vp, vp, i, i, vp, vp, vp, i, vp]),
             "pp_kernel_residual_dev": (i, [vp, i, d, d, vp, i, i, vp, vp, vp, i, vp]),
             "pp_kernel_residual_batch_dev": (i, [vp, i, C.POINTER(_ResidualJob), vp]),
+            "pp_kernel_residual_batch_lowp_dev": (i, [vp, i, C.POINTER(_ResidualJob), vp]),
             "pp_hmatrix_assemble_dense_dev": (i, [vp, i, d, d, vp, i, vp]),
             "pp_hmatrix_construct_dev": (i, [vp, i, d, d, vp, i, vp]),
             "pp_datamap2d_check_overlap": (i, [C.c_uint64, C.c_size_t, C.c_size_t, C.c_size_t,
@@ -160,6 +161,8 @@ def lib():
             "pp_vm_execute": (i, [vp, vp, i, vp, ll, vp, ll, i, vp]),
             "pp_lowrank_accum_noalloc": (i, [vp, vp, i, vp, i, vp, i, vp, i, vp, i, i, i, i, i, d, vp]),
             "pp_gmres_create": (i, [vp, i, vp, i, vp, vp, vp, vp, C.POINTER(vp)]),
+            "pp_context_set_device_dag": (i, [vp, i]),
+            "pp_hmatrix_dag_info": (i, [vp, i, i, C.POINTER(d), C.POINTER(i)]),
             "pp_gmres_destroy": (None, [vp]),
             "pp_gmres_start": (i, [vp, vp]),
             "pp_gmres_arnoldi": (i, [vp, i, vp]),
@@ -250,6 +253,11 @@ class Context:
     def sm_count(self):
         return lib().pp_device_sm_count(self._h)
 
+    def set_device_dag(self, on=True):
+        """Build the dependency DAG of programs made from now on on the device (same edges,
+        types and orders as the host build; the host build runs when the device one cannot)."""
+        self.check(lib().pp_context_set_device_dag(self._h, int(bool(on))), "set_device_dag")
+
     # --- FP64 residuals (device pointers of torch tensors)
     def dense_residual(self, A, x, b, r, stream=None):
         n, nrhs = x.shape
@@ -271,17 +279,19 @@ class Context:
                                                 x.data_ptr(), b.data_ptr(), r.data_ptr(), nrhs,
                                                 _stream_handle(stream)), "kernel_residual")
 
-    def kernel_residual_batch(self, jobs, stream=None):
+    def kernel_residual_batch(self, jobs, stream=None, lowp=False):
         """jobs: (kernel, p0, shift, pts, x, dx or None, b, r) per problem (device tensors);
-        every job does x += dx (when given), then r = b - A x, in a few batched launches."""
+        every job does x += dx (when given), then r = b - A x, in a few batched launches.
+        lowp: entries of jobs with <= 4 right-hand sides evaluated in FP32 (Krylov products
+        only; a residual that certifies a result must not use it)."""
         arr = (_ResidualJob * max(1, len(jobs)))()
         for q, (kernel, p0, shift, pts, x, dx, b, r) in enumerate(jobs):
             n, nrhs = x.shape
             arr[q] = _ResidualJob(int(kernel), int(pts.shape[1]), int(n), int(nrhs), float(p0), float(shift),
                                   pts.data_ptr(), x.data_ptr(), None if dx is None else dx.data_ptr(),
                                   b.data_ptr(), r.data_ptr())
-        self.check(lib().pp_kernel_residual_batch_dev(self._h, len(jobs), arr, _stream_handle(stream)),
-                   "kernel_residual_batch")
+        fn = lib().pp_kernel_residual_batch_lowp_dev if lowp else lib().pp_kernel_residual_batch_dev
+        self.check(fn(self._h, len(jobs), arr, _stream_handle(stream)), "kernel_residual_batch")
         return residual_batch_launches([(j[0], j[3].shape[1], j[4].shape[1], j[5] is not None) for j in jobs])
 
 
@@ -469,6 +479,12 @@ class Hierarchical:
                     arena_elems={ARENAS[i]: info.arena_elems[i] for i in range(5)},
                     host_build_ms=info.host_build_ms)
 
+    def dag_info(self, which=0, nrhs=1):
+        """(DAG build milliseconds, built on the device) of the factor / solve program."""
+        ms, dev = C.c_double(), C.c_int()
+        self.ctx.check(lib().pp_hmatrix_dag_info(self._h, which, nrhs, C.byref(ms), C.byref(dev)), "dag_info")
+        return ms.value, bool(dev.value)
+
     def encode_program(self, which, nrhs, bases):
         """Task table bound to the given arena base addresses (ints); returns
         (tasks structured array, succ, indeg, ready)."""
@@ -643,11 +659,15 @@ class BatchGMRES:
     preconditioned spectrum is clustered.  A cycle of m steps is one batched solve, one batched
     matrix-free product and one Arnoldi launch per step, then x += Z y and the true residual
     r = b - A x from the points; no host synchronization inside a cycle (capturable).  The
-    Krylov bases are torch tensors owned here: (2 m + 1) n doubles per instance."""
+    Krylov bases are torch tensors owned here: (2 m + 1) n doubles per instance.
+    lowp: the products inside a cycle evaluate the kernel entries in FP32 (a few 1e-7 relative,
+    far below what one cycle gains when rho(I - (LU)^-1 A) is large); the residual at every
+    restart, which decides convergence and certifies the answer, stays FP64."""
 
-    def __init__(self, batch, probs, m=32, stream=None):
+    def __init__(self, batch, probs, m=32, stream=None, lowp=True):
         import torch
         self.batch, self.probs, self.stream, self.m = batch, probs, stream, int(m)
+        self.lowp = bool(lowp)
         dev = torch.device("cuda", torch.cuda.current_device())
         f64 = torch.float64
         self.pts = [torch.from_numpy(np.ascontiguousarray(p.points)).to(dev) for p in probs]
@@ -686,7 +706,7 @@ class BatchGMRES:
             self.launches += 2
             self.launches += ctx.kernel_residual_batch(
                 [(p.kernel, p.p0, p.shift, pts, z, None, self.zero[:p.n], V[j + 1].view(-1, 1))
-                 for p, pts, z, V in zip(self.probs, self.pts, zj, self.V)], self.stream)
+                 for p, pts, z, V in zip(self.probs, self.pts, zj, self.V)], self.stream, lowp=self.lowp)
             ctx.check(L.pp_gmres_arnoldi(self._h, j, sh), "gmres_arnoldi")
         ctx.check(L.pp_gmres_finish(self._h, sh), "gmres_finish")
         self.launches += 2 + self.m

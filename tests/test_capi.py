@@ -140,3 +140,12 @@ def test_device_assembly_refuses_host_context(pp, hctx):
     st = pp.lib().pp_hmatrix_assemble_dense_dev(h.handle, int(prob.kernel), float(prob.p0), float(prob.shift),
                                                 pts.ctypes.data, 2, None)
     assert st == pp.PP_CUDA_ERROR
+
+
+def test_device_dag_needs_device_context(pp, hctx):
+    """The device DAG build is refused for a host-only context (no silent host build claim)."""
+    with pytest.raises(pp.PPError):
+        hctx.set_device_dag(True)
+    h = pp.Hierarchical.dense(hctx, 512, 128)
+    ms, on_dev = h.dag_info(0)
+    assert not on_dev and ms >= 0.0
