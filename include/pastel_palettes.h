@@ -306,6 +306,11 @@ typedef struct pp_residual_job {
  * jobs' needs (grown on the first call of a larger total: make that call before capturing a
  * CUDA graph); calls on different streams must not overlap. */
 pp_status pp_kernel_residual_batch_dev(pp_context* ctx, int njobs, const pp_residual_job* jobs, void* stream);
+/* The same with the kernel entries of jobs of at most 4 right-hand sides evaluated in FP32
+ * (hardware reciprocal square root, exponential and division; a few 1e-7 relative per entry;
+ * sums still in FP64).  No counterpart in the reference.  Meant for the products inside Krylov
+ * cycles (pp_gmres_*), whose answer a FP64 residual then certifies; never for that residual. */
+pp_status pp_kernel_residual_batch_lowp_dev(pp_context* ctx, int njobs, const pp_residual_job* jobs, void* stream);
 
 /* --- batched restarted GMRES around the H-LU solve -------------------------
  * No counterpart in the reference (it has no solve or refinement path).  For a batch of

@@ -780,7 +780,20 @@ pp_status pp_hmatrix_construct_dev(pp_hmatrix* h, int kernel, double p0, double 
   return launch_plan(h, h->construct, s, 0);
 }
 
+namespace {
+pp_status residual_batch(pp_context* ctx, int njobs, const pp_residual_job* jobs, void* stream, bool lowp);
+}
+
 pp_status pp_kernel_residual_batch_dev(pp_context* ctx, int njobs, const pp_residual_job* jobs, void* stream) {
+  return residual_batch(ctx, njobs, jobs, stream, false);
+}
+
+pp_status pp_kernel_residual_batch_lowp_dev(pp_context* ctx, int njobs, const pp_residual_job* jobs, void* stream) {
+  return residual_batch(ctx, njobs, jobs, stream, true);
+}
+
+namespace {
+pp_status residual_batch(pp_context* ctx, int njobs, const pp_residual_job* jobs, void* stream, bool lowp) {
   if (!has_device(ctx)) return fail(ctx, PP_CUDA_ERROR, "no CUDA device in this context");
   if (njobs < 0 || (njobs > 0 && !jobs)) return fail(ctx, PP_INVALID_ARG, "kernel residual batch: bad argument");
   size_t need = 0;
@@ -820,9 +833,10 @@ pp_status pp_kernel_residual_batch_dev(pp_context* ctx, int njobs, const pp_resi
     o.part = ctx->d_resid + off;
     off += pp_kernel_residual_part_elems(j.n, j.nrhs);
   }
-  PP_CUDA(pp_kernel_residual_batch(dj.data(), njobs, (cudaStream_t)stream));
+  PP_CUDA(pp_kernel_residual_batch(dj.data(), njobs, (cudaStream_t)stream, lowp));
   return PP_OK;
 }
+}  // namespace
 
 int pp_datamap2d_check_overlap(uintptr_t pa, size_t pitch_a, size_t width_a, size_t height_a, uintptr_t pb,
                                size_t pitch_b, size_t width_b, size_t height_b) {

@@ -2311,6 +2311,23 @@ __device__ __forceinline__ double kernel_eval_nr(double d2, double p0, double in
   return (1.0 + s) * exp(-s);
 }
 
+// The same entry evaluated in FP32 with the hardware's approximate reciprocal square root,
+// exponential and division: relative error of a few 1e-7 (the exponential's argument is
+// rounded to FP32, so for the exp / Matern kernels the error grows like |argument| * 6e-8).
+// Used only by the low-precision products of the Krylov steps, never by a residual that
+// certifies a result.
+template <int KIND>
+__device__ __forceinline__ float kernel_eval_f32(float d2, float p0, float inv_p0) {
+  const float d = d2 * rsqrtf(fmaxf(d2, 1e-30f));
+  if (KIND <= 1) {
+    constexpr float c = KIND == 1 ? 12.566370614359172f : 1.0f;
+    return __fdividef(1.0f, c * (d + p0));
+  }
+  if (KIND == 2) return __expf(-d * inv_p0);
+  const float sv = 1.7320508f * d * inv_p0;
+  return (1.0f + sv) * __expf(-sv);
+}
+
 // C[m x k] = K(P_I, P_J) B (PP_OP_KMUL): a thread per row of C, the columns j of the kernel
 // matrix in chunks of KM_JC whose points and B rows are staged in shared memory (read by all
 // threads as broadcasts); points padded to three coordinates with zeros
@@ -2491,6 +2508,32 @@ __device__ __forceinline__ void residual_steps(const double* sp, const double* s
   }
 }
 
+// residual_steps with the entries evaluated in FP32 from FP32 copies of the points (spf, pif);
+// the products are still accumulated in FP64
+template <int KIND, int DIM, int NR, bool COL, bool EDGE, bool DUP>
+__device__ __forceinline__ void residual_steps_lowp(const float* spf, const double* sx, double* colw,
+                                                    const float (&pif)[DIM], const double (&xi)[NR], double (&acc)[NR],
+                                                    int lane, int jn, float p0, float inv_p0) {
+#pragma unroll 4
+  for (int st = 0; st < KR_SEG; ++st) {
+    const int jj = DUP ? lane + st : (lane + st) & (KR_SEG - 1);
+    if (EDGE && ((lane + st) & (KR_SEG - 1)) >= jn) continue;
+    float d2 = 0.0f;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      const float u = pif[d] - spf[jj * DIM + d];
+      d2 = fmaf(u, u, d2);
+    }
+    const double a = (double)kernel_eval_f32<KIND>(d2, p0, inv_p0);
+#pragma unroll
+    for (int q = 0; q < NR; ++q) acc[q] = fma(a, sx[jj * NR + q], acc[q]);
+    if (COL) {
+#pragma unroll
+      for (int q = 0; q < NR; ++q) colw[jj * NR + q] = fma(a, xi[q], colw[jj * NR + q]);
+    }
+  }
+}
+
 // Symmetric form of the partial products (kernel matrices are symmetric): a CTA takes the
 // tile pair (I, J), I <= J, of KR_SEG x KR_SEG tiles of one job and evaluates each entry once.
 // Thread t owns row I*KR_SEG + t: a_ij x_j goes to its register sums (part[J][i]); for I < J,
@@ -2499,12 +2542,14 @@ __device__ __forceinline__ void residual_steps(const double* sp, const double* s
 // s, so the lanes of a warp never touch the same column) and added in warp order at the end.
 // Every (segment, row) partial is written once, by one CTA: deterministic, no atomics, and the
 // same bits whatever the other jobs of the launch.
-template <int KIND, int DIM, int NR>
+// LOWP: entries evaluated in FP32 (residual_steps_lowp), for the Krylov steps' products.
+template <int KIND, int DIM, int NR, bool LOWP>
 __global__ void __launch_bounds__(KR_SEG) kernel_residual_sym(const __grid_constant__ ResidLaunch L) {
   constexpr int W = KR_SEG / 32;
   constexpr bool DUP = NR == 1;             // one RHS: tile stored twice over (residual_steps)
   constexpr int SW = DUP ? 2 * KR_SEG : KR_SEG;
   __shared__ double sp[SW * DIM];
+  __shared__ float spf[LOWP ? SW * DIM : 1];
   __shared__ double sx[SW * NR];
   __shared__ double col[W][SW * NR];
   const ResidLaunch::Job& jb = L.job[resid_job_of(L, (long long)blockIdx.x)];
@@ -2528,6 +2573,7 @@ __global__ void __launch_bounds__(KR_SEG) kernel_residual_sym(const __grid_const
   for (int e = t; e < SW * DIM; e += KR_SEG) {
     const int e0 = e % (KR_SEG * DIM), jj = e0 / DIM;
     sp[e] = j0 + jj < n ? pts[(size_t)j0 * DIM + e0] : 0.0;
+    if (LOWP) spf[e] = (float)sp[e];
   }
   for (int e = t; e < SW * NR; e += KR_SEG) {
     const int e0 = e % (KR_SEG * NR), jj = e0 / NR, q = e0 % NR;
@@ -2546,7 +2592,20 @@ __global__ void __launch_bounds__(KR_SEG) kernel_residual_sym(const __grid_const
   __syncthreads();
   const bool offdiag = I != J;
   const int jn = min(KR_SEG, n - j0);
-  if (jn == KR_SEG && I * KR_SEG + KR_SEG <= n) {  // full tiles: no per-entry predicates
+  const bool full = jn == KR_SEG && I * KR_SEG + KR_SEG <= n;  // full tiles: no per-entry predicates
+  if constexpr (LOWP) {
+    float pif[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) pif[d] = (float)pi[d];
+    const float p0f = (float)p0, ip0f = (float)inv_p0;
+    if (full) {
+      if (offdiag) residual_steps_lowp<KIND, DIM, NR, true, false, DUP>(spf, sx, col[w], pif, xi, acc, lane, jn, p0f, ip0f);
+      else residual_steps_lowp<KIND, DIM, NR, false, false, DUP>(spf, sx, col[w], pif, xi, acc, lane, jn, p0f, ip0f);
+    } else if (i < n) {
+      if (offdiag) residual_steps_lowp<KIND, DIM, NR, true, true, DUP>(spf, sx, col[w], pif, xi, acc, lane, jn, p0f, ip0f);
+      else residual_steps_lowp<KIND, DIM, NR, false, true, DUP>(spf, sx, col[w], pif, xi, acc, lane, jn, p0f, ip0f);
+    }
+  } else if (full) {
     if (offdiag) residual_steps<KIND, DIM, NR, true, false, DUP>(sp, sx, col[w], pi, xi, acc, lane, jn, p0, inv_p0);
     else residual_steps<KIND, DIM, NR, false, false, DUP>(sp, sx, col[w], pi, xi, acc, lane, jn, p0, inv_p0);
   } else if (i < n) {  // ragged edge of the matrix
@@ -2597,19 +2656,24 @@ __global__ void residual_update(const __grid_constant__ ResidLaunch L) {
 }
 
 template <int KIND, int DIM>
-cudaError_t launch_residual_sym(const ResidLaunch& L, unsigned pairs, int nr, cudaStream_t s) {
-  if (nr == 1)
-    kernel_residual_sym<KIND, DIM, 1><<<pairs, KR_SEG, 0, s>>>(L);
-  else
-    kernel_residual_sym<KIND, DIM, 4><<<pairs, KR_SEG, 0, s>>>(L);
+cudaError_t launch_residual_sym(const ResidLaunch& L, unsigned pairs, int nr, bool lowp, cudaStream_t s) {
+  if (lowp) {
+    if (nr == 1) kernel_residual_sym<KIND, DIM, 1, true><<<pairs, KR_SEG, 0, s>>>(L);
+    else kernel_residual_sym<KIND, DIM, 4, true><<<pairs, KR_SEG, 0, s>>>(L);
+  } else if (nr == 1) {
+    kernel_residual_sym<KIND, DIM, 1, false><<<pairs, KR_SEG, 0, s>>>(L);
+  } else {
+    kernel_residual_sym<KIND, DIM, 4, false><<<pairs, KR_SEG, 0, s>>>(L);
+  }
   return cudaGetLastError();
 }
 
 template <int KIND>
-cudaError_t launch_residual_sym_dim(int dim, const ResidLaunch& L, unsigned pairs, int nr, cudaStream_t s) {
-  if (dim == 1) return launch_residual_sym<KIND, 1>(L, pairs, nr, s);
-  if (dim == 2) return launch_residual_sym<KIND, 2>(L, pairs, nr, s);
-  return launch_residual_sym<KIND, 3>(L, pairs, nr, s);
+cudaError_t launch_residual_sym_dim(int dim, const ResidLaunch& L, unsigned pairs, int nr, bool lowp,
+                                    cudaStream_t s) {
+  if (dim == 1) return launch_residual_sym<KIND, 1>(L, pairs, nr, lowp, s);
+  if (dim == 2) return launch_residual_sym<KIND, 2>(L, pairs, nr, lowp, s);
+  return launch_residual_sym<KIND, 3>(L, pairs, nr, lowp, s);
 }
 
 template <int KIND, int DIM>
@@ -2814,8 +2878,10 @@ cudaError_t preload(F f) {
 }
 template <int KIND, int DIM>
 cudaError_t preload_residual() {
-  cudaError_t e = preload(kernel_residual_sym<KIND, DIM, 1>);
-  if (e == cudaSuccess) e = preload(kernel_residual_sym<KIND, DIM, 4>);
+  cudaError_t e = preload(kernel_residual_sym<KIND, DIM, 1, false>);
+  if (e == cudaSuccess) e = preload(kernel_residual_sym<KIND, DIM, 4, false>);
+  if (e == cudaSuccess) e = preload(kernel_residual_sym<KIND, DIM, 1, true>);
+  if (e == cudaSuccess) e = preload(kernel_residual_sym<KIND, DIM, 4, true>);
   if (e == cudaSuccess) e = preload(kernel_residual_part<KIND, DIM, 8>);
   if (e == cudaSuccess) e = preload(kernel_residual_part<KIND, DIM, 16>);
   return e;
@@ -2861,7 +2927,7 @@ cudaError_t pp_dense_residual(const double* A, int lda, int n, const double* x, 
   return cudaGetLastError();
 }
 
-cudaError_t pp_kernel_residual_batch(const pp_resid_job* jobs, int njobs, cudaStream_t s) {
+cudaError_t pp_kernel_residual_batch(const pp_resid_job* jobs, int njobs, cudaStream_t s, bool lowp) {
   if (njobs <= 0) return cudaSuccess;
   if (!jobs) return cudaErrorInvalidValue;
   std::vector<int> all, upd;
@@ -2895,10 +2961,10 @@ cudaError_t pp_kernel_residual_batch(const pp_resid_job* jobs, int njobs, cudaSt
           }
           if (pairs >= (1LL << 31)) return cudaErrorInvalidValue;
           switch (kern) {
-            case 0: e = launch_residual_sym_dim<0>(dim, L, (unsigned)pairs, nr, s); break;
-            case 1: e = launch_residual_sym_dim<1>(dim, L, (unsigned)pairs, nr, s); break;
-            case 2: e = launch_residual_sym_dim<2>(dim, L, (unsigned)pairs, nr, s); break;
-            default: e = launch_residual_sym_dim<3>(dim, L, (unsigned)pairs, nr, s); break;
+            case 0: e = launch_residual_sym_dim<0>(dim, L, (unsigned)pairs, nr, lowp, s); break;
+            case 1: e = launch_residual_sym_dim<1>(dim, L, (unsigned)pairs, nr, lowp, s); break;
+            case 2: e = launch_residual_sym_dim<2>(dim, L, (unsigned)pairs, nr, lowp, s); break;
+            default: e = launch_residual_sym_dim<3>(dim, L, (unsigned)pairs, nr, lowp, s); break;
           }
           if (e != cudaSuccess) return e;
         }

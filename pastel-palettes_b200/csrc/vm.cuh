@@ -73,7 +73,10 @@ struct pp_resid_job {
 };
 /* the update, residual and reduction of every job in three or more launches (jobs grouped by
  * kernel, dimension and right-hand-side width); results equal those of one job per call */
-cudaError_t pp_kernel_residual_batch(const pp_resid_job* jobs, int njobs, cudaStream_t s);
+cudaError_t pp_kernel_residual_batch(const pp_resid_job* jobs, int njobs, cudaStream_t s, bool lowp = false);
+/* lowp: jobs of at most 4 right-hand sides evaluate the kernel entries in FP32 (relative error
+ * of a few 1e-7 per entry, products still summed in FP64), for the products inside Krylov
+ * cycles; wider jobs stay FP64 */
 /* one dense block of an H-matrix to assemble from points: rows [r0, r0 + m), columns
  * [c0, c0 + n) of the matrix, stored row-major at a with leading dimension ld */
 struct pp_assemble_block {

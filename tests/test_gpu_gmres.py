@@ -75,7 +75,32 @@ def stalled_instances(pp, ctx):
     return out
 
 
-def test_gmres_converges_where_refinement_stalls(pp, gctx):
+@pytest.mark.parametrize("kernel,p0,dim", [("inv", 1e-3, 2), ("laplace", 1e-3, 3), ("exp", 0.1, 2), ("matern32", 0.2, 3)])
+def test_lowp_products_within_their_bound(pp, gctx, kernel, p0, dim):
+    """FP32-evaluated entries: the product is within 5e-6 * |A| |x| of the FP64 one (which is
+    checked against the dense matrix elsewhere)."""
+    probs = [pp.make_kernel_problem(gctx, n, dim, kernel, p0, 128, 8, seed=21 + n)[1] for n in (700, 1536)]
+    jobs64, jobs32, want = [], [], []
+    for p in probs:
+        pts = torch.from_numpy(np.ascontiguousarray(p.points)).cuda()
+        for nr in (1, 3):
+            x = torch.from_numpy(np.random.default_rng(p.n + nr).uniform(-1, 1, (p.n, nr))).cuda()
+            b = torch.zeros_like(x)
+            r64, r32 = torch.empty_like(x), torch.empty_like(x)
+            jobs64.append((p.kernel, p.p0, p.shift, pts, x, None, b, r64))
+            jobs32.append((p.kernel, p.p0, p.shift, pts, x, None, b, r32))
+            want.append((np.abs(p.dense()) @ np.abs(x.cpu().numpy())))
+    gctx.kernel_residual_batch(jobs64)
+    gctx.kernel_residual_batch(jobs32, lowp=True)
+    torch.cuda.synchronize()
+    for j64, j32, bound in zip(jobs64, jobs32, want):
+        d = np.abs(j64[7].cpu().numpy() - j32[7].cpu().numpy())
+        assert np.all(d <= 5e-6 * bound), (d / bound).max()
+        assert (d > 0).any()  # really the FP32 path
+
+
+@pytest.mark.parametrize("lowp", [False, True])
+def test_gmres_converges_where_refinement_stalls(pp, gctx, lowp):
     inst = stalled_instances(pp, gctx)
     hs = [h for h, _ in inst]
     probs = [p for _, p in inst]
@@ -90,7 +115,7 @@ def test_gmres_converges_where_refinement_stalls(pp, gctx):
     with torch.cuda.stream(s):
         _, hist = ir.solve(bs, tol=1e-10, max_iter=30)
     assert hist[-1] > 1e-8
-    gm = pp.BatchGMRES(batch, probs, m=32, stream=s)
+    gm = pp.BatchGMRES(batch, probs, m=32, stream=s, lowp=lowp)
     with torch.cuda.stream(s):
         xs, ghist = gm.solve(bs, tol=1e-10, max_cycles=12)
     batch.sync(s)
