@@ -132,6 +132,17 @@ long long pp_hmatrix_block_elems(const pp_hmatrix* h);
 #define PP_PRECISION_BF16 2
 pp_status pp_hmatrix_set_precision(pp_hmatrix* h, int precision);
 int pp_hmatrix_get_precision(const pp_hmatrix* h);
+/* Partial pivoting inside every GETRF block (on = 1; 0 is the reference's no-pivot LU, the
+ * default), for matrices that are not diagonally dominant.  Uses the reference's pivot
+ * helpers' idea (src/kernel.cu:958-1051: largest-magnitude row, row swaps, permutation applied
+ * to the rows of the right-hand blocks), which the reference itself never calls: each GETRF
+ * block (at most the tile, 64 rows) picks its pivot rows among its own rows, stores its row
+ * permutation beside the leaf (arena tail), and every triangular solve against that block's
+ * L — in the factorization (the blocks to its right, dense or the U factor of a low-rank block)
+ * and in the solve (the right-hand sides) — permutes its right-hand side first.  The solve then
+ * substitutes (no explicit inverses).  A block that needs no swap gives the unpivoted bits.
+ * Drops the matrix's programs; FP64, TF32 and BF16 forms alike. */
+pp_status pp_hmatrix_set_pivoting(pp_hmatrix* h, int on);
 /* output tile edge (64, the default, or 128) that the factor's products are split into;
  * larger tiles give fewer, longer GEMM instructions (the autotuner tries both).  Results do not
  * depend on it: every element still accumulates its k products in ascending order.  Rebuilds

@@ -19,6 +19,10 @@
  * mixed-precision pair (no reference counterpart): SHADOW (an operand rounded to BF16 in the
  * tensor core's tiled layout) and the BF16 GEMM (products of the shadows summed in FP64 here; the
  * tensor cores sum in FP32, so the two agree to a tolerance, not bitwise).
+ * And the engine's opt-in partial pivoting inside GETRF blocks (PP_PIVOT): o_getrf_piv (pivot row
+ * = largest magnitude, first of equal ones, as the reference's unused blockReduceMax_Index /
+ * blockSwapRows at src/kernel.cu:958-1051 pick and swap; then o_getrf's elimination) and
+ * o_permute_rows (a TRSML's right-hand side put in the block's pivot order before o_trsml).
  * `rhypot(1, t)` of the reference is written here from its definition, 1 / hypot(1, t).
  *
  * Parity pins: dense routines must agree bitwise with the CUDA path; the Givens-based
@@ -51,6 +55,45 @@ void o_getrf(double* M, int nx, int ny, int ld) {
       at(M, ld, row, i) = left;
       for (int col = i + 1; col < nx; ++col) at(M, ld, row, col) = std::fma(at(M, ld, i, col), -left, at(M, ld, row, col));
     }
+}
+
+// GETRF with partial pivoting inside the block (the engine's PP_PIVOT): at step i the row
+// r >= i of largest |a_ri| (the first of equal ones), whole rows i and r swapped, then the
+// unpivoted elimination above; perm_out[i] = the original row of row i (as a double).  The
+// reference's pivot helpers pick and swap rows this way (src/kernel.cu:958-1051:
+// blockReduceMax_Index takes the largest magnitude, blockSwapRows exchanges whole rows) but
+// the reference never calls them.
+void o_getrf_piv(double* M, int nx, int ny, int ld, double* perm_out) {
+  std::vector<int> perm(ny);
+  for (int i = 0; i < ny; ++i) perm[i] = i;
+  const int mn = std::min(nx, ny);
+  for (int i = 0; i < mn; ++i) {
+    int r = i;
+    double best = -1.0;
+    for (int row = i; row < ny; ++row) {
+      const double v = std::fabs(at(M, ld, row, i));
+      if (v > best) { best = v; r = row; }
+    }
+    if (r != i) {
+      for (int col = 0; col < nx; ++col) std::swap(at(M, ld, i, col), at(M, ld, r, col));
+      std::swap(perm[i], perm[r]);
+    }
+    for (int row = i + 1; row < ny; ++row) {
+      const double left = at(M, ld, row, i) / at(M, ld, i, i);
+      at(M, ld, row, i) = left;
+      for (int col = i + 1; col < nx; ++col) at(M, ld, row, col) = std::fma(at(M, ld, i, col), -left, at(M, ld, row, col));
+    }
+  }
+  for (int i = 0; i < ny; ++i) perm_out[i] = (double)perm[i];
+}
+
+// rows of B (ny_b x nx_b) put in the order of a pivoted block's permutation: row i := old row perm[i]
+void o_permute_rows(double* B, const double* perm, int nx_b, int ny_b, int ld_b) {
+  std::vector<double> tmp((size_t)nx_b * ny_b);
+  for (int i = 0; i < ny_b; ++i)
+    for (int col = 0; col < nx_b; ++col) tmp[(size_t)i * nx_b + col] = at(B, ld_b, (int)perm[i], col);
+  for (int i = 0; i < ny_b; ++i)
+    for (int col = 0; col < nx_b; ++col) at(B, ld_b, i, col) = tmp[(size_t)i * nx_b + col];
 }
 
 void o_trsml(double* B, const double* L, int nx_b, int ny_b, int nx_l, int ld_b, int ld_l) {
@@ -340,8 +383,23 @@ int run_one(const pp_task& T, std::vector<double>& tmp) {
   const bool t1 = T.flags & PP_T(1), t2 = T.flags & PP_T(2), t3 = T.flags & PP_T(3), t4 = T.flags & PP_T(4);
   switch (T.op) {
     case PP_OP_NOP: return 0;
-    case PP_OP_GETRF: o_getrf(T.p[0], T.n, T.m, T.ld[0]); return 0;
-    case PP_OP_TRSML: o_trsml(T.p[0], T.p[1], T.n, T.m, T.m, T.ld[0], T.ld[1]); return 0;
+    case PP_OP_GETRF:
+      if (T.flags & PP_PIVOT) {
+        if (!T.p[1]) return -1;
+        o_getrf_piv(T.p[0], T.n, T.m, T.ld[0], T.p[1]);
+      } else {
+        o_getrf(T.p[0], T.n, T.m, T.ld[0]);
+      }
+      return 0;
+    case PP_OP_TRSML:
+      if (T.flags & PP_PIVOT) {
+        if (!T.p[2]) return -1;
+        for (int i = 0; i < T.m; ++i)
+          if (!(T.p[2][i] >= 0.0 && T.p[2][i] < T.m)) return -1;
+        o_permute_rows(T.p[0], T.p[2], T.n, T.m, T.ld[0]);
+      }
+      o_trsml(T.p[0], T.p[1], T.n, T.m, T.m, T.ld[0], T.ld[1]);
+      return 0;
     case PP_OP_TRSMR: o_trsmr(T.p[0], T.p[1], T.n, T.m, T.n, T.ld[0], T.ld[1]); return 0;
     case PP_OP_TRSMRT: o_trsmrt(T.p[0], T.p[1], T.m, T.n, T.m, T.ld[0], T.ld[1]); return 0;
     case PP_OP_TRSMU: o_trsmu(T.p[0], T.p[1], T.m, T.n, T.ld[0], T.ld[1]); return 0;

@@ -162,6 +162,7 @@ def lib():
             "pp_lowrank_accum_noalloc": (i, [vp, vp, i, vp, i, vp, i, vp, i, vp, i, i, i, i, i, d, vp]),
             "pp_gmres_create": (i, [vp, i, vp, i, vp, vp, vp, vp, C.POINTER(vp)]),
             "pp_context_set_device_dag": (i, [vp, i]),
+            "pp_hmatrix_set_pivoting": (i, [vp, i]),
             "pp_hmatrix_dag_info": (i, [vp, i, i, C.POINTER(d), C.POINTER(i)]),
             "pp_gmres_destroy": (None, [vp]),
             "pp_gmres_start": (i, [vp, vp]),
@@ -446,6 +447,11 @@ class Hierarchical:
                                                       pts.data_ptr(), int(pts.shape[1]), _stream_handle(stream)),
                        "construct")
         return pts
+
+    def set_pivoting(self, on=True):
+        """Partial pivoting inside every GETRF block (block-local row permutations applied by
+        the triangular solves against that block); drops the built programs."""
+        self.ctx.check(lib().pp_hmatrix_set_pivoting(self._h, int(bool(on))), "set_pivoting")
 
     def set_gemm_tile(self, edge):
         """Output tile edge (64 or 128) of the product instructions; results do not change."""
@@ -968,10 +974,11 @@ def fill_kernel_hmatrix(h, prob, seed=7, rank_tol=None):
             h.set_lowrank(b["id"], U, V)
 
 
-def make_dense_problem(ctx, n=1024, leaf=256, seed=1234):
-    """Configuration 1: A = U[-1,1]^{n x n} + n I, all-dense 2x2 tree down to `leaf`."""
+def make_dense_problem(ctx, n=1024, leaf=256, seed=1234, shift=None):
+    """Configuration 1: A = U[-1,1]^{n x n} + shift I (shift n by default: strictly diagonally
+    dominant), all-dense 2x2 tree down to `leaf`."""
     rng = np.random.default_rng(seed)
-    A = rng.uniform(-1.0, 1.0, (n, n)) + n * np.eye(n)
+    A = rng.uniform(-1.0, 1.0, (n, n)) + (n if shift is None else shift) * np.eye(n)
     h = Hierarchical.dense(ctx, n, leaf)
     for b in h.blocks():
         if b["kind"] == DENSE:

@@ -95,6 +95,7 @@ struct pp_hmatrix {
   int precision = PP_PREC_FP64;  // contraction precision of the factor's GEMM instructions
   int tile = 0;                  // dense tile of its programs (0: the context's)
   int gemm_tile = 64;            // output tile edge of its product tasks (64 or 128)
+  int pivoting = 0;              // 1: partial pivoting inside the GETRF blocks (PP_PIVOT)
   std::vector<double> rand_host;
   VmPlan factor;
   std::map<int, std::unique_ptr<VmPlan>> solves;
@@ -187,6 +188,7 @@ pp_status build_program(pp_hmatrix* h, int which, int nrhs, VmPlan& plan) {
   try {
     pp::Generator g(plan.prog, *h->H, h->tile > 0 ? h->tile : ctx->cfg.tile, h->H->n, ctx->cfg.reference_isa == 0);
     g.use_inverses(ctx->cfg.reference_isa == 0);
+    if (h->pivoting) g.use_pivoting(true);
     if (which == 0) g.set_gemm_tile(h->gemm_tile);  // the solve's products keep 64
     if (which == 0) {
       if (h->precision == PP_PREC_BF16) g.set_precision(PP_PREC_BF16);
@@ -561,6 +563,19 @@ pp_status pp_hmatrix_set_precision(pp_hmatrix* h, int precision) {
 }
 
 int pp_hmatrix_get_precision(const pp_hmatrix* h) { return h ? h->precision : -1; }
+
+pp_status pp_hmatrix_set_pivoting(pp_hmatrix* h, int on) {
+  if (!h || (on != 0 && on != 1)) return PP_INVALID_ARG;
+  if (on == h->pivoting) return PP_OK;
+  h->pivoting = on;
+  h->last = nullptr;
+  h->factor.release();
+  h->factor.prog = pp::Program();
+  h->factor.built = false;
+  for (auto& kv : h->solves) kv.second->release();
+  h->solves.clear();
+  return PP_OK;
+}
 
 pp_status pp_hmatrix_set_gemm_tile(pp_hmatrix* h, int edge) {
   if (!h) return PP_INVALID_ARG;

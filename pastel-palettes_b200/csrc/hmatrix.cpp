@@ -36,6 +36,9 @@ void Hierarchical::add_inverses() {
       nd.invL = add_obj(nd.m, nd.m);
       nd.invU = add_obj(nd.m, nd.m);
     }
+  // after the inverses, so that their offsets do not depend on it
+  for (auto& nd : nodes)
+    if (nd.kind == HNode::D && nd.r0 == nd.c0 && nd.m == nd.n) nd.piv = add_obj(nd.m, 1);
 }
 
 Hierarchical* Hierarchical::dense_tiled(int n, int leaf) {

@@ -44,6 +44,8 @@ struct HNode {
   int kmax = 0;      // LR: storage capacity (columns of U and V)
   int ch[4] = {-1, -1, -1, -1};  // H: children, row-major 2 x 2
   int invL = -1, invU = -1;      // D on the diagonal: L^-1 and U^-1 of its factors (solve)
+  int piv = -1;                  // D on the diagonal: m x 1 row permutations of its pivoted
+                                 // factorization (one per GETRF tile, tile-local indices)
 };
 
 class Hierarchical {

@@ -355,6 +355,7 @@ bool Program::encode_reference(int workers, std::vector<std::vector<int32_t>>& s
       // the solves' inverse preparation writes only the arena tail and nothing waits on it:
       // the reference (which has no solve) gets the factorization proper
       if (x.op == PP_OP_TRINV) continue;
+      if (x.flags & PP_PIVOT) { err = "pivoted programs have no reference-format stream"; return false; }
       auto T = [&](int k) { return (x.flags & PP_T(k)) ? 1 : 0; };
       int32_t p[6] = {0}, o[6] = {0};
       for (int k = 0; k < 6; ++k)
@@ -435,6 +436,9 @@ Generator::Generator(Program& P, Hierarchical& H, int tile, int max_n_rand, bool
   inv_obj_.assign(P.objs.size(), {-1, -1});
   for (auto& nd : H.nodes)
     if (nd.kind == HNode::D && nd.invL >= 0) inv_obj_[node_obj_[nd.obj]] = {node_obj_[nd.invL], node_obj_[nd.invU]};
+  piv_obj_.assign(P.objs.size(), -1);
+  for (auto& nd : H.nodes)
+    if (nd.kind == HNode::D && nd.piv >= 0) piv_obj_[node_obj_[nd.obj]] = node_obj_[nd.piv];
   int kmax = 1;
   for (auto& nd : H.nodes)
     if (nd.kind == HNode::LR) kmax = std::max(kmax, nd.kmax);
@@ -820,12 +824,30 @@ void Generator::construct_program(int kernel, int dim, double p0, double tol) {
   }
 }
 
+// The rows of a diagonal leaf's pivot object that belong to a diagonal block of that leaf.
+View Generator::pivot_view(const View& tile) const {
+  if (tile.t || tile.r0 != tile.c0 || tile.m != tile.n || tile.obj < 0 || tile.obj >= (int)piv_obj_.size() ||
+      piv_obj_[tile.obj] < 0)
+    throw std::logic_error("pivoting: a GETRF / TRSML block that is not a diagonal block of a diagonal leaf");
+  View v;
+  v.obj = piv_obj_[tile.obj];
+  v.r0 = tile.r0;
+  v.c0 = 0;
+  v.m = tile.m;
+  v.n = 1;
+  return v;
+}
+
 void Generator::getrf(const Mat& A) {
   if (A.kind == Mat::LR) throw std::logic_error("getrf on a low-rank block");
   const int s = tri_split(A, T_);
   if (s < 0) {
     HTask& t = emit(PP_OP_GETRF);
     bind(t, 0, A.d, true);
+    if (pivot_) {
+      bind(t, 1, pivot_view(A.d), true);
+      t.t.flags |= PP_PIVOT;
+    }
     t.t.m = A.m;
     t.t.n = A.n;
     t.flops = flops_getrf(A.m, A.n);
@@ -863,7 +885,8 @@ void Generator::trsml(const Mat& L, const Mat& B) {
   if (B.kind == Mat::D && !B.d.t && mixed_inverse(L, invL, invU) &&
       split_product(B.d, whole(invL, L.m), B.d, (int64_t)B.n * L.m * (L.m - 1)))
     return;
-  const int s = tri_split(L, tri_limit(B.n));
+  // with pivoting the triangles are the GETRF blocks themselves (T_, split as getrf splits)
+  const int s = tri_split(L, pivot_ ? T_ : tri_limit(B.n));
   if (s < 0) {
     if (B.kind != Mat::D || B.d.t) throw std::logic_error("trsml: target must be a dense untransposed block");
     for (int c = 0; c < B.n; c += T_) {
@@ -871,6 +894,10 @@ void Generator::trsml(const Mat& L, const Mat& B) {
       HTask& t = emit(PP_OP_TRSML);
       bind(t, 0, B.d.sub(0, c, B.m, w), true);
       bind(t, 1, L.d, false);
+      if (pivot_) {
+        bind(t, 2, pivot_view(L.d), false);
+        t.t.flags |= PP_PIVOT;
+      }
       t.t.m = B.m;
       t.t.n = w;
       t.flops = (int64_t)w * B.m * (B.m - 1);

@@ -169,7 +169,13 @@ class Generator {
   void getrf_program();            // H-LU factorization of the whole matrix
   // explicit inverses of the diagonal leaves' triangular factors (TRINV), which the solve
   // program then applies with TRMV instead of substituting; set before building programs
-  void use_inverses(bool on) { inverses_ = on; }
+  void use_inverses(bool on) { inverses_ = on && !pivot_; }
+  // partial pivoting inside every GETRF block (PP_PIVOT), applied lazily by the TRSML
+  // instructions against that block; the solves then substitute (no explicit inverses)
+  void use_pivoting(bool on) {
+    pivot_ = on;
+    if (on) inverses_ = false;
+  }
   // edge of the output tiles products are split into (64 or 128; larger tiles: fewer, longer
   // tasks)
   void set_gemm_tile(int t) { gemm_tile_ = t >= 128 ? 128 : 64; }
@@ -205,6 +211,9 @@ class Generator {
   int max_n_rand_;
   bool split_k_;
   bool inverses_ = false;
+  bool pivot_ = false;
+  std::vector<int> piv_obj_;  // program object of a diagonal leaf -> its pivot object (or -1)
+  View pivot_view(const View& tile) const;
   int gemm_tile_ = 64;
   bool solve_ = false;  // building a solve program
   int prec_ = PP_PREC_FP64;

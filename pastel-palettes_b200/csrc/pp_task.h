@@ -73,6 +73,16 @@ enum pp_op {
 /* flags bit 1 (ACCUM): adaptive rank — truncate to the singular values above beta times the
  * largest and store the new rank (as a double) at p[5] when p[5] is set */
 #define PP_ADAPT_RANK 2
+/* flags bit 2 (GETRF, TRSML): partial pivoting inside the block.  GETRF picks, at step i, the
+ * row r >= i of largest |a_ri| (the first of equal ones), swaps whole rows i and r of the block,
+ * then eliminates as without pivoting; it writes the block's row permutation to p[1] (m doubles
+ * holding row indices: row i of the factored block came from row p[1][i]).  TRSML reads the
+ * permutation of its L block from p[2] and solves L X = P B, row i of P B being row p[2][i] of
+ * B.  The permutations stay block-local and are applied lazily: a solve against the block's L
+ * permutes its right-hand side first, the blocks below the pivoted block are left as they are.
+ * No reference counterpart in use (the reference's pivot helpers, src/kernel.cu:958-1051, are
+ * never called). */
+#define PP_PIVOT 4
 /* precision of the contraction inside GEMM-class tasks */
 #define PP_PREC_FP64 0
 #define PP_PREC_TF32 1

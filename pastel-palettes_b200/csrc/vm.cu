@@ -984,6 +984,70 @@ __device__ __noinline__ void dev_getrf(double* A, int lda, int m, int n, double*
   __syncthreads();
 }
 
+// A[m x n] := L\U of P A with partial pivoting inside the block (m, n <= TL), P written to
+// Pout (m doubles of row indices).  Step i: the row r >= i of largest |a_ri| (the first of
+// equal ones; warp 0 scans, lanes take rows i + lane + 32 t in ascending order, the shuffle
+// tree keeps the larger value and, on a tie, the smaller row), whole rows i and r swapped,
+// then l_r = a_ri / a_ii and a_rc = fma(a_ic, -l_r, a_rc) for r, c > i — the elimination of
+// the unpivoted routine, so a block that needs no swap gets the same bits.  The block lives in
+// shared memory (row stride LDS) for the whole factorization.
+__device__ __noinline__ void dev_getrf_piv(double* A, int lda, int m, int n, double* Pout, double* smem) {
+  double* S = smem;
+  int* perm = reinterpret_cast<int*>(smem + TL * LDS);
+  int* pivot = perm + TL;
+  load_tile(S, A, lda, m, n);
+  for (int i = threadIdx.x; i < m; i += NT) perm[i] = i;
+  __syncthreads();
+  const int mn = min(m, n), lane = threadIdx.x & 31;
+  for (int i = 0; i < mn; ++i) {
+    if (threadIdx.x < 32) {
+      double best = -1.0;
+      int bi = i;
+      for (int r = i + lane; r < m; r += 32) {
+        const double v = fabs(S[r * LDS + i]);
+        if (v > best) { best = v; bi = r; }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+      }
+      if (lane == 0) *pivot = bi;
+    }
+    __syncthreads();
+    const int r = *pivot;
+    if (r != i) {
+      for (int c = threadIdx.x; c < n; c += NT) {
+        const double t = S[i * LDS + c];
+        S[i * LDS + c] = S[r * LDS + c];
+        S[r * LDS + c] = t;
+      }
+      if (threadIdx.x == 0) {
+        const int t = perm[i];
+        perm[i] = perm[r];
+        perm[r] = t;
+      }
+    }
+    __syncthreads();
+    const double d = S[i * LDS + i];
+    for (int rr = i + 1 + threadIdx.x; rr < m; rr += NT) S[rr * LDS + i] = S[rr * LDS + i] / d;
+    __syncthreads();
+    const int w = n - i - 1;
+    for (int e = threadIdx.x; e < (m - i - 1) * w; e += NT) {
+      const int rr = i + 1 + e / w, c = i + 1 + e % w;
+      S[rr * LDS + c] = fma(S[i * LDS + c], -S[rr * LDS + i], S[rr * LDS + c]);
+    }
+    __syncthreads();
+  }
+  for (int e = threadIdx.x; e < m * n; e += NT) {
+    const int rr = e / n, c = e % n;
+    A[(size_t)rr * lda + c] = S[rr * LDS + c];
+  }
+  for (int i = threadIdx.x; i < m; i += NT) Pout[i] = (double)perm[i];
+  __syncthreads();
+}
+
 // ------------------------------------------------------------------------- TRSM sweeps
 // One triangular sweep over independent lines (the columns of B for TRSML / TRSMRT /
 // TRSMU, the rows of B for TRSMR) against a triangle T staged in shared memory (ld LDS).
@@ -1048,9 +1112,13 @@ struct Sweep {
 };
 
 // B: lines of length len (<= TL), line q at B + q * lstride, position p at + p * pstride.
+// perm (shared memory, optional): position p of a line is loaded from position perm[p] (the
+// row permutation of a pivoted L block); results are stored in natural order.  A line lives in
+// the registers of its lanes between its loads and its stores, so the permuted load is safe in
+// place.
 template <int R, int PIV, bool CT, bool BACK>
 __device__ __forceinline__ void tri_sweep(double* B, size_t lstride, size_t pstride, int nlines, int len,
-                                          const double* T, const double* rd) {
+                                          const double* T, const double* rd, const int* perm = nullptr) {
   constexpr int LPP = NT / R;  // lines per pass
   const int lane = threadIdx.x & 31, g = lane % R;
   const int q_in = (threadIdx.x / 32) * (32 / R) + lane / R;
@@ -1066,7 +1134,8 @@ __device__ __forceinline__ void tri_sweep(double* B, size_t lstride, size_t pstr
 #pragma unroll
     for (int j = 0; j < Sweep<R, PIV, CT, BACK>::NJ; ++j) {
       const int p = g + R * j;
-      S.x[j] = (q < nlines && p < len) ? ldcg(&B[q * lstride + p * pstride]) : 0.0;
+      const int src = (perm && p < len) ? perm[p] : p;
+      S.x[j] = (q < nlines && p < len) ? ldcg(&B[q * lstride + src * pstride]) : 0.0;
     }
     S.run();
 #pragma unroll
@@ -1079,9 +1148,9 @@ __device__ __forceinline__ void tri_sweep(double* B, size_t lstride, size_t pstr
 
 template <int PIV, bool CT, bool BACK>
 __device__ __forceinline__ void tri_lines(double* B, size_t lstride, size_t pstride, int nlines, int len,
-                                          const double* T, const double* rd) {
-  if (nlines <= 16) tri_sweep<16, PIV, CT, BACK>(B, lstride, pstride, nlines, len, T, rd);
-  else tri_sweep<4, PIV, CT, BACK>(B, lstride, pstride, nlines, len, T, rd);
+                                          const double* T, const double* rd, const int* perm = nullptr) {
+  if (nlines <= 16) tri_sweep<16, PIV, CT, BACK>(B, lstride, pstride, nlines, len, T, rd, perm);
+  else tri_sweep<4, PIV, CT, BACK>(B, lstride, pstride, nlines, len, T, rd, perm);
 }
 
 // B[m x n] := L^-1 B, L unit lower m x m (m <= TL); columns independent
@@ -1089,6 +1158,21 @@ __device__ __noinline__ void dev_trsml(double* B, int ldb, const double* L, int 
   load_tile(smem, L, ldl, m, m);
   __syncthreads();
   tri_lines<0, false, false>(B, 1, (size_t)ldb, n, m, smem, nullptr);
+  __syncthreads();
+}
+
+// B[m x n] := L^-1 P B (m <= TL), P the row permutation of a pivoted GETRF of L's block
+// (P[i]: the row of B that row i of P B takes; m doubles holding indices)
+__device__ __noinline__ void dev_trsml_piv(double* B, int ldb, const double* L, int ldl, const double* P, int m, int n,
+                                           double* smem) {
+  int* perm = reinterpret_cast<int*>(smem + TL * LDS);
+  load_tile(smem, L, ldl, m, m);
+  for (int i = threadIdx.x; i < m; i += NT) {
+    const int v = (int)ldcg(&P[i]);
+    perm[i] = (v >= 0 && v < m) ? v : i;  // indices come from the block's GETRF; guard anyway
+  }
+  __syncthreads();
+  tri_lines<0, false, false>(B, 1, (size_t)ldb, n, m, smem, nullptr, perm);
   __syncthreads();
 }
 
@@ -2011,9 +2095,19 @@ __device__ bool run_task(const pp_task& T, double* smem, TcCtx& tc, int& err) {
     case PP_OP_NOP: return true;
     case PP_OP_GETRF:
       if (T.m > TL || T.n > TL) return false;
-      dev_getrf(T.p[0], T.ld[0], T.m, T.n, smem);
+      if (T.flags & PP_PIVOT) {
+        if (!T.p[1]) return false;
+        dev_getrf_piv(T.p[0], T.ld[0], T.m, T.n, T.p[1], smem);
+      } else {
+        dev_getrf(T.p[0], T.ld[0], T.m, T.n, smem);
+      }
       return true;
     case PP_OP_TRSML:
+      if (T.flags & PP_PIVOT) {  // one pivoted block per instruction
+        if (T.m > TL || !T.p[2]) return false;
+        dev_trsml_piv(T.p[0], T.ld[0], T.p[1], T.ld[1], T.p[2], T.m, T.n, smem);
+        return true;
+      }
       if (T.m > PP_VM_TRI) return false;
       if (T.m > TL) dev_trsml_big(T.p[0], T.ld[0], T.p[1], T.ld[1], T.m, T.n, smem);
       else dev_trsml(T.p[0], T.ld[0], T.p[1], T.ld[1], T.m, T.n, smem);
