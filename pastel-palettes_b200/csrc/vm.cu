@@ -2603,7 +2603,10 @@ __device__ __forceinline__ void residual_steps(const double* sp, const double* s
 }
 
 // residual_steps with the entries evaluated in FP32 from FP32 copies of the points (spf, pif);
-// the products are still accumulated in FP64
+// the products are still accumulated in FP64.  The skewed walk keeps the lanes of a warp on
+// distinct columns only while they take their steps together: columns past the ragged edge are
+// masked (entry 0) instead of skipped, and the column sums' read-modify-writes of one step end
+// with a warp barrier, so no lane can run a step ahead of another into the same column.
 template <int KIND, int DIM, int NR, bool COL, bool EDGE, bool DUP>
 __device__ __forceinline__ void residual_steps_lowp(const float* spf, const double* sx, double* colw,
                                                     const float (&pif)[DIM], const double (&xi)[NR], double (&acc)[NR],
@@ -2611,19 +2614,21 @@ __device__ __forceinline__ void residual_steps_lowp(const float* spf, const doub
 #pragma unroll 4
   for (int st = 0; st < KR_SEG; ++st) {
     const int jj = DUP ? lane + st : (lane + st) & (KR_SEG - 1);
-    if (EDGE && ((lane + st) & (KR_SEG - 1)) >= jn) continue;
+    const bool live = !EDGE || ((lane + st) & (KR_SEG - 1)) < jn;
     float d2 = 0.0f;
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
       const float u = pif[d] - spf[jj * DIM + d];
       d2 = fmaf(u, u, d2);
     }
-    const double a = (double)kernel_eval_f32<KIND>(d2, p0, inv_p0);
+    const float a32 = kernel_eval_f32<KIND>(d2, p0, inv_p0);
+    const double a = live ? (double)a32 : 0.0;
 #pragma unroll
     for (int q = 0; q < NR; ++q) acc[q] = fma(a, sx[jj * NR + q], acc[q]);
     if (COL) {
 #pragma unroll
       for (int q = 0; q < NR; ++q) colw[jj * NR + q] = fma(a, xi[q], colw[jj * NR + q]);
+      __syncwarp();
     }
   }
 }
