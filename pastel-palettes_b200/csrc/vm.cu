@@ -2585,19 +2585,23 @@ __device__ __forceinline__ void residual_steps(const double* sp, const double* s
 #pragma unroll 4
   for (int st = 0; st < KR_SEG; ++st) {
     const int jj = DUP ? lane + st : (lane + st) & (KR_SEG - 1);
-    if (EDGE && ((lane + st) & (KR_SEG - 1)) >= jn) continue;
+    // past the ragged edge the entry is masked, not skipped: a lane that skipped steps could
+    // run ahead of the others into a column another lane is still updating
+    const bool live = !EDGE || ((lane + st) & (KR_SEG - 1)) < jn;
     double d2 = 0.0;
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
       const double u = pi[d] - sp[jj * DIM + d];
       d2 = fma(u, u, d2);
     }
-    const double a = kernel_eval_nr<KIND>(d2, p0, inv_p0);
+    const double ak = kernel_eval_nr<KIND>(d2, p0, inv_p0);
+    const double a = live ? ak : 0.0;
 #pragma unroll
     for (int q = 0; q < NR; ++q) acc[q] = fma(a, sx[jj * NR + q], acc[q]);
     if (COL) {
 #pragma unroll
       for (int q = 0; q < NR; ++q) colw[jj * NR + q] = fma(a, xi[q], colw[jj * NR + q]);
+      if (EDGE) __syncwarp();
     }
   }
 }
