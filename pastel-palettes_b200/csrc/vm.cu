@@ -2586,7 +2586,10 @@ __device__ __forceinline__ void residual_steps(const double* sp, const double* s
   for (int st = 0; st < KR_SEG; ++st) {
     const int jj = DUP ? lane + st : (lane + st) & (KR_SEG - 1);
     // past the ragged edge the entry is masked, not skipped: a lane that skipped steps could
-    // run ahead of the others into a column another lane is still updating
+    // run ahead of the others into a column another lane is still updating.  For the same
+    // reason each step's column-sum updates end with a warp barrier: seen from one thread the
+    // next step's column is another address, so without it the compiler may load it before
+    // the neighbouring lane has stored its update there
     const bool live = !EDGE || ((lane + st) & (KR_SEG - 1)) < jn;
     double d2 = 0.0;
 #pragma unroll
@@ -2601,7 +2604,7 @@ __device__ __forceinline__ void residual_steps(const double* sp, const double* s
     if (COL) {
 #pragma unroll
       for (int q = 0; q < NR; ++q) colw[jj * NR + q] = fma(a, xi[q], colw[jj * NR + q]);
-      if (EDGE) __syncwarp();
+      __syncwarp();
     }
   }
 }

@@ -18,6 +18,10 @@ reports, per program (factor, solve):
   python pastel-palettes_b200/trace_tool.py --workload laplace3d [--n 65536] [--form bf16|fp64]
       the mixed-precision configuration instead (3-D Laplace, leaf 512, eta 1, adaptive rank
       <= 32 at 1e-8, built on the device): its factor and its 8-RHS solve
+  python pastel-palettes_b200/trace_tool.py --workload gmres [--instances 512] [--restart 32]
+      device times of the parts of one GMRES step over the uneven batch
+  python pastel-palettes_b200/trace_tool.py --workload dag [--n 65536]
+      the mixed configuration's factor program DAG built on the host and on the device
 """
 import argparse
 import collections
@@ -121,6 +125,89 @@ def trace_laplace3d(pp, ctx, torch, args):
                 tasks, tr, ef, et)
 
 
+def time_gmres(pp, ctx, torch, args):
+    """Per-component device times of one GMRES step over the uneven batch (512 instances, N
+    log-uniform in [1024, 16384], exp(-r/0.1) + 1e-2 I on U[0,1]^2, weak admissibility, leaf
+    128, rank <= 24 at 1e-7, built on the device): the merged solve, the batched product in FP64
+    and with FP32-evaluated entries, the last Arnoldi launch of a cycle, one whole cycle, and the
+    merged factor (CUDA events on the batch's stream, best of 3)."""
+    rng = np.random.default_rng(4096)
+    s = torch.cuda.Stream()
+    hs, probs = [], []
+    with torch.cuda.stream(s):
+        for i in range(args.instances):
+            n = int(round(np.exp(rng.uniform(np.log(1024), np.log(16384))) / 64)) * 64
+            h, prob = pp.make_kernel_problem(ctx, n, 2, "exp", 0.1, 128, 24, shift=1e-2, seed=4096 + 31 * i,
+                                             rank_tol=1e-7, construct="device", stream=s)
+            h.keep_original(s)
+            hs.append(h)
+            probs.append(prob)
+    s.synchronize()
+    batch = pp.Batch(ctx, hs)
+    batch.autotune(s)
+    bs = [torch.from_numpy(pp.rhs(p.n, 1, seed=3 + i)).cuda() for i, p in enumerate(probs)]
+    gm = pp.BatchGMRES(batch, probs, m=args.restart, stream=s, lowp=True)
+
+    def timeit(fn, reps=3):
+        best = float("inf")
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(s):
+                a.record(s)
+                fn()
+                b.record(s)
+            b.synchronize()
+            best = min(best, a.elapsed_time(b))
+        return best
+
+    with torch.cuda.stream(s):
+        batch.factor(s)
+        gm.reset(bs)
+        gm.cycle(bs)
+    s.synchronize()
+    v0 = [V[0].view(-1, 1) for V in gm.V]
+    z0 = [Z[0].view(-1, 1) for Z in gm.Z]
+    prod = [(p.kernel, p.p0, p.shift, pts, z, None, gm.zero[:p.n], V[1].view(-1, 1))
+            for p, pts, z, V in zip(probs, gm.pts, z0, gm.V)]
+    L = pp.lib()
+    res = {
+        "instances": len(probs), "n_total": int(sum(p.n for p in probs)),
+        "kernel_evaluations_per_product": float(sum(p.n * (p.n + 1) / 2 for p in probs)),
+        "merged_solve_ms": timeit(lambda: batch.solve(v0, z0, s)),
+        "product_fp64_ms": timeit(lambda: ctx.kernel_residual_batch(prod, s)),
+        "product_fp32_entries_ms": timeit(lambda: ctx.kernel_residual_batch(prod, s, lowp=True)),
+        "arnoldi_last_step_ms": timeit(lambda: L.pp_gmres_arnoldi(gm._h, args.restart - 1, pp._stream_handle(s))),
+        "cycle_ms": timeit(lambda: gm.cycle(bs), 1),
+        "restore_and_factor_ms": timeit(lambda: (batch.restore(s), batch.factor(s)), 1),
+    }
+    for k, v in res.items():
+        print(f"{k:32s} {v:.6g}" if isinstance(v, float) else f"{k:32s} {v}")
+
+
+def time_dag(pp, torch, args):
+    """DAG build of the mixed configuration's factor program (3-D Laplace, leaf 512, eta 1,
+    rank <= 32, BF16 form) on the host and on the device: the program's tasks and edges, the
+    DAG build's wall time, the whole program build's."""
+    import time
+    n = args.n if args.n != 8192 else 65536
+    rng = np.random.default_rng(1234)
+    pts = rng.uniform(0, 1, (n, 3))
+    pts = pts[pp.morton_order(pts)]
+    for mode in ("host", "device"):
+        ctx = pp.Context(device=0)
+        if mode == "device":
+            ctx.set_device_dag(True)
+        h = pp.Hierarchical.geometric(ctx, pts, 512, 1, 1.0, 32)
+        h.set_rank_tolerance(1e-8)
+        h.set_precision(pp.BF16)
+        t0 = time.perf_counter()
+        info = h.program_info(0)
+        wall = time.perf_counter() - t0
+        ms, on_dev = h.dag_info(0)
+        print(f"{mode:6s} tasks {info['n_tasks']} edges {info['n_edges']} dag {ms:.1f} ms (on device: {on_dev}) "
+              f"program build {info['host_build_ms']:.1f} ms (wall {1e3 * wall:.1f} ms)")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--n", type=int, default=8192)
@@ -129,7 +216,9 @@ def main():
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--gemm-tile", type=int, default=128, help="output tile edge of the factor's products")
     ap.add_argument("--out", default=None, help="also save the raw trace (npz)")
-    ap.add_argument("--workload", default="hodlr", choices=["hodlr", "laplace3d"])
+    ap.add_argument("--workload", default="hodlr", choices=["hodlr", "laplace3d", "gmres", "dag"])
+    ap.add_argument("--instances", type=int, default=512, help="gmres: instances of the uneven batch")
+    ap.add_argument("--restart", type=int, default=32, help="gmres: restart length")
     ap.add_argument("--form", default="bf16", choices=["bf16", "fp64"])
     args = ap.parse_args()
     import torch
@@ -138,6 +227,12 @@ def main():
     ctx = pp.Context(device=0)
     if args.workload == "laplace3d":
         trace_laplace3d(pp, ctx, torch, args)
+        return
+    if args.workload == "gmres":
+        time_gmres(pp, ctx, torch, args)
+        return
+    if args.workload == "dag":
+        time_dag(pp, torch, args)
         return
     h, prob = pp.make_kernel_problem(ctx, args.n, 2, "inv", 1e-3, args.leaf, args.rank, seed=1234)
     h.set_gemm_tile(args.gemm_tile)
