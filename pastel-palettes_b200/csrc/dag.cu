@@ -156,6 +156,10 @@ bool build_dag_device(Program& prog, std::string& err, double* device_ms) {
     for (const Region& r : prog.tasks[t].regions)
       h.push_back(Access{r.obj, t, r.r0, r.c0, r.r0 + r.nr, r.c0 + r.nc, r.ro ? 1 : 0, 0});
   const long long na = (long long)h.size();
+  if (na >= (1LL << 31) - 1) {  // the sorts and scans count items in int
+    err = "more than 2^31 accesses";
+    return false;
+  }
   auto t0 = std::chrono::steady_clock::now();
   std::vector<unsigned long long> ekeys;
   std::vector<unsigned char> etypes;
@@ -212,6 +216,10 @@ bool build_dag_device(Program& prog, std::string& err, double* device_ms) {
     DAG_CUDA(cudaStreamSynchronize(s));
     if (over) {
       err = "a dependency walk met more than " + std::to_string(kWalkWrites) + " partial writes";
+      return false;
+    }
+    if (total >= (1LL << 31) - 1) {
+      err = "more than 2^31 dependency pairs before merging";
       return false;
     }
     if (total > 0) {
