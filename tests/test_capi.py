@@ -149,3 +149,38 @@ def test_device_dag_needs_device_context(pp, hctx):
     h = pp.Hierarchical.dense(hctx, 512, 128)
     ms, on_dev = h.dag_info(0)
     assert not on_dev and ms >= 0.0
+
+
+def test_gmres_and_pivot_entry_points_validate_arguments(pp, hctx):
+    """Host-side argument checks of the GMRES, low-precision product and pivoting entry points:
+    refused before anything reaches a device."""
+    import ctypes as C
+    L = pp.lib()
+    g = C.c_void_p()
+    n = (C.c_int * 1)(128)
+    ptrs = (C.c_void_p * 1)(C.c_void_p(0x1000))
+    # a host-only context has no device to run on
+    assert L.pp_gmres_create(hctx.handle, 1, n, 8, ptrs, ptrs, ptrs, ptrs, C.byref(g)) == pp.PP_CUDA_ERROR
+    assert L.pp_gmres_start(None, None) == pp.PP_INVALID_ARG
+    assert L.pp_gmres_arnoldi(None, 0, None) == pp.PP_INVALID_ARG
+    assert L.pp_gmres_finish(None, None) == pp.PP_INVALID_ARG
+    job = pp._ResidualJob()
+    assert L.pp_kernel_residual_batch_lowp_dev(hctx.handle, 1, C.byref(job), None) == pp.PP_CUDA_ERROR
+    h = pp.Hierarchical.dense(hctx, 256, 64)
+    assert L.pp_hmatrix_set_pivoting(h.handle, 2) == pp.PP_INVALID_ARG
+    assert L.pp_hmatrix_set_pivoting(None, 1) == pp.PP_INVALID_ARG
+    h.set_pivoting(True)
+    info = h.program_info(0)
+    assert info["op_count"]["trinv"] == 0 and info["op_count"]["getrf"] > 0
+    h.set_pivoting(False)
+    assert h.program_info(0)["op_count"]["trinv"] > 0
+
+
+def test_pivoted_programs_have_no_reference_stream(pp):
+    """The reference's int32 stream format has no pivoting: export is refused, not silently
+    unpivoted."""
+    ctx = pp.Context(device=-1, reference_isa=1)
+    h = pp.Hierarchical.dense(ctx, 256, 64)
+    h.set_pivoting(True)
+    with pytest.raises(pp.PPError):
+        h.refstreams(1)
