@@ -937,6 +937,9 @@ def main():
         legs["uneven_batch"] = uneven_batch_leg(pp, ctx, args.uneven, 3, 1)
         print(f"bench: uneven batch leg {time.perf_counter() - t_leg:.0f} s", file=sys.stderr, flush=True)
     t_leg = time.perf_counter()
+    # admission builds programs while other requests' persistent launches hold every SM: a
+    # DAG build on the device would queue behind them, so the server builds on the host
+    ctx.set_device_dag(False)
     if args.serve_requests > 0:
         legs["serving"] = serving_leg(pp, ctx, args.serve_requests, [float(x) for x in args.serve_rates.split(",")],
                                       seed=2024 + rank)
