@@ -3,8 +3,9 @@
 The device build must give the same program to the VM: every task record, successor list
 (order included: successors are sorted by bottom level, ties in program order), in-degree and
 initial ready order, for the factor and solve programs of the benchmark configurations' trees
-(C1 all-dense, C2 HODLR, the 3-D leaf-512 tree of the mixed configuration in FP64 and BF16
-form, standard admissibility in 2-D).  Only the tree matters to the DAG, so no matrix is
+(all-dense N = 1024 with 256 leaves; HODLR N = 8192 with 256 leaves and rank 16; 3-D Laplace
+N = 8192 with 512 leaves, eta 1, rank <= 32, in FP64 and BF16 form; standard admissibility in
+2-D, N = 4096 with 128 leaves).  Only the tree matters to the DAG, so no matrix is
 filled."""
 import numpy as np
 import pytest
@@ -15,20 +16,20 @@ torch = pytest.importorskip("torch")
 
 
 def tree(pp, ctx, case):
-    if case == "c1_dense":
+    if case == "dense_n1024_leaf256":
         return pp.Hierarchical.dense(ctx, 1024, 256), 1
     rng = np.random.default_rng(1234)
-    if case == "c2_hodlr":
+    if case == "hodlr_n8192_leaf256":
         pts = rng.uniform(0, 1, (8192, 2))
         return pp.Hierarchical.geometric(ctx, pts[pp.morton_order(pts)], 256, 0, 1.0, 16), 1
-    if case in ("c3_shape_fp64", "c3_shape_bf16"):
+    if case in ("laplace3d_n8192_leaf512_fp64", "laplace3d_n8192_leaf512_bf16"):
         pts = rng.uniform(0, 1, (8192, 3))
         h = pp.Hierarchical.geometric(ctx, pts[pp.morton_order(pts)], 512, 1, 1.0, 32)
         h.set_rank_tolerance(1e-8)
         if case.endswith("bf16"):
             h.set_precision(pp.BF16)
         return h, 8
-    if case == "standard_2d":
+    if case == "standard2d_n4096_leaf128":
         pts = rng.uniform(0, 1, (4096, 2))
         h = pp.Hierarchical.geometric(ctx, pts[pp.morton_order(pts)], 128, 1, 1.0, 24)
         h.set_rank_tolerance(1e-7)
@@ -36,7 +37,8 @@ def tree(pp, ctx, case):
     raise ValueError(case)
 
 
-@pytest.mark.parametrize("case", ["c1_dense", "c2_hodlr", "c3_shape_fp64", "c3_shape_bf16", "standard_2d"])
+@pytest.mark.parametrize("case", ["dense_n1024_leaf256", "hodlr_n8192_leaf256", "laplace3d_n8192_leaf512_fp64",
+                                  "laplace3d_n8192_leaf512_bf16", "standard2d_n4096_leaf128"])
 def test_device_dag_equals_host_dag(pp, case):
     ctx_h, ctx_d = pp.Context(device=0), pp.Context(device=0)
     ctx_d.set_device_dag(True)

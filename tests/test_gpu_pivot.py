@@ -1,7 +1,7 @@
 """Partial pivoting inside the GETRF blocks on the GPU (PP_PIVOT) against the oracle running
 the same programs (oracle/oracle.cpp o_getrf_piv / o_permute_rows).
 
-* C1's tree (N = 1024, leaf 256, 64-row GETRF blocks) on U[-1,1] without the diagonal shift
+* the all-dense tree of N = 1024 with 256-row leaves (64-row GETRF blocks) on U[-1,1] without the diagonal shift
   and with a zero leading entry: the factorization bitwise equal to the oracle's (same pivot
   rows: largest magnitude, first of equal ones), the solve within 1e-12 of the oracle's, and
   FP64 refinement to a backward error <= 1e-12 against the dense matrix;
