@@ -43,6 +43,8 @@ def lib():
         L.oracle_run_parallel.restype = i
         L.oracle_dense_getrf.argtypes = [vp, i, i]
         L.oracle_dense_getrf.restype = None
+        L.oracle_getrf_piv.argtypes = [vp, i, i, vp]
+        L.oracle_getrf_piv.restype = None
         L.oracle_gemm.argtypes = [d, d, vp, vp, vp, i, i, i, i, i, i, i, i]
         L.oracle_gemm.restype = None
         L.oracle_accum.argtypes = [vp, vp, vp, vp, i, i, i, i, i, i, i, i, d, vp, i]
@@ -132,6 +134,15 @@ def dense_getrf(A):
     M = np.ascontiguousarray(A, dtype=np.float64).copy()
     lib().oracle_dense_getrf(M.ctypes.data, M.shape[0], M.shape[1])
     return M
+
+
+def getrf_piv(A):
+    """One block's LU with partial pivoting (largest magnitude, first of equal ones): returns
+    (L\\U of P A, perm) with row i of P A = row perm[i] of A."""
+    M = np.ascontiguousarray(A, dtype=np.float64).copy()
+    perm = np.zeros(M.shape[0])
+    lib().oracle_getrf_piv(M.ctypes.data, M.shape[0], M.shape[1], perm.ctypes.data)
+    return M, perm.astype(np.int64)
 
 
 def gemm(alpha, beta, M, A, B, a_T=False, b_T=False):

@@ -587,6 +587,9 @@ int oracle_run_parallel(const pp_task* tasks, int n, const int32_t* succ, const 
 // the reference reproduces element by element).
 void oracle_dense_getrf(double* A, int n, int lda) { o_getrf(A, n, n, lda); }
 
+// One block's LU with partial pivoting (the engine's PP_PIVOT GETRF); perm: n doubles.
+void oracle_getrf_piv(double* A, int n, int lda, double* perm) { o_getrf_piv(A, n, n, lda, perm); }
+
 // Single routines, for unit tests against the CUDA path.
 void oracle_gemm(double alpha, double beta, double* M, const double* A, const double* B, int m, int n, int k, int ld_m,
                  int ld_a, int ld_b, int a_T, int b_T) {

@@ -64,3 +64,23 @@ def test_pivoted_program_without_swaps_has_the_unpivoted_bits(pp, hctx):
     for ((r, c, m, n), x0), (_, x1) in zip(dense_blocks(pp, h, f0.matrix), dense_blocks(pp, h, f1.matrix)):
         assert np.array_equal(x0, x1)
         assert np.array_equal(x1, F[r:r + m, c:c + n].ravel())
+
+
+def test_block_getrf_piv_matches_lapack():
+    """The restated pivoted block LU against LAPACK's dgetrf (scipy): the same pivot rows
+    (both take the first row of largest magnitude) and the same factors to rounding (LAPACK
+    blocks its updates in another order)."""
+    import scipy.linalg as sl
+    rng = np.random.default_rng(17)
+    for n in (7, 64):
+        A = rng.uniform(-1, 1, (n, n))
+        F, perm = O.getrf_piv(A)
+        lu, piv = sl.lu_factor(A)
+        p = np.arange(n)
+        for i, r in enumerate(piv):  # LAPACK's swap sequence as a permutation
+            p[[i, r]] = p[[r, i]]
+        assert np.array_equal(perm, p)
+        assert np.abs(F - lu).max() <= 1e-12 * np.abs(lu).max()
+        L = np.tril(F, -1) + np.eye(n)
+        U = np.triu(F)
+        assert np.abs(L @ U - A[perm]).max() <= 1e-13
