@@ -2609,6 +2609,37 @@ __device__ __forceinline__ void residual_steps(const double* sp, const double* s
   }
 }
 
+// residual_steps with the entries evaluated in FP32 from FP32 copies of the points (spf, pif);
+// the products are still accumulated in FP64.  The skewed walk keeps the lanes of a warp on
+// distinct columns only while they take their steps together: columns past the ragged edge are
+// masked (entry 0) instead of skipped, and the column sums' read-modify-writes of one step end
+// with a warp barrier, so no lane can run a step ahead of another into the same column.
+template <int KIND, int DIM, int NR, bool COL, bool EDGE, bool DUP>
+__device__ __forceinline__ void residual_steps_lowp(const float* spf, const double* sx, double* colw,
+                                                    const float (&pif)[DIM], const double (&xi)[NR], double (&acc)[NR],
+                                                    int lane, int jn, float p0, float inv_p0) {
+#pragma unroll 4
+  for (int st = 0; st < KR_SEG; ++st) {
+    const int jj = DUP ? lane + st : (lane + st) & (KR_SEG - 1);
+    const bool live = !EDGE || ((lane + st) & (KR_SEG - 1)) < jn;
+    float d2 = 0.0f;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      const float u = pif[d] - spf[jj * DIM + d];
+      d2 = fmaf(u, u, d2);
+    }
+    const float a32 = kernel_eval_f32<KIND>(d2, p0, inv_p0);
+    const double a = live ? (double)a32 : 0.0;
+#pragma unroll
+    for (int q = 0; q < NR; ++q) acc[q] = fma(a, sx[jj * NR + q], acc[q]);
+    if (COL) {
+#pragma unroll
+      for (int q = 0; q < NR; ++q) colw[jj * NR + q] = fma(a, xi[q], colw[jj * NR + q]);
+      __syncwarp();
+    }
+  }
+}
+
 // Symmetric form of the partial products (kernel matrices are symmetric): a CTA takes the
 // tile pair (I, J), I <= J, of KR_SEG x KR_SEG tiles of one job and evaluates each entry once.
 // Thread t owns row I*KR_SEG + t: a_ij x_j goes to its register sums (part[J][i]); for I < J,
@@ -2617,12 +2648,14 @@ __device__ __forceinline__ void residual_steps(const double* sp, const double* s
 // s, so the lanes of a warp never touch the same column) and added in warp order at the end.
 // Every (segment, row) partial is written once, by one CTA: deterministic, no atomics, and the
 // same bits whatever the other jobs of the launch.
-template <int KIND, int DIM, int NR>
+// LOWP: entries evaluated in FP32 (residual_steps_lowp), for the Krylov steps' products.
+template <int KIND, int DIM, int NR, bool LOWP>
 __global__ void __launch_bounds__(KR_SEG) kernel_residual_sym(const __grid_constant__ ResidLaunch L) {
   constexpr int W = KR_SEG / 32;
   constexpr bool DUP = NR == 1;             // one RHS: tile stored twice over (residual_steps)
   constexpr int SW = DUP ? 2 * KR_SEG : KR_SEG;
   __shared__ double sp[SW * DIM];
+  __shared__ float spf[LOWP ? SW * DIM : 1];
   __shared__ double sx[SW * NR];
   __shared__ double col[W][SW * NR];
   const ResidLaunch::Job& jb = L.job[resid_job_of(L, (long long)blockIdx.x)];
@@ -2646,6 +2679,7 @@ __global__ void __launch_bounds__(KR_SEG) kernel_residual_sym(const __grid_const
   for (int e = t; e < SW * DIM; e += KR_SEG) {
     const int e0 = e % (KR_SEG * DIM), jj = e0 / DIM;
     sp[e] = j0 + jj < n ? pts[(size_t)j0 * DIM + e0] : 0.0;
+    if (LOWP) spf[e] = (float)sp[e];
   }
   for (int e = t; e < SW * NR; e += KR_SEG) {
     const int e0 = e % (KR_SEG * NR), jj = e0 / NR, q = e0 % NR;
@@ -2665,7 +2699,19 @@ __global__ void __launch_bounds__(KR_SEG) kernel_residual_sym(const __grid_const
   const bool offdiag = I != J;
   const int jn = min(KR_SEG, n - j0);
   const bool full = jn == KR_SEG && I * KR_SEG + KR_SEG <= n;  // full tiles: no per-entry predicates
-  if (full) {
+  if constexpr (LOWP) {
+    float pif[DIM];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) pif[d] = (float)pi[d];
+    const float p0f = (float)p0, ip0f = (float)inv_p0;
+    if (full) {
+      if (offdiag) residual_steps_lowp<KIND, DIM, NR, true, false, DUP>(spf, sx, col[w], pif, xi, acc, lane, jn, p0f, ip0f);
+      else residual_steps_lowp<KIND, DIM, NR, false, false, DUP>(spf, sx, col[w], pif, xi, acc, lane, jn, p0f, ip0f);
+    } else if (i < n) {
+      if (offdiag) residual_steps_lowp<KIND, DIM, NR, true, true, DUP>(spf, sx, col[w], pif, xi, acc, lane, jn, p0f, ip0f);
+      else residual_steps_lowp<KIND, DIM, NR, false, true, DUP>(spf, sx, col[w], pif, xi, acc, lane, jn, p0f, ip0f);
+    }
+  } else if (full) {
     if (offdiag) residual_steps<KIND, DIM, NR, true, false, DUP>(sp, sx, col[w], pi, xi, acc, lane, jn, p0, inv_p0);
     else residual_steps<KIND, DIM, NR, false, false, DUP>(sp, sx, col[w], pi, xi, acc, lane, jn, p0, inv_p0);
   } else if (i < n) {  // ragged edge of the matrix
@@ -2695,120 +2741,6 @@ __global__ void __launch_bounds__(KR_SEG) kernel_residual_sym(const __grid_const
   }
 }
 
-// The products inside Krylov cycles: kernel_residual_sym's tile pairs and skewed column walk,
-// with the entries evaluated in FP32 (kernel_eval_f32) from FP32 copies of the points and two
-// rows per thread (rows t and t + KR_SEG / 2 of the tile): each staged column's point and
-// right-hand side, and each column-sum update in shared memory, serve two entries, which halves
-// the shared-memory traffic that bounds the one-row form.  Sums stay FP64.  Columns past a
-// ragged edge are masked; rows past it have x_i = 0 and are never written; each step's
-// column-sum updates end with a warp barrier (see residual_steps).
-#define KL_THREADS (KR_SEG / 2)
-template <int KIND, int DIM, int NR>
-__global__ void __launch_bounds__(KL_THREADS) kernel_residual_sym_lowp(const __grid_constant__ ResidLaunch L) {
-  constexpr int W = KL_THREADS / 32;
-  constexpr bool DUP = NR == 1;
-  constexpr int SW = DUP ? 2 * KR_SEG : KR_SEG;
-  __shared__ float sp[SW * DIM];
-  __shared__ double sx[SW * NR];
-  __shared__ double col[W][SW * NR];
-  const ResidLaunch::Job& jb = L.job[resid_job_of(L, (long long)blockIdx.x)];
-  const double* __restrict__ pts = jb.pts;
-  const double* __restrict__ x = jb.x;
-  double* __restrict__ part = jb.part;
-  const int n = jb.n, nrhs = jb.nrhs, T = jb.T;
-  const long long b = (long long)blockIdx.x - jb.first;
-  const double tt = 2.0 * T + 1.0;
-  int I = (int)floor((tt - sqrt(tt * tt - 8.0 * (double)b)) * 0.5);
-  auto row_start = [&](int r) { return (long long)r * T - (long long)r * (r - 1) / 2; };
-  while (I > 0 && row_start(I) > b) --I;
-  while (row_start(I + 1) <= b) ++I;
-  const int J = I + (int)(b - row_start(I));
-  const int t = threadIdx.x, w = t >> 5, lane = t & 31;
-  const int j0 = J * KR_SEG;
-  const int i0[2] = {I * KR_SEG + t, I * KR_SEG + KL_THREADS + t};
-  for (int e = t; e < SW * DIM; e += KL_THREADS) {
-    const int e0 = e % (KR_SEG * DIM), jj = e0 / DIM;
-    sp[e] = j0 + jj < n ? (float)pts[(size_t)j0 * DIM + e0] : 0.0f;
-  }
-  for (int e = t; e < SW * NR; e += KL_THREADS) {
-    const int e0 = e % (KR_SEG * NR), jj = e0 / NR, q = e0 % NR;
-    sx[e] = (j0 + jj < n && q < nrhs) ? x[(size_t)(j0 + jj) * nrhs + q] : 0.0;
-  }
-  for (int e = t; e < W * SW * NR; e += KL_THREADS) (&col[0][0])[e] = 0.0;
-  float pi[2][DIM];
-  double xi[2][NR], acc[2][NR];
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int ir = min(i0[h], n - 1);
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) pi[h][d] = (float)pts[(size_t)ir * DIM + d];
-#pragma unroll
-    for (int q = 0; q < NR; ++q) {
-      xi[h][q] = (i0[h] < n && q < nrhs) ? x[(size_t)ir * nrhs + q] : 0.0;
-      acc[h][q] = 0.0;
-    }
-  }
-  __syncthreads();
-  const bool offdiag = I != J;
-  const int jn = min(KR_SEG, n - j0);
-  const float p0 = (float)jb.p0, inv_p0 = (float)(1.0 / jb.p0);
-  double* colw = col[w];
-#pragma unroll 2
-  for (int st = 0; st < KR_SEG; ++st) {
-    const int jj = DUP ? lane + st : (lane + st) & (KR_SEG - 1);
-    const bool live = ((lane + st) & (KR_SEG - 1)) < jn;
-    double a[2];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      float d2 = 0.0f;
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) {
-        const float u = pi[h][d] - sp[jj * DIM + d];
-        d2 = fmaf(u, u, d2);
-      }
-      const float v = kernel_eval_f32<KIND>(d2, p0, inv_p0);
-      a[h] = live ? (double)v : 0.0;
-    }
-#pragma unroll
-    for (int q = 0; q < NR; ++q) {
-      const double xj = sx[jj * NR + q];
-      acc[0][q] = fma(a[0], xj, acc[0][q]);
-      acc[1][q] = fma(a[1], xj, acc[1][q]);
-    }
-    if (offdiag) {
-#pragma unroll
-      for (int q = 0; q < NR; ++q) colw[jj * NR + q] = fma(a[1], xi[1][q], fma(a[0], xi[0][q], colw[jj * NR + q]));
-      __syncwarp();
-    }
-  }
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    if (i0[h] >= n) continue;
-    if (!offdiag) {  // the diagonal entry's shift
-#pragma unroll
-      for (int q = 0; q < NR; ++q) acc[h][q] = fma(jb.shift, xi[h][q], acc[h][q]);
-    }
-    for (int q = 0; q < nrhs; ++q) part[((size_t)J * n + i0[h]) * nrhs + q] = acc[h][q];
-  }
-  if (offdiag) {
-    __syncthreads();
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int c = t + h * KL_THREADS, jrow = j0 + c;
-      if (jrow >= n) continue;
-      for (int q = 0; q < nrhs; ++q) {
-        double v = 0.0;
-#pragma unroll
-        for (int ww = 0; ww < W; ++ww) {
-          v += col[ww][c * NR + q];
-          if (DUP) v += col[ww][(c + KR_SEG) * NR + q];
-        }
-        part[((size_t)I * n + jrow) * nrhs + q] = v;
-      }
-    }
-  }
-}
-
 // r = b - (sum of the job's segments in order), one thread per (row, rhs) element
 __global__ void residual_reduce(const __grid_constant__ ResidLaunch L) {
   const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -2832,12 +2764,12 @@ __global__ void residual_update(const __grid_constant__ ResidLaunch L) {
 template <int KIND, int DIM>
 cudaError_t launch_residual_sym(const ResidLaunch& L, unsigned pairs, int nr, bool lowp, cudaStream_t s) {
   if (lowp) {
-    if (nr == 1) kernel_residual_sym_lowp<KIND, DIM, 1><<<pairs, KL_THREADS, 0, s>>>(L);
-    else kernel_residual_sym_lowp<KIND, DIM, 4><<<pairs, KL_THREADS, 0, s>>>(L);
+    if (nr == 1) kernel_residual_sym<KIND, DIM, 1, true><<<pairs, KR_SEG, 0, s>>>(L);
+    else kernel_residual_sym<KIND, DIM, 4, true><<<pairs, KR_SEG, 0, s>>>(L);
   } else if (nr == 1) {
-    kernel_residual_sym<KIND, DIM, 1><<<pairs, KR_SEG, 0, s>>>(L);
+    kernel_residual_sym<KIND, DIM, 1, false><<<pairs, KR_SEG, 0, s>>>(L);
   } else {
-    kernel_residual_sym<KIND, DIM, 4><<<pairs, KR_SEG, 0, s>>>(L);
+    kernel_residual_sym<KIND, DIM, 4, false><<<pairs, KR_SEG, 0, s>>>(L);
   }
   return cudaGetLastError();
 }
@@ -3052,10 +2984,10 @@ cudaError_t preload(F f) {
 }
 template <int KIND, int DIM>
 cudaError_t preload_residual() {
-  cudaError_t e = preload(kernel_residual_sym<KIND, DIM, 1>);
-  if (e == cudaSuccess) e = preload(kernel_residual_sym<KIND, DIM, 4>);
-  if (e == cudaSuccess) e = preload(kernel_residual_sym_lowp<KIND, DIM, 1>);
-  if (e == cudaSuccess) e = preload(kernel_residual_sym_lowp<KIND, DIM, 4>);
+  cudaError_t e = preload(kernel_residual_sym<KIND, DIM, 1, false>);
+  if (e == cudaSuccess) e = preload(kernel_residual_sym<KIND, DIM, 4, false>);
+  if (e == cudaSuccess) e = preload(kernel_residual_sym<KIND, DIM, 1, true>);
+  if (e == cudaSuccess) e = preload(kernel_residual_sym<KIND, DIM, 4, true>);
   if (e == cudaSuccess) e = preload(kernel_residual_part<KIND, DIM, 8>);
   if (e == cudaSuccess) e = preload(kernel_residual_part<KIND, DIM, 16>);
   return e;
