@@ -365,6 +365,12 @@ pp_status pp_context_set_device_dag(pp_context* ctx, int on);
  * ran on the device (builds the program first if needed) */
 pp_status pp_hmatrix_dag_info(pp_hmatrix* h, int which, int nrhs, double* dag_ms, int* on_device);
 
+/* The data regions of every instruction of the factor (which 0) or solve (1) program, the
+ * reference's Operation data list (rts/ops.h:22-36: read-only flag and 2-D region per operand):
+ * 7 int32 per region (task, storage object, first row, first column, rows, columns, read-only),
+ * in program order; out == NULL only sets *count. */
+pp_status pp_hmatrix_program_regions(pp_hmatrix* h, int which, int nrhs, long long* count, int32_t* out);
+
 /* --- rts (DAG primitives, rts/ops.h, rts/dependency.h) ------------------- */
 /* DataMap2D::checkOverlap (rts/ops.cpp:7-40); regions: ptr, pitch, width (bytes), height */
 int pp_datamap2d_check_overlap(uintptr_t ptr_a, size_t pitch_a, size_t width_a, size_t height_a, uintptr_t ptr_b,

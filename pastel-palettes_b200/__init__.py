@@ -163,6 +163,7 @@ def lib():
             "pp_gmres_create": (i, [vp, i, vp, i, vp, vp, vp, vp, C.POINTER(vp)]),
             "pp_context_set_device_dag": (i, [vp, i]),
             "pp_hmatrix_set_pivoting": (i, [vp, i]),
+            "pp_hmatrix_program_regions": (i, [vp, i, i, C.POINTER(ll), vp]),
             "pp_hmatrix_dag_info": (i, [vp, i, i, C.POINTER(d), C.POINTER(i)]),
             "pp_gmres_destroy": (None, [vp]),
             "pp_gmres_start": (i, [vp, vp]),
@@ -484,6 +485,16 @@ class Hierarchical:
                     op_count={OP_NAMES[i]: info.op_count[i] for i in range(len(OP_NAMES))},
                     arena_elems={ARENAS[i]: info.arena_elems[i] for i in range(5)},
                     host_build_ms=info.host_build_ms)
+
+    def regions(self, which=0, nrhs=1):
+        """Every instruction's data regions: int32 rows (task, object, row0, col0, rows, cols,
+        read_only) in program order."""
+        k = C.c_longlong()
+        self.ctx.check(lib().pp_hmatrix_program_regions(self._h, which, nrhs, C.byref(k), None), "program_regions")
+        out = np.zeros((max(k.value, 1), 7), dtype=np.int32)
+        self.ctx.check(lib().pp_hmatrix_program_regions(self._h, which, nrhs, C.byref(k), out.ctypes.data),
+                       "program_regions")
+        return out[: k.value]
 
     def dag_info(self, which=0, nrhs=1):
         """(DAG build milliseconds, built on the device) of the factor / solve program."""

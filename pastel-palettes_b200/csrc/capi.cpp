@@ -1770,6 +1770,31 @@ pp_status pp_gmres_status(pp_gmres* g, double* out) {
   return PP_OK;
 }
 
+// ---------------------------------------------------------------- program regions
+pp_status pp_hmatrix_program_regions(pp_hmatrix* h, int which, int nrhs, long long* count, int32_t* out) {
+  if (!h || !count || (which != 0 && which != 1) || (which == 1 && nrhs <= 0)) return PP_INVALID_ARG;
+  VmPlan* plan = which == 0 ? &h->factor : solve_plan(h, nrhs);
+  pp_status st = build_program(h, which, nrhs, *plan);
+  if (st != PP_OK) return st;
+  long long k = 0;
+  for (size_t t = 0; t < plan->prog.tasks.size(); ++t)
+    for (const pp::Region& r : plan->prog.tasks[t].regions) {
+      if (out) {
+        int32_t* o = out + 7 * k;
+        o[0] = (int32_t)t;
+        o[1] = r.obj;
+        o[2] = r.r0;
+        o[3] = r.c0;
+        o[4] = r.nr;
+        o[5] = r.nc;
+        o[6] = r.ro ? 1 : 0;
+      }
+      ++k;
+    }
+  *count = k;
+  return PP_OK;
+}
+
 // ---------------------------------------------------------------- DAG build placement
 pp_status pp_context_set_device_dag(pp_context* ctx, int on) {
   if (!ctx || (on != 0 && on != 1)) return PP_INVALID_ARG;
