@@ -390,7 +390,7 @@ def serving_leg(pp, ctx, n_requests, rates, seed=2024, smin=2048, smax=65536):
                         f"diagonal shift computed by the client before submission"}
 
 
-def uneven_batch_leg(pp, ctx, n_inst, steps, warmup, seed=4096, smin=1024, smax=16384, restart=32):
+def uneven_batch_leg(pp, ctx, n_inst, steps, warmup, seed=4096, smin=1024, smax=16384, restart=64):
     """Configuration-4 batch: n_inst H-matrices of uneven size in one merged persistent launch.
     N log-uniform in [smin, smax] (multiple of 64), points U[0,1]^2, kernel exp(-r / 0.1) + 1e-2 I,
     weak admissibility, leaf 128, adaptive rank at 1e-7 capped at 24, FP64 instructions (at leaf
