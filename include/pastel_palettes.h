@@ -335,7 +335,7 @@ pp_status pp_kernel_residual_batch_lowp_dev(pp_context* ctx, int njobs, const pp
  *   r = b - A x.
  * Each call is one launch on `stream`, one CTA per instance (largest first), no host
  * synchronization and no allocation (capturable).  1 <= m <= PP_GMRES_MAX_RESTART. */
-#define PP_GMRES_MAX_RESTART 64
+#define PP_GMRES_MAX_RESTART 128
 typedef struct pp_gmres pp_gmres;
 pp_status pp_gmres_create(pp_context* ctx, int count, const int* n, int m, double* const* V, double* const* Z,
                           double* const* x, double* const* r, pp_gmres** out);

@@ -93,7 +93,7 @@ cudaError_t pp_axpy(double* x, const double* dx, size_t count, cudaStream_t s);
 cudaError_t pp_absmax2(const double* x, const double* r, size_t count, unsigned long long* out, cudaStream_t s);
 
 /* ---- batched restarted GMRES around the H-LU solve (krylov.cu) ---- */
-#define PP_GMRES_MAX_RESTART 64  /* largest restart length (Arnoldi steps per cycle) */
+#define PP_GMRES_MAX_RESTART 128 /* largest restart length (Arnoldi steps per cycle) */
 /* one instance of a batched GMRES: device pointers, n rows, restart length m */
 struct pp_gmres_slot {
   int n, m;
